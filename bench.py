@@ -1,0 +1,415 @@
+"""Benchmark: Mparticles/s of one FMM solve on one B200, with its accuracy.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c1|c2|c3] [--impl ours|reference]
+
+A step is one full solve (tree build through outputs in input order) of the
+configuration's seeded synthetic particle set.  ``value`` times solves on
+device-resident inputs (CUDA events on the solver's stream, K solves after W
+warm-up solves, barrier + synchronise around the timed region, max over
+ranks); ``e2e`` times the same solve through the public host-buffer entry
+point (pinned host inputs copied in and results copied out every step).
+Every solve rebuilds the tree and re-reads every particle; the working set
+exceeds L2 (126 MB) for the 16M-particle configuration, and for the smaller
+ones an L2 flush (a 256 MB write) runs between timed steps.
+
+Multi-GPU: the solver does not shard one problem (no collective); with
+``--gpus N`` every rank solves its own independent copy of the
+configuration (weak scaling, replicas), rank 0 prints the line.
+
+``--impl reference`` times the reference's own CPU FMM (compiled from its
+sources into oracle/_ref) on the host cores, on a bounded sample of the same
+configuration; only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    # 3D uniform, 131,072 particles, FP64, p = 8 (N = 9), uniform depth 5 (max 64 per leaf)
+    "c1": dict(dim=3, n=131072, gen="uniform3d", seed=12345, N=9, depth=5, precision="fp64",
+               workload="3D uniform 131,072 particles, FP64, p=8 (N=9), uniform octree depth 5"),
+    # 2D clustered, 4,194,304 particles, p = 20 (N = 21), FP64
+    "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=9, precision="fp64",
+               workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
+                        "p=20 (N=21), uniform quadtree depth 9"),
+    # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform)
+    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=11, depth=8, precision="fp64",
+               workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, p=10 (N=11), octree depth 8"),
+}
+DEFAULT_CONFIG = "c1"
+METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def make_particles(cfg):
+    from laplace_fmm_b200 import workloads as W
+    return getattr(W, cfg["gen"])(cfg["n"], seed=cfg["seed"])
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0])); mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- peaks
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16_tflops": d.get("bf16_tflops", 1590.0),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def fp64_peak_tflops(torch):
+    """Dense FP64 throughput measured here (cuBLAS DGEMM 8192^3, best of 5):
+    the denominator for the FP64 kernels, which MEASURED_PEAKS.json lacks."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b); torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def launches_per_solve(depth, dim, radix_passes, targets):
+    """Kernels the library enqueues for one solve (tree + FMM passes)."""
+    scan = 3
+    tree = 2 + 1 + radix_passes * (1 + scan + 1) + 1 + 1 + scan + 1 + 1
+    tree += (depth - 1) * (1 + scan + 1 + 1) + depth + 1 + (depth - 1)
+    if dim == 3:
+        fmm = 1 + (depth - 1) + max(0, depth - 2) + max(0, depth - 3) + 1
+    else:
+        fmm = 1 + (depth - 1) + max(0, depth - 2) + 1
+    return tree + fmm
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    from laplace_fmm_b200 import Context
+    from laplace_fmm_b200._lib import PRECISION, LfmmStats
+    from laplace_fmm_b200.workloads import rel_l2, sample_targets
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    dim, n, N, depth = cfg["dim"], cfg["n"], cfg["N"], cfg["depth"]
+    prec = PRECISION[cfg["precision"]]
+    pos, q = make_particles(cfg)
+    ctx = Context(local_rank)
+    L = ctx.lib
+    solve_dev = L.lfmm3d_solve_device if dim == 3 else L.lfmm2d_solve_device
+    solve_host = L.lfmm3d_solve if dim == 3 else L.lfmm2d_solve
+    d_src = torch.from_numpy(pos).cuda()
+    d_q = torch.from_numpy(q).cuda()
+    d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_fld = torch.empty(n, dim, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    vp = ctypes.c_void_p
+
+    def step_dev():
+        ctx.check(solve_dev(ctx.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), 0, None, N, depth, 1e-8, prec,
+                            vp(d_pot.data_ptr()), vp(d_fld.data_ptr()), None), "solve_device")
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            step_dev()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # per-phase split (separate timed solve with phase events)
+    ctx_t = Context(local_rank, timing=True)
+    st = LfmmStats()
+    ctx_t.check(solve_dev(ctx_t.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), 0, None, N, depth, 1e-8, prec,
+                          vp(d_pot.data_ptr()), vp(d_fld.data_ptr()), ctypes.byref(st)), "solve_device(timed)")
+    torch.cuda.synchronize()
+    stats = st.as_dict()
+    ctx_t.close()
+    # accuracy on 4096 seeded targets against the FP64 direct sum (on the GPU)
+    idx = sample_targets(n)
+    tgt = torch.from_numpy(np.ascontiguousarray(pos[idx])).cuda()
+    e_pot = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+    e_fld = torch.empty(len(idx), dim, dtype=torch.float64, device="cuda")
+    direct = L.lfmm3d_direct_device if dim == 3 else L.lfmm2d_direct_device
+    step_dev()
+    ctx.check(direct(ctx.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), len(idx), vp(tgt.data_ptr()),
+                     vp(e_pot.data_ptr()), vp(e_fld.data_ptr())), "direct")
+    torch.cuda.synchronize()
+    fp, ff = d_pot.cpu().numpy()[idx], d_fld.cpu().numpy()[idx]
+    ep, ef = e_pot.cpu().numpy(), e_fld.cpu().numpy()
+    self_term = q[idx] * (1e4 if dim == 3 else np.log(1e-4))
+    acc = {"rel_l2_pot_noself": rel_l2(fp - self_term, ep - self_term), "rel_l2_pot": rel_l2(fp, ep),
+           "rel_l2_field": rel_l2(ff, ef), "targets": int(len(idx))}
+    # end to end through the host API with pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        h_src = torch.from_numpy(pos).pin_memory(); h_q = torch.from_numpy(q).pin_memory()
+        h_pot = torch.empty(n, dtype=torch.float64).pin_memory()
+        h_fld = torch.empty(n, dim, dtype=torch.float64).pin_memory()
+
+        def step_host():
+            ctx.check(solve_host(ctx.handle, n, vp(h_src.data_ptr()), vp(h_q.data_ptr()), 0, None, N, depth, 1e-8,
+                                 prec, vp(h_pot.data_ptr()), vp(h_fld.data_ptr()), None), "solve")
+
+        for _ in range(max(1, args.warmup)):
+            step_host()
+        tot = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            step_host()
+            e.record(stream)
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        e2e_ms = tot / args.steps
+        if dist:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * n / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
+               "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
+    return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx)
+
+
+def m2l_flops(N):
+    """Algorithmic flops of one rotation-based M2L: two y-rotations, the
+    z-translation and two z-rotations (the reference's operator count)."""
+    nx2 = N * (N + 1) // 2
+    return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
+
+
+def roofline(cfg, stats, peaks, fp64_tflops):
+    """Roofline of the dominant phase (device time from the phase events)."""
+    phases = {"leaves": stats["ms_leaves"], "m2l": stats["ms_m2l"], "tree": stats["ms_tree"],
+              "upward": stats["ms_upward"], "l2l": stats["ms_l2l"]}
+    dom = max(phases, key=phases.get)
+    ms = phases[dom]
+    fp64 = cfg["precision"] == "fp64"
+    if dom == "leaves":
+        flops = 20.0 * stats["n_p2p_pairs"]
+        achieved = flops / (ms * 1e-3) / 1e12
+        peak = fp64_tflops if fp64 else 2 * 148 * 128 * 1.965e9 / 1e12
+        return {"kernel": "leaves_kernel (P2P + L2P)", "bound": "fp64" if fp64 else "fp32",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "measured DGEMM" if fp64 else "spec FP32 SIMT", "algorithmic_flops": flops,
+                "phase_ms": ms, "traffic": None}
+    if dom == "m2l":
+        flops = float(m2l_flops(cfg["N"])) * stats["n_far_pairs"]
+        achieved = flops / (ms * 1e-3) / 1e12
+        peak = fp64_tflops if fp64 else peaks["bf16_tflops"]
+        return {"kernel": "m2l_kernel", "bound": "fp64" if fp64 else "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "algorithmic_flops": flops, "phase_ms": ms,
+                "traffic": None}
+    # tree / upward: HBM-bound passes over the particles
+    nbytes = stats["n_particles"] * (2 * 32 + 2 * 8 + 4)
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "algorithmic_bytes": nbytes, "phase_ms": ms, "traffic": None}
+
+
+# ---------------------------------------------------------------- CPU legs
+def cpu_sample(cfg):
+    """Bounded sample of the configuration for the host-core baselines: the
+    full problem for the small configurations, 1/8 of the particles with one
+    level less (same particles per leaf) for the large ones."""
+    if cfg["n"] <= 200000:
+        return cfg["n"], cfg["depth"], "full problem"
+    n = cfg["n"] // 8
+    return n, cfg["depth"] - 1, f"first {n} particles of the seeded set (1/8), depth {cfg['depth'] - 1}"
+
+
+def cpu_solver():
+    from oracle.oracle import ORACLE_SO, REF_SO, Oracle, Reference, build
+    if REF_SO.exists():
+        return Reference(), "reference"
+    if not ORACLE_SO.exists():
+        build(("oracle",))
+    return Oracle(), "port"
+
+
+def run_cpu(cfg, pos, q, steps):
+    solver, kind = cpu_solver()
+    cores = os.cpu_count() or 1
+    solver.set_threads(cores)
+    n, depth, sample = cpu_sample(cfg)
+    p, qq = pos[:n], q[:n]
+    fn = solver.fmm3d if cfg["dim"] == 3 else solver.fmm2d
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn(p, qq, N=cfg["N"], depth=depth)
+        times.append(time.perf_counter() - t0)
+    s = float(np.median(times))
+    return {"value": n / s / 1e6, "unit": "Mparticles/s", "cores": cores, "kind": kind, "sample": sample,
+            "seconds_per_solve": s}
+
+
+def base_config(cfg, world):
+    return {"workload": cfg["workload"], "particles": cfg["n"], "order_p": cfg["N"] - 1, "N_degrees": cfg["N"],
+            "tree_depth": cfg["depth"], "precision": cfg["precision"],
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "inputs > L2" if cfg["n"] * 32 > 126e6 else "L2 flushed (256 MB write) between steps"}
+
+
+def main():
+    args = parse()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "RANK" not in os.environ:
+        world = 1
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        pos, q = make_particles(cfg)
+        for _ in range(max(0, min(args.warmup, 1))):
+            run_cpu(cfg, pos, q, 1)
+        cb = run_cpu(cfg, pos, q, args.steps)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Mparticles/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": cb["seconds_per_solve"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+                "config": base_config(cfg, 1),
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": "Mparticles/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    r = run_ours(args, cfg, rank, world, local_rank)
+    torch, dist = r["torch"], r["dist"]
+    line = None
+    if rank == 0:
+        peaks = measured_peaks()
+        fp64 = fp64_peak_tflops(torch)
+        stats = r["stats"]
+        radix_passes = (cfg["dim"] * (cfg["depth"] - 1) + 7) // 8
+        line = {
+            "metric": METRIC, "value": world * cfg["n"] / (r["ms"] * 1e-3) / 1e6, "unit": "Mparticles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if cfg["precision"] == "fp64" else "f32/tf32", "data": "synthetic (seeded PCG64)",
+            "config": base_config(cfg, world), "accuracy": r["acc"], "phases_ms": {
+                k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves", "ms_total")},
+            "tree": {k: stats[k] for k in ("n_cells", "n_leaves", "n_far_pairs", "n_close_pairs", "n_p2p_pairs")},
+            "roofline": roofline(cfg, stats, peaks, fp64), "fp64_peak_tflops_measured": fp64,
+            "peaks_source": peaks["source"], "e2e": r["e2e"], "clocks": r["clocks"],
+            "gpu_launches": args.steps * launches_per_solve(cfg["depth"], cfg["dim"], radix_passes, False),
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            pos, q = make_particles(cfg)
+            cb = run_cpu(cfg, pos, q, 2)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

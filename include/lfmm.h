@@ -1,0 +1,148 @@
+/*
+ * lfmm.h -- C ABI of the B200 (sm_100a) Laplace fast multipole method.
+ *
+ * Drop-in boundary for the reference's solver classes: every entry point
+ * takes plain pointers and sizes, returns an int status (0 = success, < 0 =
+ * error, message via lfmm_last_error), never throws or aborts.  One context
+ * per host thread; a context owns a CUDA stream, a device arena reused across
+ * solves, and the rotation tables (the reference's process-global
+ * InitMathConstants / cudaCopyMathConstants state, made per-context).
+ *
+ * Reference interfaces replaced (paths relative to the reference's src/):
+ *   lfmm3d_solve   fmm::gpu::FastMultipole3d<double>(particles, eps, N, tree_depth)
+ *                  cuda/multipole3d.h:16, and the source/target overload :17;
+ *                  the CPU twins cpu/multipole3d.h:19-21
+ *   lfmm2d_solve   fmm::gpu::FastMultipole(particles, eps, N, tree_depth)
+ *                  cuda/multipole.h:11, source/target overload :12;
+ *                  CPU twins cpu/multipole.h:13-15
+ *   lfmm3d_direct / lfmm2d_direct
+ *                  fmm::gpu::ComputeExact<Potential3d|Force3d|Potential2d|Force2d>
+ *                  common/simple_math.h:283-313 (common/simple_math.cu:25-130)
+ *   lfmm_tree_*    fmm::MortonTree<dim,...> public members (levels, level_sizes,
+ *                  positions_map, closeneighbours, farneighbours),
+ *                  cpu/morton_tree.h:24-45
+ *
+ * Conventions kept from the reference:
+ *   - N is the number of degrees (order p = N - 1), clamped to 18 (3D) / 30
+ *     (2D); LFMM_AUTO picks N from eps and the depth from the particle count
+ *     with the reference's formulas (cpu/multipole3d.cpp:1328-1337,
+ *     cpu/multipole.cpp:478-486).
+ *   - Potential includes the self term q_i / 1e-4 (3D) or q_i log(1e-4) (2D);
+ *     all distances are clamped at 1e-4.
+ *   - Source+target solves: targets carry q = 0 and outputs are for targets
+ *     only, in input order.  Source-only solves: outputs for every source in
+ *     input order.  As in the reference, a source-only solve in which some
+ *     charge is exactly 0 evaluates only the zero-charge particles.
+ *   - 3D field = -grad(potential) = sum q (r_i - r_j) / |r_i - r_j|^3,
+ *     xyz per particle; 2D "force" = sum q / (z_i - z_j) as (re, im).
+ */
+#ifndef LFMM_H
+#define LFMM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LFMM_AUTO 2147483647
+
+/* status codes */
+#define LFMM_OK 0
+#define LFMM_ERR_ARG (-1)
+#define LFMM_ERR_CUDA (-2)
+#define LFMM_ERR_OOM (-3)
+#define LFMM_ERR_DEVICE (-4)
+#define LFMM_ERR_UNSUPPORTED (-5)
+
+/* precision: plain FP64 (the reference's arithmetic), or the mixed form */
+#define LFMM_PRECISION_FP64 0
+#define LFMM_PRECISION_MIXED 1
+
+typedef struct lfmm_ctx lfmm_ctx;
+
+typedef struct {
+	int device;   /* CUDA device ordinal */
+	int verbose;  /* 0: silent */
+	int timing;   /* 1: record per-phase CUDA events into lfmm_stats */
+} lfmm_options;
+
+typedef struct {
+	int order_N;            /* resolved number of degrees */
+	int depth;              /* resolved tree depth (levels) */
+	size_t n_particles;     /* particles in the tree (sources + targets) */
+	size_t n_cells, n_leaves, targets_num;
+	size_t n_far_pairs;     /* M2L interactions */
+	size_t n_close_pairs;   /* leaf-leaf near-field interactions (full lists) */
+	size_t n_p2p_pairs;     /* particle-particle evaluations in the near field */
+	float ms_tree, ms_upward, ms_m2l, ms_l2l, ms_leaves, ms_total; /* device time, when timing */
+} lfmm_stats;
+
+int lfmm_create(lfmm_ctx** ctx, const lfmm_options* opt);
+void lfmm_destroy(lfmm_ctx* ctx);
+const char* lfmm_last_error(const lfmm_ctx* ctx);
+int lfmm_version(void);
+/* the context's CUDA stream (cudaStream_t), for callers that order work on it */
+void* lfmm_stream(lfmm_ctx* ctx);
+
+/* ---- 3D ----------------------------------------------------------------
+ * Host buffers.  src_xyz: n_src x 3, src_q: n_src, tgt_xyz: n_tgt x 3 (or
+ * NULL with n_tgt = 0).  pot: n_out, field: n_out x 3, n_out = n_tgt ? n_tgt
+ * : n_src.  Blocking: returns when the results are in the host buffers. */
+int lfmm3d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                 const double* tgt_xyz, int N, int tree_depth, double eps, int precision, double* pot,
+                 double* field, lfmm_stats* stats);
+/* Same with device buffers; enqueued on the context's stream, returns after
+ * the solve has been issued and its host-side sizing syncs are done (the
+ * results are complete once the stream is synchronised). */
+int lfmm3d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                        const double* tgt_xyz, int N, int tree_depth, double eps, int precision, double* pot,
+                        double* field, lfmm_stats* stats);
+
+/* ---- 2D ---------------------------------------------------------------- */
+int lfmm2d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                 const double* tgt_xy, int N, int tree_depth, double eps, int precision, double* pot,
+                 double* field, lfmm_stats* stats);
+int lfmm2d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                        const double* tgt_xy, int N, int tree_depth, double eps, int precision, double* pot,
+                        double* field, lfmm_stats* stats);
+
+/* ---- FP64 direct sums (the accuracy oracle on the GPU) -------------------
+ * Every target against every source, same clamp and self term as the FMM.
+ * Host and device-buffer variants. */
+int lfmm3d_direct(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                  const double* tgt_xyz, double* pot, double* field);
+int lfmm3d_direct_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                         const double* tgt_xyz, double* pot, double* field);
+int lfmm2d_direct(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                  const double* tgt_xy, double* pot, double* field);
+int lfmm2d_direct_device(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                         const double* tgt_xy, double* pot, double* field);
+
+/* ---- tree inspection (the reference's MortonTree members) ----------------
+ * lfmm_tree_build builds the uniform tree of [targets | sources] on the
+ * device (host input buffers, q = NULL means all targets) and keeps it in the
+ * context until the next call.  Level L cells are read with
+ * lfmm_tree_level (codes, particle / child ranges, target ranges, parents,
+ * centres as dim doubles each); lists with lfmm_tree_lists (close lists are
+ * the full symmetric lists; far lists in the reference's order);
+ * positions[i] = tree position of input particle i. */
+int lfmm_tree_build(lfmm_ctx* ctx, int dim, size_t n_src, const double* src_pts, const double* src_q, size_t n_tgt,
+                    const double* tgt_pts, int tree_depth, size_t* level_sizes, size_t* targets_num);
+int lfmm_tree_level(lfmm_ctx* ctx, int level, unsigned long long* code, long long* beg, long long* end,
+                    long long* tbeg, long long* tend, long long* parent, double* center);
+int lfmm_tree_list_sizes(lfmm_ctx* ctx, int level, long long* n_close, long long* n_far);
+int lfmm_tree_lists(lfmm_ctx* ctx, int level, long long* close, long long* far);
+int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
+
+/* ---- rotation tables (tests) --------------------------------------------
+ * Wigner small-d matrix for table slot `slot` (layout n(n+1)(4n-1)/6 +
+ * m(2n+1) + k + n, N = 18) and its canonical angle; returns the number of
+ * slots, or < 0. */
+int lfmm_wignerd_slot(lfmm_ctx* ctx, int slot, double* theta, double* d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LFMM_H */

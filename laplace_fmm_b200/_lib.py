@@ -1,0 +1,130 @@
+"""ctypes binding of ``liblfmm.so`` (the C ABI in ``include/lfmm.h``).
+
+The shared library is the product: every solve runs in its CUDA kernels.
+Loading fails loudly when the library is missing; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblfmm.so"
+
+AUTO = 2147483647
+PRECISION = {"fp64": 0, "mixed": 1}
+STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_DEVICE", -5: "ERR_UNSUPPORTED"}
+
+# Every symbol include/lfmm.h declares (checked by the CPU tests).
+EXPORTS = [
+    "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream",
+    "lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device",
+    "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
+    "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
+    "lfmm_wignerd_slot",
+]
+
+
+class LfmmOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("verbose", ctypes.c_int), ("timing", ctypes.c_int)]
+
+
+class LfmmStats(ctypes.Structure):
+    _fields_ = [
+        ("order_N", ctypes.c_int), ("depth", ctypes.c_int),
+        ("n_particles", ctypes.c_size_t), ("n_cells", ctypes.c_size_t), ("n_leaves", ctypes.c_size_t),
+        ("targets_num", ctypes.c_size_t), ("n_far_pairs", ctypes.c_size_t), ("n_close_pairs", ctypes.c_size_t),
+        ("n_p2p_pairs", ctypes.c_size_t),
+        ("ms_tree", ctypes.c_float), ("ms_upward", ctypes.c_float), ("ms_m2l", ctypes.c_float),
+        ("ms_l2l", ctypes.c_float), ("ms_leaves", ctypes.c_float), ("ms_total", ctypes.c_float),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LfmmError(RuntimeError):
+    pass
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load(path: Path | str = LIB_PATH):
+    """Load the library (no GPU needed just to load it)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not Path(path).exists():
+            raise LfmmError(f"{path} is not built: run `python -m laplace_fmm_b200.build`")
+        L = ctypes.CDLL(str(path))
+        P, SZ, I, D = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double
+        L.lfmm_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(LfmmOptions)]
+        L.lfmm_destroy.argtypes = [P]
+        L.lfmm_destroy.restype = None
+        L.lfmm_last_error.argtypes = [P]
+        L.lfmm_last_error.restype = ctypes.c_char_p
+        L.lfmm_stream.argtypes = [P]
+        L.lfmm_stream.restype = P
+        solve = [P, SZ, P, P, SZ, P, I, I, D, I, P, P, ctypes.POINTER(LfmmStats)]
+        for f in ("lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device"):
+            getattr(L, f).argtypes = solve
+        for f in ("lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device"):
+            getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, P, P]
+        L.lfmm_tree_build.argtypes = [P, I, SZ, P, P, SZ, P, I, P, P]
+        L.lfmm_tree_level.argtypes = [P, I, P, P, P, P, P, P, P]
+        L.lfmm_tree_list_sizes.argtypes = [P, I, P, P]
+        L.lfmm_tree_lists.argtypes = [P, I, P, P]
+        L.lfmm_tree_positions.argtypes = [P, P]
+        L.lfmm_wignerd_slot.argtypes = [P, I, ctypes.POINTER(D), P]
+        _lib = L
+        return L
+
+
+class Context:
+    """One solver context (CUDA stream + device arena + rotation tables)."""
+
+    def __init__(self, device: int = 0, timing: bool = False):
+        self.lib = load()
+        self.handle = ctypes.c_void_p()
+        opt = LfmmOptions(device, 0, 1 if timing else 0)
+        st = self.lib.lfmm_create(ctypes.byref(self.handle), ctypes.byref(opt))
+        if st != 0:
+            raise LfmmError(f"lfmm_create failed ({STATUS.get(st, st)}): no usable CUDA device {device}?")
+        self.device = device
+
+    def check(self, st: int, what: str):
+        if st != 0:
+            msg = self.lib.lfmm_last_error(self.handle).decode()
+            raise LfmmError(f"{what}: {STATUS.get(st, st)}: {msg}")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.lfmm_stream(self.handle)
+
+    def close(self):
+        if self.handle:
+            self.lib.lfmm_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    with _lock:
+        ctx = _default.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        with _lock:
+            _default[device] = ctx
+    return ctx

@@ -1,0 +1,475 @@
+// C ABI (include/lfmm.h): contexts, host/device solves, direct sums, tree
+// inspection.  No exceptions cross this boundary; every entry returns a
+// status and records a message for lfmm_last_error.
+#include "../../include/lfmm.h"
+#include "fmm2d.cuh"
+#include "direct.cuh"
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <algorithm>
+
+struct lfmm_ctx {
+	lfmm::Context c;
+	lfmm::DevTree tree;
+	bool has_tree = false;
+};
+
+namespace lfmm {
+
+Arena::~Arena() { release(); }
+
+void Arena::release()
+{
+	for (void* p : extra_) cudaFree(p);
+	extra_.clear();
+	if (base_) cudaFree(base_);
+	base_ = nullptr; cap_ = used_ = extra_total_ = 0;
+}
+
+void* Arena::take(size_t bytes)
+{
+	bytes = (bytes + 255) & ~size_t(255);
+	if (used_ + bytes <= cap_) {
+		void* p = base_ + used_;
+		used_ += bytes;
+		high_ = std::max(high_, used_ + extra_total_);
+		return p;
+	}
+	void* p = nullptr;
+	if (cudaMalloc(&p, bytes) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+	extra_.push_back(p);
+	extra_total_ += bytes;
+	high_ = std::max(high_, used_ + extra_total_);
+	return p;
+}
+
+void Arena::settle()
+{
+	if (!extra_.empty()) {
+		cudaDeviceSynchronize();
+		for (void* p : extra_) cudaFree(p);
+		extra_.clear();
+		size_t want = high_ + (high_ >> 3);
+		if (base_) cudaFree(base_);
+		base_ = nullptr; cap_ = 0;
+		if (cudaMalloc(&base_, want) == cudaSuccess) cap_ = want;
+		else { cudaGetLastError(); base_ = nullptr; }
+	}
+	extra_total_ = 0;
+	used_ = 0;
+}
+
+int cuda_fail(Context& ctx, cudaError_t e, const char* where)
+{
+	ctx.last_error = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") at " + where;
+	return ERR_CUDA;
+}
+
+} // namespace lfmm
+
+using namespace lfmm;
+
+namespace {
+
+int resolve_order(int dim, int N, double eps)
+{
+	if (dim == 3) {
+		eps = std::max(eps, 1.e-11);
+		if (N == AUTO) return std::min(MAXN3, (int)(54.2 - 10.73 * std::sqrt(std::log(2.4 * eps) + 25.5)));
+		return std::min(MAXN3, N);
+	}
+	if (N == AUTO) return std::min(MAXN2, (int)(-1.18 * std::log(1.65 * eps)));
+	return std::min(MAXN2, N);
+}
+
+int resolve_depth(int dim, int depth, size_t n)
+{
+	if (depth != AUTO) return depth;
+	if (dim == 3) return (int)std::max(2.0, 1 + std::log((double)n / 100.0) / std::log(8.0));
+	return (int)std::max(3.0, 2 + std::log((double)n / 100.0) / std::log(4.0));
+}
+
+int check_flags(Context& c)
+{
+	unsigned f = 0;
+	LFMM_CUDA(c, cudaMemcpyAsync(&f, c.dev_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+	LFMM_CUDA(c, cudaStreamSynchronize(c.stream));
+	if (f) {
+		cudaMemsetAsync(c.dev_flags, 0, sizeof(unsigned), c.stream);
+		c.last_error = "device-side check failed (flags " + std::to_string(f) + ")";
+		return ERR_DEVICE;
+	}
+	return OK;
+}
+
+void fill_stats(lfmm_stats* out, const SolveStats& s)
+{
+	if (!out) return;
+	out->order_N = s.N; out->depth = s.depth;
+	out->n_particles = s.n_particles; out->n_cells = s.n_cells; out->n_leaves = s.n_leaves;
+	out->targets_num = s.targets_num; out->n_far_pairs = s.n_far_pairs; out->n_close_pairs = s.n_close_pairs;
+	out->n_p2p_pairs = s.n_p2p_pairs;
+	out->ms_tree = s.ms_tree; out->ms_upward = s.ms_upward; out->ms_m2l = s.ms_m2l; out->ms_l2l = s.ms_l2l;
+	out->ms_leaves = s.ms_leaves; out->ms_total = s.ms_total;
+}
+
+int select_device(lfmm_ctx* ctx)
+{
+	cudaError_t e = cudaSetDevice(ctx->c.device);
+	if (e != cudaSuccess) return cuda_fail(ctx->c, e, "cudaSetDevice");
+	return OK;
+}
+
+// Device solve shared by the host and device entry points.
+int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                 int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats,
+                 bool arena_reset)
+{
+	Context& c = ctx->c;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return ERR_ARG; }
+	if ((ns && (!src || !q)) || (nt && !tgt) || !pot || !field) { c.last_error = "null buffer"; return ERR_ARG; }
+	if (precision != LFMM_PRECISION_FP64 && precision != LFMM_PRECISION_MIXED) { c.last_error = "unknown precision"; return ERR_ARG; }
+	int Nr = resolve_order(dim, N, eps);
+	int Dr = resolve_depth(dim, depth, ns + nt);
+	if (Nr < 1) { c.last_error = "order must be >= 1"; return ERR_ARG; }
+	if (Dr < 1) { c.last_error = "tree depth must be >= 1"; return ERR_ARG; }
+	if (arena_reset) c.arena.reset();
+	ctx->has_tree = false;
+	ParticleInput in;
+	in.dim = dim; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q; in.tgt = tgt;
+	SolveStats ss;
+	int st = dim == 3 ? fmm3d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr)
+	                  : fmm2d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
+	if (st) return st;
+	fill_stats(stats, ss);
+	return OK;
+}
+
+int solve_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+               int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+{
+	Context& c = ctx->c;
+	if (select_device(ctx)) return ERR_CUDA;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return ERR_ARG; }
+	if ((ns && (!src || !q)) || (nt && !tgt) || !pot || !field) { c.last_error = "null buffer"; return ERR_ARG; }
+	c.arena.reset();
+	const size_t nout = nt ? nt : ns;
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(nt, 1)));
+	double* dpot = static_cast<double*>(c.arena.take(sizeof(double) * nout));
+	double* dfld = static_cast<double*>(c.arena.take(sizeof(double) * dim * nout));
+	if (!dsrc || !dq || !dtgt || !dpot || !dfld) { c.last_error = "device allocation failed"; return ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * dim * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
+	int st = solve_device(ctx, dim, ns, dsrc, dq, nt, dtgt, N, depth, eps, precision, dpot, dfld, stats, false);
+	if (st == OK) {
+		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * dim * nout, cudaMemcpyDeviceToHost, s));
+		st = check_flags(c);
+	}
+	c.arena.settle();
+	return st;
+}
+
+int direct_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                double* pot, double* field)
+{
+	Context& c = ctx->c;
+	if (select_device(ctx)) return ERR_CUDA;
+	if ((ns && (!src || !q)) || (nt && (!tgt || !pot || !field))) { c.last_error = "null buffer"; return ERR_ARG; }
+	c.arena.reset();
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(nt, 1)));
+	double* dpot = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(nt, 1)));
+	double* dfld = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(nt, 1)));
+	if (!dsrc || !dq || !dtgt || !dpot || !dfld) { c.last_error = "device allocation failed"; return ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * dim * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
+	int st = direct_device(c, dim, ns, dsrc, dq, nt, dtgt, dpot, dfld);
+	if (st == OK && nt) {
+		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * dim * nt, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(c, cudaStreamSynchronize(s));
+	}
+	c.arena.settle();
+	return st;
+}
+
+int need_tree(lfmm_ctx* ctx, int level)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (!ctx->has_tree) { ctx->c.last_error = "no tree: call lfmm_tree_build first"; return LFMM_ERR_ARG; }
+	if (level < 0 || level >= ctx->tree.depth) { ctx->c.last_error = "level out of range"; return LFMM_ERR_ARG; }
+	return LFMM_OK;
+}
+
+template <typename D, typename S>
+int fetch(Context& c, D* dst, const S* src, size_t n)
+{
+	std::vector<S> tmp(n);
+	if (n) LFMM_CUDA(c, cudaMemcpy(tmp.data(), src, sizeof(S) * n, cudaMemcpyDeviceToHost));
+	for (size_t i = 0; i < n; ++i) dst[i] = (D)tmp[i];
+	return OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int lfmm_version(void) { return 100; }
+
+int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
+{
+	if (!out) return LFMM_ERR_ARG;
+	*out = nullptr;
+	lfmm_ctx* ctx = new (std::nothrow) lfmm_ctx();
+	if (!ctx) return LFMM_ERR_OOM;
+	Context& c = ctx->c;
+	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+		cudaGetLastError();
+		delete ctx;
+		return LFMM_ERR_CUDA;
+	}
+	if (c.device < 0 || c.device >= ndev || cudaSetDevice(c.device) != cudaSuccess) { delete ctx; return LFMM_ERR_ARG; }
+	if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaMalloc(&c.dev_flags, sizeof(unsigned)) != cudaSuccess ||
+	    cudaMemset(c.dev_flags, 0, sizeof(unsigned)) != cudaSuccess) {
+		delete ctx;
+		return LFMM_ERR_CUDA;
+	}
+	for (auto& e : c.ev) cudaEventCreate(&e);
+	if (tables_build(c) != OK) {
+		lfmm_destroy(ctx);
+		return LFMM_ERR_CUDA;
+	}
+	*out = ctx;
+	return LFMM_OK;
+}
+
+void lfmm_destroy(lfmm_ctx* ctx)
+{
+	if (!ctx) return;
+	Context& c = ctx->c;
+	cudaSetDevice(c.device);
+	if (c.stream) cudaStreamSynchronize(c.stream);
+	c.arena.release();
+	tables_free(c.tables);
+	for (auto& e : c.ev) if (e) cudaEventDestroy(e);
+	if (c.dev_flags) cudaFree(c.dev_flags);
+	if (c.stream) cudaStreamDestroy(c.stream);
+	delete ctx;
+}
+
+const char* lfmm_last_error(const lfmm_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "null context"; }
+
+void* lfmm_stream(lfmm_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+int lfmm3d_solve(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt, int N,
+                 int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	return solve_host(ctx, 3, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats);
+}
+
+int lfmm3d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                        int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats, true);
+	if (st == OK && stats) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
+int lfmm2d_solve(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt, int N,
+                 int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	return solve_host(ctx, 2, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats);
+}
+
+int lfmm2d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                        int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = solve_device(ctx, 2, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats, true);
+	if (st == OK && stats) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
+int lfmm3d_direct(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                  double* pot, double* field)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	return direct_host(ctx, 3, ns, src, q, nt, tgt, pot, field);
+}
+
+int lfmm2d_direct(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                  double* pot, double* field)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	return direct_host(ctx, 2, ns, src, q, nt, tgt, pot, field);
+}
+
+int lfmm3d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                         double* pot, double* field)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	return direct_device(ctx->c, 3, ns, src, q, nt, tgt, pot, field);
+}
+
+int lfmm2d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                         double* pot, double* field)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	return direct_device(ctx->c, 2, ns, src, q, nt, tgt, pot, field);
+}
+
+// ---- tree inspection -------------------------------------------------------
+
+int lfmm_tree_build(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
+                    const double* tgt, int depth, size_t* level_sizes, size_t* targets_num)
+{
+	if (!ctx || (dim != 2 && dim != 3)) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return LFMM_ERR_ARG; }
+	c.arena.reset();
+	ctx->has_tree = false;
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(nt, 1)));
+	if (!dsrc || !dq || !dtgt) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * dim * ns, cudaMemcpyHostToDevice, s));
+		if (q) LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+		else LFMM_CUDA(c, cudaMemsetAsync(dq, 0, sizeof(double) * ns, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
+	ParticleInput in;
+	in.dim = dim; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
+	int st = tree_build(c, in, resolve_depth(dim, depth, ns + nt), ctx->tree);
+	if (st) return st;
+	st = check_flags(c);
+	if (st) return st;
+	ctx->has_tree = true;
+	for (int L = 0; L < ctx->tree.depth && level_sizes; ++L) level_sizes[L] = ctx->tree.lsize[L];
+	if (targets_num) *targets_num = ctx->tree.targets_num;
+	return LFMM_OK;
+}
+
+int lfmm_tree_level(lfmm_ctx* ctx, int L, unsigned long long* code, long long* beg, long long* end, long long* tbeg,
+                    long long* tend, long long* parent, double* center)
+{
+	int st = need_tree(ctx, L);
+	if (st) return st;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	size_t o = t.loff[L], m = t.lsize[L];
+	if (code && (st = fetch(c, code, t.code + o, m))) return st;
+	if (beg && (st = fetch(c, beg, t.beg + o, m))) return st;
+	if (end && (st = fetch(c, end, t.end + o, m))) return st;
+	if (tbeg && (st = fetch(c, tbeg, t.tbeg + o, m))) return st;
+	if (tend && (st = fetch(c, tend, t.tend + o, m))) return st;
+	if (parent && (st = fetch(c, parent, t.parent + o, m))) return st;
+	if (center) {
+		std::vector<double> x(m), y(m), z(m);
+		if ((st = fetch(c, x.data(), t.cx + o, m)) || (st = fetch(c, y.data(), t.cy + o, m))) return st;
+		if (t.dim == 3 && (st = fetch(c, z.data(), t.cz + o, m))) return st;
+		for (size_t i = 0; i < m; ++i) {
+			center[t.dim * i] = x[i]; center[t.dim * i + 1] = y[i];
+			if (t.dim == 3) center[3 * i + 2] = z[i];
+		}
+	}
+	return LFMM_OK;
+}
+
+int lfmm_tree_list_sizes(lfmm_ctx* ctx, int L, long long* n_close, long long* n_far)
+{
+	int st = need_tree(ctx, L);
+	if (st) return st;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	size_t o = t.loff[L], m = t.lsize[L];
+	if (n_close && (st = fetch(c, n_close, t.close_cnt + o, m))) return st;
+	if (n_far && (st = fetch(c, n_far, t.far_cnt + o, m))) return st;
+	return LFMM_OK;
+}
+
+int lfmm_tree_lists(lfmm_ctx* ctx, int L, long long* close, long long* far)
+{
+	int st = need_tree(ctx, L);
+	if (st) return st;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	size_t o = t.loff[L], m = t.lsize[L];
+	std::vector<int32_t> cnt(m);
+	if ((st = fetch(c, cnt.data(), t.close_cnt + o, m))) return st;
+	if (close) {
+		std::vector<int32_t> idx(m * t.close_stride);
+		if ((st = fetch(c, idx.data(), t.close_idx + o * t.close_stride, m * t.close_stride))) return st;
+		size_t a = 0;
+		for (size_t i = 0; i < m; ++i)
+			for (int k = 0; k < cnt[i]; ++k) close[a++] = idx[i * t.close_stride + k];
+	}
+	if (far && L >= 2) {
+		std::vector<int32_t> fc(m);
+		if ((st = fetch(c, fc.data(), t.far_cnt + o, m))) return st;
+		size_t total = 0;
+		for (auto v : fc) total += (size_t)v;
+		uint32_t* off = static_cast<uint32_t*>(c.arena.take(sizeof(uint32_t) * (m + 1)));
+		int32_t* idx = static_cast<int32_t*>(c.arena.take(sizeof(int32_t) * (total + 1)));
+		if (!off || !idx) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+		if ((st = tree_far_lists(c, t, L, off, idx, total))) return st;
+		if ((st = check_flags(c))) return st;
+		if ((st = fetch(c, far, idx, total))) return st;
+	}
+	return LFMM_OK;
+}
+
+int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions)
+{
+	int st = need_tree(ctx, 0);
+	if (st) return st;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	std::vector<uint32_t> orig(t.n);
+	if ((st = fetch(c, orig.data(), t.orig, t.n))) return st;
+	for (size_t s = 0; s < t.n; ++s) positions[orig[s]] = (long long)s;
+	return LFMM_OK;
+}
+
+int lfmm_wignerd_slot(lfmm_ctx* ctx, int slot, double* theta, double* d)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Tables& T = ctx->c.tables;
+	if (slot < 0 || slot >= T.d.n_dslots) return T.d.n_dslots;
+	if (theta) *theta = T.theta_of_slot[slot];
+	if (d) {
+		cudaError_t e = cudaMemcpy(d, T.d.dmat + (size_t)slot * dsize(MAXN3), sizeof(double) * dsize(MAXN3),
+		                           cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) return cuda_fail(ctx->c, e, "lfmm_wignerd_slot");
+	}
+	return T.d.n_dslots;
+}
+
+} // extern "C"

@@ -1,0 +1,78 @@
+// Solver context: stream, device arena, math tables, error state.
+#pragma once
+#include "common.cuh"
+#include <string>
+#include <vector>
+
+namespace lfmm {
+
+// Bump allocator over one device block.  A solve that outgrows the block
+// takes extra cudaMalloc chunks; at the end of the solve they are released and
+// the block is regrown to the high-water mark, so repeated solves of the same
+// shape allocate nothing.
+class Arena {
+public:
+	~Arena();
+	void reset() { used_ = 0; }
+	void* take(size_t bytes);               // nullptr on cudaMalloc failure
+	void settle();                          // end of solve: consolidate chunks
+	size_t capacity() const { return cap_; }
+	size_t high_water() const { return high_; }
+	void release();
+private:
+	char* base_ = nullptr;
+	size_t cap_ = 0, used_ = 0, high_ = 0, extra_total_ = 0;
+	std::vector<void*> extra_;
+};
+
+// Rotation / translation tables, built once per context on the GPU (FP64).
+// DevTables is the plain-pointer view passed to kernels.
+struct DevTables {
+	// Wigner small-d matrices (N = 18 layout) for each theta slot
+	double* dmat = nullptr;
+	int n_dslots = 0;
+	// (cos m phi, sin m phi), m < 18, for each phi slot
+	double2* emat = nullptr;
+	int n_eslots = 0;
+	// per integer direction (dx+3)*49+(dy+3)*7+(dz+3):
+	// {dslot(theta), dslot(-theta), eslot(phi), eslot(-phi)}, -1 if absent
+	int4* dirinfo = nullptr;
+	// K(n,m) and the translation coefficient cubes [j][k][n] (18^3)
+	double* knm = nullptr;
+	double* m2l = nullptr;
+	double* m2m = nullptr;
+	double* l2l = nullptr;
+};
+
+struct Tables {
+	DevTables d;
+	// host copies of the canonical angles (tests)
+	std::vector<double> theta_of_slot, phi_of_slot;
+	std::vector<int4> dirinfo_host;
+};
+
+struct Context {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	Arena arena;
+	Tables tables;
+	unsigned* dev_flags = nullptr;      // device error flags
+	std::string last_error;
+	int verbose = 0;
+	cudaEvent_t ev[16] = {};
+	int timing = 0;
+};
+
+int tables_build(Context& ctx);
+void tables_free(Tables& t);
+
+// set last_error from a CUDA error; returns ERR_CUDA
+int cuda_fail(Context& ctx, cudaError_t e, const char* where);
+
+#define LFMM_CUDA(ctx, call)                                                   \
+	do {                                                                       \
+		cudaError_t e__ = (call);                                              \
+		if (e__ != cudaSuccess) return ::lfmm::cuda_fail((ctx), e__, #call);  \
+	} while (0)
+
+} // namespace lfmm

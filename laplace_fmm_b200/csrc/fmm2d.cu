@@ -1,0 +1,318 @@
+// 2D Laplace FMM, FP64, following the reference's CPU solver
+// (cpu/multipole.cpp): P2M 22-36, M2M 38-53, M2L 66-84, L2L 86-97, passes
+// 99-231 (per level: L2L from the parent, then M2L from the far list),
+// leaves 233-449 (P2P + L2P for potential and field).
+// Warp per box with one expansion coefficient per lane (N <= 30), block per
+// leaf for the near field.
+#include "fmm2d.cuh"
+
+namespace lfmm {
+
+namespace {
+
+constexpr int WPB2 = 4;
+constexpr int BINOM_N = 2 * MAXN2;
+__constant__ double c_binom[BINOM_N * BINOM_N];   // Pascal triangle, C(n,k) at n*60+k
+
+struct Exp2 {
+	int N;
+	double2* outer;
+	double2* inner;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{ return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b)
+{
+	double d = b.x * b.x + b.y * b.y;
+	return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 cpow_u(double2 b, int e)
+{
+	double2 r = make_double2(1.0, 0.0);
+	while (e) { if (e & 1) r = cmul(r, b); e >>= 1; b = cmul(b, b); }
+	return r;
+}
+__device__ __forceinline__ void coords2(uint64_t code, int* c) { c[0] = (int)compact2(code >> 1); c[1] = (int)compact2(code); }
+
+// a_k = -sum q (z - z0)^k / k, a_0 = sum q
+__global__ void __launch_bounds__(WPB2 * 32) p2m2d_kernel(DevTree t, Exp2 E)
+{
+	__shared__ double2 sacc[WPB2][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int LL = t.depth - 1;
+	size_t leaf = (size_t)blockIdx.x * WPB2 + w;
+	if (leaf >= t.lsize[LL]) return;
+	size_t g = t.loff[LL] + leaf;
+	const int N = E.N;
+	sacc[w][lane] = make_double2(0.0, 0.0);
+	__syncwarp();
+	const double cx = t.cx[g], cy = t.cy[g];
+	for (uint32_t base = t.beg[g]; base < t.end[g]; base += 32) {
+		uint32_t i = base + lane;
+		double q = 0.0;
+		double2 z = make_double2(0.0, 0.0);
+		if (i < t.end[g]) { q = t.q[i]; z = make_double2(t.x[i] - cx, t.y[i] - cy); }
+		for (int k = 0; k < N; ++k) {
+			double vr, vi;
+			if (k == 0) { vr = q; vi = 0.0; }
+			else { double2 p = cpow_u(z, k); vr = q * p.x; vi = q * p.y; }
+			vr = warp_sum(vr); vi = warp_sum(vi);
+			if (lane == 0) { sacc[w][k].x += vr; sacc[w][k].y += vi; }
+		}
+	}
+	__syncwarp();
+	if (lane < N) {
+		double2 a = sacc[w][lane];
+		if (lane > 0) a = make_double2(-a.x / lane, -a.y / lane);
+		E.outer[g * N + lane] = a;
+	}
+}
+
+// b_j += sum_{i=1..j} a_i z0^(j-i) C(j-1, i-1) - a_0 z0^j / j, b_0 += a_0 ; z0 = child - parent
+__global__ void __launch_bounds__(WPB2 * 32) m2m2d_kernel(DevTree t, Exp2 E, int L)
+{
+	__shared__ double2 sa[WPB2][32];
+	__shared__ double2 sp[WPB2][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t c = (size_t)blockIdx.x * WPB2 + w;
+	if (c >= t.lsize[L]) return;
+	const int N = E.N;
+	size_t g = t.loff[L] + c, cb = t.loff[L + 1];
+	double2 acc = make_double2(0.0, 0.0);
+	for (uint32_t k = t.beg[g]; k < t.end[g]; ++k) {
+		size_t gk = cb + k;
+		double2 z0 = make_double2(t.cx[gk] - t.cx[g], t.cy[gk] - t.cy[g]);
+		__syncwarp();
+		if (lane < N) { sa[w][lane] = E.outer[gk * N + lane]; sp[w][lane] = cpow_u(z0, lane); }
+		__syncwarp();
+		int j = lane;
+		if (j < N) {
+			if (j == 0) { acc.x += sa[w][0].x; acc.y += sa[w][0].y; }
+			else {
+				double2 s = make_double2(0.0, 0.0);
+				for (int i = 1; i <= j; ++i) {
+					double2 v = cmul(sa[w][i], sp[w][j - i]);
+					double bc = c_binom[(j - 1) * BINOM_N + (i - 1)];
+					s.x += v.x * bc; s.y += v.y * bc;
+				}
+				double2 a0z = cmul(sa[w][0], sp[w][j]);
+				acc.x += s.x - a0z.x / j; acc.y += s.y - a0z.y / j;
+			}
+		}
+	}
+	if (lane < N) E.outer[g * N + lane] = acc;
+}
+
+// Per level L >= 2: b = L2L(parent inner) (overwrite), then += M2L over the
+// far list.  L2L as b_k = sum_{n>=k} a_n C(n,k) (-z0)^(n-k), z0 = parent - child
+// (the reference's in-place Horner shift, cpu/multipole.cpp:86-97).
+// M2L: z0 = source - target; b_0 += a_0 conj(log(-z0)) + sum_j w_j,
+// b_i += (-a_0 / i + sum_j w_j C(i+j-1, j-1)) / z0^i, w_j = (-1)^j a_j / z0^j.
+__global__ void __launch_bounds__(WPB2 * 32) down2d_kernel(DevTree t, Exp2 E, int L)
+{
+	__shared__ double2 sa[WPB2][32];
+	__shared__ double2 sw[WPB2][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t c = (size_t)blockIdx.x * WPB2 + w;
+	if (c >= t.lsize[L]) return;
+	const int N = E.N;
+	size_t off = t.loff[L], poff = t.loff[L - 1], g = off + c;
+	int32_t p = t.parent[g];
+	size_t gp = poff + p;
+	double2 acc = make_double2(0.0, 0.0);
+	if (L >= 3) {
+		double2 mz = make_double2(-(t.cx[gp] - t.cx[g]), -(t.cy[gp] - t.cy[g]));
+		if (lane < N) sa[w][lane] = E.inner[gp * N + lane];
+		__syncwarp();
+		if (lane < N) {
+			double2 pw = make_double2(1.0, 0.0);
+			for (int n = lane; n < N; ++n) {
+				double2 v = cmul(sa[w][n], pw);
+				double bc = c_binom[n * BINOM_N + lane];
+				acc.x += v.x * bc; acc.y += v.y * bc;
+				pw = cmul(pw, mz);
+			}
+		}
+	}
+	int me[2];
+	coords2(t.code[g], me);
+	int npc = t.close_cnt[gp];
+	const int32_t* pl = t.close_idx + gp * t.close_stride;
+	const double cx = t.cx[g], cy = t.cy[g];
+	for (int e = 0; e <= npc; ++e) {
+		int32_t pn = e < npc ? pl[e] : p;
+		for (uint32_t k = t.beg[poff + pn]; k < t.end[poff + pn]; ++k) {
+			if (k == c) continue;
+			size_t gk = off + k;
+			int o[2];
+			coords2(t.code[gk], o);
+			if (max(abs(o[0] - me[0]), abs(o[1] - me[1])) <= 1) continue;
+			double2 z0 = make_double2(t.cx[gk] - cx, t.cy[gk] - cy);
+			__syncwarp();
+			double2 zl = make_double2(1.0, 0.0);
+			if (lane < N) {
+				double2 a = E.outer[gk * N + lane];
+				sa[w][lane] = a;
+				zl = cpow_u(z0, lane);
+				sw[w][lane] = lane == 0 ? a : cdiv(make_double2(dsgn(lane) * a.x, dsgn(lane) * a.y), zl);
+			}
+			__syncwarp();
+			if (lane < N) {
+				double2 a0 = sa[w][0];
+				if (lane == 0) {
+					double2 mz = make_double2(-z0.x, -z0.y);
+					double2 lg = make_double2(log(sqrt(mz.x * mz.x + mz.y * mz.y)), -atan2(mz.y, mz.x));
+					double2 v = cmul(a0, lg);
+					double sr = v.x, si = v.y;
+					for (int j = 1; j < N; ++j) { sr += sw[w][j].x; si += sw[w][j].y; }
+					acc.x += sr; acc.y += si;
+				} else {
+					int i = lane;
+					double sr = 0.0, si = 0.0;
+					for (int j = 1; j < N; ++j) {
+						double bc = c_binom[(i + j - 1) * BINOM_N + (j - 1)];
+						sr += sw[w][j].x * bc; si += sw[w][j].y * bc;
+					}
+					double2 num = make_double2(-a0.x / i + sr, -a0.y / i + si);
+					double2 v = cdiv(num, zl);
+					acc.x += v.x; acc.y += v.y;
+				}
+			}
+		}
+	}
+	if (lane < N) E.inner[g * N + lane] = acc;
+}
+
+constexpr int LT2 = 128;
+
+__global__ void __launch_bounds__(LT2) leaves2d_kernel(DevTree t, Exp2 E, double* __restrict__ pot_out,
+                                                       double* __restrict__ fld_out)
+{
+	__shared__ double sx[LT2], sy[LT2], sq[LT2];
+	__shared__ double2 sL[32];
+	const int LL = t.depth - 1;
+	size_t leaf = blockIdx.x;
+	if (leaf >= t.lsize[LL]) return;
+	size_t off = t.loff[LL], g = off + leaf;
+	const bool tmode = t.targets_num > 0;
+	const uint32_t tb = tmode ? t.tbeg[g] : t.beg[g];
+	const uint32_t te = tmode ? t.tend[g] : t.end[g];
+	if (tb >= te) return;
+	const int N = E.N;
+	if (threadIdx.x < N) sL[threadIdx.x] = E.inner[g * N + threadIdx.x];
+	const int ncl = t.close_cnt[g];
+	const int32_t* cl = t.close_idx + g * t.close_stride;
+	const double cx = t.cx[g], cy = t.cy[g];
+	for (uint32_t t0 = tb; t0 < te; t0 += LT2) {
+		uint32_t i = t0 + threadIdx.x;
+		const bool valid = i < te;
+		double xi = 0.0, yi = 0.0;
+		if (valid) { xi = t.x[i]; yi = t.y[i]; }
+		double pot = 0.0, fr = 0.0, fi = 0.0;
+		for (int e = -1; e < ncl; ++e) {
+			size_t sc = e < 0 ? g : off + cl[e];
+			const uint32_t sb = t.beg[sc], se = t.end[sc];
+			for (uint32_t s0 = sb; s0 < se; s0 += LT2) {
+				const int cnt = min((uint32_t)LT2, se - s0);
+				__syncthreads();
+				if (threadIdx.x < cnt) {
+					uint32_t j = s0 + threadIdx.x;
+					sx[threadIdx.x] = t.x[j]; sy[threadIdx.x] = t.y[j]; sq[threadIdx.x] = t.q[j];
+				}
+				__syncthreads();
+				if (valid) {
+					for (int j = 0; j < cnt; ++j) {
+						double dx = xi - sx[j], dy = yi - sy[j];
+						double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
+						pot += sq[j] * 0.5 * log(r2);
+						double qr = sq[j] / r2;
+						fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
+					}
+				}
+			}
+		}
+		__syncthreads();
+		if (valid) {
+			double2 dz = make_double2(xi - cx, yi - cy), pw = make_double2(1.0, 0.0);
+			for (int k = 0; k < N; ++k) {
+				double2 Lk = sL[k];
+				pot += Lk.x * pw.x - Lk.y * pw.y;
+				if (k + 1 < N) {
+					double2 v = cmul(sL[k + 1], pw);
+					fr += (k + 1) * v.x; fi += (k + 1) * v.y;
+				}
+				pw = cmul(pw, dz);
+			}
+			uint32_t o = t.orig[i];
+			pot_out[o] = pot;
+			fld_out[2 * (size_t)o] = fr; fld_out[2 * (size_t)o + 1] = fi;
+		}
+	}
+}
+
+bool g_binom_ready = false;
+
+} // namespace
+
+int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, double* pot, double* field,
+                       SolveStats* stats)
+{
+	if (N < 1 || N > MAXN2) { ctx.last_error = "order out of range (1 <= N <= 30)"; return ERR_ARG; }
+	if (!g_binom_ready) {
+		static double b[BINOM_N * BINOM_N];
+		for (int i = 0; i < BINOM_N * BINOM_N; ++i) b[i] = 0.0;
+		b[0] = 1.0;
+		for (int i = 1; i < BINOM_N; ++i) {
+			b[i * BINOM_N] = 1.0; b[i * BINOM_N + i] = 1.0;
+			for (int j = 1; j < i; ++j) b[i * BINOM_N + j] = b[(i - 1) * BINOM_N + j] + b[(i - 1) * BINOM_N + j - 1];
+		}
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_binom, b, sizeof(b)));
+		g_binom_ready = true;
+	}
+	cudaStream_t s = ctx.stream;
+	const bool timing = ctx.timing != 0;
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
+	DevTree t;
+	int st = tree_build(ctx, in, depth, t);
+	if (st) return st;
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
+	Exp2 E;
+	E.N = N;
+	E.outer = static_cast<double2*>(ctx.arena.take(sizeof(double2) * t.ncells * N));
+	E.inner = static_cast<double2*>(ctx.arena.take(sizeof(double2) * t.ncells * N));
+	if (!E.outer || !E.inner) { ctx.last_error = "fmm2d: device allocation failed"; return ERR_OOM; }
+	const int LL = depth - 1;
+	const size_t n_out = in.nt ? in.nt : in.ns;
+	LFMM_CUDA(ctx, cudaMemsetAsync(pot, 0, sizeof(double) * n_out, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(field, 0, sizeof(double) * 2 * n_out, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(E.inner, 0, sizeof(double2) * t.ncells * N, s));
+	p2m2d_kernel<<<div_up(t.lsize[LL], WPB2), WPB2 * 32, 0, s>>>(t, E);
+	for (int L = depth - 2; L >= 0; --L) m2m2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
+	for (int L = 2; L < depth; ++L) down2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
+	if (timing) { LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s)); LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s)); }
+	leaves2d_kernel<<<(unsigned)t.lsize[LL], LT2, 0, s>>>(t, E, pot, field);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[5], s));
+	LFMM_CUDA(ctx, cudaGetLastError());
+	if (stats) {
+		unsigned long long h[3];
+		unsigned long long* counters = static_cast<unsigned long long*>(ctx.arena.take(32));
+		if (!counters) { ctx.last_error = "fmm2d: device allocation failed"; return ERR_OOM; }
+		if ((st = tree_count_pairs(ctx, t, counters, h))) return st;
+		stats->n_far_pairs = h[0]; stats->n_close_pairs = h[1]; stats->n_p2p_pairs = h[2];
+		stats->N = N; stats->depth = depth;
+		stats->n_particles = t.n; stats->n_cells = t.ncells; stats->n_leaves = t.lsize[LL];
+		stats->targets_num = t.targets_num;
+		if (timing) {
+			cudaEventElapsedTime(&stats->ms_tree, ctx.ev[0], ctx.ev[1]);
+			cudaEventElapsedTime(&stats->ms_upward, ctx.ev[1], ctx.ev[2]);
+			cudaEventElapsedTime(&stats->ms_m2l, ctx.ev[2], ctx.ev[3]);
+			cudaEventElapsedTime(&stats->ms_leaves, ctx.ev[4], ctx.ev[5]);
+			cudaEventElapsedTime(&stats->ms_total, ctx.ev[0], ctx.ev[5]);
+		}
+	}
+	return OK;
+}
+
+} // namespace lfmm

@@ -1,0 +1,55 @@
+// Uniform-depth Morton quadtree / octree on the device, bit-exact with the
+// reference's MortonTree (reference cpu/morton_tree.cpp:286-493).
+#pragma once
+#include "context.cuh"
+
+namespace lfmm {
+
+constexpr int MAX_LEVELS = 22;
+
+struct DevTree {
+	int dim = 3, depth = 0;
+	size_t n = 0;              // particles in the tree: [targets | sources]
+	size_t nt = 0;             // leading input particles that are targets (q = 0)
+	size_t targets_num = 0;    // particles with q == 0 (switches P2P to target mode)
+	double* geo = nullptr;     // device: shift x, y, z, scale
+	// particles in tree order (SoA)
+	double *x = nullptr, *y = nullptr, *z = nullptr, *q = nullptr;
+	uint32_t* orig = nullptr;  // input index of tree particle s
+	uint64_t* pcode = nullptr;
+	// cells of all levels, concatenated; level L occupies [loff[L], loff[L] + lsize[L])
+	size_t lsize[MAX_LEVELS] = {}, loff[MAX_LEVELS] = {};
+	size_t ncells = 0;
+	uint64_t* code = nullptr;
+	uint32_t *beg = nullptr, *end = nullptr;    // particles (leaves) or level-local children
+	uint32_t *tbeg = nullptr, *tend = nullptr;  // leaf target range
+	int32_t* parent = nullptr;                  // level-local parent index
+	double *cx = nullptr, *cy = nullptr, *cz = nullptr;
+	// close lists, fixed stride (26 in 3D, 8 in 2D), level-local indices
+	int close_stride = 26;
+	int32_t* close_cnt = nullptr;
+	int32_t* close_idx = nullptr;
+	int32_t* far_cnt = nullptr;                 // per cell, for statistics
+	size_t n_far_pairs = 0, n_close_pairs = 0;
+};
+
+// Input particles: targets (nt, q = 0) followed by sources (ns, with q).
+struct ParticleInput {
+	int dim = 3;
+	size_t ns = 0, nt = 0;
+	const double* src = nullptr;   // device, ns x dim interleaved
+	const double* srcq = nullptr;  // device, ns
+	const double* tgt = nullptr;   // device, nt x dim interleaved
+};
+
+int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t);
+
+// Fill a CSR far list of level L (level-local source indices) in the
+// reference's order; far_off must hold lsize[L] + 1 entries.
+int tree_far_lists(Context& ctx, const DevTree& t, int L, uint32_t* far_off, int32_t* far_idx, size_t cap);
+
+// Interaction counts (synchronises): out[0] far pairs, out[1] leaf close
+// pairs (full lists), out[2] particle pairs in the near field.  dev: 3 words.
+int tree_count_pairs(Context& ctx, const DevTree& t, unsigned long long* dev, unsigned long long* out);
+
+} // namespace lfmm

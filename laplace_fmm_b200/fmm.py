@@ -1,0 +1,158 @@
+"""Host-side mirror of the reference's solver interface, over the C ABI.
+
+Names, argument meaning and results follow the reference's classes:
+
+* ``FastMultipole3d(particles, eps=1e-8, N=FMM_AUTO, tree_depth=FMM_AUTO)`` and
+  ``FastMultipole3d(sources, targets, ...)`` -- reference
+  ``fmm::gpu::FastMultipole3d<double>`` (cuda/multipole3d.h:16-17) and its CPU
+  twin (cpu/multipole3d.h:19-21).  Results in ``.potentials`` (n,) and
+  ``.forces`` (n, 3), input order; targets must carry q = 0.
+* ``FastMultipole(...)`` -- reference ``fmm::gpu::FastMultipole``
+  (cuda/multipole.h:11-12): 2D, ``.forces`` complex (n,).
+* ``compute_exact(kind, sources, targets=None)`` -- reference
+  ``fmm::gpu::ComputeExact<kind>`` (common/simple_math.h:283-313) without the
+  text file: returns the direct-sum values.
+* ``init_math_constants`` / ``cuda_copy_math_constants`` /
+  ``cuda_clear_math_constants`` -- the reference's process-global table set-up
+  (common/special_functions.h:154-156); here the tables live in each context,
+  so these are no-ops kept for call compatibility.
+
+Particles are accepted as ``(positions, charges)`` pairs or as numpy
+structured arrays with the reference's particle layout (``particle3d_dtype``:
+centre xyz, q, morton_code = 40 bytes; ``particle2d_dtype``: 32 bytes).
+"""
+from __future__ import annotations
+
+import ctypes
+from enum import Enum
+
+import numpy as np
+
+from ._lib import AUTO, PRECISION, Context, LfmmStats, default_context
+
+FMM_AUTO = AUTO
+FORCE_EPS = 1.0e-4
+
+particle3d_dtype = np.dtype([("center", "<f8", (3,)), ("q", "<f8"), ("morton_code", "<u8")])
+particle2d_dtype = np.dtype([("center", "<c16"), ("q", "<f8"), ("morton_code", "<u8")])
+
+
+class InteractionType(Enum):
+    """Reference common/utils.h:17-23."""
+    Potential2d = 0
+    Force2d = 1
+    Potential3d = 2
+    Force3d = 3
+
+
+def _split(particles, dim):
+    """(positions (n, dim) float64 C-contiguous, charges (n,) float64)."""
+    if isinstance(particles, np.ndarray) and particles.dtype.names:
+        c = particles["center"]
+        if dim == 2 and np.iscomplexobj(c):
+            pos = np.stack([c.real, c.imag], axis=1)
+        else:
+            pos = np.asarray(c, dtype=np.float64).reshape(-1, dim)
+        q = np.asarray(particles["q"], dtype=np.float64)
+    else:
+        pos, q = particles
+        pos = np.asarray(pos)
+        if dim == 2 and np.iscomplexobj(pos):
+            pos = np.stack([pos.real, pos.imag], axis=1)
+        pos = pos.reshape(-1, dim)
+        q = np.asarray(q, dtype=np.float64).reshape(-1)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    if len(pos) != len(q):
+        raise ValueError("positions and charges differ in length")
+    return pos, q
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None and a.size else None
+
+
+class _Solver:
+    dim = 3
+
+    def __init__(self, *args, eps: float = 1.0e-8, N: int = FMM_AUTO, tree_depth: int = FMM_AUTO,
+                 precision: str = "fp64", ctx: Context | None = None):
+        # reference overloads: (particles, eps, N, depth) and (sources, targets, eps, N, depth)
+        args = list(args)
+        if not args:
+            raise TypeError("particles required")
+        sources = args.pop(0)
+        targets = None
+        if args and not isinstance(args[0], (int, float)):
+            targets = args.pop(0)
+        if args:
+            eps = args.pop(0)
+        if args:
+            N = args.pop(0)
+        if args:
+            tree_depth = args.pop(0)
+        ctx = ctx or default_context()
+        dim = self.dim
+        spos, sq = _split(sources, dim)
+        tpos = None
+        if targets is not None:
+            tpos, tq = _split(targets, dim) if not isinstance(targets, np.ndarray) or targets.dtype.names \
+                else (np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1, dim)), None)
+        nt = 0 if tpos is None else len(tpos)
+        nout = nt if nt else len(spos)
+        pot = np.zeros(nout)
+        fld = np.zeros((nout, dim))
+        stats = LfmmStats()
+        fn = ctx.lib.lfmm3d_solve if dim == 3 else ctx.lib.lfmm2d_solve
+        st = fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos), int(N), int(tree_depth), float(eps),
+                PRECISION[precision], _ptr(pot), _ptr(fld), ctypes.byref(stats))
+        ctx.check(st, f"lfmm{dim}d_solve")
+        self.potentials = pot
+        self.forces = fld if dim == 3 else fld[:, 0] + 1j * fld[:, 1]
+        self.stats = stats.as_dict()
+        self.N = stats.order_N
+        self.tree_depth = stats.depth
+
+
+class FastMultipole3d(_Solver):
+    """3D rotation-based Laplace FMM (reference fmm::gpu::FastMultipole3d<double>)."""
+    dim = 3
+
+
+class FastMultipole(_Solver):
+    """2D complex Laplace FMM (reference fmm::gpu::FastMultipole)."""
+    dim = 2
+
+
+def compute_exact(kind: InteractionType, sources, targets=None, ctx: Context | None = None):
+    """FP64 direct sum on the GPU; returns potentials (n,) or fields."""
+    ctx = ctx or default_context()
+    dim = 3 if kind in (InteractionType.Potential3d, InteractionType.Force3d) else 2
+    spos, sq = _split(sources, dim)
+    if targets is None:
+        tpos = spos
+    elif isinstance(targets, np.ndarray) and targets.dtype.names:
+        tpos = _split(targets, dim)[0]
+    else:
+        tpos = np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1, dim))
+    pot = np.zeros(len(tpos))
+    fld = np.zeros((len(tpos), dim))
+    fn = ctx.lib.lfmm3d_direct if dim == 3 else ctx.lib.lfmm2d_direct
+    ctx.check(fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), len(tpos), _ptr(tpos), _ptr(pot), _ptr(fld)),
+              "direct")
+    if kind in (InteractionType.Potential2d, InteractionType.Potential3d):
+        return pot
+    return fld if dim == 3 else fld[:, 0] + 1j * fld[:, 1]
+
+
+def init_math_constants(N: int = 18):
+    """Reference fmm::detail::InitMathConstants: tables are per context here."""
+    return None
+
+
+def cuda_copy_math_constants():
+    return None
+
+
+def cuda_clear_math_constants():
+    return None
