@@ -62,7 +62,19 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default=None, help="override the configuration's")
+    ap.add_argument("--order", type=int, default=None, help="override N (degrees)")
+    ap.add_argument("--depth", type=int, default=None, help="override the tree depth")
+    a = ap.parse_args()
+    cfg = dict(CONFIGS[a.config])
+    if a.precision:
+        cfg["precision"] = a.precision
+    if a.order:
+        cfg["N"] = a.order
+    if a.depth:
+        cfg["depth"] = a.depth
+    a.cfg = cfg
+    return a
 
 
 def make_particles(cfg):
@@ -356,7 +368,7 @@ def base_config(cfg, world):
 
 def main():
     args = parse()
-    cfg = CONFIGS[args.config]
+    cfg = args.cfg
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <algorithm>
+#include <cstdlib>
 
 struct lfmm_ctx {
 	lfmm::Context c;
@@ -139,8 +140,13 @@ int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const dou
 	ParticleInput in;
 	in.dim = dim; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q; in.tgt = tgt;
 	SolveStats ss;
-	int st = dim == 3 ? fmm3d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr)
-	                  : fmm2d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
+	int st;
+	if (dim == 3 && precision == LFMM_PRECISION_MIXED)
+		st = fmm3d_solve_mixed(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
+	else if (dim == 3)
+		st = fmm3d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
+	else   // 2D: one FP64 form (the mixed request runs it too)
+		st = fmm2d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
 	if (st) return st;
 	fill_stats(stats, ss);
 	return OK;
@@ -237,6 +243,8 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	if (!ctx) return LFMM_ERR_OOM;
 	Context& c = ctx->c;
 	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
+	// M2L engine: dense direction GEMMs (default) or per-pair rotations
+	if (const char* e = std::getenv("LFMM_M2L")) c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : 0;
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
 		cudaGetLastError();
@@ -266,6 +274,8 @@ void lfmm_destroy(lfmm_ctx* ctx)
 	cudaSetDevice(c.device);
 	if (c.stream) cudaStreamSynchronize(c.stream);
 	c.arena.release();
+	for (auto& e : c.opcache) cudaFree(e.ptr);
+	c.opcache.clear();
 	tables_free(c.tables);
 	for (auto& e : c.ev) if (e) cudaEventDestroy(e);
 	if (c.dev_flags) cudaFree(c.dev_flags);

@@ -42,6 +42,13 @@ struct DevTables {
 	double* m2l = nullptr;
 	double* m2m = nullptr;
 	double* l2l = nullptr;
+	// FP32 copies for the mixed form (same layouts)
+	float* dmat_f = nullptr;
+	float2* emat_f = nullptr;
+	float* knm_f = nullptr;
+	float* m2l_f = nullptr;
+	float* m2m_f = nullptr;
+	float* l2l_f = nullptr;
 };
 
 struct Tables {
@@ -51,11 +58,24 @@ struct Tables {
 	std::vector<int4> dirinfo_host;
 };
 
+// Dense M2L operators [343][MT][MT] of one (order, cell size, precision),
+// kept across solves (repeated solves of one geometry rebuild nothing).
+struct OpCacheEntry {
+	int N = 0, prec = 0;
+	double h = 0.0;
+	void* ptr = nullptr;
+	size_t bytes = 0;
+	unsigned long long stamp = 0;
+};
+
 struct Context {
 	int device = 0;
 	cudaStream_t stream = nullptr;
 	Arena arena;
 	Tables tables;
+	std::vector<OpCacheEntry> opcache;
+	unsigned long long opcache_clock = 0;
+	int m2l_engine = 0;               // 0: dense direction GEMM where supported, 1: per-pair rotations
 	unsigned* dev_flags = nullptr;      // device error flags
 	std::string last_error;
 	int verbose = 0;

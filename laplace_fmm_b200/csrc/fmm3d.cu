@@ -7,6 +7,8 @@
 // expansion coefficients, per-box data is staged in shared memory, there are
 // no atomics and no per-thread local arrays.
 #include "fmm3d.cuh"
+#include "m2l_gemm.cuh"
+#include <algorithm>
 
 namespace lfmm {
 
@@ -408,6 +410,39 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaves_kernel(DevTree t, Exp E, 
 	}
 }
 
+// Dense M2L operators of one level: column r of T_d is the rotation-based
+// M2L (the same translate_warp as the per-pair path) applied to the r-th
+// unit vector, for the far offset d * h.  out: [343][MT][MT], pre-zeroed.
+__global__ void __launch_bounds__(WPB * 32) m2l_ops_kernel(int N, int MT, double h, DevTables T, double* out,
+                                                           unsigned* flags)
+{
+	__shared__ Smem sm[WPB];
+	__shared__ double2 unit[WPB][NX2MAX];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int Nx2 = N * (N + 1) / 2, R = 2 * Nx2;
+	size_t task = (size_t)blockIdx.x * WPB + w;
+	int dirid = (int)(task / R), r = (int)(task % R);
+	if (dirid >= 343) return;
+	int dx = dirid / 49 - 3, dy = (dirid / 7) % 7 - 3, dz = dirid % 7 - 3;
+	if (max(max(abs(dx), abs(dy)), abs(dz)) <= 1) return;
+	for (int c = lane; c < Nx2; c += 32)
+		unit[w][c] = make_double2(c == r / 2 && !(r & 1) ? 1.0 : 0.0, c == r / 2 && (r & 1) ? 1.0 : 0.0);
+	__syncwarp();
+	double2 acc[CMAX];
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) acc[k] = make_double2(0.0, 0.0);
+	translate_warp<OP_M2L>(unit[w], dx * h, dy * h, dz * h, dirid, acc, N, Nx2, sm[w], T, flags);
+	double* op = out + (size_t)dirid * MT * MT;
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) {
+		int c = lane + 32 * k;
+		if (c < Nx2) {
+			op[(size_t)(2 * c) * MT + r] = acc[k].x;
+			op[(size_t)(2 * c + 1) * MT + r] = acc[k].y;
+		}
+	}
+}
+
 bool g_const_ready = false;
 
 int upload_constants(Context& ctx)
@@ -423,6 +458,33 @@ int upload_constants(Context& ctx)
 }
 
 } // namespace
+
+// Dense FP64 M2L operators for cell size h, cached in the context.
+double* m2l_ops_fp64(Context& ctx, int N, double h)
+{
+	for (auto& e : ctx.opcache)
+		if (e.N == N && e.prec == 0 && e.h == h) { e.stamp = ++ctx.opcache_clock; return static_cast<double*>(e.ptr); }
+	if (upload_constants(ctx)) return nullptr;
+	const int MT = m2l_padded(N), R = N * (N + 1);
+	size_t bytes = sizeof(double) * 343 * (size_t)MT * MT;
+	if (ctx.opcache.size() >= 24) {     // evict the least recently used
+		auto it = std::min_element(ctx.opcache.begin(), ctx.opcache.end(),
+		                           [](const OpCacheEntry& a, const OpCacheEntry& b) { return a.stamp < b.stamp; });
+		cudaStreamSynchronize(ctx.stream);
+		cudaFree(it->ptr);
+		ctx.opcache.erase(it);
+	}
+	OpCacheEntry e;
+	e.N = N; e.prec = 0; e.h = h; e.bytes = bytes; e.stamp = ++ctx.opcache_clock;
+	if (cudaMalloc(&e.ptr, bytes) != cudaSuccess) { cudaGetLastError(); ctx.last_error = "m2l operators: out of memory"; return nullptr; }
+	cudaMemsetAsync(e.ptr, 0, bytes, ctx.stream);
+	size_t tasks = (size_t)343 * R;
+	m2l_ops_kernel<<<div_up(tasks, WPB), WPB * 32, 0, ctx.stream>>>(N, MT, h, ctx.tables.d, static_cast<double*>(e.ptr),
+	                                                                 ctx.dev_flags);
+	if (cudaGetLastError() != cudaSuccess) { cudaFree(e.ptr); ctx.last_error = "m2l operators: launch failed"; return nullptr; }
+	ctx.opcache.push_back(e);
+	return static_cast<double*>(e.ptr);
+}
 
 int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, double* pot, double* field,
                        SolveStats* stats, DevTree* tree_out, double2** inner_out, double2** outer_out)
@@ -455,8 +517,22 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 		m2m_kernel<<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, E, L, ctx.tables.d, ctx.dev_flags);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
 	// downward
-	for (int L = 2; L < depth; ++L)
-		m2l_kernel<<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, E, L, ctx.tables.d, ctx.dev_flags);
+	const bool gemm = ctx.m2l_engine == 0 && m2l_gemm_supported(N);
+	for (int L = 2; L < depth; ++L) {
+		if (gemm) {
+			double h = t.geo_host[3] / (double)(1ull << L);
+			double* ops = m2l_ops_fp64(ctx, N, h);
+			if (!ops) return ERR_OOM;
+			M2LPlan plan;
+			if ((st = m2l_plan_build(ctx, t, L, plan))) return st;
+			const size_t off = t.loff[L] * E.Nx2;
+			if ((st = m2l_gemm<double>(ctx, plan, ops, reinterpret_cast<const double*>(E.outer + off),
+			                           reinterpret_cast<double*>(E.inner + off), N)))
+				return st;
+		} else {
+			m2l_kernel<<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, E, L, ctx.tables.d, ctx.dev_flags);
+		}
+	}
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s));
 	for (int L = 3; L < depth; ++L)
 		l2l_kernel<<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, E, L, ctx.tables.d, ctx.dev_flags);

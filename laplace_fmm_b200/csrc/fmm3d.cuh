@@ -18,4 +18,14 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
                        SolveStats* stats, DevTree* tree_out = nullptr, double2** inner_out = nullptr,
                        double2** outer_out = nullptr);
 
+// Mixed-precision form (FP32 scaled expansions below level 4, FP32 near field
+// with FP64 tile accumulation); same arguments.
+int fmm3d_solve_mixed(Context& ctx, const ParticleInput& in, int N, int depth, double* pot, double* field,
+                      SolveStats* stats);
+
+// Dense FP64 M2L operators [343][MT][MT] for cell size h (h = 1: the
+// level-independent scaled operators), cached in the context.
+double* m2l_ops_fp64(Context& ctx, int N, double h);
+float* m2l_ops_fp32(Context& ctx, int N);
+
 } // namespace lfmm

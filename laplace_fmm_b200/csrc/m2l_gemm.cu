@@ -1,0 +1,249 @@
+// Direction-grouped M2L GEMMs (see m2l_gemm.cuh), SIMT register-tiled form
+// for FP64 (plain) and FP32.
+#include "m2l_gemm.cuh"
+#include "primitives.cuh"
+#include <mutex>
+
+namespace lfmm {
+
+namespace {
+
+__constant__ int16_t c_slot_dir[8][M2L_SLOTS];
+__constant__ int16_t c_dir_slot[8][343];
+
+__device__ __forceinline__ void coords3(uint64_t code, int* c)
+{ c[0] = (int)compact3(code >> 2); c[1] = (int)compact3(code >> 1); c[2] = (int)compact3(code); }
+
+// Fill the V table of level L: slot of each far source in the target's
+// octant class; the candidates are the children of the parent's close cells
+// and of the parent (reference cpu/morton_tree.cpp:147-208).
+__global__ void vtab_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsigned* flags)
+{
+	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	size_t m = t.lsize[L];
+	if (c >= m) return;
+	size_t off = t.loff[L], poff = t.loff[L - 1];
+	int me[3];
+	coords3(t.code[off + c], me);
+	int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
+	int32_t* row = vtab + c * M2L_SLOTS;
+	int32_t p = t.parent[off + c];
+	int npc = t.close_cnt[poff + p];
+	const int32_t* pl = t.close_idx + (poff + p) * t.close_stride;
+	for (int e = 0; e <= npc; ++e) {
+		int32_t pn = e < npc ? pl[e] : p;
+		for (uint32_t k = t.beg[poff + pn]; k < t.end[poff + pn]; ++k) {
+			if (k == c) continue;
+			int o[3];
+			coords3(t.code[off + k], o);
+			int dx = o[0] - me[0], dy = o[1] - me[1], dz = o[2] - me[2];
+			if (max(max(abs(dx), abs(dy)), abs(dz)) <= 1) continue;
+			int slot = c_dir_slot[oct][(dx + 3) * 49 + (dy + 3) * 7 + (dz + 3)];
+			if (slot < 0) { atomicOr(flags, DEV_ERR_DIRECTION); continue; }
+			row[slot] = (int32_t)k;
+		}
+	}
+}
+
+__global__ void count_oct_kernel(DevTree t, int L, uint32_t* __restrict__ oct_count)
+{
+	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= t.lsize[L]) return;
+	int me[3];
+	coords3(t.code[t.loff[L] + c], me);
+	int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
+	atomicAdd(&oct_count[oct], 1u);
+}
+
+__global__ void scatter_oct_kernel(DevTree t, int L, uint32_t* __restrict__ oct_count, int32_t* __restrict__ order)
+{
+	__shared__ uint32_t base[8];
+	if (threadIdx.x < 8) {
+		uint32_t a = 0;
+		for (int o = 0; o < (int)threadIdx.x; ++o) a += oct_count[o];
+		base[threadIdx.x] = a;
+	}
+	__syncthreads();
+	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= t.lsize[L]) return;
+	int me[3];
+	coords3(t.code[t.loff[L] + c], me);
+	int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
+	uint32_t pos = atomicAdd(&oct_count[8 + oct], 1u);
+	order[base[oct] + pos] = (int32_t)c;
+}
+
+// C[MT x 64] = sum over the octant's offsets of T_dir[MT x MT] * B[MT x 64];
+// 256 threads, thread (ty, tx) owns rows ty + 16 i and columns tx + 16 j.
+template <typename real, int TM, int TN>
+__global__ void __launch_bounds__(256) m2l_gemm_kernel(const real* __restrict__ ops, const real* __restrict__ mult,
+                                                       real* __restrict__ loc, const int32_t* __restrict__ vtab,
+                                                       const int32_t* __restrict__ order,
+                                                       const uint32_t* __restrict__ oct_count, int R)
+{
+	constexpr int MT = 16 * TM;
+	constexpr int BN = 16 * TN;
+	constexpr int BK = 16;
+	__shared__ real As[BK][MT];
+	__shared__ real Bs[BK][BN];
+	__shared__ int32_t src[BN];
+	__shared__ int32_t tgt[BN];
+	__shared__ int s_oct, s_n;
+	const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+	if (tid == 0) {
+		// locate this block's (octant, tile)
+		uint32_t b = blockIdx.x, start = 0;
+		int oct = -1, nn = 0;
+		for (int o = 0; o < 8; ++o) {
+			uint32_t cnt = oct_count[o];
+			uint32_t tiles = (cnt + BN - 1) / BN;
+			if (b < tiles) { oct = o; start += b * BN; nn = (int)min((uint32_t)BN, cnt - b * BN); break; }
+			b -= tiles; start += cnt;
+		}
+		s_oct = oct; s_n = nn;
+		tgt[0] = (int32_t)start;
+	}
+	__syncthreads();
+	const int oct = s_oct, nt = s_n;
+	if (oct < 0) return;
+	const uint32_t start = (uint32_t)tgt[0];
+	__syncthreads();
+	if (tid < BN) tgt[tid] = tid < nt ? order[start + tid] : -1;
+	real acc[TM][TN];
+#pragma unroll
+	for (int i = 0; i < TM; ++i)
+#pragma unroll
+		for (int j = 0; j < TN; ++j) acc[i][j] = real(0);
+	__syncthreads();
+	for (int slot = 0; slot < M2L_SLOTS; ++slot) {
+		int mine = -1;
+		if (tid < BN && tgt[tid] >= 0) mine = vtab[(size_t)tgt[tid] * M2L_SLOTS + slot];
+		if (tid < BN) src[tid] = mine;
+		if (!__syncthreads_or(mine >= 0)) continue;
+		const real* A = ops + (size_t)c_slot_dir[oct][slot] * MT * MT;
+		for (int k0 = 0; k0 < MT; k0 += BK) {
+			for (int idx = tid; idx < BK * MT; idx += 256) {
+				int k = idx & (BK - 1), r = idx / BK;
+				As[k][r] = A[(size_t)r * MT + k0 + k];
+			}
+			for (int idx = tid; idx < BK * BN; idx += 256) {
+				int k = idx & (BK - 1), c = idx / BK;
+				int s = src[c];
+				int kk = k0 + k;
+				Bs[k][c] = (s >= 0 && kk < R) ? mult[(size_t)s * R + kk] : real(0);
+			}
+			__syncthreads();
+#pragma unroll
+			for (int k = 0; k < BK; ++k) {
+				real a[TM], b[TN];
+#pragma unroll
+				for (int i = 0; i < TM; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+				for (int j = 0; j < TN; ++j) b[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+				for (int i = 0; i < TM; ++i)
+#pragma unroll
+					for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+			}
+			__syncthreads();
+		}
+	}
+#pragma unroll
+	for (int j = 0; j < TN; ++j) {
+		int c = tx + 16 * j;
+		int tg = c < BN ? tgt[c] : -1;
+		if (tg < 0) continue;
+#pragma unroll
+		for (int i = 0; i < TM; ++i) {
+			int r = ty + 16 * i;
+			if (r < R) loc[(size_t)tg * R + r] = acc[i][j];
+		}
+	}
+}
+
+template <typename real, int TM>
+void launch_gemm(unsigned grid, cudaStream_t s, const real* ops, const real* mult, real* loc, const M2LPlan& p, int R)
+{
+	m2l_gemm_kernel<real, TM, 4><<<grid, 256, 0, s>>>(ops, mult, loc, p.vtab, p.order, p.oct_count, R);
+}
+
+} // namespace
+
+const M2LSlots& m2l_slots()
+{
+	static M2LSlots S;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		for (int o = 0; o < 8; ++o) {
+			for (int d = 0; d < 343; ++d) S.dir_slot[o][d] = -1;
+			int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
+			int s = 0;
+			for (int dx = -2 - ox; dx <= 3 - ox; ++dx)
+				for (int dy = -2 - oy; dy <= 3 - oy; ++dy)
+					for (int dz = -2 - oz; dz <= 3 - oz; ++dz) {
+						if (std::max(std::max(std::abs(dx), std::abs(dy)), std::abs(dz)) <= 1) continue;
+						int id = (dx + 3) * 49 + (dy + 3) * 7 + (dz + 3);
+						S.slot_dir[o][s] = (int16_t)id;
+						S.dir_slot[o][id] = (int16_t)s;
+						++s;
+					}
+		}
+	});
+	return S;
+}
+
+int m2l_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan)
+{
+	static bool uploaded = false;
+	if (!uploaded) {
+		const M2LSlots& S = m2l_slots();
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_slot_dir, S.slot_dir, sizeof(S.slot_dir)));
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_dir_slot, S.dir_slot, sizeof(S.dir_slot)));
+		uploaded = true;
+	}
+	size_t m = t.lsize[L];
+	plan.cells = m;
+	plan.vtab = static_cast<int32_t*>(ctx.arena.take(sizeof(int32_t) * m * M2L_SLOTS));
+	plan.order = static_cast<int32_t*>(ctx.arena.take(sizeof(int32_t) * 2 * m));
+	plan.oct_count = static_cast<uint32_t*>(ctx.arena.take(sizeof(uint32_t) * 16));
+	if (!plan.vtab || !plan.order || !plan.oct_count) { ctx.last_error = "m2l plan: allocation failed"; return ERR_OOM; }
+	cudaStream_t s = ctx.stream;
+	LFMM_CUDA(ctx, cudaMemsetAsync(plan.vtab, 0xff, sizeof(int32_t) * m * M2L_SLOTS, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(plan.oct_count, 0, sizeof(uint32_t) * 16, s));
+	count_oct_kernel<<<div_up(m, 256), 256, 0, s>>>(t, L, plan.oct_count);
+	scatter_oct_kernel<<<div_up(m, 256), 256, 0, s>>>(t, L, plan.oct_count, plan.order);
+	vtab_kernel<<<div_up(m, 128), 128, 0, s>>>(t, L, plan.vtab, ctx.dev_flags);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+template <typename real>
+int m2l_gemm(Context& ctx, const M2LPlan& plan, const real* ops, const real* mult, real* loc, int N)
+{
+	const int R = N * (N + 1);
+	const int MT = m2l_padded(N);
+	unsigned grid = (unsigned)(plan.cells / M2L_TILE + 8);
+	cudaStream_t s = ctx.stream;
+	switch (MT / 16) {
+	case 1: launch_gemm<real, 1>(grid, s, ops, mult, loc, plan, R); break;
+	case 2: launch_gemm<real, 2>(grid, s, ops, mult, loc, plan, R); break;
+	case 3: launch_gemm<real, 3>(grid, s, ops, mult, loc, plan, R); break;
+	case 4: launch_gemm<real, 4>(grid, s, ops, mult, loc, plan, R); break;
+	case 5: launch_gemm<real, 5>(grid, s, ops, mult, loc, plan, R); break;
+	case 6: launch_gemm<real, 6>(grid, s, ops, mult, loc, plan, R); break;
+	case 7: launch_gemm<real, 7>(grid, s, ops, mult, loc, plan, R); break;
+	case 8: launch_gemm<real, 8>(grid, s, ops, mult, loc, plan, R); break;
+	case 9: launch_gemm<real, 9>(grid, s, ops, mult, loc, plan, R); break;
+	case 10: launch_gemm<real, 10>(grid, s, ops, mult, loc, plan, R); break;
+	case 11: launch_gemm<real, 11>(grid, s, ops, mult, loc, plan, R); break;
+	case 12: launch_gemm<real, 12>(grid, s, ops, mult, loc, plan, R); break;
+	default: ctx.last_error = "m2l gemm: order too large"; return ERR_UNSUPPORTED;
+	}
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+template int m2l_gemm<double>(Context&, const M2LPlan&, const double*, const double*, double*, int);
+template int m2l_gemm<float>(Context&, const M2LPlan&, const float*, const float*, float*, int);
+
+} // namespace lfmm

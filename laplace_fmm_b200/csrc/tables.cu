@@ -86,6 +86,12 @@ __global__ void wignerd_kernel(const double* __restrict__ thetas, int nslots, do
 		}
 }
 
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n)
+{
+	size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (float)in[i];
+}
+
 __global__ void exp_kernel(const double* __restrict__ phis, int nslots, double2* __restrict__ out)
 {
 	int slot = blockIdx.x, m = threadIdx.x;
@@ -182,6 +188,22 @@ int tables_build(Context& ctx)
 	wignerd_kernel<<<T.n_dslots, 32, 0, s>>>(d_th, T.n_dslots, T.dmat);
 	exp_kernel<<<T.n_eslots, 32, 0, s>>>(d_ph, T.n_eslots, T.emat);
 	LFMM_CUDA(ctx, cudaGetLastError());
+	// FP32 copies (mixed form)
+	size_t nd = (size_t)dsize(MAXN3) * T.n_dslots, ne = (size_t)2 * MAXN3 * T.n_eslots;
+	LFMM_CUDA(ctx, cudaMalloc(&T.dmat_f, sizeof(float) * nd));
+	LFMM_CUDA(ctx, cudaMalloc(&T.emat_f, sizeof(float) * ne));
+	LFMM_CUDA(ctx, cudaMalloc(&T.knm_f, sizeof(float) * K.size()));
+	LFMM_CUDA(ctx, cudaMalloc(&T.m2l_f, sizeof(float) * C));
+	LFMM_CUDA(ctx, cudaMalloc(&T.m2m_f, sizeof(float) * C));
+	LFMM_CUDA(ctx, cudaMalloc(&T.l2l_f, sizeof(float) * C));
+	to_float_kernel<<<div_up(nd, 256), 256, 0, s>>>(T.dmat, T.dmat_f, nd);
+	to_float_kernel<<<div_up(ne, 256), 256, 0, s>>>(reinterpret_cast<const double*>(T.emat),
+	                                                 reinterpret_cast<float*>(T.emat_f), ne);
+	to_float_kernel<<<div_up(K.size(), 256), 256, 0, s>>>(T.knm, T.knm_f, K.size());
+	to_float_kernel<<<div_up(C, 256), 256, 0, s>>>(T.m2l, T.m2l_f, C);
+	to_float_kernel<<<div_up(C, 256), 256, 0, s>>>(T.m2m, T.m2m_f, C);
+	to_float_kernel<<<div_up(C, 256), 256, 0, s>>>(T.l2l, T.l2l_f, C);
+	LFMM_CUDA(ctx, cudaGetLastError());
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	cudaFree(d_th);
 	cudaFree(d_ph);
@@ -193,6 +215,8 @@ void tables_free(Tables& TH)
 	DevTables& T = TH.d;
 	cudaFree(T.dmat); cudaFree(T.emat); cudaFree(T.dirinfo); cudaFree(T.knm);
 	cudaFree(T.m2l); cudaFree(T.m2m); cudaFree(T.l2l);
+	cudaFree(T.dmat_f); cudaFree(T.emat_f); cudaFree(T.knm_f);
+	cudaFree(T.m2l_f); cudaFree(T.m2m_f); cudaFree(T.l2l_f);
 	TH = Tables();
 }
 

@@ -376,6 +376,7 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t)
 	else gather_kernel<2><<<div_up(n, TB), TB, 0, s>>>(in, n, sk, sv, t, newlev, hist);
 	unsigned hh[MAX_LEVELS + 2];
 	LFMM_CUDA(ctx, cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, s));
+	LFMM_CUDA(ctx, cudaMemcpyAsync(t.geo_host, t.geo, sizeof(t.geo_host), cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	size_t acc = 0;
 	for (int L = 0; L < depth; ++L) { acc += hh[L]; t.lsize[L] = acc; }

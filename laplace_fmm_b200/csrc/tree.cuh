@@ -13,6 +13,7 @@ struct DevTree {
 	size_t nt = 0;             // leading input particles that are targets (q = 0)
 	size_t targets_num = 0;    // particles with q == 0 (switches P2P to target mode)
 	double* geo = nullptr;     // device: shift x, y, z, scale
+	double geo_host[4] = {};   // host copy
 	// particles in tree order (SoA)
 	double *x = nullptr, *y = nullptr, *z = nullptr, *q = nullptr;
 	uint32_t* orig = nullptr;  // input index of tree particle s

@@ -139,6 +139,27 @@ def test_wigner_tables_match_oracle(ctx, oracle):
         assert np.abs(d - oracle.wignerd(18, th.value)).max() < 1e-11
 
 
+@pytest.mark.parametrize("N,depth", [(9, 5), (13, 4), (6, 6)])
+def test_m2l_engines_agree(ctx, oracle, N, depth):
+    """Dense direction-GEMM M2L and per-pair rotations: both at parity."""
+    import os
+    from laplace_fmm_b200 import Context
+    os.environ["LFMM_M2L"] = "rotation"
+    try:
+        rot = Context(0)
+    finally:
+        del os.environ["LFMM_M2L"]
+    g = rng(N * 100 + depth)
+    n = 60000
+    src = g.random((n, 3)); q = g.uniform(-1, 1, n)
+    a = FastMultipole3d((src, q), N=N, tree_depth=depth)
+    b = FastMultipole3d((src, q), N=N, tree_depth=depth, ctx=rot)
+    pot, fld = oracle.fmm3d(src, q, N=N, depth=depth)
+    assert rel_l2(a.potentials, pot) < TOL and rel_l2(a.forces, fld) < TOL
+    assert rel_l2(b.potentials, pot) < TOL and rel_l2(b.forces, fld) < TOL
+    rot.close()
+
+
 def test_bad_arguments(ctx):
     from laplace_fmm_b200 import LfmmError
     with pytest.raises(LfmmError):
