@@ -75,6 +75,8 @@ typedef struct {
 	size_t n_far_pairs;     /* M2L interactions */
 	size_t n_close_pairs;   /* leaf-leaf near-field interactions (full lists) */
 	size_t n_p2p_pairs;     /* particle-particle evaluations in the near field */
+	size_t n_m2p;           /* adaptive tree: target-particle x W-cell evaluations */
+	size_t n_w, n_x;        /* adaptive tree: W and X list entries */
 	float ms_tree, ms_upward, ms_m2l, ms_l2l, ms_leaves, ms_total; /* device time, when timing */
 } lfmm_stats;
 
@@ -98,6 +100,27 @@ int lfmm3d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const doubl
 int lfmm3d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                         const double* tgt_xyz, int N, int tree_depth, double eps, int precision, double* pot,
                         double* field, lfmm_stats* stats);
+
+/* Extended 3D solve: the reference's arguments plus the leaf size and the
+ * precision.  max_leaf = 0 keeps the reference's uniform tree of depth
+ * tree_depth; max_leaf > 0 builds an adaptive octree (cells split while they
+ * hold more than max_leaf particles, at most tree_depth levels) with U, V, W, X
+ * lists.  precision FP64 with max_leaf = 0 is the reference-parity path
+ * (same as lfmm3d_solve); every other combination runs the scaled-expansion
+ * solver (N <= 13). */
+typedef struct {
+	int N;            /* degrees (order p + 1), or LFMM_AUTO (from eps) */
+	int tree_depth;   /* uniform depth / maximum adaptive depth, or LFMM_AUTO */
+	int max_leaf;     /* 0: uniform tree; > 0: adaptive split threshold */
+	int precision;    /* LFMM_PRECISION_FP64 or LFMM_PRECISION_MIXED */
+	double eps;       /* tolerance used by LFMM_AUTO order selection */
+} lfmm_solve_opts;
+
+int lfmm3d_solve_ex(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                    const double* tgt_xyz, const lfmm_solve_opts* opts, double* pot, double* field, lfmm_stats* stats);
+int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                           const double* tgt_xyz, const lfmm_solve_opts* opts, double* pot, double* field,
+                           lfmm_stats* stats);
 
 /* ---- 2D ---------------------------------------------------------------- */
 int lfmm2d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,

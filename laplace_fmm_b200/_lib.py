@@ -19,7 +19,8 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_DEVICE
 # Every symbol include/lfmm.h declares (checked by the CPU tests).
 EXPORTS = [
     "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream",
-    "lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device",
+    "lfmm3d_solve", "lfmm3d_solve_device", "lfmm3d_solve_ex", "lfmm3d_solve_ex_device",
+    "lfmm2d_solve", "lfmm2d_solve_device",
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
     "lfmm_wignerd_slot",
@@ -35,13 +36,19 @@ class LfmmStats(ctypes.Structure):
         ("order_N", ctypes.c_int), ("depth", ctypes.c_int),
         ("n_particles", ctypes.c_size_t), ("n_cells", ctypes.c_size_t), ("n_leaves", ctypes.c_size_t),
         ("targets_num", ctypes.c_size_t), ("n_far_pairs", ctypes.c_size_t), ("n_close_pairs", ctypes.c_size_t),
-        ("n_p2p_pairs", ctypes.c_size_t),
+        ("n_p2p_pairs", ctypes.c_size_t), ("n_m2p", ctypes.c_size_t), ("n_w", ctypes.c_size_t),
+        ("n_x", ctypes.c_size_t),
         ("ms_tree", ctypes.c_float), ("ms_upward", ctypes.c_float), ("ms_m2l", ctypes.c_float),
         ("ms_l2l", ctypes.c_float), ("ms_leaves", ctypes.c_float), ("ms_total", ctypes.c_float),
     ]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LfmmSolveOpts(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("tree_depth", ctypes.c_int), ("max_leaf", ctypes.c_int),
+                ("precision", ctypes.c_int), ("eps", ctypes.c_double)]
 
 
 class LfmmError(RuntimeError):
@@ -72,6 +79,9 @@ def load(path: Path | str = LIB_PATH):
         solve = [P, SZ, P, P, SZ, P, I, I, D, I, P, P, ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device"):
             getattr(L, f).argtypes = solve
+        for f in ("lfmm3d_solve_ex", "lfmm3d_solve_ex_device"):
+            getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, P,
+                                      ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, P, P]
         L.lfmm_tree_build.argtypes = [P, I, SZ, P, P, SZ, P, I, P, P]

@@ -111,6 +111,7 @@ void fill_stats(lfmm_stats* out, const SolveStats& s)
 	out->n_particles = s.n_particles; out->n_cells = s.n_cells; out->n_leaves = s.n_leaves;
 	out->targets_num = s.targets_num; out->n_far_pairs = s.n_far_pairs; out->n_close_pairs = s.n_close_pairs;
 	out->n_p2p_pairs = s.n_p2p_pairs;
+	out->n_m2p = s.n_m2p; out->n_w = s.n_w; out->n_x = s.n_x;
 	out->ms_tree = s.ms_tree; out->ms_upward = s.ms_upward; out->ms_m2l = s.ms_m2l; out->ms_l2l = s.ms_l2l;
 	out->ms_leaves = s.ms_leaves; out->ms_total = s.ms_total;
 }
@@ -125,7 +126,7 @@ int select_device(lfmm_ctx* ctx)
 // Device solve shared by the host and device entry points.
 int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                  int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats,
-                 bool arena_reset)
+                 bool arena_reset, int max_leaf = 0)
 {
 	Context& c = ctx->c;
 	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return ERR_ARG; }
@@ -141,8 +142,9 @@ int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const dou
 	in.dim = dim; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q; in.tgt = tgt;
 	SolveStats ss;
 	int st;
-	if (dim == 3 && precision == LFMM_PRECISION_MIXED)
-		st = fmm3d_solve_mixed(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
+	if (dim == 2 && max_leaf > 0) { c.last_error = "adaptive trees are 3D only"; return ERR_UNSUPPORTED; }
+	if (dim == 3 && (precision == LFMM_PRECISION_MIXED || max_leaf > 0))
+		st = fmm3d_solve_scaled(c, in, Nr, Dr, max_leaf, precision, pot, field, stats ? &ss : nullptr);
 	else if (dim == 3)
 		st = fmm3d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
 	else   // 2D: one FP64 form (the mixed request runs it too)
@@ -153,7 +155,8 @@ int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const dou
 }
 
 int solve_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
-               int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
+               int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats,
+               int max_leaf = 0)
 {
 	Context& c = ctx->c;
 	if (select_device(ctx)) return ERR_CUDA;
@@ -173,7 +176,8 @@ int solve_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const doubl
 		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
 	}
 	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
-	int st = solve_device(ctx, dim, ns, dsrc, dq, nt, dtgt, N, depth, eps, precision, dpot, dfld, stats, false);
+	int st = solve_device(ctx, dim, ns, dsrc, dq, nt, dtgt, N, depth, eps, precision, dpot, dfld, stats, false,
+	                      max_leaf);
 	if (st == OK) {
 		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
 		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * dim * nout, cudaMemcpyDeviceToHost, s));
@@ -244,7 +248,9 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	Context& c = ctx->c;
 	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
 	// M2L engine: dense direction GEMMs (default) or per-pair rotations
-	if (const char* e = std::getenv("LFMM_M2L")) c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : 0;
+	// (rotation: per-pair rotations on the plain path; simt: no tensor cores on the FP32 levels)
+	if (const char* e = std::getenv("LFMM_M2L"))
+		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 2 : 0);
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
 		cudaGetLastError();
@@ -300,6 +306,26 @@ int lfmm3d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const doubl
 	if (!ctx) return LFMM_ERR_ARG;
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats, true);
+	if (st == OK && stats) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
+int lfmm3d_solve_ex(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                    const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	return solve_host(ctx, 3, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                  o->max_leaf);
+}
+
+int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                           const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                      true, o->max_leaf);
 	if (st == OK && stats) st = check_flags(ctx->c);
 	ctx->c.arena.settle();
 	return st;

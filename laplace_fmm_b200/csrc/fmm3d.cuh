@@ -8,6 +8,7 @@ struct SolveStats {
 	int N = 0, depth = 0;
 	size_t n_particles = 0, n_cells = 0, n_leaves = 0, targets_num = 0;
 	size_t n_far_pairs = 0, n_close_pairs = 0, n_p2p_pairs = 0;
+	size_t n_m2p = 0, n_w = 0, n_x = 0;
 	float ms_tree = 0, ms_upward = 0, ms_m2l = 0, ms_l2l = 0, ms_leaves = 0, ms_total = 0;
 };
 
@@ -18,10 +19,12 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
                        SolveStats* stats, DevTree* tree_out = nullptr, double2** inner_out = nullptr,
                        double2** outer_out = nullptr);
 
-// Mixed-precision form (FP32 scaled expansions below level 4, FP32 near field
-// with FP64 tile accumulation); same arguments.
-int fmm3d_solve_mixed(Context& ctx, const ParticleInput& in, int N, int depth, double* pot, double* field,
-                      SolveStats* stats);
+// Scaled-expansion solver on the adaptive-form tree (max_leaf = 0: uniform
+// depth `depth`; > 0: adaptive, at most `depth` levels): precision 0 = FP64,
+// 1 = mixed (FP32 expansions / near field, FP64 M2L on levels 2-3, FP64 tile
+// sums and self term).  N <= 13.
+int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
+                       double* pot, double* field, SolveStats* stats, DevTree* tree_out = nullptr);
 
 // Dense FP64 M2L operators [343][MT][MT] for cell size h (h = 1: the
 // level-independent scaled operators), cached in the context.

@@ -1,0 +1,201 @@
+// 3D FMM in scaled expansions on the adaptive-form tree (uniform when
+// max_leaf = 0): plain FP64 or mixed (FP32 expansions and near field, FP64
+// M2L accumulation on levels 2-3, FP64 tile sums and self term).
+// Passes: P2M (every leaf, any level) -> M2M -> M2L (V, direction GEMMs) ->
+// P2L (X) -> L2L -> leaves: P2P (self + U), M2P (W), L2P.
+#include "scaled_kernels.cuh"
+#include "m2l_tc.cuh"
+#include <algorithm>
+
+namespace lfmm {
+
+using namespace scaled;
+
+namespace {
+
+bool g_scaled_const_ready = false;
+
+int upload_scaled_constants(Context& ctx)
+{
+	if (g_scaled_const_ready) return OK;
+	unsigned char n_of[NX2MAX], m_of[NX2MAX];
+	for (int n = 0; n < MAXN3; ++n)
+		for (int m = 0; m <= n; ++m) { n_of[tix(n, m)] = (unsigned char)n; m_of[tix(n, m)] = (unsigned char)m; }
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_n_of, n_of, sizeof(n_of)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_m_of, m_of, sizeof(m_of)));
+	g_scaled_const_ready = true;
+	return OK;
+}
+
+template <typename real> Tab<real> tables_of(const DevTables& T);
+template <> Tab<double> tables_of<double>(const DevTables& T) { return Tab<double>{T.dmat, T.emat, T.m2m, T.l2l, T.knm, T.dirinfo}; }
+template <> Tab<float> tables_of<float>(const DevTables& T) { return Tab<float>{T.dmat_f, T.emat_f, T.m2m_f, T.l2l_f, T.knm_f, T.dirinfo}; }
+
+template <typename real> const real* ops_of(Context& ctx, int N);
+template <> const double* ops_of<double>(Context& ctx, int N) { return m2l_ops_fp64(ctx, N, 1.0); }
+template <> const float* ops_of<float>(Context& ctx, int N) { return m2l_ops_fp32(ctx, N); }
+
+template <typename real>
+int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, SolveStats* stats)
+{
+	using v2 = typename V2<real>::t;
+	cudaStream_t s = ctx.stream;
+	const bool timing = ctx.timing != 0;
+	const int Nx2 = N * (N + 1) / 2, R = 2 * Nx2;
+	const size_t n = t.n, C = t.ncells;
+	const Tab<real> T = tables_of<real>(ctx.tables.d);
+	const real* knm = T.knm;
+	real* xr = static_cast<real*>(ctx.arena.take(sizeof(real) * n));
+	real* yr = static_cast<real*>(ctx.arena.take(sizeof(real) * n));
+	real* zr = static_cast<real*>(ctx.arena.take(sizeof(real) * n));
+	real* qr = static_cast<real*>(ctx.arena.take(sizeof(real) * n));
+	v2* outer = static_cast<v2*>(ctx.arena.take(sizeof(v2) * C * Nx2));
+	v2* inner = static_cast<v2*>(ctx.arena.take(sizeof(v2) * C * Nx2));
+	size_t bmax = 0;
+	for (int L = 0; L < t.depth; ++L) bmax = std::max(bmax, t.lsize[L]);
+	const bool coarse64 = sizeof(real) == sizeof(float);
+	double* cv_in = coarse64 ? static_cast<double*>(ctx.arena.take(sizeof(double) * bmax * R)) : nullptr;
+	double* cv_out = coarse64 ? static_cast<double*>(ctx.arena.take(sizeof(double) * bmax * R)) : nullptr;
+	if (!xr || !yr || !zr || !qr || !outer || !inner || (coarse64 && (!cv_in || !cv_out))) {
+		ctx.last_error = "scaled solve: allocation failed";
+		return ERR_OOM;
+	}
+	const size_t n_out = t.nt ? t.nt : t.n - t.nt;
+	LFMM_CUDA(ctx, cudaMemsetAsync(pot, 0, sizeof(double) * n_out, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(field, 0, sizeof(double) * 3 * n_out, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(outer, 0, sizeof(v2) * C * Nx2, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(inner, 0, sizeof(v2) * C * Nx2, s));
+	const unsigned nl = (unsigned)t.nleaves;
+	relcoords_kernel<real><<<nl, 128, 0, s>>>(t, xr, yr, zr, qr);
+	p2m_scaled_kernel<real><<<div_up(nl, WPB), WPB * 32, 0, s>>>(t, xr, yr, zr, qr, N, knm, outer);
+	for (int L = t.depth - 2; L >= 0; --L)
+		m2m_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, outer + t.loff[L + 1] * Nx2,
+		                                                                     outer + t.loff[L] * Nx2, N, T, ctx.dev_flags);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
+	int st;
+	if (t.depth > 2) {
+		const real* ops = ops_of<real>(ctx, N);
+		const double* opd = coarse64 ? m2l_ops_fp64(ctx, N, 1.0) : nullptr;
+		if (!ops || (coarse64 && !opd)) return ERR_OOM;
+		for (int L = 2; L < t.depth; ++L) {
+			if (t.lsize[L] == 0) continue;
+			M2LPlan plan;
+			if ((st = m2l_plan_build(ctx, t, L, plan))) return st;
+			const real* mL = reinterpret_cast<const real*>(outer + t.loff[L] * Nx2);
+			real* lL = reinterpret_cast<real*>(inner + t.loff[L] * Nx2);
+			if (coarse64 && L <= 3) {
+				// FP64 accumulation on the coarse levels
+				size_t m = t.lsize[L] * (size_t)R;
+				convert_kernel<real><<<div_up(m, 256), 256, 0, s>>>(mL, cv_in, m);
+				if ((st = m2l_gemm<double>(ctx, plan, opd, cv_in, cv_out, N))) return st;
+				convert_back_kernel<real><<<div_up(m, 256), 256, 0, s>>>(cv_out, lL, m);
+			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 0 && m2l_tc_supported(N) &&
+			           t.lsize[L] >= 4096) {
+				// FP32 levels with enough tiles: tcgen05 TF32 hi/lo GEMM
+				const uint4* tc = m2l_ops_tc(ctx, N);
+				if (!tc) return ERR_OOM;
+				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N)))
+					return st;
+			} else {
+				if ((st = m2l_gemm<real>(ctx, plan, ops, mL, lL, N))) return st;
+			}
+		}
+	}
+	if (t.adaptive && t.n_x > 0)
+		p2l_kernel<real><<<div_up(C, WPB), WPB * 32, 0, s>>>(t, N, knm, inner);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s));
+	for (int L = 3; L < t.depth; ++L)
+		if (t.lsize[L])
+			l2l_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, inner + t.loff[L - 1] * Nx2,
+			                                                                     inner + t.loff[L] * Nx2, N, T, ctx.dev_flags);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s));
+	leaves_scaled_kernel<real><<<nl, LT, 0, s>>>(t, xr, yr, zr, qr, outer, inner, N, knm, pot, field);
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[5], s));
+	LFMM_CUDA(ctx, cudaGetLastError());
+	(void)stats;
+	return OK;
+}
+
+__global__ void adaptive_counts_kernel(DevTree t, unsigned long long* out)
+{
+	size_t li = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long p2p = 0, m2p = 0, u = 0;
+	if (li < t.nleaves) {
+		size_t g = t.leaves[li];
+		unsigned long long nt = t.tend[g] - t.tbeg[g];
+		unsigned long long ns = t.send[g] - t.pbeg[g];
+		for (uint32_t e = t.u_off[li]; e < t.u_off[li + 1]; ++e) { size_t k = t.u_idx[e]; ns += t.send[k] - t.pbeg[k]; }
+		p2p = nt * ns;
+		m2p = nt * (t.w_off[li + 1] - t.w_off[li]);
+		u = t.u_off[li + 1] - t.u_off[li];
+	}
+	unsigned long long far = 0;
+	for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < t.ncells; c += (size_t)gridDim.x * blockDim.x)
+		far += (unsigned long long)t.far_cnt[c];
+	p2p = warp_sum(p2p); m2p = warp_sum(m2p); u = warp_sum(u); far = warp_sum(far);
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(out, far); atomicAdd(out + 1, u); atomicAdd(out + 2, p2p); atomicAdd(out + 3, m2p);
+	}
+}
+
+} // namespace
+
+float* m2l_ops_fp32(Context& ctx, int N)
+{
+	for (auto& e : ctx.opcache)
+		if (e.N == N && e.prec == 1) { e.stamp = ++ctx.opcache_clock; return static_cast<float*>(e.ptr); }
+	double* d = m2l_ops_fp64(ctx, N, 1.0);
+	if (!d) return nullptr;
+	const int MT = m2l_padded(N);
+	size_t cnt = (size_t)343 * MT * MT;
+	OpCacheEntry e;
+	e.N = N; e.prec = 1; e.h = 1.0; e.bytes = cnt * sizeof(float); e.stamp = ++ctx.opcache_clock;
+	if (cudaMalloc(&e.ptr, e.bytes) != cudaSuccess) { cudaGetLastError(); ctx.last_error = "m2l operators: out of memory"; return nullptr; }
+	convert_back_kernel<float><<<div_up(cnt, 256), 256, 0, ctx.stream>>>(d, static_cast<float*>(e.ptr), cnt);
+	ctx.opcache.push_back(e);
+	return static_cast<float*>(e.ptr);
+}
+
+int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
+                       double* pot, double* field, SolveStats* stats, DevTree* tree_out)
+{
+	if (N < 1 || N > MAXN3) { ctx.last_error = "order out of range (1 <= N <= 18)"; return ERR_ARG; }
+	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 13"; return ERR_UNSUPPORTED; }
+	if (max_leaf < 0) { ctx.last_error = "max_leaf must be >= 0"; return ERR_ARG; }
+	int st = upload_scaled_constants(ctx);
+	if (st) return st;
+	cudaStream_t s = ctx.stream;
+	const bool timing = ctx.timing != 0;
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
+	DevTree t;
+	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t))) return st;
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
+	st = precision == 1 ? solve_t<float>(ctx, t, N, pot, field, stats) : solve_t<double>(ctx, t, N, pot, field, stats);
+	if (st) return st;
+	if (tree_out) *tree_out = t;
+	if (stats) {
+		unsigned long long* dc = static_cast<unsigned long long*>(ctx.arena.take(64));
+		if (!dc) return ERR_OOM;
+		LFMM_CUDA(ctx, cudaMemsetAsync(dc, 0, 64, s));
+		adaptive_counts_kernel<<<div_up(std::max<size_t>(t.nleaves, 1), 256), 256, 0, s>>>(t, dc);
+		unsigned long long h[4];
+		LFMM_CUDA(ctx, cudaMemcpyAsync(h, dc, 32, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+		stats->N = N; stats->depth = t.depth;
+		stats->n_particles = t.n; stats->n_cells = t.ncells; stats->n_leaves = t.nleaves;
+		stats->targets_num = t.targets_num;
+		stats->n_far_pairs = h[0]; stats->n_close_pairs = h[1]; stats->n_p2p_pairs = h[2];
+		stats->n_m2p = h[3]; stats->n_w = t.n_w; stats->n_x = t.n_x;
+		if (timing) {
+			cudaEventElapsedTime(&stats->ms_tree, ctx.ev[0], ctx.ev[1]);
+			cudaEventElapsedTime(&stats->ms_upward, ctx.ev[1], ctx.ev[2]);
+			cudaEventElapsedTime(&stats->ms_m2l, ctx.ev[2], ctx.ev[3]);
+			cudaEventElapsedTime(&stats->ms_l2l, ctx.ev[3], ctx.ev[4]);
+			cudaEventElapsedTime(&stats->ms_leaves, ctx.ev[4], ctx.ev[5]);
+			cudaEventElapsedTime(&stats->ms_total, ctx.ev[0], ctx.ev[5]);
+		}
+	}
+	return OK;
+}
+
+} // namespace lfmm

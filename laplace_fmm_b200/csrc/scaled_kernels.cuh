@@ -1,0 +1,509 @@
+// Device kernels of the scaled-expansion 3D solver (plain FP64 or mixed
+// FP32), included only by fmm3d_scaled.cu.  Scaled expansions: multipole
+// a_nm / h^n and local L_nm h^(n+1) for a cell of size h; every operator is
+// then level-independent and every coefficient O(total charge):
+//   M2L   rho / h = |d|                      (one operator per far offset d)
+//   M2M   (rho / h_child)^n, row j times 2^-j
+//   L2L   (rho / h_parent)^(n-j), row j times 2^-(j+1)
+//   P2M / L2P / P2L / M2P with r / h; potential times 1/h, field times 1/h^2.
+#pragma once
+#include "fmm3d.cuh"
+#include "m2l_gemm.cuh"
+
+namespace lfmm {
+namespace scaled {
+
+constexpr int CMAX = (MAXN3 * (MAXN3 + 1) / 2 + 31) / 32;
+constexpr int NX2MAX = MAXN3 * (MAXN3 + 1) / 2;
+constexpr int WPB = 4;
+
+__constant__ unsigned char c_n_of[NX2MAX];
+__constant__ unsigned char c_m_of[NX2MAX];
+
+template <typename real> struct V2;
+template <> struct V2<double> { using t = double2; static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); } };
+template <> struct V2<float> { using t = float2; static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); } };
+
+template <typename real>
+struct Tab {
+	const real* dmat;
+	const typename V2<real>::t* emat;
+	const real* m2m;
+	const real* l2l;
+	const real* knm;
+	const int4* dirinfo;
+};
+
+template <typename real>
+__device__ __forceinline__ typename V2<real>::t cmulv(typename V2<real>::t a, typename V2<real>::t b)
+{ return V2<real>::make(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+__device__ __forceinline__ void coords3(uint64_t code, int* c)
+{ c[0] = (int)compact3(code >> 2); c[1] = (int)compact3(code >> 1); c[2] = (int)compact3(code); }
+__device__ __forceinline__ int dir_id(int dx, int dy, int dz) { return (dx + 3) * 49 + (dy + 3) * 7 + (dz + 3); }
+
+template <typename real>
+struct SmemT {
+	typename V2<real>::t a[NX2MAX];
+	typename V2<real>::t b[NX2MAX];
+	real rn[2 * MAXN3 + 2];
+};
+
+template <typename real>
+__device__ __forceinline__ void rotate_y_t(const typename V2<real>::t* __restrict__ in, typename V2<real>::t* __restrict__ out,
+                                           const real* __restrict__ D, int Nx2)
+{
+	const int lane = threadIdx.x & 31;
+#pragma unroll
+	for (int t = 0; t < CMAX; ++t) {
+		int c = lane + 32 * t;
+		if (c < Nx2) {
+			int n = c_n_of[c], m = c_m_of[c];
+			const real* Dr = D + dix(n, m, 0);
+			real vr = 0, vi = 0;
+			const typename V2<real>::t* row = in + tix(n, 0);
+			for (int k = 1; k <= n; ++k) {
+				real z1 = Dr[k], z2 = Dr[-k];
+				typename V2<real>::t w = row[k];
+				vr = fma(w.x, z1 + z2, vr);
+				vi = fma(w.y, z1 - z2, vi);
+			}
+			real d0 = Dr[0];
+			vr = fma(d0, row[0].x, vr);
+			vi = fma(d0, row[0].y, vi);
+			out[c] = V2<real>::make(vr, vi);
+		}
+	}
+}
+
+enum { SOP_M2M = 0, SOP_L2L = 1 };
+
+// Scaled M2M / L2L along one of the 8 diagonal offsets (warp-cooperative).
+template <int OP, typename real>
+__device__ void translate_scaled(const typename V2<real>::t* __restrict__ src, int dirid,
+                                 typename V2<real>::t (&acc)[CMAX], int N, int Nx2, SmemT<real>& sm,
+                                 const Tab<real>& T, unsigned* flags)
+{
+	const int lane = threadIdx.x & 31;
+	int4 di = T.dirinfo[dirid];
+	if (di.x < 0 || di.y < 0 || di.z < 0 || di.w < 0) {
+		if (lane == 0) atomicOr(flags, DEV_ERR_DIRECTION);
+		return;
+	}
+	const real* D1 = T.dmat + (size_t)di.x * dsize(MAXN3);
+	const real* D2 = T.dmat + (size_t)di.y * dsize(MAXN3);
+	const typename V2<real>::t* E1 = T.emat + di.z * MAXN3;
+	const typename V2<real>::t* E2 = T.emat + di.w * MAXN3;
+	// M2M: rho / h_child = sqrt(3)/2 ; L2L: rho / h_parent = sqrt(3)/4
+	const double rho = OP == SOP_M2M ? 0.86602540378443864676 : 0.43301270189221932338;
+	for (int i = lane; i < N; i += 32) {
+		double p = 1.0;
+		for (int j = 0; j < i; ++j) p *= rho;
+		sm.rn[i] = (real)p;
+	}
+#pragma unroll
+	for (int t = 0; t < CMAX; ++t) {
+		int c = lane + 32 * t;
+		if (c < Nx2) sm.a[c] = cmulv<real>(src[c], E1[c_m_of[c]]);
+	}
+	__syncwarp();
+	rotate_y_t<real>(sm.a, sm.b, D1, Nx2);
+	__syncwarp();
+	const real* cube = OP == SOP_M2M ? T.m2m : T.l2l;
+#pragma unroll
+	for (int t = 0; t < CMAX; ++t) {
+		int c = lane + 32 * t;
+		if (c < Nx2) {
+			int j = c_n_of[c], k = c_m_of[c];
+			const real* cf = cube + (j * MAXN3 + k) * MAXN3;
+			real sr = 0, si = 0;
+			if (OP == SOP_M2M) {
+				for (int n = 0; j - n >= k; ++n) {
+					real f = cf[n] * sm.rn[n];
+					typename V2<real>::t w = sm.b[tix(j - n, k)];
+					sr = fma(f, w.x, sr); si = fma(f, w.y, si);
+				}
+				real s = (real)ldexp(1.0, -j);
+				sr *= s; si *= s;
+			} else {
+				for (int n = j; n < N; ++n) {
+					real f = cf[n] * sm.rn[n - j];
+					typename V2<real>::t w = sm.b[tix(n, k)];
+					sr = fma(f, w.x, sr); si = fma(f, w.y, si);
+				}
+				real s = (real)ldexp(1.0, -(j + 1));
+				sr *= s; si *= s;
+			}
+			sm.a[c] = V2<real>::make(sr, si);
+		}
+	}
+	__syncwarp();
+	rotate_y_t<real>(sm.a, sm.b, D2, Nx2);
+	__syncwarp();
+#pragma unroll
+	for (int t = 0; t < CMAX; ++t) {
+		int c = lane + 32 * t;
+		if (c < Nx2) {
+			typename V2<real>::t v = cmulv<real>(sm.b[c], E2[c_m_of[c]]);
+			acc[t].x += v.x; acc[t].y += v.y;
+		}
+	}
+	__syncwarp();
+}
+
+// parent (level L, array par) = sum of scaled M2M from its children (level L+1, array chi)
+template <typename real>
+__global__ void __launch_bounds__(WPB * 32) m2m_scaled_kernel(DevTree t, int L, const typename V2<real>::t* __restrict__ chi,
+                                                              typename V2<real>::t* __restrict__ par, int N,
+                                                              Tab<real> T, unsigned* flags)
+{
+	__shared__ SmemT<real> sm[WPB];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t c = (size_t)blockIdx.x * WPB + w;
+	if (c >= t.lsize[L]) return;
+	const int Nx2 = N * (N + 1) / 2;
+	size_t g = t.loff[L] + c, cb = t.loff[L + 1];
+	if (t.beg[g] >= t.end[g]) return;     // a leaf keeps its P2M expansion
+	typename V2<real>::t acc[CMAX];
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) acc[k] = V2<real>::make(0, 0);
+	for (uint32_t k = t.beg[g]; k < t.end[g]; ++k) {
+		uint64_t oct = t.code[cb + k] & 7ull;
+		int d = dir_id(2 * (int)((oct >> 2) & 1) - 1, 2 * (int)((oct >> 1) & 1) - 1, 2 * (int)(oct & 1) - 1);
+		translate_scaled<SOP_M2M, real>(chi + (size_t)k * Nx2, d, acc, N, Nx2, sm[w], T, flags);
+	}
+	typename V2<real>::t* out = par + c * Nx2;
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) {
+		int cc = lane + 32 * k;
+		if (cc < Nx2) out[cc] = acc[k];
+	}
+}
+
+// child (level L, array chi) += scaled L2L from its parent (level L-1, array par)
+template <typename real>
+__global__ void __launch_bounds__(WPB * 32) l2l_scaled_kernel(DevTree t, int L, const typename V2<real>::t* __restrict__ par,
+                                                              typename V2<real>::t* __restrict__ chi, int N,
+                                                              Tab<real> T, unsigned* flags)
+{
+	__shared__ SmemT<real> sm[WPB];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t c = (size_t)blockIdx.x * WPB + w;
+	if (c >= t.lsize[L]) return;
+	const int Nx2 = N * (N + 1) / 2;
+	size_t g = t.loff[L] + c;
+	int32_t p = t.parent[g];
+	typename V2<real>::t* out = chi + c * Nx2;
+	typename V2<real>::t acc[CMAX];
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) {
+		int cc = lane + 32 * k;
+		acc[k] = cc < Nx2 ? out[cc] : V2<real>::make(0, 0);
+	}
+	uint64_t oct = t.code[g] & 7ull;
+	int d = dir_id(1 - 2 * (int)((oct >> 2) & 1), 1 - 2 * (int)((oct >> 1) & 1), 1 - 2 * (int)(oct & 1));
+	translate_scaled<SOP_L2L, real>(par + (size_t)p * Nx2, d, acc, N, Nx2, sm[w], T, flags);
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) {
+		int cc = lane + 32 * k;
+		if (cc < Nx2) out[cc] = acc[k];
+	}
+}
+
+template <typename real> __device__ __forceinline__ real rsq(real x);
+template <> __device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double rsq<double>(double x) { return rsqrt(x); }
+template <typename real> __device__ __forceinline__ void sc(real a, real* s, real* c);
+template <> __device__ __forceinline__ void sc<float>(float a, float* s, float* c) { sincosf(a, s, c); }
+template <> __device__ __forceinline__ void sc<double>(double a, double* s, double* c) { sincos(a, s, c); }
+
+// Leaf-relative coordinates (real) and charges, block per leaf.
+template <typename real>
+__global__ void relcoords_kernel(DevTree t, real* __restrict__ xr, real* __restrict__ yr, real* __restrict__ zr,
+                                 real* __restrict__ qr)
+{
+	if (blockIdx.x >= t.nleaves) return;
+	size_t g = t.leaves[blockIdx.x];
+	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+	for (uint32_t i = t.pbeg[g] + threadIdx.x; i < t.pend[g]; i += blockDim.x) {
+		xr[i] = (real)(t.x[i] - cx); yr[i] = (real)(t.y[i] - cy); zr[i] = (real)(t.z[i] - cz);
+		qr[i] = (real)t.q[i];
+	}
+}
+
+// Regular (P2M) or singular (P2L) harmonics of the warp's particles summed
+// into sacc: regular  q (r/h)^n K P_nm e^{-i m phi}
+//            singular q (r/h)^-(n+1) K P_nm e^{-i m phi}
+template <bool SINGULAR, typename real>
+__device__ __forceinline__ void accumulate_harmonics(real q, real r, real th, real ph, int N, const real* __restrict__ knm,
+                                                     typename V2<real>::t* sacc)
+{
+	const int lane = threadIdx.x & 31;
+	real y, x;
+	sc<real>(th, &y, &x);
+	const real ir = real(1) / r;
+	real Pmm = 1, rpow = SINGULAR ? ir : real(1);
+	for (int m = 0; m < N; ++m) {
+		if (m > 0) { Pmm = Pmm * y * (real)(1 - 2 * m); rpow *= SINGULAR ? ir : r; }
+		real sm_, cm_;
+		sc<real>(m * ph, &sm_, &cm_);
+		real Pn = Pmm, Pn1 = 0, rn = rpow;
+		for (int n = m; n < N; ++n) {
+			if (n > m) {
+				real Pnew = (n == m + 1) ? Pmm * x * (real)(2 * n - 1)
+				                         : ((real)(2 * n - 1) * x * Pn - (real)(n + m - 1) * Pn1) / (real)(n - m);
+				Pn1 = Pn; Pn = Pnew; rn *= SINGULAR ? ir : r;
+			}
+			real f = q * rn * knm[tix(n, m)] * Pn;
+			real vr = warp_sum(f * cm_), vi = warp_sum(-f * sm_);
+			if (lane == 0) { typename V2<real>::t a = sacc[tix(n, m)]; sacc[tix(n, m)] = V2<real>::make(a.x + vr, a.y + vi); }
+		}
+	}
+}
+
+// P2M, warp per leaf, in the leaf's scaled frame
+template <typename real>
+__global__ void __launch_bounds__(WPB * 32) p2m_scaled_kernel(DevTree t, const real* __restrict__ xr, const real* __restrict__ yr,
+                                                              const real* __restrict__ zr, const real* __restrict__ qr,
+                                                              int N, const real* __restrict__ knm,
+                                                              typename V2<real>::t* __restrict__ outer)
+{
+	__shared__ typename V2<real>::t sacc[WPB][NX2MAX];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t li = (size_t)blockIdx.x * WPB + w;
+	if (li >= t.nleaves) return;
+	const size_t g = t.leaves[li];
+	const int Nx2 = N * (N + 1) / 2;
+	for (int c = lane; c < Nx2; c += 32) sacc[w][c] = V2<real>::make(0, 0);
+	__syncwarp();
+	const real ih = (real)(ldexp(1.0, t.lev[g]) / t.geo_host[3]);
+	const uint32_t b = t.pbeg[g], e = t.send[g];
+	for (uint32_t base = b; base < e; base += 32) {
+		uint32_t i = base + lane;
+		real q = 0, r = 1, th = 1, ph = 0;
+		if (i < e) { q = qr[i]; dec_to_sph<real>(xr[i] * ih, yr[i] * ih, zr[i] * ih, r, th, ph); }
+		accumulate_harmonics<false, real>(q, r, th, ph, N, knm, sacc[w]);
+	}
+	__syncwarp();
+	typename V2<real>::t* out = outer + g * Nx2;
+	for (int c = lane; c < Nx2; c += 32) out[c] = sacc[w][c];
+}
+
+// P2L over the X list, warp per cell: inner[g] += singular harmonics of every
+// X leaf's sources about g's centre (scaled by g's size).
+template <typename real>
+__global__ void __launch_bounds__(WPB * 32) p2l_kernel(DevTree t, int N, const real* __restrict__ knm,
+                                                       typename V2<real>::t* __restrict__ inner)
+{
+	__shared__ typename V2<real>::t sacc[WPB][NX2MAX];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t g = (size_t)blockIdx.x * WPB + w;
+	if (g >= t.ncells) return;
+	const uint32_t xb = t.x_off[g], xe = t.x_off[g + 1];
+	if (xb == xe) return;
+	const int Nx2 = N * (N + 1) / 2;
+	for (int c = lane; c < Nx2; c += 32) sacc[w][c] = V2<real>::make(0, 0);
+	__syncwarp();
+	const double ih = ldexp(1.0, t.lev[g]) / t.geo_host[3];
+	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+	for (uint32_t e = xb; e < xe; ++e) {
+		const int32_t C = t.x_idx[e];
+		const uint32_t b = t.pbeg[C], en = t.send[C];
+		for (uint32_t base = b; base < en; base += 32) {
+			uint32_t i = base + lane;
+			real q = 0, r = 1, th = 1, ph = 0;
+			if (i < en) {
+				q = (real)t.q[i];
+				dec_to_sph<real>((real)((t.x[i] - cx) * ih), (real)((t.y[i] - cy) * ih), (real)((t.z[i] - cz) * ih), r, th, ph);
+			}
+			accumulate_harmonics<true, real>(q, r, th, ph, N, knm, sacc[w]);
+		}
+	}
+	__syncwarp();
+	typename V2<real>::t* out = inner + g * Nx2;
+	for (int c = lane; c < Nx2; c += 32) {
+		typename V2<real>::t a = out[c], b = sacc[w][c];
+		out[c] = V2<real>::make(a.x + b.x, a.y + b.y);
+	}
+}
+
+// Expansion evaluated at one target, in the expansion's scaled frame:
+// LOCAL  phi = sum (2 - d_m0) Re(r^n Y_nm L_nm)      (reference L2P form,
+//        cpu/multipole3d.cpp:1152-1208)
+// MULTI  phi = sum (2 - d_m0) Re(r^-(n+1) Y_nm a_nm)  (M2P)
+// with Y_nm = K_nm P_nm e^{i m phi}; returns phi and -grad phi.
+template <bool LOCAL, typename real>
+__device__ void eval_expansion(const typename V2<real>::t* __restrict__ Lc, real dx, real dy, real dz, int N,
+                               const real* __restrict__ knm, real& pot, real& fx, real& fy, real& fz)
+{
+	real r, th, ph;
+	dec_to_sph<real>(dx, dy, dz, r, th, ph);
+	real y, x;
+	sc<real>(th, &y, &x);
+	const real ir = real(1) / r;
+	real phi = 0, mt0 = 0, mt1 = 0, mt2 = 0;
+	// LOCAL: rn = r^(n-1) ; MULTI: rn = r^-(n+2)
+	real Pmm = 1, rpow = LOCAL ? ir : ir * ir;
+	for (int m = 0; m < N; ++m) {
+		if (m > 0) { Pmm = Pmm * y * (real)(1 - 2 * m); rpow *= LOCAL ? r : ir; }
+		real sm_, cm_;
+		sc<real>(m * ph, &sm_, &cm_);
+		const real mult = m ? real(2) : real(1);
+		real Pn = Pmm, Pn1 = 0, rn = rpow;
+		for (int n = m; n < N; ++n) {
+			real Pnext = (n == m) ? Pmm * x * (real)(2 * n + 1)
+			                      : ((real)(2 * n + 1) * x * Pn - (real)(n + m) * Pn1) / (real)(n + 1 - m);
+			real K = knm[tix(n, m)];
+			real Yr = Pn * cm_ * K, Yi = Pn * sm_ * K;
+			typename V2<real>::t A = Lc[tix(n, m)];
+			real cr = A.x * rn, ci = A.y * rn;
+			real ycr = Yr * cr - Yi * ci;                 // Re(Y A) r^(n-1) or r^-(n+2)
+			real gq = K * ((real)(1 - m + n) * Pnext - (real)(n + 1) * x * Pn) / y;
+			if (LOCAL) {
+				phi += mult * (r * ycr);
+				mt0 -= mult * ((real)n * ycr);
+			} else {
+				phi += mult * (r * ycr);
+				mt0 += mult * ((real)(n + 1) * ycr);
+			}
+			mt1 -= mult * (cr * cm_ * gq - ci * sm_ * gq);
+			mt2 -= mult * (cr * (-(real)m * Yi) - ci * ((real)m * Yr));
+			Pn1 = Pn; Pn = Pnext; rn *= LOCAL ? r : ir;
+		}
+	}
+	pot = phi;
+	real s2, c2;
+	sc<real>(ph, &s2, &c2);
+	fx = mt0 * y * c2 + mt1 * x * c2 - mt2 * s2 / y;
+	fy = mt0 * y * s2 + mt1 * x * s2 + mt2 * c2 / y;
+	fz = mt0 * x - mt1 * y;
+}
+
+template <typename real>
+__global__ void convert_kernel(const real* __restrict__ in, double* __restrict__ out, size_t n)
+{
+	size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (double)in[i];
+}
+template <typename real>
+__global__ void convert_back_kernel(const double* __restrict__ in, real* __restrict__ out, size_t n)
+{
+	size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (real)in[i];
+}
+
+constexpr int LT = 128;
+
+// One block per leaf: near field over the leaf and its U list (leaf-relative
+// coordinates, source leaves shifted by the FP64 centre difference rounded
+// once, per-tile partial sums carried in FP64), M2P over the W list, L2P of
+// the leaf's local expansion, and the self term q_i / 1e-4 in FP64.
+template <typename real>
+__global__ void __launch_bounds__(LT) leaves_scaled_kernel(DevTree t, const real* __restrict__ xr, const real* __restrict__ yr,
+                                                           const real* __restrict__ zr, const real* __restrict__ qr,
+                                                           const typename V2<real>::t* __restrict__ outer,
+                                                           const typename V2<real>::t* __restrict__ inner, int N,
+                                                           const real* __restrict__ knm, double* __restrict__ pot_out,
+                                                           double* __restrict__ fld_out)
+{
+	// source tile in the target leaf's frame: offset = hi + lo (FP32 pairs; the
+	// FP64 offset split once when staged, so pair differences keep ~1e-7
+	// relative accuracy however close the pair); lo unused in FP64
+	__shared__ real sx[LT], sy[LT], sz[LT], sq[LT];
+	__shared__ real lx[LT], ly[LT], lz[LT];
+	__shared__ typename V2<real>::t sL[NX2MAX];
+	__shared__ typename V2<real>::t sM[NX2MAX];
+	if (blockIdx.x >= t.nleaves) return;
+	const size_t li = blockIdx.x;
+	const size_t g = t.leaves[li];
+	const uint32_t tb = t.tbeg[g], te = t.tend[g];
+	if (tb >= te) return;
+	const bool tmode = t.targets_num > 0;
+	const int Nx2 = N * (N + 1) / 2;
+	const double scale = t.geo_host[3];
+	const double ihg = ldexp(1.0, t.lev[g]) / scale;
+	for (int c = threadIdx.x; c < Nx2; c += LT) sL[c] = inner[g * Nx2 + c];
+	const uint32_t ub = t.u_off[li], ue = t.u_off[li + 1];
+	const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
+	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+	for (uint32_t t0 = tb; t0 < te; t0 += LT) {
+		const uint32_t i = t0 + threadIdx.x;
+		const bool valid = i < te;
+		constexpr bool SPLIT = sizeof(real) == sizeof(float);
+		real xi = 0, yi = 0, zi = 0, xl = 0, yl = 0, zl = 0;
+		if (valid) {
+			const double ax_ = t.x[i] - cx, ay_ = t.y[i] - cy, az_ = t.z[i] - cz;
+			xi = (real)ax_; yi = (real)ay_; zi = (real)az_;
+			if (SPLIT) { xl = (real)(ax_ - (double)xi); yl = (real)(ay_ - (double)yi); zl = (real)(az_ - (double)zi); }
+		}
+		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+		for (int64_t e = (int64_t)ub - 1; e < (int64_t)ue; ++e) {
+			const size_t sc_ = e < (int64_t)ub ? g : (size_t)t.u_idx[e];
+			const uint32_t sb = t.pbeg[sc_], se = t.send[sc_];
+			for (uint32_t s0 = sb; s0 < se; s0 += LT) {
+				const int cnt = min((uint32_t)LT, se - s0);
+				__syncthreads();
+				if (threadIdx.x < cnt) {
+					const uint32_t j = s0 + threadIdx.x;
+					const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
+					const real hx = (real)dx_, hy = (real)dy_, hz = (real)dz_;
+					sx[threadIdx.x] = hx; sy[threadIdx.x] = hy; sz[threadIdx.x] = hz;
+					if (SPLIT) {
+						lx[threadIdx.x] = (real)(dx_ - (double)hx); ly[threadIdx.x] = (real)(dy_ - (double)hy);
+						lz[threadIdx.x] = (real)(dz_ - (double)hz);
+					}
+					sq[threadIdx.x] = qr[j];
+				}
+				__syncthreads();
+				if (valid) {
+					const int self = (sc_ == g) ? (int)i - (int)s0 : -1;
+					// partial sums over 8 sources, carried in FP64 (compensated per target)
+					for (int j0 = 0; j0 < cnt; j0 += 8) {
+					const int j1 = min(cnt, j0 + 8);
+					real p = 0, ax = 0, ay = 0, az = 0;
+					for (int j = j0; j < j1; ++j) {
+						real dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
+						if (SPLIT) { dx += xl - lx[j]; dy += yl - ly[j]; dz += zl - lz[j]; }
+						real r2 = fmax(fma(dx, dx, fma(dy, dy, dz * dz)), (real)FORCE_EPS2);
+						real inv = rsq<real>(r2);
+						real qi = (j == self) ? real(0) : sq[j] * inv;
+						real qi3 = qi * inv * inv;
+						p += qi;
+						ax = fma(dx, qi3, ax); ay = fma(dy, qi3, ay); az = fma(dz, qi3, az);
+					}
+					pot += p; fx += ax; fy += ay; fz += az;
+					}
+				}
+			}
+		}
+		// M2P over the W list
+		for (uint32_t e = wb; e < we; ++e) {
+			const size_t D = t.w_idx[e];
+			__syncthreads();
+			for (int c = threadIdx.x; c < Nx2; c += LT) sM[c] = outer[D * Nx2 + c];
+			__syncthreads();
+			if (valid) {
+				const double ihd = ldexp(1.0, t.lev[D]) / scale;
+				real mp, mx_, my_, mz_;
+				eval_expansion<false, real>(sM, (real)((t.x[i] - t.cx[D]) * ihd), (real)((t.y[i] - t.cy[D]) * ihd),
+				                            (real)((t.z[i] - t.cz[D]) * ihd), N, knm, mp, mx_, my_, mz_);
+				pot += (double)mp * ihd;
+				fx += (double)mx_ * ihd * ihd; fy += (double)my_ * ihd * ihd; fz += (double)mz_ * ihd * ihd;
+			}
+		}
+		__syncthreads();
+		if (valid) {
+			real lp, lx, ly, lz;
+			eval_expansion<true, real>(sL, (real)(xi * ihg), (real)(yi * ihg), (real)(zi * ihg), N, knm, lp, lx, ly, lz);
+			pot += (double)lp * ihg;
+			fx += (double)lx * ihg * ihg; fy += (double)ly * ihg * ihg; fz += (double)lz * ihg * ihg;
+			if (!tmode) pot += t.q[i] * (1.0 / FORCE_EPS);
+			const uint32_t o = t.orig[i];
+			pot_out[o] = pot;
+			fld_out[3 * (size_t)o] = fx; fld_out[3 * (size_t)o + 1] = fy; fld_out[3 * (size_t)o + 2] = fz;
+		}
+	}
+}
+
+} // namespace scaled
+} // namespace lfmm

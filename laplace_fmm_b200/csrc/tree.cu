@@ -331,7 +331,7 @@ T* take(Context& ctx, size_t count)
 
 } // namespace
 
-int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t)
+int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, bool partition, bool lists)
 {
 	const int dim = in.dim;
 	const size_t n = in.ns + in.nt;
@@ -417,7 +417,7 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t)
 		else centres_kernel<2><<<div_up(t.lsize[L], TB), TB, 0, s>>>(t, L, t.loff[L], t.lsize[L]);
 	}
 	// target partition
-	if (t.targets_num > 0) {
+	if (partition && t.targets_num > 0) {
 		double* x2 = reinterpret_cast<double*>(keys2 == sk ? keys : keys2);   // reuse the free sort buffer
 		double* y2 = take<double>(ctx, n);
 		double* z2 = dim == 3 ? take<double>(ctx, n) : nullptr;
@@ -433,11 +433,18 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t)
 	} else {
 		source_targets_kernel<<<div_up(t.lsize[LL], TB), TB, 0, s>>>(t, t.loff[LL], t.lsize[LL]);
 	}
-	// lists
-	LFMM_CUDA(ctx, cudaMemsetAsync(t.close_cnt, 0, sizeof(int32_t) * C, s));
-	LFMM_CUDA(ctx, cudaMemsetAsync(t.far_cnt, 0, sizeof(int32_t) * C, s));
-	for (int L = 1; L < depth; ++L) {
-		if (dim == 3) lists_kernel<3><<<div_up(t.lsize[L], 128), 128, 0, s>>>(t, L, ctx.dev_flags);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return lists ? tree_lists(ctx, t) : OK;
+}
+
+int tree_lists(Context& ctx, DevTree& t)
+{
+	cudaStream_t s = ctx.stream;
+	LFMM_CUDA(ctx, cudaMemsetAsync(t.close_cnt, 0, sizeof(int32_t) * t.ncells, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(t.far_cnt, 0, sizeof(int32_t) * t.ncells, s));
+	for (int L = 1; L < t.depth; ++L) {
+		if (t.lsize[L] == 0) continue;
+		if (t.dim == 3) lists_kernel<3><<<div_up(t.lsize[L], 128), 128, 0, s>>>(t, L, ctx.dev_flags);
 		else lists_kernel<2><<<div_up(t.lsize[L], 128), 128, 0, s>>>(t, L, ctx.dev_flags);
 	}
 	LFMM_CUDA(ctx, cudaGetLastError());

@@ -32,6 +32,20 @@ struct DevTree {
 	int32_t* close_idx = nullptr;
 	int32_t* far_cnt = nullptr;                 // per cell, for statistics
 	size_t n_far_pairs = 0, n_close_pairs = 0;
+	// adaptive form (tree_build_adaptive); global cell indices unless noted
+	bool adaptive = false;
+	int max_leaf = 0;
+	uint32_t *pbeg = nullptr, *pend = nullptr;  // particles of every cell
+	uint32_t* send = nullptr;                   // leaves: sources are [pbeg, send)
+	uint8_t* is_leaf = nullptr;
+	uint8_t* lev = nullptr;
+	int32_t* leaves = nullptr;                  // global indices of the leaves
+	size_t nleaves = 0;
+	uint32_t *u_off = nullptr, *w_off = nullptr; // per leaf (position in leaves[]), CSR
+	int32_t *u_idx = nullptr, *w_idx = nullptr;  // global cell indices
+	uint32_t* x_off = nullptr;                  // per cell, CSR
+	int32_t* x_idx = nullptr;                   // global indices of leaves
+	size_t n_u = 0, n_w = 0, n_x = 0;
 };
 
 // Input particles: targets (nt, q = 0) followed by sources (ns, with q).
@@ -43,7 +57,21 @@ struct ParticleInput {
 	const double* tgt = nullptr;   // device, nt x dim interleaved
 };
 
-int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t);
+// partition: split each leaf into sources then q == 0 targets; lists: build
+// the close lists and far counts.
+int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, bool partition = true,
+               bool lists = true);
+
+// Close lists (fixed stride) and far counts of every level from the child
+// ranges; used by both builders.
+int tree_lists(Context& ctx, DevTree& t);
+
+// Adaptive octree from the uniform one: a cell is split while it holds more
+// than max_leaf particles and is above level depth-1 (max_leaf = 0 splits
+// every cell: the uniform tree in adaptive form).  Leaves may sit on any
+// level; beg/end hold child ranges (empty for leaves), pbeg/pend particle
+// ranges; U/W/X lists are built (3D only).
+int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& t);
 
 // Fill a CSR far list of level L (level-local source indices) in the
 // reference's order; far_off must hold lsize[L] + 1 entries.

@@ -28,7 +28,7 @@ from enum import Enum
 
 import numpy as np
 
-from ._lib import AUTO, PRECISION, Context, LfmmStats, default_context
+from ._lib import AUTO, PRECISION, Context, LfmmSolveOpts, LfmmStats, default_context
 
 FMM_AUTO = AUTO
 FORCE_EPS = 1.0e-4
@@ -76,7 +76,7 @@ class _Solver:
     dim = 3
 
     def __init__(self, *args, eps: float = 1.0e-8, N: int = FMM_AUTO, tree_depth: int = FMM_AUTO,
-                 precision: str = "fp64", ctx: Context | None = None):
+                 precision: str = "fp64", max_leaf: int = 0, ctx: Context | None = None):
         # reference overloads: (particles, eps, N, depth) and (sources, targets, eps, N, depth)
         args = list(args)
         if not args:
@@ -103,9 +103,14 @@ class _Solver:
         pot = np.zeros(nout)
         fld = np.zeros((nout, dim))
         stats = LfmmStats()
-        fn = ctx.lib.lfmm3d_solve if dim == 3 else ctx.lib.lfmm2d_solve
-        st = fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos), int(N), int(tree_depth), float(eps),
-                PRECISION[precision], _ptr(pot), _ptr(fld), ctypes.byref(stats))
+        if dim == 3 and max_leaf:
+            opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
+            st = ctx.lib.lfmm3d_solve_ex(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos),
+                                         ctypes.byref(opts), _ptr(pot), _ptr(fld), ctypes.byref(stats))
+        else:
+            fn = ctx.lib.lfmm3d_solve if dim == 3 else ctx.lib.lfmm2d_solve
+            st = fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos), int(N), int(tree_depth),
+                    float(eps), PRECISION[precision], _ptr(pot), _ptr(fld), ctypes.byref(stats))
         ctx.check(st, f"lfmm{dim}d_solve")
         self.potentials = pot
         self.forces = fld if dim == 3 else fld[:, 0] + 1j * fld[:, 1]
