@@ -45,11 +45,12 @@ CONFIGS = {
     "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=9, precision="fp64",
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
                         "p=20 (N=21), uniform quadtree depth 9"),
-    # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform)
-    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=11, depth=8, precision="fp64",
-               workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, p=10 (N=11), octree depth 8"),
+    # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
+    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=13, depth=10, max_leaf=64, precision="mixed",
+               workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels, "
+                        "<=64 per leaf), p=12 (N=13), mixed precision"),
 }
-DEFAULT_CONFIG = "c1"
+DEFAULT_CONFIG = "c3"
 METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
 
 
@@ -62,6 +63,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the mixed one")
+    ap.add_argument("--max-leaf", type=int, default=None, help="override the adaptive split threshold (0: uniform)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None, help="override the configuration's")
     ap.add_argument("--order", type=int, default=None, help="override N (degrees)")
     ap.add_argument("--depth", type=int, default=None, help="override the tree depth")
@@ -73,6 +76,8 @@ def parse():
         cfg["N"] = a.order
     if a.depth:
         cfg["depth"] = a.depth
+    if a.max_leaf is not None:
+        cfg["max_leaf"] = a.max_leaf
     a.cfg = cfg
     return a
 
@@ -161,13 +166,39 @@ def fp64_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def launches_per_solve(depth, dim, radix_passes, targets):
-    """Kernels the library enqueues for one solve (tree + FMM passes)."""
+def fp32_peak_tflops(torch):
+    """Dense FP32 (SIMT, TF32 off) throughput measured here: cuBLAS SGEMM 8192^3."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    torch.matmul(a, b); torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def launches_per_solve(depth, dim, radix_passes, adaptive, precision):
+    """Kernels the library enqueues for one solve (tree + FMM passes), counted
+    from the launch sites."""
     scan = 3
     tree = 2 + 1 + radix_passes * (1 + scan + 1) + 1 + 1 + scan + 1 + 1
-    tree += (depth - 1) * (1 + scan + 1 + 1) + depth + 1 + (depth - 1)
+    tree += (depth - 1) * (1 + scan + 1 + 1) + depth + 1
+    lists = depth - 1
+    if adaptive or precision != "fp64":
+        tree += depth + depth * (1 + scan) + depth + 1 + scan + 1 + 1 + lists + 2 + 2 + 3 * scan
+        m2l = max(0, depth - 2) * (3 + 1 + 1) + 2 * 2          # plan + GEMM (+ split reduce), FP64 coarse converts
+        fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + 1
+        return tree + fmm
+    tree += lists
     if dim == 3:
-        fmm = 1 + (depth - 1) + max(0, depth - 2) + max(0, depth - 3) + 1
+        fmm = 1 + (depth - 1) + max(0, depth - 2) * 5 + max(0, depth - 3) + 1
     else:
         fmm = 1 + (depth - 1) + max(0, depth - 2) + 1
     return tree + fmm
@@ -177,7 +208,7 @@ def launches_per_solve(depth, dim, radix_passes, targets):
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     from laplace_fmm_b200 import Context
-    from laplace_fmm_b200._lib import PRECISION, LfmmStats
+    from laplace_fmm_b200._lib import PRECISION, LfmmSolveOpts, LfmmStats
     from laplace_fmm_b200.workloads import rel_l2, sample_targets
     torch.cuda.set_device(local_rank)
     dist = None
@@ -186,12 +217,11 @@ def run_ours(args, cfg, rank, world, local_rank):
         dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank),
                                 timeout=__import__("datetime").timedelta(seconds=300))
     dim, n, N, depth = cfg["dim"], cfg["n"], cfg["N"], cfg["depth"]
+    max_leaf = cfg.get("max_leaf", 0)
     prec = PRECISION[cfg["precision"]]
     pos, q = make_particles(cfg)
     ctx = Context(local_rank)
     L = ctx.lib
-    solve_dev = L.lfmm3d_solve_device if dim == 3 else L.lfmm2d_solve_device
-    solve_host = L.lfmm3d_solve if dim == 3 else L.lfmm2d_solve
     d_src = torch.from_numpy(pos).cuda()
     d_q = torch.from_numpy(q).cuda()
     d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
@@ -200,9 +230,23 @@ def run_ours(args, cfg, rank, world, local_rank):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     vp = ctypes.c_void_p
 
+    def call(c, device, precision, stats=None, host=None):
+        """One solve through the C ABI (device buffers, or pinned host buffers)."""
+        src, qq, pot, fld = host if host else (d_src, d_q, d_pot, d_fld)
+        sp = ctypes.byref(stats) if stats is not None else None
+        if dim == 3:
+            opts = LfmmSolveOpts(N, depth, max_leaf, precision, 1e-8)
+            fn = L.lfmm3d_solve_ex_device if device else L.lfmm3d_solve_ex
+            st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, ctypes.byref(opts),
+                    vp(pot.data_ptr()), vp(fld.data_ptr()), sp)
+        else:
+            fn = L.lfmm2d_solve_device if device else L.lfmm2d_solve
+            st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, N, depth, 1e-8, precision,
+                    vp(pot.data_ptr()), vp(fld.data_ptr()), sp)
+        c.check(st, "solve")
+
     def step_dev():
-        ctx.check(solve_dev(ctx.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), 0, None, N, depth, 1e-8, prec,
-                            vp(d_pot.data_ptr()), vp(d_fld.data_ptr()), None), "solve_device")
+        call(ctx, True, prec)
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -232,10 +276,27 @@ def run_ours(args, cfg, rank, world, local_rank):
     # per-phase split (separate timed solve with phase events)
     ctx_t = Context(local_rank, timing=True)
     st = LfmmStats()
-    ctx_t.check(solve_dev(ctx_t.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), 0, None, N, depth, 1e-8, prec,
-                          vp(d_pot.data_ptr()), vp(d_fld.data_ptr()), ctypes.byref(st)), "solve_device(timed)")
+    call(ctx_t, True, prec)                       # warm the operator cache of this context
+    call(ctx_t, True, prec, stats=st)
     torch.cuda.synchronize()
     stats = st.as_dict()
+    # the plain FP64 form of the same configuration (the comparison the metric names)
+    plain = None
+    if dim == 3 and prec != 0 and not args.no_plain:
+        for _ in range(2):
+            call(ctx_t, True, 0)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t0.record()
+        for _ in range(reps):
+            call(ctx_t, True, 0)
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t1.record()
+        t1.synchronize()
+        pms = t0.elapsed_time(t1) / reps
+        plain = {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms, "precision": "fp64"}
     ctx_t.close()
     # accuracy on 4096 seeded targets against the FP64 direct sum (on the GPU)
     idx = sample_targets(n)
@@ -260,8 +321,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         h_fld = torch.empty(n, dim, dtype=torch.float64).pin_memory()
 
         def step_host():
-            ctx.check(solve_host(ctx.handle, n, vp(h_src.data_ptr()), vp(h_q.data_ptr()), 0, None, N, depth, 1e-8,
-                                 prec, vp(h_pot.data_ptr()), vp(h_fld.data_ptr()), None), "solve")
+            call(ctx, False, prec, host=(h_src, h_q, h_pot, h_fld))
 
         for _ in range(max(1, args.warmup)):
             step_host()
@@ -283,7 +343,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         e2e = {"value": world * n / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
                "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
-    return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx)
+    return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx,
+                plain=plain)
 
 
 def m2l_flops(N):
@@ -293,28 +354,32 @@ def m2l_flops(N):
     return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
 
 
-def roofline(cfg, stats, peaks, fp64_tflops):
-    """Roofline of the dominant phase (device time from the phase events)."""
+def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops):
+    """Roofline of the dominant phase (device time from the phase events).
+    P2P: 20 flops per particle pair; M2L: the rotation method's algorithmic
+    flops per V pair (executed dense-GEMM flops reported beside it)."""
     phases = {"leaves": stats["ms_leaves"], "m2l": stats["ms_m2l"], "tree": stats["ms_tree"],
               "upward": stats["ms_upward"], "l2l": stats["ms_l2l"]}
     dom = max(phases, key=phases.get)
     ms = phases[dom]
     fp64 = cfg["precision"] == "fp64"
+    peak = fp64_tflops if fp64 else fp32_tflops
+    src = "measured cuBLAS DGEMM" if fp64 else "measured cuBLAS SGEMM (TF32 off)"
     if dom == "leaves":
         flops = 20.0 * stats["n_p2p_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
-        peak = fp64_tflops if fp64 else 2 * 148 * 128 * 1.965e9 / 1e12
-        return {"kernel": "leaves_kernel (P2P + L2P)", "bound": "fp64" if fp64 else "fp32",
+        return {"kernel": "leaves kernel (P2P + M2P + L2P)", "bound": "fp64" if fp64 else "fp32",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "measured DGEMM" if fp64 else "spec FP32 SIMT", "algorithmic_flops": flops,
-                "phase_ms": ms, "traffic": None}
+                "peak_source": src, "algorithmic_flops": flops, "phase_ms": ms, "traffic": None}
     if dom == "m2l":
         flops = float(m2l_flops(cfg["N"])) * stats["n_far_pairs"]
+        R = cfg["N"] * (cfg["N"] + 1)
+        executed = 2.0 * R * R * stats["n_far_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
-        peak = fp64_tflops if fp64 else peaks["bf16_tflops"]
-        return {"kernel": "m2l_kernel", "bound": "fp64" if fp64 else "tensor", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "algorithmic_flops": flops, "phase_ms": ms,
-                "traffic": None}
+        return {"kernel": "m2l_gemm_kernel (direction-grouped GEMM)", "bound": "fp64" if fp64 else "fp32",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": src, "algorithmic_flops": flops, "executed_dense_flops": executed,
+                "executed_tflops": executed / (ms * 1e-3) / 1e12, "phase_ms": ms, "traffic": None}
     # tree / upward: HBM-bound passes over the particles
     nbytes = stats["n_particles"] * (2 * 32 + 2 * 8 + 4)
     achieved = nbytes / (ms * 1e-3) / 1e9
@@ -397,6 +462,7 @@ def main():
     if rank == 0:
         peaks = measured_peaks()
         fp64 = fp64_peak_tflops(torch)
+        fp32 = fp32_peak_tflops(torch)
         stats = r["stats"]
         radix_passes = (cfg["dim"] * (cfg["depth"] - 1) + 7) // 8
         line = {
@@ -407,10 +473,15 @@ def main():
             "config": base_config(cfg, world), "accuracy": r["acc"], "phases_ms": {
                 k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves", "ms_total")},
             "tree": {k: stats[k] for k in ("n_cells", "n_leaves", "n_far_pairs", "n_close_pairs", "n_p2p_pairs")},
-            "roofline": roofline(cfg, stats, peaks, fp64), "fp64_peak_tflops_measured": fp64,
+            "roofline": roofline(cfg, stats, peaks, fp64, fp32), "fp64_peak_tflops_measured": fp64,
+            "fp32_peak_tflops_measured": fp32,
             "peaks_source": peaks["source"], "e2e": r["e2e"], "clocks": r["clocks"],
-            "gpu_launches": args.steps * launches_per_solve(cfg["depth"], cfg["dim"], radix_passes, False),
+            "gpu_launches": args.steps * launches_per_solve(stats["depth"], cfg["dim"], radix_passes,
+                                                            cfg.get("max_leaf", 0) > 0, cfg["precision"]),
         }
+        if r["plain"]:
+            line["plain_fp64"] = r["plain"]
+            line["speedup_vs_plain_fp64"] = r["plain"]["ms_per_step"] / r["ms"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()

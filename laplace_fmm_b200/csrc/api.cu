@@ -67,6 +67,8 @@ int cuda_fail(Context& ctx, cudaError_t e, const char* where)
 	return ERR_CUDA;
 }
 
+Context& ctx_of(lfmm_ctx* c) { return c->c; }
+
 } // namespace lfmm
 
 using namespace lfmm;
@@ -248,9 +250,10 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	Context& c = ctx->c;
 	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
 	// M2L engine: dense direction GEMMs (default) or per-pair rotations
-	// (rotation: per-pair rotations on the plain path; simt: no tensor cores on the FP32 levels)
+	// rotation: per-pair rotations on the plain path; simt: SIMT GEMMs only (the
+	// default); tc: tcgen05 TF32 hi/lo GEMMs on large FP32 levels
 	if (const char* e = std::getenv("LFMM_M2L"))
-		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 2 : 0);
+		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "tc") == 0 ? 3 : 0);
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
 		cudaGetLastError();

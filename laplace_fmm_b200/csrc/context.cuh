@@ -75,7 +75,7 @@ struct Context {
 	Tables tables;
 	std::vector<OpCacheEntry> opcache;
 	unsigned long long opcache_clock = 0;
-	int m2l_engine = 0;               // 0: auto (tcgen05 on large FP32 levels), 1: per-pair rotations, 2: SIMT only
+	int m2l_engine = 0;               // 0: dense SIMT GEMMs, 1: per-pair rotations (plain path), 3: tcgen05 on large FP32 levels
 	unsigned* dev_flags = nullptr;      // device error flags
 	std::string last_error;
 	int verbose = 0;

@@ -89,9 +89,10 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 				convert_kernel<real><<<div_up(m, 256), 256, 0, s>>>(mL, cv_in, m);
 				if ((st = m2l_gemm<double>(ctx, plan, opd, cv_in, cv_out, N))) return st;
 				convert_back_kernel<real><<<div_up(m, 256), 256, 0, s>>>(cv_out, lL, m);
-			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 0 && m2l_tc_supported(N) &&
+			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N) &&
 			           t.lsize[L] >= 4096) {
-				// FP32 levels with enough tiles: tcgen05 TF32 hi/lo GEMM
+				// opt-in: tcgen05 TF32 hi/lo GEMM on the large FP32 levels (its TMEM
+				// accumulation keeps ~1e-5 relative accuracy, short of the SIMT GEMM's)
 				const uint4* tc = m2l_ops_tc(ctx, N);
 				if (!tc) return ERR_OOM;
 				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N)))

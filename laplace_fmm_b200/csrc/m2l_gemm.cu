@@ -5,6 +5,7 @@
 #include "fmm3d.cuh"
 #include "primitives.cuh"
 #include <mutex>
+#include <cstdlib>
 
 namespace lfmm {
 
@@ -317,11 +318,13 @@ constexpr uint32_t TC_IDESC = (1u << 4)        // D: FP32
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Round to TF32 (nearest, ties away); the low 13 bits of the cvt result are
+// not specified, so they are cleared to make the value exact as an FP32.
 __device__ __forceinline__ uint32_t tf32_rna(float x)
 {
 	uint32_t r;
 	asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-	return r;
+	return r & 0xffffe000u;
 }
 
 // K-major operand, 128-byte swizzle, 8-row groups 1024 bytes apart
@@ -363,7 +366,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const uint4* __re
 	constexpr int A_BYTES = 2 * MH * HALF;          // hi halves, then lo halves
 	constexpr int B_BYTES = 2 * TC_BN * 128;        // hi, then lo
 	constexpr int STAGE = A_BYTES + B_BYTES;
-	constexpr uint32_t TMEM_COLS = MH == 1 ? 128 : 256;
+	// two accumulators: main (hi x hi) and correction (hi x lo + lo x hi).  The
+	// tensor core aligns each product to the largest addend before adding, so
+	// the small corrections keep their bits only if summed on their own.
+	constexpr uint32_t TMEM_COLS = MH == 1 ? 256 : 512;
+	constexpr uint32_t CORR = MH * TC_BN;     // column offset of the correction accumulator
 	extern __shared__ uint8_t dsm[];
 	__shared__ uint64_t bars[2];
 	__shared__ uint32_t tmem_sh;
@@ -465,9 +472,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const uint4* __re
 						const uint64_t ah = umma_desc_sw128(sa + h * HALF + ks * 32);
 						const uint64_t al = umma_desc_sw128(sa + MH * HALF + h * HALF + ks * 32);
 						const uint32_t d = tmem + (uint32_t)(h * TC_BN);
-						mma_tf32(d, ah, bh, (it == 0 && ks == 0) ? 0u : 1u);
-						mma_tf32(d, ah, bl, 1u);
-						mma_tf32(d, al, bh, 1u);
+						const uint32_t first = (it == 0 && ks == 0) ? 0u : 1u;
+						mma_tf32(d, ah, bh, first);
+						mma_tf32(d + CORR, ah, bl, first);
+						mma_tf32(d + CORR, al, bh, 1u);
 					}
 				}
 				asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -488,7 +496,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const uint4* __re
 #pragma unroll
 		for (int h = 0; h < MH; ++h) {
 			for (int cc = 0; cc < TC_BN / 16; ++cc) {
-				uint32_t r[16];
+				uint32_t r[16], rc[16];
 				if (it > 0) {
 					const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * TC_BN + cc * 16);
 					asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -496,17 +504,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const uint4* __re
 					               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
 					               "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
 					             : "r"(ta));
+					asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+					             : "=r"(rc[0]), "=r"(rc[1]), "=r"(rc[2]), "=r"(rc[3]), "=r"(rc[4]), "=r"(rc[5]), "=r"(rc[6]),
+					               "=r"(rc[7]), "=r"(rc[8]), "=r"(rc[9]), "=r"(rc[10]), "=r"(rc[11]), "=r"(rc[12]),
+					               "=r"(rc[13]), "=r"(rc[14]), "=r"(rc[15])
+					             : "r"(ta + CORR));
 					asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 				} else {
 #pragma unroll
-					for (int j = 0; j < 16; ++j) r[j] = 0u;
+					for (int j = 0; j < 16; ++j) { r[j] = 0u; rc[j] = 0u; }
 				}
 				const int row = h * 128 + warp * 32 + lane;
 				if (row < R) {
 #pragma unroll
 					for (int j = 0; j < 16; ++j) {
 						const int tg = tgt[cc * 16 + j];
-						if (tg >= 0) loc[(size_t)tg * R + row] = __uint_as_float(r[j]);
+						if (tg >= 0) loc[(size_t)tg * R + row] = __uint_as_float(r[j]) + __uint_as_float(rc[j]);
 					}
 				}
 			}
