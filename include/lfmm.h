@@ -158,6 +158,30 @@ int lfmm_tree_list_sizes(lfmm_ctx* ctx, int level, long long* n_close, long long
 int lfmm_tree_lists(lfmm_ctx* ctx, int level, long long* close, long long* far);
 int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
 
+/* ---- learned order selection (no counterpart in the reference) -----------
+ * The reference picks one order from eps by a fixed formula
+ * (cpu/multipole3d.cpp:1328-1331).  Here a small MLP (16 per-leaf features ->
+ * 64 -> 64 -> 6, FP32, ReLU) predicts log10 of each leaf box's error at the
+ * orders p = 4, 6, ..., 14; a solve takes the lowest p whose predicted
+ * particle-weighted error meets the tolerance.  All pointers to MLP data are
+ * device pointers (FP32); parameters are W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[6][64] b3[6]. */
+#define LFMM_MLP_IN 16
+#define LFMM_MLP_HIDDEN 64
+#define LFMM_MLP_OUT 6
+#define LFMM_MLP_PARAMS (64 * 16 + 64 + 64 * 64 + 64 + 6 * 64 + 6)
+
+/* Y[n][6] = MLP(X[n][16]) */
+int lfmm_mlp_forward(lfmm_ctx* ctx, const float* params, int n, const float* X, float* Y);
+/* Masked mean-squared-error loss sum M (Y - T)^2 / sum M over T, M [n][6];
+ * grad[LFMM_MLP_PARAMS]; work >= n * (6 + 128) + 2 floats; *loss on the host.
+ * Synchronises. */
+int lfmm_mlp_grad(lfmm_ctx* ctx, const float* params, int n, const float* X, const float* T, const float* M,
+                  float* grad, float* work, float* loss);
+/* One Adam step (step >= 1) on params with moments m, v. */
+int lfmm_mlp_adam(lfmm_ctx* ctx, float* params, const float* grad, float* m, float* v, int step, float lr,
+                  float beta1, float beta2, float eps);
+
 /* ---- rotation tables (tests) --------------------------------------------
  * Wigner small-d matrix for table slot `slot` (layout n(n+1)(4n-1)/6 +
  * m(2n+1) + k + n, N = 18) and its canonical angle; returns the number of

@@ -24,6 +24,7 @@ EXPORTS = [
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
     "lfmm_wignerd_slot",
+    "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
 ]
 
 
@@ -90,6 +91,10 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_tree_lists.argtypes = [P, I, P, P]
         L.lfmm_tree_positions.argtypes = [P, P]
         L.lfmm_wignerd_slot.argtypes = [P, I, ctypes.POINTER(D), P]
+        L.lfmm_mlp_forward.argtypes = [P, P, I, P, P]
+        L.lfmm_mlp_grad.argtypes = [P, P, I, P, P, P, P, P, ctypes.POINTER(ctypes.c_float)]
+        F = ctypes.c_float
+        L.lfmm_mlp_adam.argtypes = [P, P, P, P, P, I, F, F, F, F]
         _lib = L
         return L
 

@@ -1,0 +1,133 @@
+"""Learned order selection: host side of the MLP kernels in ``csrc/mlp.cu``.
+
+The network maps 16 features of a leaf box to log10 of that box's relative
+error at the orders p = 4, 6, ..., 14 (``ORDERS``).  Training, inference and
+the optimiser all run in the library's CUDA kernels (``lfmm_mlp_forward``,
+``lfmm_mlp_grad``, ``lfmm_mlp_adam``); torch only holds the device buffers.
+The reference has no counterpart: it derives one order from eps by a fixed
+formula (cpu/multipole3d.cpp:1328-1331), which stays the fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from ._lib import Context, LfmmError, default_context
+
+N_IN, N_HIDDEN, N_OUT = 16, 64, 6
+N_PARAMS = N_HIDDEN * N_IN + N_HIDDEN + N_HIDDEN * N_HIDDEN + N_HIDDEN + N_OUT * N_HIDDEN + N_OUT
+ORDERS = tuple(range(4, 15, 2))          # expansion order p of each output (N = p + 1 degrees)
+WEIGHTS = Path(__file__).resolve().parent / "order_mlp.npz"
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise LfmmError("the order MLP runs on the GPU; no CUDA device is visible")
+    return torch
+
+
+def he_init(seed: int = 0) -> np.ndarray:
+    """He-uniform weights, zero biases, packed in the kernels' layout."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for rows, cols in ((N_HIDDEN, N_IN), (N_HIDDEN, N_HIDDEN), (N_OUT, N_HIDDEN)):
+        bound = np.sqrt(6.0 / cols)
+        parts += [rng.uniform(-bound, bound, size=rows * cols), np.zeros(rows)]
+    return np.concatenate(parts).astype(np.float32)
+
+
+class OrderMLP:
+    """Parameters on the device plus the Adam state; every op is a CUDA kernel."""
+
+    def __init__(self, params: np.ndarray | None = None, ctx: Context | None = None, seed: int = 0,
+                 x_mean: np.ndarray | None = None, x_std: np.ndarray | None = None):
+        torch = _torch()
+        self.ctx = ctx or default_context(0)
+        dev = torch.device("cuda", self.ctx.device)
+        p = he_init(seed) if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        if p.shape != (N_PARAMS,):
+            raise ValueError(f"expected {N_PARAMS} parameters, got {p.shape}")
+        self.params = torch.from_numpy(p.copy()).to(dev)
+        self.grad = torch.zeros(N_PARAMS, dtype=torch.float32, device=dev)
+        self.m = torch.zeros_like(self.grad)
+        self.v = torch.zeros_like(self.grad)
+        self.step_count = 0
+        self.x_mean = np.zeros(N_IN, np.float32) if x_mean is None else np.asarray(x_mean, np.float32)
+        self.x_std = np.ones(N_IN, np.float32) if x_std is None else np.asarray(x_std, np.float32)
+        self._dev = dev
+
+    # -- device helpers ----------------------------------------------------
+    def _to_dev(self, a: np.ndarray):
+        torch = _torch()
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(self._dev)
+
+    def _sync_lib(self):
+        """Wait for the library's stream (torch work is ordered before each
+        call by a device synchronise)."""
+        torch = _torch()
+        s = torch.cuda.ExternalStream(self.ctx.stream, device=self._dev)
+        s.synchronize()
+
+    def normalise(self, X: np.ndarray) -> np.ndarray:
+        return ((np.asarray(X, np.float32) - self.x_mean) / self.x_std).astype(np.float32)
+
+    # -- network ops -------------------------------------------------------
+    def forward(self, X: np.ndarray, normalised: bool = False) -> np.ndarray:
+        """log10 error predictions [n][6] for feature rows X [n][16]."""
+        torch = _torch()
+        Xn = np.asarray(X, np.float32) if normalised else self.normalise(X)
+        n = len(Xn)
+        if n == 0:
+            return np.zeros((0, N_OUT), np.float32)
+        dX = self._to_dev(Xn)
+        dY = torch.empty((n, N_OUT), dtype=torch.float32, device=self._dev)
+        torch.cuda.synchronize(self._dev)
+        self.ctx.check(self.ctx.lib.lfmm_mlp_forward(self.ctx.handle, self.params.data_ptr(), n, dX.data_ptr(),
+                                                     dY.data_ptr()), "lfmm_mlp_forward")
+        self._sync_lib()
+        return dY.cpu().numpy()
+
+    def loss_grad(self, X, T, M, normalised: bool = True):
+        """Masked MSE loss and its gradient (left in ``self.grad``)."""
+        torch = _torch()
+        Xn = np.asarray(X, np.float32) if normalised else self.normalise(X)
+        n = len(Xn)
+        dX, dT, dM = self._to_dev(Xn), self._to_dev(T), self._to_dev(M)
+        work = torch.empty(n * (N_OUT + 2 * N_HIDDEN) + 2, dtype=torch.float32, device=self._dev)
+        loss = ctypes.c_float()
+        torch.cuda.synchronize(self._dev)
+        self.ctx.check(self.ctx.lib.lfmm_mlp_grad(self.ctx.handle, self.params.data_ptr(), n, dX.data_ptr(),
+                                                  dT.data_ptr(), dM.data_ptr(), self.grad.data_ptr(),
+                                                  work.data_ptr(), ctypes.byref(loss)), "lfmm_mlp_grad")
+        self._sync_lib()
+        return float(loss.value)
+
+    def adam_step(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8):
+        self.step_count += 1
+        torch = _torch()
+        torch.cuda.synchronize(self._dev)
+        self.ctx.check(self.ctx.lib.lfmm_mlp_adam(self.ctx.handle, self.params.data_ptr(), self.grad.data_ptr(),
+                                                  self.m.data_ptr(), self.v.data_ptr(), self.step_count, lr, beta1,
+                                                  beta2, eps), "lfmm_mlp_adam")
+        self._sync_lib()
+
+    def train_step(self, X, T, M, lr: float = 1e-3) -> float:
+        loss = self.loss_grad(X, T, M)
+        self.adam_step(lr)
+        return loss
+
+    def params_host(self) -> np.ndarray:
+        return self.params.cpu().numpy()
+
+    # -- persistence ---------------------------------------------------------
+    def save(self, path: Path | str = WEIGHTS, **meta):
+        np.savez(path, params=self.params_host(), x_mean=self.x_mean, x_std=self.x_std,
+                 **{k: np.asarray(v) for k, v in meta.items()})
+
+    @classmethod
+    def load(cls, path: Path | str = WEIGHTS, ctx: Context | None = None) -> "OrderMLP":
+        z = np.load(path)
+        return cls(z["params"], ctx=ctx, x_mean=z["x_mean"], x_std=z["x_std"])
