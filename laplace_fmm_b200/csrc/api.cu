@@ -268,6 +268,7 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 		return LFMM_ERR_CUDA;
 	}
 	for (auto& e : c.ev) cudaEventCreate(&e);
+	cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
 	if (tables_build(c) != OK) {
 		lfmm_destroy(ctx);
 		return LFMM_ERR_CUDA;
@@ -371,7 +372,10 @@ int lfmm3d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const doub
 {
 	if (!ctx) return LFMM_ERR_ARG;
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
-	return direct_device(ctx->c, 3, ns, src, q, nt, tgt, pot, field);
+	ctx->c.arena.reset();
+	int st = direct_device(ctx->c, 3, ns, src, q, nt, tgt, pot, field);
+	ctx->c.arena.settle();
+	return st;
 }
 
 int lfmm2d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
@@ -379,7 +383,10 @@ int lfmm2d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const doub
 {
 	if (!ctx) return LFMM_ERR_ARG;
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
-	return direct_device(ctx->c, 2, ns, src, q, nt, tgt, pot, field);
+	ctx->c.arena.reset();
+	int st = direct_device(ctx->c, 2, ns, src, q, nt, tgt, pot, field);
+	ctx->c.arena.settle();
+	return st;
 }
 
 // ---- tree inspection -------------------------------------------------------

@@ -70,6 +70,7 @@ struct OpCacheEntry {
 
 struct Context {
 	int device = 0;
+	int num_sms = 148;
 	cudaStream_t stream = nullptr;
 	Arena arena;
 	Tables tables;

@@ -2,6 +2,12 @@
 // the reference's clamp of r at 1e-4 and its self term (reference
 // common/simple_math.h:130-216 pair kernels, simple_math.cu:9-23 the GPU
 // ComputeExact).  Thread per target, sources staged through shared memory.
+//
+// With few targets (the sampled accuracy check: thousands of targets against
+// millions of sources) one block per 128 targets would leave most SMs idle, so
+// the sources are split into S chunks: block (tile, chunk) writes its partial
+// sums to scratch [S][nt][4] and a second kernel adds the S partials of each
+// target in chunk order (deterministic).
 #include "direct.cuh"
 
 namespace lfmm {
@@ -10,79 +16,134 @@ namespace {
 
 constexpr int DT = 128;
 
-__global__ void __launch_bounds__(DT) direct3d_kernel(size_t ns, const double* __restrict__ src,
-                                                      const double* __restrict__ q, size_t nt,
-                                                      const double* __restrict__ tgt, double* __restrict__ pot,
-                                                      double* __restrict__ fld)
+// Sums of target i over sources [s_lo, s_hi): out[0] = potential, out[1..dim] = field.
+template <int DIM>
+__device__ __forceinline__ void direct_range(size_t s_lo, size_t s_hi, const double* __restrict__ src,
+                                             const double* __restrict__ q, double xi, double yi, double zi,
+                                             double out[4])
 {
 	__shared__ double sx[DT], sy[DT], sz[DT], sq[DT];
-	size_t i = (size_t)blockIdx.x * DT + threadIdx.x;
-	const bool valid = i < nt;
-	double xi = 0, yi = 0, zi = 0;
-	if (valid) { xi = tgt[3 * i]; yi = tgt[3 * i + 1]; zi = tgt[3 * i + 2]; }
 	double p = 0, fx = 0, fy = 0, fz = 0;
-	for (size_t s0 = 0; s0 < ns; s0 += DT) {
-		int cnt = (int)min((size_t)DT, ns - s0);
+	for (size_t s0 = s_lo; s0 < s_hi; s0 += DT) {
+		int cnt = (int)min((size_t)DT, s_hi - s0);
 		__syncthreads();
 		if (threadIdx.x < cnt) {
 			size_t j = s0 + threadIdx.x;
-			sx[threadIdx.x] = src[3 * j]; sy[threadIdx.x] = src[3 * j + 1]; sz[threadIdx.x] = src[3 * j + 2];
+			sx[threadIdx.x] = src[DIM * j]; sy[threadIdx.x] = src[DIM * j + 1];
+			if (DIM == 3) sz[threadIdx.x] = src[DIM * j + 2];
 			sq[threadIdx.x] = q[j];
 		}
 		__syncthreads();
-		for (int j = 0; j < cnt; ++j) {
-			double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
-			double r = fmax(sqrt(dx * dx + dy * dy + dz * dz), FORCE_EPS);
-			double qr = sq[j] / r;
-			double qr3 = qr / (r * r);
-			p += qr;
-			fx = fma(dx, qr3, fx); fy = fma(dy, qr3, fy); fz = fma(dz, qr3, fz);
+		if (DIM == 3) {
+			for (int j = 0; j < cnt; ++j) {
+				double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
+				double r = fmax(sqrt(dx * dx + dy * dy + dz * dz), FORCE_EPS);
+				double qr = sq[j] / r;
+				double qr3 = qr / (r * r);
+				p += qr;
+				fx = fma(dx, qr3, fx); fy = fma(dy, qr3, fy); fz = fma(dz, qr3, fz);
+			}
+		} else {
+			for (int j = 0; j < cnt; ++j) {
+				double dx = xi - sx[j], dy = yi - sy[j];
+				double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
+				p += sq[j] * 0.5 * log(r2);
+				double qr = sq[j] / r2;
+				fx = fma(dx, qr, fx); fy = fma(-dy, qr, fy);
+			}
 		}
 	}
-	if (valid) { pot[i] = p; fld[3 * i] = fx; fld[3 * i + 1] = fy; fld[3 * i + 2] = fz; }
+	out[0] = p; out[1] = fx; out[2] = fy; out[3] = fz;
 }
 
-__global__ void __launch_bounds__(DT) direct2d_kernel(size_t ns, const double* __restrict__ src,
-                                                      const double* __restrict__ q, size_t nt,
-                                                      const double* __restrict__ tgt, double* __restrict__ pot,
-                                                      double* __restrict__ fld)
+// grid (target tiles, source chunks).  part == nullptr: one chunk, results
+// straight to pot/fld; else partials to part[(chunk * nt + i) * 4 + k].
+template <int DIM>
+__global__ void __launch_bounds__(DT) direct_kernel(size_t ns, size_t chunk, const double* __restrict__ src,
+                                                    const double* __restrict__ q, size_t nt,
+                                                    const double* __restrict__ tgt, double* __restrict__ pot,
+                                                    double* __restrict__ fld, double* __restrict__ part)
 {
-	__shared__ double sx[DT], sy[DT], sq[DT];
-	size_t i = (size_t)blockIdx.x * DT + threadIdx.x;
+	const size_t i = (size_t)blockIdx.x * DT + threadIdx.x;
 	const bool valid = i < nt;
-	double xi = 0, yi = 0;
-	if (valid) { xi = tgt[2 * i]; yi = tgt[2 * i + 1]; }
-	double p = 0, fr = 0, fi = 0;
-	for (size_t s0 = 0; s0 < ns; s0 += DT) {
-		int cnt = (int)min((size_t)DT, ns - s0);
-		__syncthreads();
-		if (threadIdx.x < cnt) {
-			size_t j = s0 + threadIdx.x;
-			sx[threadIdx.x] = src[2 * j]; sy[threadIdx.x] = src[2 * j + 1]; sq[threadIdx.x] = q[j];
-		}
-		__syncthreads();
-		for (int j = 0; j < cnt; ++j) {
-			double dx = xi - sx[j], dy = yi - sy[j];
-			double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
-			p += sq[j] * 0.5 * log(r2);
-			double qr = sq[j] / r2;
-			fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
-		}
+	double xi = 0, yi = 0, zi = 0;
+	if (valid) {
+		xi = tgt[DIM * i]; yi = tgt[DIM * i + 1];
+		if (DIM == 3) zi = tgt[DIM * i + 2];
 	}
-	if (valid) { pot[i] = p; fld[2 * i] = fr; fld[2 * i + 1] = fi; }
+	const size_t lo = (size_t)blockIdx.y * chunk, hi = min(ns, lo + chunk);
+	double r[4];
+	direct_range<DIM>(lo, hi, src, q, xi, yi, zi, r);
+	if (!valid) return;
+	if (part) {
+		double2* o = reinterpret_cast<double2*>(part + ((size_t)blockIdx.y * nt + i) * 4);
+		o[0] = make_double2(r[0], r[1]);
+		o[1] = make_double2(r[2], r[3]);
+	} else {
+		pot[i] = r[0];
+		for (int k = 0; k < DIM; ++k) fld[DIM * i + k] = r[1 + k];
+	}
+}
+
+template <int DIM>
+__global__ void direct_reduce_kernel(size_t nt, int S, const double* __restrict__ part, double* __restrict__ pot,
+                                     double* __restrict__ fld)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nt) return;
+	double a[4] = {0, 0, 0, 0};
+	for (int s = 0; s < S; ++s) {
+		const double2* o = reinterpret_cast<const double2*>(part + ((size_t)s * nt + i) * 4);
+		double2 u = o[0], v = o[1];
+		a[0] += u.x; a[1] += u.y; a[2] += v.x; a[3] += v.y;
+	}
+	pot[i] = a[0];
+	for (int k = 0; k < DIM; ++k) fld[DIM * i + k] = a[1 + k];
 }
 
 } // namespace
+
+int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks)
+{
+	const size_t tiles = (nt + DT - 1) / DT;
+	const size_t want = (size_t)num_sms * 8;           // blocks for a full GPU (several per SM)
+	if (tiles >= want || ns < 4 * (size_t)DT) return 1;
+	size_t s = (want + tiles - 1) / tiles;
+	s = std::min(s, (ns + 4 * DT - 1) / (4 * DT));     // at least 4 source tiles per chunk
+	s = std::min(s, max_chunks);
+	return (int)std::max<size_t>(s, 1);
+}
+
+int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
+                  const double* tgt, double* pot, double* fld, double* part, int S)
+{
+	if (nt == 0) return OK;
+	if (S <= 1 || !part) S = 1, part = nullptr;
+	const size_t chunk = S > 1 ? ((ns + S - 1) / S + DT - 1) / DT * DT : std::max<size_t>(ns, 1);
+	S = S > 1 ? (int)((ns + chunk - 1) / chunk) : 1;
+	if (S <= 1) part = nullptr;
+	dim3 grid(div_up(nt, DT), S);
+	if (dim == 3) direct_kernel<3><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
+	else direct_kernel<2><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
+	if (part) {
+		if (dim == 3) direct_reduce_kernel<3><<<div_up(nt, 256), 256, 0, ctx.stream>>>(nt, S, part, pot, fld);
+		else direct_reduce_kernel<2><<<div_up(nt, 256), 256, 0, ctx.stream>>>(nt, S, part, pot, fld);
+	}
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
 
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                   double* pot, double* fld)
 {
 	if (nt == 0) return OK;
-	unsigned grid = div_up(nt, DT);
-	if (dim == 3) direct3d_kernel<<<grid, DT, 0, ctx.stream>>>(ns, src, q, nt, tgt, pot, fld);
-	else direct2d_kernel<<<grid, DT, 0, ctx.stream>>>(ns, src, q, nt, tgt, pot, fld);
-	LFMM_CUDA(ctx, cudaGetLastError());
-	return OK;
+	int S = direct_chunks(ns, nt, ctx.num_sms, 1024);
+	double* part = nullptr;
+	if (S > 1) {
+		part = static_cast<double*>(ctx.arena.take(sizeof(double) * 4 * nt * (size_t)S));
+		if (!part) S = 1;       // fall back to one chunk (no scratch)
+	}
+	return direct_launch(ctx, dim, ns, src, q, nt, tgt, pot, fld, part, S);
 }
 
 } // namespace lfmm

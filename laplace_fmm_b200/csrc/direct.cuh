@@ -4,7 +4,13 @@
 
 namespace lfmm {
 
-// Enqueue on ctx.stream; all pointers are device pointers.
+// Source chunks for nt targets (1: no split), at most max_chunks.
+int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks);
+// Enqueue with S source chunks; part: scratch of 4 * nt * S doubles (written
+// before it is read; nothing needs to start at zero), unused when S == 1.
+int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
+                  const double* tgt, double* pot, double* fld, double* part, int S);
+// Enqueue on ctx.stream, scratch from the arena; all pointers are device pointers.
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                   double* pot, double* fld);
 

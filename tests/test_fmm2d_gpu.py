@@ -67,3 +67,16 @@ def test_accuracy_vs_direct(ctx):
     fe = compute_exact(InteractionType.Force2d, (src, q), src[idx])
     assert rel_l2(f.potentials[idx], pe) < 1e-9
     assert rel_l2(f.forces[idx], fe) < 1e-8
+
+
+@pytest.mark.parametrize("ns,nt", [(4000, 500), (100000, 37), (3, 2000)])
+def test_direct_matches_oracle(ctx, oracle, ns, nt):
+    """Few targets against many sources take the source-split direct sum."""
+    g = rng(ns + nt)
+    src = g.random((ns, 2)); q = g.uniform(-1, 1, ns)
+    tgt = g.random((nt, 2))
+    pe = compute_exact(InteractionType.Potential2d, (src, q), tgt)
+    fe = compute_exact(InteractionType.Force2d, (src, q), tgt)
+    po, fo = oracle.direct2d(src, q, tgt)
+    assert rel_l2(pe, po) < 1e-13
+    assert rel_l2(np.stack([fe.real, fe.imag], 1), fo) < 1e-13
