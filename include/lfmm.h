@@ -158,6 +158,23 @@ int lfmm_tree_list_sizes(lfmm_ctx* ctx, int level, long long* n_close, long long
 int lfmm_tree_lists(lfmm_ctx* ctx, int level, long long* close, long long* far);
 int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
 
+/* ---- direct sum without allocation (no counterpart in the reference) -----
+ * Same result as lfmm3d_direct_device, but the call allocates no device
+ * memory: its source-chunk scratch is a static device array of
+ * LFMM_DIRECT_NOALLOC_SCRATCH_BYTES per device, so calls with more than
+ * LFMM_DIRECT_NOALLOC_MAX_TARGETS targets are rejected (LFMM_ERR_ARG).  For
+ * callers that must not allocate inside their step (an allocator that has
+ * reserved the device's memory, or a loop where cudaMalloc / cudaFree would
+ * synchronise the device).  The first call on each device looks up the
+ * array's address (and may load the module): make it before any stream
+ * capture.  The array is shared by every context on the device, so calls
+ * that overlap in time on one device race; serialise them.  Nothing in the
+ * scratch needs to start at zero.  All pointers are device pointers. */
+#define LFMM_DIRECT_NOALLOC_MAX_TARGETS 65536
+#define LFMM_DIRECT_NOALLOC_SCRATCH_BYTES (8u << 20)
+int lfmm3d_direct_device_noalloc(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q,
+                                 size_t n_tgt, const double* tgt_xyz, double* pot, double* field);
+
 /* ---- learned order selection (no counterpart in the reference) -----------
  * The reference picks one order from eps by a fixed formula
  * (cpu/multipole3d.cpp:1328-1331).  Here a small MLP (16 per-leaf features ->

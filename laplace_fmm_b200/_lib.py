@@ -22,6 +22,7 @@ EXPORTS = [
     "lfmm3d_solve", "lfmm3d_solve_device", "lfmm3d_solve_ex", "lfmm3d_solve_ex_device",
     "lfmm2d_solve", "lfmm2d_solve_device",
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
+    "lfmm3d_direct_device_noalloc",
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
@@ -83,7 +84,8 @@ def load(path: Path | str = LIB_PATH):
         for f in ("lfmm3d_solve_ex", "lfmm3d_solve_ex_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, P,
                                       ctypes.POINTER(LfmmStats)]
-        for f in ("lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device"):
+        for f in ("lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
+                  "lfmm3d_direct_device_noalloc"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, P, P]
         L.lfmm_tree_build.argtypes = [P, I, SZ, P, P, SZ, P, I, P, P]
         L.lfmm_tree_level.argtypes = [P, I, P, P, P, P, P, P, P]
