@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None, help="override the configuration's")
     ap.add_argument("--order", type=int, default=None, help="override N (degrees)")
     ap.add_argument("--depth", type=int, default=None, help="override the tree depth")
+    ap.add_argument("--particles", type=int, default=None,
+                    help="override the particle count (small cases for profiling; not a bench line)")
     a = ap.parse_args()
     cfg = dict(CONFIGS[a.config])
     if a.precision:
@@ -76,6 +78,9 @@ def parse():
         cfg["N"] = a.order
     if a.depth:
         cfg["depth"] = a.depth
+    if a.particles:
+        cfg["n"] = a.particles
+        cfg["workload"] += f" [particle count overridden: {a.particles:,}]"
     if a.max_leaf is not None:
         cfg["max_leaf"] = a.max_leaf
     a.cfg = cfg

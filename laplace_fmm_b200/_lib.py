@@ -42,6 +42,7 @@ class LfmmStats(ctypes.Structure):
         ("n_x", ctypes.c_size_t),
         ("ms_tree", ctypes.c_float), ("ms_upward", ctypes.c_float), ("ms_m2l", ctypes.c_float),
         ("ms_l2l", ctypes.c_float), ("ms_leaves", ctypes.c_float), ("ms_total", ctypes.c_float),
+        ("ms_m2l_kernel", ctypes.c_float), ("n_m2l_kernel", ctypes.c_int),
     ]
 
     def as_dict(self):

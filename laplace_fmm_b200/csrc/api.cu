@@ -116,6 +116,7 @@ void fill_stats(lfmm_stats* out, const SolveStats& s)
 	out->n_m2p = s.n_m2p; out->n_w = s.n_w; out->n_x = s.n_x;
 	out->ms_tree = s.ms_tree; out->ms_upward = s.ms_upward; out->ms_m2l = s.ms_m2l; out->ms_l2l = s.ms_l2l;
 	out->ms_leaves = s.ms_leaves; out->ms_total = s.ms_total;
+	out->ms_m2l_kernel = s.ms_m2l_kernel; out->n_m2l_kernel = s.n_m2l_kernel;
 }
 
 int select_device(lfmm_ctx* ctx)
@@ -249,11 +250,12 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	if (!ctx) return LFMM_ERR_OOM;
 	Context& c = ctx->c;
 	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
-	// M2L engine: dense direction GEMMs (default) or per-pair rotations
-	// rotation: per-pair rotations on the plain path; simt: SIMT GEMMs only (the
-	// default); tc: tcgen05 TF32 hi/lo GEMMs on large FP32 levels
+	// M2L engine (LFMM_M2L): tc (default) = tcgen05 TF32 hi/lo GEMMs on the FP32
+	// levels and SIMT GEMMs elsewhere; simt = SIMT GEMMs only; rotation =
+	// per-pair rotations on the plain path
+	c.m2l_engine = 3;
 	if (const char* e = std::getenv("LFMM_M2L"))
-		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "tc") == 0 ? 3 : 0);
+		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 0 : 3);
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
 		cudaGetLastError();
@@ -268,6 +270,7 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 		return LFMM_ERR_CUDA;
 	}
 	for (auto& e : c.ev) cudaEventCreate(&e);
+	for (auto& e : c.kev) cudaEventCreate(&e);
 	cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
 	if (tables_build(c) != OK) {
 		lfmm_destroy(ctx);
@@ -288,6 +291,7 @@ void lfmm_destroy(lfmm_ctx* ctx)
 	c.opcache.clear();
 	tables_free(c.tables);
 	for (auto& e : c.ev) if (e) cudaEventDestroy(e);
+	for (auto& e : c.kev) if (e) cudaEventDestroy(e);
 	if (c.dev_flags) cudaFree(c.dev_flags);
 	if (c.stream) cudaStreamDestroy(c.stream);
 	delete ctx;

@@ -76,11 +76,13 @@ struct Context {
 	Tables tables;
 	std::vector<OpCacheEntry> opcache;
 	unsigned long long opcache_clock = 0;
-	int m2l_engine = 0;               // 0: dense SIMT GEMMs, 1: per-pair rotations (plain path), 3: tcgen05 on large FP32 levels
+	int m2l_engine = 3;               // 0: dense SIMT GEMMs, 1: per-pair rotations (plain path), 3: tcgen05 on FP32 levels
 	unsigned* dev_flags = nullptr;      // device error flags
 	std::string last_error;
 	int verbose = 0;
 	cudaEvent_t ev[16] = {};
+	cudaEvent_t kev[32] = {};          // pairs around the tensor-core M2L launches (timing)
+	int kev_used = 0;
 	int timing = 0;
 };
 

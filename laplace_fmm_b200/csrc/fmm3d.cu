@@ -517,7 +517,7 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 		m2m_kernel<<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, E, L, ctx.tables.d, ctx.dev_flags);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
 	// downward
-	const bool gemm = ctx.m2l_engine == 0 && m2l_gemm_supported(N);
+	const bool gemm = ctx.m2l_engine != 1 && m2l_gemm_supported(N);     // FP64: SIMT GEMMs unless rotations asked
 	for (int L = 2; L < depth; ++L) {
 		if (gemm) {
 			double h = t.geo_host[3] / (double)(1ull << L);

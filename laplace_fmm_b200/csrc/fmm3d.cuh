@@ -10,6 +10,8 @@ struct SolveStats {
 	size_t n_far_pairs = 0, n_close_pairs = 0, n_p2p_pairs = 0;
 	size_t n_m2p = 0, n_w = 0, n_x = 0;
 	float ms_tree = 0, ms_upward = 0, ms_m2l = 0, ms_l2l = 0, ms_leaves = 0, ms_total = 0;
+	float ms_m2l_kernel = 0;     // inside the tensor-core M2L kernel launches
+	int n_m2l_kernel = 0;        // those launches
 };
 
 // Solve on device-resident inputs; pot (n_out) and field (n_out x 3) are

@@ -89,10 +89,8 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 				convert_kernel<real><<<div_up(m, 256), 256, 0, s>>>(mL, cv_in, m);
 				if ((st = m2l_gemm<double>(ctx, plan, opd, cv_in, cv_out, N))) return st;
 				convert_back_kernel<real><<<div_up(m, 256), 256, 0, s>>>(cv_out, lL, m);
-			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N) &&
-			           t.lsize[L] >= 4096) {
-				// opt-in: tcgen05 TF32 hi/lo GEMM on the large FP32 levels (its TMEM
-				// accumulation keeps ~1e-5 relative accuracy, short of the SIMT GEMM's)
+			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N)) {
+				// tcgen05 TF32 hi/lo GEMM on the FP32 levels
 				const uint4* tc = m2l_ops_tc(ctx, N);
 				if (!tc) return ERR_OOM;
 				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N)))
@@ -161,12 +159,13 @@ int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, 
                        double* pot, double* field, SolveStats* stats, DevTree* tree_out)
 {
 	if (N < 1 || N > MAXN3) { ctx.last_error = "order out of range (1 <= N <= 18)"; return ERR_ARG; }
-	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 13"; return ERR_UNSUPPORTED; }
+	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 15"; return ERR_UNSUPPORTED; }
 	if (max_leaf < 0) { ctx.last_error = "max_leaf must be >= 0"; return ERR_ARG; }
 	int st = upload_scaled_constants(ctx);
 	if (st) return st;
 	cudaStream_t s = ctx.stream;
 	const bool timing = ctx.timing != 0;
+	ctx.kev_used = 0;
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
 	DevTree t;
 	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t))) return st;
@@ -194,6 +193,12 @@ int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, 
 			cudaEventElapsedTime(&stats->ms_l2l, ctx.ev[3], ctx.ev[4]);
 			cudaEventElapsedTime(&stats->ms_leaves, ctx.ev[4], ctx.ev[5]);
 			cudaEventElapsedTime(&stats->ms_total, ctx.ev[0], ctx.ev[5]);
+			for (int k = 0; k + 1 < ctx.kev_used; k += 2) {
+				float ms = 0.f;
+				cudaEventElapsedTime(&ms, ctx.kev[k], ctx.kev[k + 1]);
+				stats->ms_m2l_kernel += ms;
+				++stats->n_m2l_kernel;
+			}
 		}
 	}
 	return OK;

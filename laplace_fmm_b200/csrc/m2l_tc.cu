@@ -1,0 +1,505 @@
+// tcgen05 M2L engine (m2l_tc.cuh).  One CTA per tile of 128 targets of one
+// octant class; D[128 targets][NC coefficients] in TMEM.  Warp roles:
+//   warps 0-3  producers: thread t gathers target t's source multipole for
+//              the K block, splits it into TF32 hi / lo and writes both rows
+//              128-byte swizzled; thread 0 also starts the bulk copy of the
+//              operator block (hi and lo, stored pre-swizzled) into the stage.
+//   warp 4     TMEM owner; lane 0 issues the MMAs (M=128, N=NC, K=8):
+//              main = B_hi T_hi (fresh per slot), corr += B_hi T_lo + B_lo T_hi.
+//   warps 5-12 epilogue: after each slot, add main to FP32 registers (warp w
+//              reads TMEM lanes 32 (w % 4) .. +31, half of the columns each).
+// Two smem stages (full: 128 arrivals + operator bytes; empty: MMA commit),
+// one main accumulator (full: MMA commit after the slot; empty: 256 epilogue
+// arrivals).  Every wait is bounded; on expiry the kernel sets
+// DEV_ERR_TIMEOUT, waits (bounded) for its copies and MMAs in flight, frees
+// TMEM and returns.
+#include "m2l_tc.cuh"
+#include "fmm3d.cuh"
+#include <mutex>
+
+namespace lfmm {
+
+namespace {
+
+__constant__ int16_t c_tc_slot_dir[8][M2L_SLOTS];
+
+constexpr int TC_M = 128;                 // targets per tile
+constexpr int NSTAGE = 2;
+constexpr int EPI_WARP0 = 5, EPI_WARPS = 8;
+constexpr int TC_THREADS = (EPI_WARP0 + EPI_WARPS) * 32;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t CORR_COL = 256;
+constexpr int WAIT_LIMIT = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Round to TF32 (nearest, ties away); the low 13 bits of the cvt result are
+// not specified, so they are cleared to make the value exact as an FP32.
+__device__ __forceinline__ uint32_t tf32_rna(float x)
+{
+	uint32_t r;
+	asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+	return r & 0xffffe000u;
+}
+
+// K-major operand, 128-byte swizzle, 8-row groups 1024 bytes apart
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
+{
+	uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+	d |= (uint64_t)1u << 16;
+	d |= (uint64_t)(1024u >> 4) << 32;
+	d |= (uint64_t)1u << 46;
+	d |= (uint64_t)2u << 61;
+	return d;
+}
+
+template <int NC>
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+	constexpr uint32_t IDESC = (1u << 4)                     // D: FP32
+	                         | (2u << 7)                     // A: TF32
+	                         | (2u << 10)                    // B: TF32
+	                         | ((uint32_t)(NC >> 3) << 17)   // N
+	                         | ((uint32_t)(TC_M >> 4) << 24); // M
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+
+// Wait for the phase of the given parity; gives up after WAIT_LIMIT polls, or
+// at once when *abort is set (abort == nullptr: a draining wait).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort)
+{
+	for (int it = 0; it < WAIT_LIMIT; ++it) {
+		uint32_t ok;
+		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+		if (ok) return true;
+		if (abort && *abort) return false;
+	}
+	return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+	             :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+
+// TMEM -> registers, 32 lanes x 16 (or 8) consecutive columns, the wait inside
+// the same asm so the values are complete when it returns.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+	uint32_t r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+	             "tcgen05.wait::ld.sync.aligned;"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	               "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+	               "=r"(r[15])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
+{
+	uint32_t r[8];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+	             "tcgen05.wait::ld.sync.aligned;"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// acc[0 .. W) += TMEM columns [col, col + W) of this warp's 32 lanes
+template <int W>
+__device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
+{
+#pragma unroll
+	for (int c = 0; c + 16 <= W; c += 16) {
+		float v[16];
+		tmem_ld16(taddr + c, v);
+#pragma unroll
+		for (int j = 0; j < 16; ++j) acc[c + j] += v[j];
+	}
+#pragma unroll
+	for (int c = W / 16 * 16; c < W; c += 8) {
+		float v[8];
+		tmem_ld8(taddr + c, v);
+#pragma unroll
+		for (int j = 0; j < 8; ++j) acc[c + j] += v[j];
+	}
+}
+
+template <int NC>
+struct TcCfg {
+	static constexpr int KB = (NC + 31) / 32;           // K blocks of 32 inputs
+	static constexpr int OP_BYTES = 2 * NC * 128;       // operator block: hi rows, then lo rows
+	static constexpr int A_BYTES = TC_M * 128;          // multipole block, one of hi / lo
+	static constexpr int STAGE = OP_BYTES + 2 * A_BYTES;
+	static constexpr int HALF = NC / 2;                 // columns per epilogue warp
+	static constexpr int SMEM = NSTAGE * STAGE + 1024;
+	static_assert(NC % 16 == 0 && NC >= 16 && NC <= 256, "MMA N");
+	static_assert(HALF % 8 == 0, "epilogue column split");
+};
+
+// grid (tiles, slot splits).  With S = gridDim.y > 1 split s handles slots
+// [s*189/S, (s+1)*189/S) and writes part[s][cell][R]; else loc[cell][R].
+template <int NC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
+              const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
+              const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
+              unsigned* flags)
+{
+	using C = TcCfg<NC>;
+	extern __shared__ uint8_t dsm[];
+	__shared__ uint64_t full_bar[NSTAGE], empty_bar[NSTAGE];
+	__shared__ uint64_t tfull_bar, tempty_bar, drain_bar;
+	__shared__ uint32_t tmem_sh;
+	__shared__ int32_t tgt[TC_M];
+	__shared__ uint32_t active_mask[(M2L_SLOTS + 31) / 32];
+	__shared__ int16_t active[M2L_SLOTS];
+	__shared__ int s_nactive, s_oct, s_n, s_abort;
+	__shared__ uint32_t s_start;
+
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int S = gridDim.y, sidx = blockIdx.y;
+	const int slot0 = sidx * M2L_SLOTS / S, slot1 = (sidx + 1) * M2L_SLOTS / S;
+	float* out = S > 1 ? part + (size_t)sidx * cells * R : loc;
+	uint8_t* base = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
+	volatile int* abort = &s_abort;
+
+	if (tid == 0) {
+		// this block's (octant, tile): tiles of each octant class in turn
+		uint32_t b = blockIdx.x, start = 0;
+		int oct = -1, nn = 0;
+		for (int o = 0; o < 8; ++o) {
+			const uint32_t cnt = oct_count[o];
+			const uint32_t tiles = (cnt + TC_M - 1) / TC_M;
+			if (b < tiles) { oct = o; start += b * TC_M; nn = (int)min((uint32_t)TC_M, cnt - b * TC_M); break; }
+			b -= tiles; start += cnt;
+		}
+		s_oct = oct; s_n = nn; s_start = start; s_abort = 0; s_nactive = 0;
+	}
+	if (tid < (M2L_SLOTS + 31) / 32) active_mask[tid] = 0u;
+	__syncthreads();
+	if (s_oct < 0) return;
+	const int oct = s_oct;
+	if (tid < TC_M) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
+	if (warp == 4) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		             :: "r"(smem_u32(&tmem_sh)), "r"(TMEM_COLS));
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	if (tid == 0) {
+		for (int s = 0; s < NSTAGE; ++s) {
+			mbar_init(smem_u32(&full_bar[s]), TC_M);
+			mbar_init(smem_u32(&empty_bar[s]), 1);
+		}
+		mbar_init(smem_u32(&tfull_bar), 1);
+		mbar_init(smem_u32(&tempty_bar), EPI_WARPS * 32);
+		mbar_init(smem_u32(&drain_bar), 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+	// slots in which at least one target of the tile has a source
+	if (warp < 4) {
+		const int myt = tgt[tid];
+		const int32_t* row = vtab + (size_t)(myt >= 0 ? myt : 0) * M2L_SLOTS;
+		for (int s = slot0; s < slot1; ++s) {
+			const unsigned any = __ballot_sync(0xffffffffu, myt >= 0 && row[s] >= 0);
+			if (lane == 0 && any) atomicOr(&active_mask[s >> 5], 1u << (s & 31));
+		}
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	if (tid == 0) {
+		int n = 0;
+		for (int s = slot0; s < slot1; ++s)
+			if (active_mask[s >> 5] & (1u << (s & 31))) active[n++] = (int16_t)s;
+		s_nactive = n;
+	}
+	__syncthreads();
+	const int nact = s_nactive;
+	const uint32_t tmem = tmem_sh;
+
+	if (warp < 4) {
+		// ---- producers: one target row each; thread 0 also copies the operator
+		const int myt = tgt[tid];
+		uint32_t it = 0;
+		for (int j = 0; j < nact; ++j) {
+			const int slot = active[j];
+			const int dir = c_tc_slot_dir[oct][slot];
+			const int src = myt >= 0 ? vtab[(size_t)myt * M2L_SLOTS + slot] : -1;
+			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
+			bool ok = true;
+			for (int kb = 0; kb < C::KB; ++kb, ++it) {
+				const uint32_t st = it % NSTAGE;
+				float v[32];
+#pragma unroll
+				for (int q = 0; q < 16; ++q) {
+					const int k = kb * 32 + 2 * q;           // R is even: a pair is in or out
+					const float2 w = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
+					v[2 * q] = w.x; v[2 * q + 1] = w.y;
+				}
+				if (it >= NSTAGE && !mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort)) {
+					ok = false;
+					break;
+				}
+				uint8_t* stage = base + st * C::STAGE;
+				if (tid == 0) {
+					mbar_expect_tx(smem_u32(&full_bar[st]), C::OP_BYTES);
+					bulk_g2s(smem_u32(stage), ops + ((size_t)dir * C::KB + kb) * C::OP_BYTES, C::OP_BYTES,
+					         smem_u32(&full_bar[st]));
+				}
+				uint8_t* rh = stage + C::OP_BYTES + tid * 128;
+				uint8_t* rl = rh + C::A_BYTES;
+#pragma unroll
+				for (int c = 0; c < 8; ++c) {
+					uint32_t h[4], l[4];
+#pragma unroll
+					for (int e = 0; e < 4; ++e) {
+						const float x = v[4 * c + e];
+						h[e] = tf32_rna(x);
+						l[e] = tf32_rna(x - __uint_as_float(h[e]));
+					}
+					const int pc = c ^ (tid & 7);
+					*reinterpret_cast<uint4*>(rh + pc * 16) = make_uint4(h[0], h[1], h[2], h[3]);
+					*reinterpret_cast<uint4*>(rl + pc * 16) = make_uint4(l[0], l[1], l[2], l[3]);
+				}
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				mbar_arrive(smem_u32(&full_bar[st]));
+			}
+			if (!ok) {
+				*abort = 1;
+				atomicOr(flags, DEV_ERR_TIMEOUT);
+				break;
+			}
+		}
+		// the operator copies still in flight land before the block exits
+		if (tid == 0)
+			for (uint32_t i = it > NSTAGE ? it - NSTAGE : 0; i < it; ++i)
+				mbar_wait(smem_u32(&full_bar[i % NSTAGE]), (i / NSTAGE) & 1u, nullptr);
+	} else if (warp == 4) {
+		// ---- MMA issue (one thread)
+		if (lane == 0) {
+			uint32_t it = 0;
+			bool ok = true;
+			for (int j = 0; j < nact && ok; ++j) {
+				if (j > 0 && !mbar_wait(smem_u32(&tempty_bar), (j - 1) & 1u, abort)) { ok = false; break; }
+				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+				for (int kb = 0; kb < C::KB; ++kb, ++it) {
+					const uint32_t st = it % NSTAGE;
+					if (!mbar_wait(smem_u32(&full_bar[st]), (it / NSTAGE) & 1u, abort)) { ok = false; break; }
+					asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+					const uint32_t sb = smem_u32(base + st * C::STAGE);
+					const uint32_t op_hi = sb, op_lo = sb + NC * 128;
+					const uint32_t a_hi = sb + C::OP_BYTES, a_lo = a_hi + C::A_BYTES;
+#pragma unroll
+					for (int ks = 0; ks < 4; ++ks) {
+						const uint64_t ah = desc_sw128(a_hi + ks * 32), al = desc_sw128(a_lo + ks * 32);
+						const uint64_t bh = desc_sw128(op_hi + ks * 32), bl = desc_sw128(op_lo + ks * 32);
+						mma_tf32<NC>(tmem, ah, bh, (kb | ks) != 0);
+						mma_tf32<NC>(tmem + CORR_COL, ah, bl, (j | kb | ks) != 0);
+						mma_tf32<NC>(tmem + CORR_COL, al, bh, 1u);
+					}
+					mma_commit(smem_u32(&empty_bar[st]));
+				}
+				if (ok) mma_commit(smem_u32(&tfull_bar));
+			}
+			if (!ok) {
+				*abort = 1;
+				atomicOr(flags, DEV_ERR_TIMEOUT);
+			}
+			// every MMA issued above has completed once this commit arrives
+			mma_commit(smem_u32(&drain_bar));
+			mbar_wait(smem_u32(&drain_bar), 0u, nullptr);
+		}
+		__syncwarp();
+	} else {
+		// ---- epilogue: per slot, main -> FP32 registers
+		constexpr int W = C::HALF;
+		const int quarter = warp & 3, half = (warp - EPI_WARP0) >> 2;
+		const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * W);
+		float acc[W];
+#pragma unroll
+		for (int c = 0; c < W; ++c) acc[c] = 0.f;
+		bool ok = true;
+		for (int j = 0; j < nact; ++j) {
+			if (!mbar_wait(smem_u32(&tfull_bar), j & 1u, abort)) { ok = false; break; }
+			asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+			tmem_accumulate<W>(taddr, acc);
+			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+			mbar_arrive(smem_u32(&tempty_bar));
+		}
+		if (!ok) {
+			*abort = 1;
+			atomicOr(flags, DEV_ERR_TIMEOUT);
+		} else {
+			if (nact > 0) tmem_accumulate<W>(taddr + CORR_COL, acc);
+			const int tg = tgt[quarter * 32 + lane];
+			if (tg >= 0 && !*abort) {
+				float* o = out + (size_t)tg * R + half * W;
+				const int lim = R - half * W;
+#pragma unroll
+				for (int c = 0; c < W; ++c)
+					if (c < lim) o[c] = acc[c];
+			}
+		}
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	if (warp == 4)
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS));
+}
+
+__global__ void tc_split_reduce_kernel(const float* __restrict__ part, float* __restrict__ loc, size_t n, int S)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	float s = part[i];
+	for (int k = 1; k < S; ++k) s += part[(size_t)k * n + i];
+	loc[i] = s;
+}
+
+// FP64 scaled operators [343][NC][NC] -> per (direction, K block): hi rows then
+// lo rows, NC rows of 32 TF32 values, 16-byte chunk c of row r at c ^ (r & 7).
+__global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int NC, int R, int KB, uint32_t* __restrict__ out)
+{
+	const size_t total = (size_t)343 * KB * 2 * NC * 32;
+	const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= total) return;
+	const int j = (int)(e % 32);
+	size_t rest = e / 32;
+	const int row = (int)(rest % NC); rest /= NC;
+	const int x = (int)(rest % 2); rest /= 2;
+	const int kb = (int)(rest % KB);
+	const int dir = (int)(rest / KB);
+	const int k = kb * 32 + j;
+	const double v = (row < R && k < R) ? ops64[((size_t)dir * NC + row) * NC + k] : 0.0;
+	const uint32_t hi = tf32_rna((float)v);
+	const uint32_t lo = tf32_rna((float)(v - (double)__uint_as_float(hi)));
+	const size_t blk = ((size_t)dir * KB + kb) * 2 + x;
+	const size_t word = blk * NC * 32 + (size_t)row * 32 + (size_t)(((j >> 2) ^ (row & 7)) * 4) + (j & 3);
+	out[word] = x == 0 ? hi : lo;
+}
+
+template <int NC>
+int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
+{
+	using C = TcCfg<NC>;
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
+	// spread the slots of few tiles over several blocks (about two waves)
+	int S = 1;
+	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
+	float* part = nullptr;
+	if (S > 1) {
+		part = static_cast<float*>(ctx.arena.take(sizeof(float) * (size_t)S * plan.cells * R));
+		if (!part) S = 1;
+	}
+	dim3 grid(tiles, S);
+	const bool timed = ctx.timing && ctx.kev_used + 2 <= 32;
+	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
+	m2l_tc_kernel<NC><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(reinterpret_cast<const uint8_t*>(ops), mult, loc,
+	                                                            plan.vtab, plan.order, plan.oct_count, R, part,
+	                                                            plan.cells, ctx.dev_flags);
+	if (timed) {
+		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
+		ctx.kev_used += 2;
+	}
+	if (S > 1) {
+		const size_t n = plan.cells * (size_t)R;
+		tc_split_reduce_kernel<<<div_up(n, 256), 256, 0, ctx.stream>>>(part, loc, n, S);
+	}
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+std::mutex g_upload_mu;
+bool g_uploaded[64] = {};
+
+int upload_slot_dirs(Context& ctx)
+{
+	std::lock_guard<std::mutex> lock(g_upload_mu);
+	if (ctx.device < 0 || ctx.device >= 64) { ctx.last_error = "device index above 63"; return ERR_ARG; }
+	if (!g_uploaded[ctx.device]) {
+		const M2LSlots& S = m2l_slots();
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_tc_slot_dir, S.slot_dir, sizeof(S.slot_dir)));
+		g_uploaded[ctx.device] = true;
+	}
+	return OK;
+}
+
+} // namespace
+
+const uint4* m2l_ops_tc(Context& ctx, int N)
+{
+	for (auto& e : ctx.opcache)
+		if (e.N == N && e.prec == 3) { e.stamp = ++ctx.opcache_clock; return static_cast<const uint4*>(e.ptr); }
+	const double* d = m2l_ops_fp64(ctx, N, 1.0);
+	if (!d) return nullptr;
+	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N);
+	const size_t words = (size_t)343 * KB * 2 * NC * 32;
+	OpCacheEntry e;
+	e.N = N; e.prec = 3; e.h = 1.0; e.bytes = words * 4; e.stamp = ++ctx.opcache_clock;
+	if (cudaMalloc(&e.ptr, e.bytes) != cudaSuccess) {
+		cudaGetLastError();
+		ctx.last_error = "tensor-core operators: out of memory";
+		return nullptr;
+	}
+	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(d, NC, R, KB, static_cast<uint32_t*>(e.ptr));
+	if (cudaGetLastError() != cudaSuccess) {
+		cudaFree(e.ptr);
+		ctx.last_error = "tensor-core operators: launch failed";
+		return nullptr;
+	}
+	ctx.opcache.push_back(e);
+	return static_cast<const uint4*>(e.ptr);
+}
+
+int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N)
+{
+	if (int st = upload_slot_dirs(ctx)) return st;
+	const int R = N * (N + 1);
+	switch (m2l_padded(N)) {
+	case 64: return launch_tc<64>(ctx, plan, ops, mult, loc, R);
+	case 80: return launch_tc<80>(ctx, plan, ops, mult, loc, R);
+	case 96: return launch_tc<96>(ctx, plan, ops, mult, loc, R);
+	case 112: return launch_tc<112>(ctx, plan, ops, mult, loc, R);
+	case 144: return launch_tc<144>(ctx, plan, ops, mult, loc, R);
+	case 160: return launch_tc<160>(ctx, plan, ops, mult, loc, R);
+	case 192: return launch_tc<192>(ctx, plan, ops, mult, loc, R);
+	case 224: return launch_tc<224>(ctx, plan, ops, mult, loc, R);
+	case 240: return launch_tc<240>(ctx, plan, ops, mult, loc, R);
+	default:
+		ctx.last_error = "tensor-core M2L: unsupported order";
+		return ERR_UNSUPPORTED;
+	}
+}
+
+} // namespace lfmm

@@ -1,8 +1,7 @@
-"""Opt-in tensor-core (tcgen05, TF32 hi/lo split) M2L engine against the
-default SIMT FP32 GEMM.  Measured accuracy of the tcgen05 engine: ~1e-5
-relative to the FP64 form (its FP32 accumulation inside TMEM keeps fewer bits
-than the SIMT GEMM's per-offset FP32 partials carried in FP64, 2e-7); the
-bound below is that measured level, not the mixed form's 1e-6."""
+"""tcgen05 M2L engine (TF32 hi/lo split, per-slot FP32 flush; the default for
+the mixed form) against the SIMT FP32 GEMM and the FP64 form.  Both mixed
+engines must stay within the mixed form's 1e-6 of the FP64 form (measured:
+3-4e-7 for the tensor-core engine, 2-3e-7 for the SIMT one)."""
 import os
 
 import pytest
@@ -11,39 +10,60 @@ from laplace_fmm_b200 import Context, FastMultipole3d
 from laplace_fmm_b200.workloads import plummer_mix3d, rel_l2, uniform3d
 
 pytestmark = pytest.mark.gpu
-TC_TOL = 3e-5
+TOL = 1e-6
 
 
-def tc_context():
-    os.environ["LFMM_M2L"] = "tc"
+def engine_context(name):
+    os.environ["LFMM_M2L"] = name
     try:
         return Context(0)
     finally:
         del os.environ["LFMM_M2L"]
 
 
+@pytest.fixture(scope="module")
+def tc():
+    c = engine_context("tc")
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def simt():
+    c = engine_context("simt")
+    yield c
+    c.close()
+
+
 def noself(p, q):
     return p - q * 1e4
 
 
-@pytest.mark.parametrize("N", [13, 9, 5])
-def test_tc_engine_uniform(ctx, N):
+@pytest.mark.parametrize("N", [13, 9, 7, 11, 14, 15])
+def test_tc_engine_uniform(tc, simt, ctx, N):
     src, q = uniform3d(262144, seed=40 + N)
-    tc = tc_context()
     a = FastMultipole3d((src, q), N=N, tree_depth=6, precision="mixed", ctx=tc)
-    b = FastMultipole3d((src, q), N=N, tree_depth=6, precision="mixed")
-    c = FastMultipole3d((src, q), N=N, tree_depth=6)
-    assert rel_l2(noself(a.potentials, q), noself(b.potentials, q)) < TC_TOL
-    assert rel_l2(a.forces, b.forces) < TC_TOL
-    assert rel_l2(noself(b.potentials, q), noself(c.potentials, q)) < 1e-6
-    tc.close()
+    b = FastMultipole3d((src, q), N=N, tree_depth=6, precision="mixed", ctx=simt)
+    c = FastMultipole3d((src, q), N=N, tree_depth=6, ctx=ctx)
+    assert rel_l2(noself(a.potentials, q), noself(c.potentials, q)) < TOL
+    assert rel_l2(a.forces, c.forces) < TOL
+    assert rel_l2(noself(b.potentials, q), noself(c.potentials, q)) < TOL
 
 
-def test_tc_engine_adaptive(ctx):
+def test_tc_engine_adaptive(tc, ctx):
     src, q = plummer_mix3d(400000, seed=41)
-    tc = tc_context()
     a = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, precision="mixed", ctx=tc)
-    b = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, precision="mixed")
-    assert rel_l2(noself(a.potentials, q), noself(b.potentials, q)) < TC_TOL
-    assert rel_l2(a.forces, b.forces) < TC_TOL
-    tc.close()
+    c = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, ctx=ctx)
+    assert rel_l2(noself(a.potentials, q), noself(c.potentials, q)) < TOL
+    assert rel_l2(a.forces, c.forces) < TOL
+
+
+def test_tc_engine_small_levels_and_targets(tc, ctx):
+    """Few cells per level (slot split over several blocks, partial tiles) and
+    separate targets."""
+    src, q = uniform3d(20000, seed=44)
+    tgt, _ = uniform3d(3000, seed=45)
+    a = FastMultipole3d((src, q), tgt, N=11, tree_depth=5, precision="mixed", ctx=tc)
+    c = FastMultipole3d((src, q), tgt, N=11, tree_depth=5, ctx=ctx)
+    assert rel_l2(a.potentials, c.potentials) < TOL
+    assert rel_l2(a.forces, c.forces) < TOL
