@@ -46,9 +46,10 @@ CONFIGS = {
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
                         "p=20 (N=21), uniform quadtree depth 9"),
     # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
-    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=13, depth=10, max_leaf=64, precision="mixed",
+    # p = 13 (N = 14): the lowest order at which both forms reach rel-L2 <= 1e-6 here
+    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=14, depth=10, max_leaf=64, precision="mixed",
                workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels, "
-                        "<=64 per leaf), p=12 (N=13), mixed precision"),
+                        "<=64 per leaf), p=13 (N=14), mixed precision"),
 }
 DEFAULT_CONFIG = "c3"
 METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
@@ -175,6 +176,25 @@ def fp32_peak_tflops(torch):
     """Dense FP32 (SIMT, TF32 off) throughput measured here: cuBLAS SGEMM 8192^3."""
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    torch.matmul(a, b); torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def tf32_peak_tflops(torch):
+    """Dense TF32 tensor-core throughput measured here: cuBLAS FP32 GEMM 8192^3
+    with TF32 allowed (the denominator for the tcgen05 M2L kernel)."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
     a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
     b = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
     torch.matmul(a, b); torch.cuda.synchronize()
@@ -359,15 +379,43 @@ def m2l_flops(N):
     return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
 
 
-def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops):
-    """Roofline of the dominant phase (device time from the phase events).
+# DRAM bytes per millisecond of m2l_tc_kernel time, from an ncu capture of a
+# 2,097,152-particle case of the default workload (1.35 GB over 6.97 ms in 4
+# launches); the kernel's traffic grows with its work, so a full launch's
+# traffic is this rate times its duration.
+M2L_TC_DRAM_BYTES_PER_MS = 1.354e9 / 6.969
+
+
+def padded(N):
+    return (N * (N + 1) + 15) // 16 * 16
+
+
+def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=None):
+    """Roofline of the dominant phase (device time from the phase events; for
+    the tensor-core M2L, the summed CUDA-event time of its kernel launches).
     P2P: 20 flops per particle pair; M2L: the rotation method's algorithmic
-    flops per V pair (executed dense-GEMM flops reported beside it)."""
+    flops per V pair (executed dense-GEMM / tensor flops reported beside it)."""
     phases = {"leaves": stats["ms_leaves"], "m2l": stats["ms_m2l"], "tree": stats["ms_tree"],
               "upward": stats["ms_upward"], "l2l": stats["ms_l2l"]}
-    dom = max(phases, key=phases.get)
+    dom = phase or max(phases, key=phases.get)
     ms = phases[dom]
     fp64 = cfg["precision"] == "fp64"
+    if dom == "m2l" and stats.get("n_m2l_kernel", 0) > 0 and stats["ms_m2l_kernel"] > 0:
+        ms = stats["ms_m2l_kernel"]
+        N = cfg["N"]
+        nc = padded(N)
+        kpad = (nc + 31) // 32 * 32
+        flops = float(m2l_flops(N)) * stats["n_far_pairs"]
+        tensor = 3.0 * 2.0 * nc * kpad * stats["n_far_pairs"]     # hi x hi + two corrections, per V pair
+        achieved = flops / (ms * 1e-3) / 1e12
+        return {"kernel": "m2l_tc_kernel (tcgen05 TF32 hi/lo, direction-grouped)", "bound": "tensor",
+                "achieved": achieved, "peak": tf32_tflops, "unit": "TFLOP/s", "frac": achieved / tf32_tflops,
+                "peak_source": "measured cuBLAS FP32 GEMM with TF32 (8192^3)", "algorithmic_flops": flops,
+                "executed_tensor_flops": tensor, "executed_tensor_tflops": tensor / (ms * 1e-3) / 1e12,
+                "executed_frac": tensor / (ms * 1e-3) / 1e12 / tf32_tflops,
+                "kernel_ms": ms, "kernel_launches": stats["n_m2l_kernel"], "phase_ms": phases["m2l"],
+                "traffic": M2L_TC_DRAM_BYTES_PER_MS * ms / stats["n_m2l_kernel"],
+                "traffic_unit": "bytes per launch (ncu capture of a 2M-particle case, scaled by kernel time)"}
     peak = fp64_tflops if fp64 else fp32_tflops
     src = "measured cuBLAS DGEMM" if fp64 else "measured cuBLAS SGEMM (TF32 off)"
     if dom == "leaves":
@@ -394,13 +442,15 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops):
 
 # ---------------------------------------------------------------- CPU legs
 def cpu_sample(cfg):
-    """Bounded sample of the configuration for the host-core baselines: the
-    full problem for the small configurations, 1/8 of the particles with one
-    level less (same particles per leaf) for the large ones."""
+    """Bounded sample of the configuration for the host-core baselines (a few
+    seconds per solve): the full problem for the small configurations; for
+    the large ones every 64th particle of the seeded set (the same mixture)
+    on a uniform tree three levels shallower (the reference has no adaptive
+    tree).  Returns (stride, depth, description)."""
     if cfg["n"] <= 200000:
-        return cfg["n"], cfg["depth"], "full problem"
-    n = cfg["n"] // 8
-    return n, cfg["depth"] - 1, f"first {n} particles of the seeded set (1/8), depth {cfg['depth'] - 1}"
+        return 1, cfg["depth"], "full problem"
+    d = max(3, cfg["depth"] - 3)
+    return 64, d, f"every 64th particle of the seeded set ({cfg['n'] // 64}), uniform depth {d}"
 
 
 def cpu_solver():
@@ -416,8 +466,9 @@ def run_cpu(cfg, pos, q, steps):
     solver, kind = cpu_solver()
     cores = os.cpu_count() or 1
     solver.set_threads(cores)
-    n, depth, sample = cpu_sample(cfg)
-    p, qq = pos[:n], q[:n]
+    stride, depth, sample = cpu_sample(cfg)
+    p, qq = np.ascontiguousarray(pos[::stride]), np.ascontiguousarray(q[::stride])
+    n = len(p)
     fn = solver.fmm3d if cfg["dim"] == 3 else solver.fmm2d
     times = []
     for _ in range(steps):
@@ -468,6 +519,7 @@ def main():
         peaks = measured_peaks()
         fp64 = fp64_peak_tflops(torch)
         fp32 = fp32_peak_tflops(torch)
+        tf32 = tf32_peak_tflops(torch)
         stats = r["stats"]
         radix_passes = (cfg["dim"] * (cfg["depth"] - 1) + 7) // 8
         line = {
@@ -476,10 +528,12 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if cfg["precision"] == "fp64" else "f32/tf32", "data": "synthetic (seeded PCG64)",
             "config": base_config(cfg, world), "accuracy": r["acc"], "phases_ms": {
-                k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves", "ms_total")},
+                k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves", "ms_total",
+                                      "ms_m2l_kernel")},
             "tree": {k: stats[k] for k in ("n_cells", "n_leaves", "n_far_pairs", "n_close_pairs", "n_p2p_pairs")},
-            "roofline": roofline(cfg, stats, peaks, fp64, fp32), "fp64_peak_tflops_measured": fp64,
-            "fp32_peak_tflops_measured": fp32,
+            "roofline": roofline(cfg, stats, peaks, fp64, fp32, tf32),
+            "roofline_leaves": roofline(cfg, stats, peaks, fp64, fp32, tf32, phase="leaves"),
+            "fp64_peak_tflops_measured": fp64, "fp32_peak_tflops_measured": fp32, "tf32_peak_tflops_measured": tf32,
             "peaks_source": peaks["source"], "e2e": r["e2e"], "clocks": r["clocks"],
             "gpu_launches": args.steps * launches_per_solve(stats["depth"], cfg["dim"], radix_passes,
                                                             cfg.get("max_leaf", 0) > 0, cfg["precision"]),
