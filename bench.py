@@ -46,10 +46,23 @@ CONFIGS = {
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
                         "p=20 (N=21), uniform quadtree depth 9"),
     # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
-    # p = 13 (N = 14): the lowest order at which both forms reach rel-L2 <= 1e-6 here
+    # mixed form at the order the network picks for rel-L2 <= 1e-6 (sampled
+    # check of 256 outputs, fixed-order fallback); the plain FP64 form beside it
+    # at p = 13 (N = 14), the lowest fixed order that reaches 1e-6 here
     "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=14, depth=10, max_leaf=64, precision="mixed",
+               learned=True, tol=1e-6, check_targets=256,
                workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels, "
-                        "<=64 per leaf), p=13 (N=14), mixed precision"),
+                        "<=64 per leaf), mixed precision at the learned order for rel-L2 <= 1e-6 "
+                        "(plain FP64 form at p=13, N=14)"),
+    # 1024 independent problems, N log-uniform in [2048, 262144] (about 60M particles),
+    # each uniform in its own unit cube or one Gaussian cluster (sigma 0.05), solved
+    # as one batch (mixed, N = 14); the plain FP64 form (p = 10, N = 11) one problem
+    # at a time beside it
+    "c5": dict(dim=3, batch=True, count=1024, seed=5150, N=14, plain_N=11, depth=10, max_leaf=64,
+               precision="mixed", n=0,
+               workload="batched 3D: 1024 problems, N log-uniform in [2048, 262144], uniform or one Gaussian "
+                        "cluster (sigma 0.05) each, mixed precision p=13 (N=14), adaptive octrees (<=10 levels, "
+                        "<=64 per leaf); plain FP64 p=10 one problem at a time beside it"),
 }
 DEFAULT_CONFIG = "c3"
 METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
@@ -65,6 +78,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the mixed one")
+    ap.add_argument("--no-learned", action="store_true", help="mixed form at the fixed order N instead of the learned one")
     ap.add_argument("--max-leaf", type=int, default=None, help="override the adaptive split threshold (0: uniform)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None, help="override the configuration's")
     ap.add_argument("--order", type=int, default=None, help="override N (degrees)")
@@ -233,7 +247,7 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision):
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     from laplace_fmm_b200 import Context
-    from laplace_fmm_b200._lib import PRECISION, LfmmSolveOpts, LfmmStats
+    from laplace_fmm_b200._lib import PRECISION, LfmmLearnedInfo, LfmmSolveOpts, LfmmStats
     from laplace_fmm_b200.workloads import rel_l2, sample_targets
     torch.cuda.set_device(local_rank)
     dist = None
@@ -254,12 +268,27 @@ def run_ours(args, cfg, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     vp = ctypes.c_void_p
+    learned = bool(cfg.get("learned")) and not args.no_learned
+    d_params = None
+    info_box = {}
+    if learned:
+        from laplace_fmm_b200.order import load_params
+        d_params = torch.from_numpy(load_params()).cuda()
 
     def call(c, device, precision, stats=None, host=None):
-        """One solve through the C ABI (device buffers, or pinned host buffers)."""
+        """One solve through the C ABI (device buffers, or pinned host buffers);
+        the configuration's precision runs the learned solve when it has one."""
         src, qq, pot, fld = host if host else (d_src, d_q, d_pot, d_fld)
         sp = ctypes.byref(stats) if stats is not None else None
-        if dim == 3:
+        if dim == 3 and learned and precision == prec:
+            opts = LfmmSolveOpts(N, depth, max_leaf, precision, cfg["tol"])
+            info = LfmmLearnedInfo()
+            fn = L.lfmm3d_solve_learned_device if device else L.lfmm3d_solve_learned
+            st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, ctypes.byref(opts),
+                    vp(d_params.data_ptr()), cfg["tol"], cfg["check_targets"], vp(pot.data_ptr()),
+                    vp(fld.data_ptr()), ctypes.byref(info), sp)
+            info_box.update(info.as_dict())
+        elif dim == 3:
             opts = LfmmSolveOpts(N, depth, max_leaf, precision, 1e-8)
             fn = L.lfmm3d_solve_ex_device if device else L.lfmm3d_solve_ex
             st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, ctypes.byref(opts),
@@ -369,7 +398,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
                "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
     return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx,
-                plain=plain)
+                plain=plain, learned=dict(info_box) if learned else None)
 
 
 def m2l_flops(N):
@@ -402,7 +431,7 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
     fp64 = cfg["precision"] == "fp64"
     if dom == "m2l" and stats.get("n_m2l_kernel", 0) > 0 and stats["ms_m2l_kernel"] > 0:
         ms = stats["ms_m2l_kernel"]
-        N = cfg["N"]
+        N = stats.get("order_N") or cfg["N"]
         nc = padded(N)
         kpad = (nc + 31) // 32 * 32
         flops = float(m2l_flops(N)) * stats["n_far_pairs"]
@@ -425,8 +454,9 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": src, "algorithmic_flops": flops, "phase_ms": ms, "traffic": None}
     if dom == "m2l":
-        flops = float(m2l_flops(cfg["N"])) * stats["n_far_pairs"]
-        R = cfg["N"] * (cfg["N"] + 1)
+        Nd = stats.get("order_N") or cfg["N"]
+        flops = float(m2l_flops(Nd)) * stats["n_far_pairs"]
+        R = Nd * (Nd + 1)
         executed = 2.0 * R * R * stats["n_far_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
         return {"kernel": "m2l_gemm_kernel (direction-grouped GEMM)", "bound": "fp64" if fp64 else "fp32",
@@ -487,9 +517,104 @@ def base_config(cfg, world):
             "l2": "inputs > L2" if cfg["n"] * 32 > 126e6 else "L2 flushed (256 MB write) between steps"}
 
 
+def run_batch(args, cfg):
+    """Batched solves: one forest solve of all problems (device buffers), the
+    plain FP64 form one problem at a time, per-problem accuracy."""
+    import torch
+    from laplace_fmm_b200 import Context
+    from laplace_fmm_b200._lib import PRECISION, LfmmSolveOpts, LfmmStats
+    from laplace_fmm_b200.workloads import batch3d, rel_l2
+    probs = batch3d(cfg["count"], seed=cfg["seed"])
+    sizes = np.array([len(p) for p, _ in probs], dtype=np.uint64)
+    offs = np.zeros(len(probs) + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(sizes)
+    pos = np.ascontiguousarray(np.concatenate([p for p, _ in probs]))
+    q = np.ascontiguousarray(np.concatenate([c for _, c in probs]))
+    n = len(pos)
+    ctx = Context(0)
+    L = ctx.lib
+    vp = ctypes.c_void_p
+    d_src, d_q = torch.from_numpy(pos).cuda(), torch.from_numpy(q).cuda()
+    d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_fld = torch.empty(n, 3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    opts = LfmmSolveOpts(cfg["N"], cfg["depth"], cfg["max_leaf"], PRECISION[cfg["precision"]], 1e-8)
+
+    def step():
+        ctx.check(L.lfmm3d_solve_batch_device(ctx.handle, len(probs), offs.ctypes.data_as(vp), vp(d_src.data_ptr()),
+                                              vp(d_q.data_ptr()), ctypes.byref(opts), vp(d_pot.data_ptr()),
+                                              vp(d_fld.data_ptr()), None), "batch")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    # per-problem accuracy: 64 evenly spread targets of every problem against its own FP64 direct sum
+    pot, fld = d_pot.cpu().numpy(), d_fld.cpu().numpy()
+    errs_p, errs_f = [], []
+    for k, (p, c) in enumerate(probs):
+        b = int(offs[k])
+        idx = np.arange(0, len(p), max(1, len(p) // 64))
+        tgt = torch.from_numpy(np.ascontiguousarray(p[idx])).cuda()
+        ep = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+        ef = torch.empty(len(idx), 3, dtype=torch.float64, device="cuda")
+        ctx.check(L.lfmm3d_direct_device(ctx.handle, len(p), vp(d_src.data_ptr() + 24 * b),
+                                         vp(d_q.data_ptr() + 8 * b), len(idx), vp(tgt.data_ptr()),
+                                         vp(ep.data_ptr()), vp(ef.data_ptr())), "direct")
+        stream.synchronize()
+        self_t = c[idx] * 1e4
+        errs_p.append(rel_l2(pot[b + idx] - self_t, ep.cpu().numpy() - self_t))
+        errs_f.append(rel_l2(fld[b + idx], ef.cpu().numpy()))
+    # the plain FP64 form, one problem at a time (uniform octree, automatic depth)
+    def plain_all():
+        for k, (p, c) in enumerate(probs):
+            b = int(offs[k])
+            ctx.check(L.lfmm3d_solve_device(ctx.handle, len(p), vp(d_src.data_ptr() + 24 * b),
+                                            vp(d_q.data_ptr() + 8 * b), 0, None, cfg["plain_N"], 2147483647, 1e-8,
+                                            0, vp(d_pot.data_ptr() + 8 * b), vp(d_fld.data_ptr() + 24 * b), None),
+                      "plain")
+
+    plain_all()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    plain_all()
+    t1.record(stream)
+    t1.synchronize()
+    pms = t0.elapsed_time(t1)
+    ep_ = np.array(errs_p); ef_ = np.array(errs_f)
+    line = {"metric": "batched 3D FMM aggregate Mparticles/s", "value": n / (ms * 1e-3) / 1e6,
+            "unit": "Mparticles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32",
+            "data": "synthetic (seeded PCG64)",
+            "config": {"workload": cfg["workload"], "problems": len(probs), "particles": int(n),
+                       "N_degrees": cfg["N"], "tree_depth": cfg["depth"], "precision": cfg["precision"],
+                       "parallelism": "single GPU", "l2": "inputs > L2"},
+            "accuracy": {"rel_l2_pot_noself_median": float(np.median(ep_)), "rel_l2_pot_noself_p95":
+                         float(np.quantile(ep_, 0.95)), "rel_l2_pot_noself_max": float(ep_.max()),
+                         "rel_l2_field_median": float(np.median(ef_)), "rel_l2_field_max": float(ef_.max()),
+                         "targets_per_problem": 64},
+            "plain_fp64_one_at_a_time": {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s",
+                                         "ms": pms, "N_degrees": cfg["plain_N"]},
+            "speedup_vs_plain_fp64": pms / ms, "clocks": clk.summary()}
+    ctx.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     cfg = args.cfg
+    if cfg.get("batch"):
+        return run_batch(args, cfg)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -538,6 +663,11 @@ def main():
             "gpu_launches": args.steps * launches_per_solve(stats["depth"], cfg["dim"], radix_passes,
                                                             cfg.get("max_leaf", 0) > 0, cfg["precision"]),
         }
+        if r["learned"]:
+            line["learned_order"] = dict(r["learned"], tol=cfg["tol"], check_targets=cfg["check_targets"])
+            line["config"]["N_degrees"] = r["learned"]["order_N"]
+            line["config"]["order_p"] = r["learned"]["order_N"] - 1
+            line["config"]["plain_fp64_N_degrees"] = cfg["N"]
         if r["plain"]:
             line["plain_fp64"] = r["plain"]
             line["speedup_vs_plain_fp64"] = r["plain"]["ms_per_step"] / r["ms"]

@@ -109,7 +109,7 @@ int lfmm3d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, cons
  * hold more than max_leaf particles, at most tree_depth levels) with U, V, W, X
  * lists.  precision FP64 with max_leaf = 0 is the reference-parity path
  * (same as lfmm3d_solve); every other combination runs the scaled-expansion
- * solver (N <= 13). */
+ * solver (N <= 15). */
 typedef struct {
 	int N;            /* degrees (order p + 1), or LFMM_AUTO (from eps) */
 	int tree_depth;   /* uniform depth / maximum adaptive depth, or LFMM_AUTO */
@@ -123,6 +123,22 @@ int lfmm3d_solve_ex(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const do
 int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                            const double* tgt_xyz, const lfmm_solve_opts* opts, double* pot, double* field,
                            lfmm_stats* stats);
+
+/* ---- batched 3D solves (no counterpart in the reference, which solves one
+ * problem per constructor call) ---------------------------------------------
+ * n_prob independent problems in one solve: problem k is the sources
+ * [offsets[k], offsets[k + 1]) of the concatenated arrays (offsets: host
+ * array of n_prob + 1 entries, offsets[0] = 0, non-decreasing, total < 2^32).
+ * One forest of octrees (each problem its own bounding box and root, as if
+ * solved alone) built and solved together: every FMM pass is one launch over
+ * all problems.  Results in input order.  opts as for lfmm3d_solve_ex (one N
+ * for the batch; tree_depth LFMM_AUTO follows the largest problem; the
+ * scaled-expansion solver). */
+int lfmm3d_solve_batch(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz, const double* src_q,
+                       const lfmm_solve_opts* opts, double* pot, double* field, lfmm_stats* stats);
+int lfmm3d_solve_batch_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
+                              const double* src_q, const lfmm_solve_opts* opts, double* pot, double* field,
+                              lfmm_stats* stats);
 
 /* ---- 2D ---------------------------------------------------------------- */
 int lfmm2d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
@@ -200,6 +216,49 @@ int lfmm_mlp_grad(lfmm_ctx* ctx, const float* params, int n, const float* X, con
 /* One Adam step (step >= 1) on params with moments m, v. */
 int lfmm_mlp_adam(lfmm_ctx* ctx, float* params, const float* grad, float* m, float* v, int step, float lr,
                   float beta1, float beta2, float eps);
+
+/* Per-leaf features of the tree that opts describes (its tree_depth and
+ * max_leaf; host buffers): feats [cap][16] in leaf order, leaf_of[n_src +
+ * n_tgt] = the leaf of every input particle (targets first, then sources);
+ * either may be NULL.  *n_leaves = the leaves of the tree (fails with
+ * LFMM_ERR_ARG when above cap).  The features: log10 particles; log10 of
+ * the far-field strength sum sqrt(n) / h over the V lists of the leaf and its
+ * ancestors (n = particles of the source cell, h = cell size); level / depth;
+ * log10 |U|, |W|, |X|, |V|, V-list entries of the leaf and its ancestors;
+ * log10 sum |q|; log10 of sum n / h over the same V lists; rms and max
+ * particle distance from the centre / cell size; log10 particles in the
+ * parent, in the problem, in the U cells; log10 |dipole| / (h sum |q|). */
+int lfmm3d_features(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                    const double* tgt_xyz, const lfmm_solve_opts* opts, float* feats, size_t cap, int* leaf_of,
+                    size_t* n_leaves);
+
+typedef struct {
+	int order_N;                /* degrees of the final solve */
+	int predicted_N;            /* degrees the network chose */
+	int fallback;               /* 1: the sampled check missed tol and the solve was rerun at N = 15 */
+	double predicted_error;     /* the network's rel-L2 estimate of the potential at predicted_N */
+	double checked_error;       /* sampled rel-L2 of the potential, self term removed (-1: no check) */
+	double checked_error_field; /* the same for the field */
+} lfmm_learned_info;
+
+/* 3D solve at the order the network picks for tolerance tol (rel-L2 of the
+ * potential without the self term).  The FP64 direct sum is first evaluated
+ * at check_targets (>= 1) outputs spread through the output range; the
+ * network predicts each leaf's absolute error at p = 4, 6, ..., 14, the
+ * leaves' errors over the samples' RMS potential give the predicted rel-L2,
+ * and the lowest p in 4..14 within tol is solved (else N = 15).  The same
+ * samples then judge the result: a solve above tol is rerun at the fixed
+ * order N = 15 (the fallback).  params: device pointer to the network
+ * (LFMM_MLP_PARAMS floats, inputs unnormalised).  opts gives the tree
+ * (tree_depth, max_leaf) and precision; opts->N and opts->eps are ignored.
+ * Synchronises.  Host and device-buffer variants. */
+int lfmm3d_solve_learned(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                         const double* tgt_xyz, const lfmm_solve_opts* opts, const float* params, double tol,
+                         int check_targets, double* pot, double* field, lfmm_learned_info* info, lfmm_stats* stats);
+int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q,
+                                size_t n_tgt, const double* tgt_xyz, const lfmm_solve_opts* opts,
+                                const float* params, double tol, int check_targets, double* pot, double* field,
+                                lfmm_learned_info* info, lfmm_stats* stats);
 
 /* ---- rotation tables (tests) --------------------------------------------
  * Wigner small-d matrix for table slot `slot` (layout n(n+1)(4n-1)/6 +

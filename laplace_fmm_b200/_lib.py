@@ -26,6 +26,8 @@ EXPORTS = [
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
+    "lfmm3d_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
+    "lfmm3d_solve_batch", "lfmm3d_solve_batch_device",
 ]
 
 
@@ -52,6 +54,15 @@ class LfmmStats(ctypes.Structure):
 class LfmmSolveOpts(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("tree_depth", ctypes.c_int), ("max_leaf", ctypes.c_int),
                 ("precision", ctypes.c_int), ("eps", ctypes.c_double)]
+
+
+class LfmmLearnedInfo(ctypes.Structure):
+    _fields_ = [("order_N", ctypes.c_int), ("predicted_N", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("predicted_error", ctypes.c_double), ("checked_error", ctypes.c_double),
+                ("checked_error_field", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class LfmmError(RuntimeError):
@@ -98,6 +109,13 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_mlp_grad.argtypes = [P, P, I, P, P, P, P, P, ctypes.POINTER(ctypes.c_float)]
         F = ctypes.c_float
         L.lfmm_mlp_adam.argtypes = [P, P, P, P, P, I, F, F, F, F]
+        L.lfmm3d_features.argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, SZ, P,
+                                      ctypes.POINTER(SZ)]
+        for f in ("lfmm3d_solve_learned", "lfmm3d_solve_learned_device"):
+            getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, D, I, P, P,
+                                      ctypes.POINTER(LfmmLearnedInfo), ctypes.POINTER(LfmmStats)]
+        for f in ("lfmm3d_solve_batch", "lfmm3d_solve_batch_device"):
+            getattr(L, f).argtypes = [P, I, P, P, P, ctypes.POINTER(LfmmSolveOpts), P, P, ctypes.POINTER(LfmmStats)]
         _lib = L
         return L
 

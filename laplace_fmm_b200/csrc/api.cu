@@ -4,6 +4,7 @@
 #include "../../include/lfmm.h"
 #include "fmm2d.cuh"
 #include "direct.cuh"
+#include "learned.cuh"
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -227,6 +228,76 @@ int need_tree(lfmm_ctx* ctx, int level)
 	return LFMM_OK;
 }
 
+// Inputs validated as for a solve; device pointers.
+int check_inputs(Context& c, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                 const lfmm_solve_opts* o)
+{
+	if (!o) { c.last_error = "null options"; return ERR_ARG; }
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return ERR_ARG; }
+	if ((ns && (!src || !q)) || (nt && !tgt)) { c.last_error = "null buffer"; return ERR_ARG; }
+	if (o->precision != LFMM_PRECISION_FP64 && o->precision != LFMM_PRECISION_MIXED) {
+		c.last_error = "unknown precision";
+		return ERR_ARG;
+	}
+	return OK;
+}
+
+int learned_dev(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                const lfmm_solve_opts* o, const float* params, double tol, int check, double* pot, double* field,
+                lfmm_learned_info* info, lfmm_stats* stats)
+{
+	Context& c = ctx->c;
+	int st = check_inputs(c, ns, src, q, nt, tgt, o);
+	if (st) return st;
+	if (!pot || !field) { c.last_error = "null buffer"; return ERR_ARG; }
+	ctx->has_tree = false;
+	ParticleInput in;
+	in.dim = 3; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q; in.tgt = tgt;
+	SolveStats ss;
+	st = solve_learned_device(c, in, resolve_depth(3, o->tree_depth, ns + nt), o->max_leaf, o->precision, params,
+	                          tol, check, pot, field, info, stats ? &ss : nullptr);
+	if (st) return st;
+	fill_stats(stats, ss);
+	return OK;
+}
+
+// Batched solve on device buffers (see lfmm3d_solve_batch).
+int batch_dev(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src, const double* q,
+              const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	Context& c = ctx->c;
+	if (!o || !offsets || nprob < 1 || !pot || !field) { c.last_error = "batch: bad arguments"; return ERR_ARG; }
+	if (offsets[0] != 0) { c.last_error = "batch: offsets[0] must be 0"; return ERR_ARG; }
+	size_t big = 0;
+	for (int k = 0; k < nprob; ++k) {
+		if (offsets[k + 1] < offsets[k]) { c.last_error = "batch: offsets must not decrease"; return ERR_ARG; }
+		big = std::max(big, offsets[k + 1] - offsets[k]);
+	}
+	const size_t n = offsets[nprob];
+	if (n == 0 || n >= 0xffffffffull) { c.last_error = "batch: total particle count out of range"; return ERR_ARG; }
+	if (!src || !q) { c.last_error = "null buffer"; return ERR_ARG; }
+	if (o->precision != LFMM_PRECISION_FP64 && o->precision != LFMM_PRECISION_MIXED) {
+		c.last_error = "unknown precision";
+		return ERR_ARG;
+	}
+	std::vector<uint32_t> h(nprob + 1);
+	for (int k = 0; k <= nprob; ++k) h[k] = (uint32_t)offsets[k];
+	uint32_t* poff = static_cast<uint32_t*>(c.arena.take(sizeof(uint32_t) * (nprob + 1)));
+	if (!poff) { c.last_error = "device allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(c, cudaMemcpyAsync(poff, h.data(), sizeof(uint32_t) * (nprob + 1), cudaMemcpyHostToDevice, c.stream));
+	ctx->has_tree = false;
+	ParticleInput in;
+	in.dim = 3; in.ns = n; in.nt = 0; in.src = src; in.srcq = q; in.poff = poff; in.nprob = nprob;
+	SolveStats ss;
+	int st = fmm3d_solve_scaled(c, in, resolve_order(3, o->N, o->eps), resolve_depth(3, o->tree_depth, big),
+	                            o->max_leaf, o->precision, pot, field, stats ? &ss : nullptr);
+	// the host copy of offsets must outlive the async copy
+	LFMM_CUDA(c, cudaStreamSynchronize(c.stream));
+	if (st) return st;
+	fill_stats(stats, ss);
+	return OK;
+}
+
 template <typename D, typename S>
 int fetch(Context& c, D* dst, const S* src, size_t n)
 {
@@ -390,6 +461,128 @@ int lfmm2d_direct_device(lfmm_ctx* ctx, size_t ns, const double* src, const doub
 	ctx->c.arena.reset();
 	int st = direct_device(ctx->c, 2, ns, src, q, nt, tgt, pot, field);
 	ctx->c.arena.settle();
+	return st;
+}
+
+// ---- batched solves ----------------------------------------------------------
+
+int lfmm3d_solve_batch_device(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src, const double* q,
+                              const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	ctx->c.arena.reset();
+	int st = batch_dev(ctx, nprob, offsets, src, q, o, pot, field, stats);
+	if (st == OK) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
+int lfmm3d_solve_batch(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src, const double* q,
+                       const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (!offsets || nprob < 1 || !src || !q || !pot || !field) { c.last_error = "batch: bad arguments"; return LFMM_ERR_ARG; }
+	const size_t n = offsets[nprob];
+	c.arena.reset();
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(n, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(n, 1)));
+	double* dpot = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(n, 1)));
+	double* dfld = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(n, 1)));
+	if (!dsrc || !dq || !dpot || !dfld) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (n) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+	}
+	int st = batch_dev(ctx, nprob, offsets, dsrc, dq, o, dpot, dfld, stats);
+	if (st == OK) {
+		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+		st = check_flags(c);
+	}
+	c.arena.settle();
+	return st;
+}
+
+// ---- learned order -----------------------------------------------------------
+
+int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+                                const double* tgt, const lfmm_solve_opts* o, const float* params, double tol,
+                                int check_targets, double* pot, double* field, lfmm_learned_info* info,
+                                lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	ctx->c.arena.reset();
+	int st = learned_dev(ctx, ns, src, q, nt, tgt, o, params, tol, check_targets, pot, field, info, stats);
+	if (st == OK) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
+int lfmm3d_solve_learned(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                         const lfmm_solve_opts* o, const float* params, double tol, int check_targets, double* pot,
+                         double* field, lfmm_learned_info* info, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = check_inputs(c, ns, src, q, nt, tgt, o);
+	if (st) return st;
+	if (!pot || !field) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
+	c.arena.reset();
+	const size_t nout = nt ? nt : ns;
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	double* dpot = static_cast<double*>(c.arena.take(sizeof(double) * nout));
+	double* dfld = static_cast<double*>(c.arena.take(sizeof(double) * 3 * nout));
+	if (!dsrc || !dq || !dtgt || !dpot || !dfld) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+	st = learned_dev(ctx, ns, dsrc, dq, nt, dtgt, o, params, tol, check_targets, dpot, dfld, info, stats);
+	if (st == OK) {
+		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * 3 * nout, cudaMemcpyDeviceToHost, s));
+		st = check_flags(c);
+	}
+	c.arena.settle();
+	return st;
+}
+
+int lfmm3d_features(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                    const lfmm_solve_opts* o, float* feats, size_t cap, int* leaf_of, size_t* n_leaves)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = check_inputs(c, ns, src, q, nt, tgt, o);
+	if (st) return st;
+	c.arena.reset();
+	ctx->has_tree = false;
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	if (!dsrc || !dq || !dtgt) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+	ParticleInput in;
+	in.dim = 3; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
+	st = features_tree(c, in, resolve_depth(3, o->tree_depth, ns + nt), o->max_leaf, feats, cap,
+	                   reinterpret_cast<int32_t*>(leaf_of), n_leaves);
+	if (st == OK) st = check_flags(c);
+	c.arena.settle();
 	return st;
 }
 

@@ -16,8 +16,23 @@ namespace {
 
 constexpr int DT = 128;
 
+// 1 / sqrt(x) for the sampled checks: an FP32 seed refined by two Newton
+// steps in FP64 (relative error ~1e-16); the FP64 square root and divide
+// where the seed's range does not reach.
+__device__ __forceinline__ double rsqrt_refined(double x)
+{
+	if (!(x > 1e-30 && x < 1e30)) return 1.0 / sqrt(x);
+	double y = (double)rsqrtf((float)x);
+	const double hx = 0.5 * x;
+	y = y * fma(-hx * y, y, 1.5);
+	y = y * fma(-hx * y, y, 1.5);
+	return y;
+}
+
 // Sums of target i over sources [s_lo, s_hi): out[0] = potential, out[1..dim] = field.
-template <int DIM>
+// FAST (3D, the sampled accuracy checks): 1/r from rsqrt_refined of the
+// clamped r^2 instead of a square root and a divide.
+template <int DIM, bool FAST = false>
 __device__ __forceinline__ void direct_range(size_t s_lo, size_t s_hi, const double* __restrict__ src,
                                              const double* __restrict__ q, double xi, double yi, double zi,
                                              double out[4])
@@ -34,7 +49,16 @@ __device__ __forceinline__ void direct_range(size_t s_lo, size_t s_hi, const dou
 			sq[threadIdx.x] = q[j];
 		}
 		__syncthreads();
-		if (DIM == 3) {
+		if (DIM == 3 && FAST) {
+			for (int j = 0; j < cnt; ++j) {
+				double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
+				const double inv = rsqrt_refined(fmax(dx * dx + dy * dy + dz * dz, FORCE_EPS2));
+				const double qr = sq[j] * inv;
+				const double qr3 = qr * inv * inv;
+				p += qr;
+				fx = fma(dx, qr3, fx); fy = fma(dy, qr3, fy); fz = fma(dz, qr3, fz);
+			}
+		} else if (DIM == 3) {
 			for (int j = 0; j < cnt; ++j) {
 				double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
 				double r = fmax(sqrt(dx * dx + dy * dy + dz * dz), FORCE_EPS);
@@ -58,7 +82,7 @@ __device__ __forceinline__ void direct_range(size_t s_lo, size_t s_hi, const dou
 
 // grid (target tiles, source chunks).  part == nullptr: one chunk, results
 // straight to pot/fld; else partials to part[(chunk * nt + i) * 4 + k].
-template <int DIM>
+template <int DIM, bool FAST = false>
 __global__ void __launch_bounds__(DT) direct_kernel(size_t ns, size_t chunk, const double* __restrict__ src,
                                                     const double* __restrict__ q, size_t nt,
                                                     const double* __restrict__ tgt, double* __restrict__ pot,
@@ -73,7 +97,7 @@ __global__ void __launch_bounds__(DT) direct_kernel(size_t ns, size_t chunk, con
 	}
 	const size_t lo = (size_t)blockIdx.y * chunk, hi = min(ns, lo + chunk);
 	double r[4];
-	direct_range<DIM>(lo, hi, src, q, xi, yi, zi, r);
+	direct_range<DIM, FAST>(lo, hi, src, q, xi, yi, zi, r);
 	if (!valid) return;
 	if (part) {
 		double2* o = reinterpret_cast<double2*>(part + ((size_t)blockIdx.y * nt + i) * 4);
@@ -115,7 +139,7 @@ int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks)
 }
 
 int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
-                  const double* tgt, double* pot, double* fld, double* part, int S)
+                  const double* tgt, double* pot, double* fld, double* part, int S, bool fast)
 {
 	if (nt == 0) return OK;
 	if (S <= 1 || !part) S = 1, part = nullptr;
@@ -123,7 +147,8 @@ int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const dou
 	S = S > 1 ? (int)((ns + chunk - 1) / chunk) : 1;
 	if (S <= 1) part = nullptr;
 	dim3 grid(div_up(nt, DT), S);
-	if (dim == 3) direct_kernel<3><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
+	if (dim == 3 && fast) direct_kernel<3, true><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
+	else if (dim == 3) direct_kernel<3><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
 	else direct_kernel<2><<<grid, DT, 0, ctx.stream>>>(ns, chunk, src, q, nt, tgt, pot, fld, part);
 	if (part) {
 		if (dim == 3) direct_reduce_kernel<3><<<div_up(nt, 256), 256, 0, ctx.stream>>>(nt, S, part, pot, fld);
@@ -134,7 +159,7 @@ int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const dou
 }
 
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
-                  double* pot, double* fld)
+                  double* pot, double* fld, bool fast)
 {
 	if (nt == 0) return OK;
 	int S = direct_chunks(ns, nt, ctx.num_sms, 1024);
@@ -143,7 +168,7 @@ int direct_device(Context& ctx, int dim, size_t ns, const double* src, const dou
 		part = static_cast<double*>(ctx.arena.take(sizeof(double) * 4 * nt * (size_t)S));
 		if (!part) S = 1;       // fall back to one chunk (no scratch)
 	}
-	return direct_launch(ctx, dim, ns, src, q, nt, tgt, pot, fld, part, S);
+	return direct_launch(ctx, dim, ns, src, q, nt, tgt, pot, fld, part, S, fast);
 }
 
 } // namespace lfmm

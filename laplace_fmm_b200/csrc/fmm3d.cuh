@@ -24,9 +24,13 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 // Scaled-expansion solver on the adaptive-form tree (max_leaf = 0: uniform
 // depth `depth`; > 0: adaptive, at most `depth` levels): precision 0 = FP64,
 // 1 = mixed (FP32 expansions / near field, FP64 M2L on levels 2-3, FP64 tile
-// sums and self term).  N <= 13.
+// sums and self term).  N <= 15.
 int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
                        double* pot, double* field, SolveStats* stats, DevTree* tree_out = nullptr);
+// The same on a tree built by tree_build_adaptive (phase events 0 and 1, the
+// tree build, are the caller's when timing).
+int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, double* pot, double* field,
+                         SolveStats* stats);
 
 // Dense FP64 M2L operators [343][MT][MT] for cell size h (h = 1: the
 // level-independent scaled operators), cached in the context.

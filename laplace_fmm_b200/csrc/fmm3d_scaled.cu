@@ -108,7 +108,8 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 			l2l_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, inner + t.loff[L - 1] * Nx2,
 			                                                                     inner + t.loff[L] * Nx2, N, T, ctx.dev_flags);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s));
-	leaves_scaled_kernel<real><<<nl, LT, 0, s>>>(t, xr, yr, zr, qr, outer, inner, N, knm, pot, field);
+	constexpr int LW = leaf_warps<real>();
+	leaves_scaled_kernel<real><<<div_up(nl, LW), LW * 32, 0, s>>>(t, qr, outer, inner, N, knm, pot, field);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[5], s));
 	LFMM_CUDA(ctx, cudaGetLastError());
 	(void)stats;
@@ -170,9 +171,24 @@ int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, 
 	DevTree t;
 	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t))) return st;
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
+	if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+	if (tree_out) *tree_out = t;
+	return OK;
+}
+
+int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, double* pot, double* field,
+                         SolveStats* stats)
+{
+	if (N < 1 || N > MAXN3 || !m2l_gemm_supported(N)) {
+		ctx.last_error = "scaled / mixed / adaptive forms support N <= 15";
+		return ERR_UNSUPPORTED;
+	}
+	int st = upload_scaled_constants(ctx);
+	if (st) return st;
+	cudaStream_t s = ctx.stream;
+	const bool timing = ctx.timing != 0;
 	st = precision == 1 ? solve_t<float>(ctx, t, N, pot, field, stats) : solve_t<double>(ctx, t, N, pot, field, stats);
 	if (st) return st;
-	if (tree_out) *tree_out = t;
 	if (stats) {
 		unsigned long long* dc = static_cast<unsigned long long*>(ctx.arena.take(64));
 		if (!dc) return ERR_OOM;

@@ -1,0 +1,25 @@
+// Learned order selection: MLP forward (mlp.cu), per-leaf features and the
+// learned solve (learned.cu).
+#pragma once
+#include "../../include/lfmm.h"
+#include "fmm3d.cuh"
+
+namespace lfmm {
+
+// Y[n][6] = MLP(X[n][16]) on ctx.stream (device pointers).
+int mlp_forward_device(Context& ctx, const float* params, int n, const float* X, float* Y);
+
+// Tree (adaptive form: max_leaf > 0 splits, 0 = uniform depth), order from
+// the network for tolerance tol, solve on that tree, optional sampled check
+// (check_targets outputs) with the fixed-order rerun on a miss.  Device
+// pointers; synchronises.
+int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int max_leaf, int precision,
+                         const float* params, double tol, int check_targets, double* pot, double* field,
+                         lfmm_learned_info* info, SolveStats* stats);
+
+// Per-leaf features [n_leaves][16] and the leaf of every input particle
+// (host buffers; either may be null).
+int features_tree(Context& ctx, const ParticleInput& in, int depth, int max_leaf, float* feats_host, size_t cap,
+                  int32_t* leaf_of_host, size_t* n_leaves);
+
+} // namespace lfmm

@@ -3,8 +3,7 @@
 // Output k predicts log10 of a leaf box's error at order p = 4 + 2k.
 //
 // Parameter layout (floats): W1[64][16] b1[64] W2[64][64] b2[64] W3[6][64] b3[6].
-#include "../../include/lfmm.h"
-#include "context.cuh"
+#include "learned.cuh"
 
 namespace lfmm {
 
@@ -167,6 +166,18 @@ __global__ void adam_kernel(float* __restrict__ P, const float* __restrict__ G, 
 }
 
 } // namespace
+
+} // namespace lfmm
+
+namespace lfmm {
+
+int mlp_forward_device(Context& c, const float* params, int n, const float* X, float* Y)
+{
+	if (n <= 0) return OK;
+	mlp_forward_kernel<<<(n + MT - 1) / MT, 64, 0, c.stream>>>(params, n, X, Y, nullptr, nullptr);
+	LFMM_CUDA(c, cudaGetLastError());
+	return OK;
+}
 
 } // namespace lfmm
 

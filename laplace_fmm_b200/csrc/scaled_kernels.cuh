@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(WPB * 32) p2m_scaled_kernel(DevTree t, const r
 	const int Nx2 = N * (N + 1) / 2;
 	for (int c = lane; c < Nx2; c += 32) sacc[w][c] = V2<real>::make(0, 0);
 	__syncwarp();
-	const real ih = (real)(ldexp(1.0, t.lev[g]) / t.geo_host[3]);
+	const real ih = (real)(1.0 / cell_size(t, g));
 	const uint32_t b = t.pbeg[g], e = t.send[g];
 	for (uint32_t base = b; base < e; base += 32) {
 		uint32_t i = base + lane;
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(WPB * 32) p2l_kernel(DevTree t, int N, const r
 	const int Nx2 = N * (N + 1) / 2;
 	for (int c = lane; c < Nx2; c += 32) sacc[w][c] = V2<real>::make(0, 0);
 	__syncwarp();
-	const double ih = ldexp(1.0, t.lev[g]) / t.geo_host[3];
+	const double ih = 1.0 / cell_size(t, g);
 	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
 	for (uint32_t e = xb; e < xe; ++e) {
 		const int32_t C = t.x_idx[e];
@@ -392,44 +392,45 @@ __global__ void convert_back_kernel(const double* __restrict__ in, real* __restr
 	if (i < n) out[i] = (real)in[i];
 }
 
-constexpr int LT = 128;
+// warps (leaves) per block of the leaf kernel (static shared memory <= 48 KB)
+template <typename real> constexpr int leaf_warps() { return sizeof(real) == sizeof(float) ? 8 : 4; }
 
-// One block per leaf: near field over the leaf and its U list (leaf-relative
-// coordinates, source leaves shifted by the FP64 centre difference rounded
-// once, per-tile partial sums carried in FP64), M2P over the W list, L2P of
-// the leaf's local expansion, and the self term q_i / 1e-4 in FP64.
-template <typename real>
-__global__ void __launch_bounds__(LT) leaves_scaled_kernel(DevTree t, const real* __restrict__ xr, const real* __restrict__ yr,
-                                                           const real* __restrict__ zr, const real* __restrict__ qr,
-                                                           const typename V2<real>::t* __restrict__ outer,
-                                                           const typename V2<real>::t* __restrict__ inner, int N,
-                                                           const real* __restrict__ knm, double* __restrict__ pot_out,
-                                                           double* __restrict__ fld_out)
+// Near and local field of every target particle: one warp per leaf, lane =
+// target (chunks of 32).  P2P over the leaf itself and its U list, sources
+// staged 32 at a time in the warp's shared memory as offsets in the target
+// leaf's frame split hi + lo (FP32 pairs keep ~1e-7 relative accuracy
+// however close the pair; lo unused in FP64), partial sums over 8 sources
+// carried in FP64; M2P over the W list; L2P of the leaf's local expansion;
+// self term in FP64; outputs written in input order.
+template <typename real, int LW = leaf_warps<real>()>
+__global__ void __launch_bounds__(LW * 32) leaves_scaled_kernel(DevTree t, const real* __restrict__ qr,
+                                                               const typename V2<real>::t* __restrict__ outer,
+                                                               const typename V2<real>::t* __restrict__ inner, int N,
+                                                               const real* __restrict__ knm, double* __restrict__ pot_out,
+                                                               double* __restrict__ fld_out)
 {
-	// source tile in the target leaf's frame: offset = hi + lo (FP32 pairs; the
-	// FP64 offset split once when staged, so pair differences keep ~1e-7
-	// relative accuracy however close the pair); lo unused in FP64
-	__shared__ real sx[LT], sy[LT], sz[LT], sq[LT];
-	__shared__ real lx[LT], ly[LT], lz[LT];
-	__shared__ typename V2<real>::t sL[NX2MAX];
-	__shared__ typename V2<real>::t sM[NX2MAX];
-	if (blockIdx.x >= t.nleaves) return;
-	const size_t li = blockIdx.x;
+	using v2 = typename V2<real>::t;
+	constexpr bool SPLIT = sizeof(real) == sizeof(float);
+	__shared__ real sx[LW][32], sy[LW][32], sz[LW][32], sq[LW][32];
+	__shared__ real lx[LW][32], ly[LW][32], lz[LW][32];
+	__shared__ v2 sL[LW][NX2MAX], sM[LW][NX2MAX];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const size_t li = (size_t)blockIdx.x * LW + w;
+	if (li >= t.nleaves) return;
 	const size_t g = t.leaves[li];
 	const uint32_t tb = t.tbeg[g], te = t.tend[g];
 	if (tb >= te) return;
 	const bool tmode = t.targets_num > 0;
 	const int Nx2 = N * (N + 1) / 2;
-	const double scale = t.geo_host[3];
-	const double ihg = ldexp(1.0, t.lev[g]) / scale;
-	for (int c = threadIdx.x; c < Nx2; c += LT) sL[c] = inner[g * Nx2 + c];
+	const double ihg = 1.0 / cell_size(t, g);
+	for (int c = lane; c < Nx2; c += 32) sL[w][c] = inner[g * Nx2 + c];
 	const uint32_t ub = t.u_off[li], ue = t.u_off[li + 1];
 	const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
 	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
-	for (uint32_t t0 = tb; t0 < te; t0 += LT) {
-		const uint32_t i = t0 + threadIdx.x;
+	__syncwarp();
+	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
+		const uint32_t i = t0 + lane;
 		const bool valid = i < te;
-		constexpr bool SPLIT = sizeof(real) == sizeof(float);
 		real xi = 0, yi = 0, zi = 0, xl = 0, yl = 0, zl = 0;
 		if (valid) {
 			const double ax_ = t.x[i] - cx, ay_ = t.y[i] - cy, az_ = t.z[i] - cz;
@@ -440,38 +441,37 @@ __global__ void __launch_bounds__(LT) leaves_scaled_kernel(DevTree t, const real
 		for (int64_t e = (int64_t)ub - 1; e < (int64_t)ue; ++e) {
 			const size_t sc_ = e < (int64_t)ub ? g : (size_t)t.u_idx[e];
 			const uint32_t sb = t.pbeg[sc_], se = t.send[sc_];
-			for (uint32_t s0 = sb; s0 < se; s0 += LT) {
-				const int cnt = min((uint32_t)LT, se - s0);
-				__syncthreads();
-				if (threadIdx.x < cnt) {
-					const uint32_t j = s0 + threadIdx.x;
+			for (uint32_t s0 = sb; s0 < se; s0 += 32) {
+				const int cnt = min(32u, se - s0);
+				__syncwarp();
+				if (lane < cnt) {
+					const uint32_t j = s0 + lane;
 					const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
 					const real hx = (real)dx_, hy = (real)dy_, hz = (real)dz_;
-					sx[threadIdx.x] = hx; sy[threadIdx.x] = hy; sz[threadIdx.x] = hz;
+					sx[w][lane] = hx; sy[w][lane] = hy; sz[w][lane] = hz;
 					if (SPLIT) {
-						lx[threadIdx.x] = (real)(dx_ - (double)hx); ly[threadIdx.x] = (real)(dy_ - (double)hy);
-						lz[threadIdx.x] = (real)(dz_ - (double)hz);
+						lx[w][lane] = (real)(dx_ - (double)hx); ly[w][lane] = (real)(dy_ - (double)hy);
+						lz[w][lane] = (real)(dz_ - (double)hz);
 					}
-					sq[threadIdx.x] = qr[j];
+					sq[w][lane] = qr[j];
 				}
-				__syncthreads();
+				__syncwarp();
 				if (valid) {
 					const int self = (sc_ == g) ? (int)i - (int)s0 : -1;
-					// partial sums over 8 sources, carried in FP64 (compensated per target)
 					for (int j0 = 0; j0 < cnt; j0 += 8) {
-					const int j1 = min(cnt, j0 + 8);
-					real p = 0, ax = 0, ay = 0, az = 0;
-					for (int j = j0; j < j1; ++j) {
-						real dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
-						if (SPLIT) { dx += xl - lx[j]; dy += yl - ly[j]; dz += zl - lz[j]; }
-						real r2 = fmax(fma(dx, dx, fma(dy, dy, dz * dz)), (real)FORCE_EPS2);
-						real inv = rsq<real>(r2);
-						real qi = (j == self) ? real(0) : sq[j] * inv;
-						real qi3 = qi * inv * inv;
-						p += qi;
-						ax = fma(dx, qi3, ax); ay = fma(dy, qi3, ay); az = fma(dz, qi3, az);
-					}
-					pot += p; fx += ax; fy += ay; fz += az;
+						const int j1 = min(cnt, j0 + 8);
+						real p = 0, ax = 0, ay = 0, az = 0;
+						for (int j = j0; j < j1; ++j) {
+							real dx = xi - sx[w][j], dy = yi - sy[w][j], dz = zi - sz[w][j];
+							if (SPLIT) { dx += xl - lx[w][j]; dy += yl - ly[w][j]; dz += zl - lz[w][j]; }
+							const real r2 = fmax(fma(dx, dx, fma(dy, dy, dz * dz)), (real)FORCE_EPS2);
+							const real inv = rsq<real>(r2);
+							const real qi = (j == self) ? real(0) : sq[w][j] * inv;
+							const real qi3 = qi * inv * inv;
+							p += qi;
+							ax = fma(dx, qi3, ax); ay = fma(dy, qi3, ay); az = fma(dz, qi3, az);
+						}
+						pot += p; fx += ax; fy += ay; fz += az;
 					}
 				}
 			}
@@ -479,24 +479,24 @@ __global__ void __launch_bounds__(LT) leaves_scaled_kernel(DevTree t, const real
 		// M2P over the W list
 		for (uint32_t e = wb; e < we; ++e) {
 			const size_t D = t.w_idx[e];
-			__syncthreads();
-			for (int c = threadIdx.x; c < Nx2; c += LT) sM[c] = outer[D * Nx2 + c];
-			__syncthreads();
+			__syncwarp();
+			for (int c = lane; c < Nx2; c += 32) sM[w][c] = outer[D * Nx2 + c];
+			__syncwarp();
 			if (valid) {
-				const double ihd = ldexp(1.0, t.lev[D]) / scale;
+				const double ihd = 1.0 / cell_size(t, D);
 				real mp, mx_, my_, mz_;
-				eval_expansion<false, real>(sM, (real)((t.x[i] - t.cx[D]) * ihd), (real)((t.y[i] - t.cy[D]) * ihd),
+				eval_expansion<false, real>(sM[w], (real)((t.x[i] - t.cx[D]) * ihd), (real)((t.y[i] - t.cy[D]) * ihd),
 				                            (real)((t.z[i] - t.cz[D]) * ihd), N, knm, mp, mx_, my_, mz_);
 				pot += (double)mp * ihd;
 				fx += (double)mx_ * ihd * ihd; fy += (double)my_ * ihd * ihd; fz += (double)mz_ * ihd * ihd;
 			}
 		}
-		__syncthreads();
 		if (valid) {
-			real lp, lx, ly, lz;
-			eval_expansion<true, real>(sL, (real)(xi * ihg), (real)(yi * ihg), (real)(zi * ihg), N, knm, lp, lx, ly, lz);
+			real lp, lx_, ly_, lz_;
+			eval_expansion<true, real>(sL[w], (real)(xi * ihg), (real)(yi * ihg), (real)(zi * ihg), N, knm, lp, lx_, ly_,
+			                           lz_);
 			pot += (double)lp * ihg;
-			fx += (double)lx * ihg * ihg; fy += (double)ly * ihg * ihg; fz += (double)lz * ihg * ihg;
+			fx += (double)lx_ * ihg * ihg; fy += (double)ly_ * ihg * ihg; fz += (double)lz_ * ihg * ihg;
 			if (!tmode) pot += t.q[i] * (1.0 / FORCE_EPS);
 			const uint32_t o = t.orig[i];
 			pot_out[o] = pot;

@@ -68,16 +68,64 @@ __global__ void bbox_final_kernel(const double* partial, int nb, double* geo)
 	geo[3] = dw + 1.e-6;
 }
 
+// Forest: the bounding box of each problem, one block per problem, with the
+// same shift / scale rule.
+template <int DIM>
+__global__ void __launch_bounds__(BBOX_THREADS) bbox_segment_kernel(const ParticleInput in, double* geo)
+{
+	const uint32_t b = in.poff[blockIdx.x], e = in.poff[blockIdx.x + 1];
+	double mn[DIM], mx[DIM];
+#pragma unroll
+	for (int d = 0; d < DIM; ++d) { mn[d] = 1e300; mx[d] = -1e300; }
+	for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+		double p[DIM];
+		load_point<DIM>(in, i, p);
+#pragma unroll
+		for (int d = 0; d < DIM; ++d) { mn[d] = fmin(mn[d], p[d]); mx[d] = fmax(mx[d], p[d]); }
+	}
+#pragma unroll
+	for (int d = 0; d < DIM; ++d)
+		for (int o = 16; o > 0; o >>= 1) {
+			mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+			mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+		}
+	__shared__ double s[BBOX_THREADS / 32][2 * DIM];
+	const int w = threadIdx.x >> 5;
+	if ((threadIdx.x & 31) == 0)
+		for (int d = 0; d < DIM; ++d) { s[w][d] = mn[d]; s[w][DIM + d] = mx[d]; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int k = 1; k < BBOX_THREADS / 32; ++k)
+			for (int d = 0; d < DIM; ++d) { s[0][d] = fmin(s[0][d], s[k][d]); s[0][DIM + d] = fmax(s[0][DIM + d], s[k][DIM + d]); }
+		double dw = s[0][DIM] - s[0][0];
+		for (int d = 1; d < DIM; ++d) dw = fmax(dw, s[0][DIM + d] - s[0][d]);
+		double* g = geo + 4 * blockIdx.x;
+		for (int d = 0; d < 3; ++d) g[d] = d < DIM ? s[0][d] - 1.e-7 : 0.0;
+		g[3] = dw + 1.e-6;
+	}
+}
+
 // code = interleave(trunc(2^(depth-1) * (x - shift) / scale)), x highest
 // (reference cpu/morton_tree.cpp:48-99); IEEE-rounded ops, no contraction.
+// Forest: the particle's problem index above the Morton bits, the problem's box.
 template <int DIM>
-__global__ void codes_kernel(const ParticleInput in, size_t n, const double* __restrict__ geo, int depth,
+__global__ void codes_kernel(const ParticleInput in, size_t n, const double* __restrict__ geo_all, int depth,
                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
 {
 	size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	double p[DIM];
 	load_point<DIM>(in, i, p);
+	uint64_t prob = 0;
+	if (in.nprob > 1) {
+		int lo = 0, hi = in.nprob;          // last k with poff[k] <= i
+		while (hi - lo > 1) {
+			const int mid = (lo + hi) >> 1;
+			if (in.poff[mid] <= i) lo = mid; else hi = mid;
+		}
+		prob = (uint64_t)lo;
+	}
+	const double* geo = geo_all + 4 * prob;
 	double scale = geo[3];
 	double bit_shift = (double)(1ull << (depth - 1));
 	uint64_t c = 0;
@@ -87,7 +135,7 @@ __global__ void codes_kernel(const ParticleInput in, size_t n, const double* __r
 		uint64_t v = (uint64_t)__dmul_rn(bit_shift, u);
 		c |= (DIM == 3 ? spread3(v) : spread2(v)) << (DIM - 1 - d);
 	}
-	keys[i] = c;
+	keys[i] = c | (prob << (DIM * (depth - 1)));
 	vals[i] = (uint32_t)i;
 }
 
@@ -120,7 +168,7 @@ __global__ void gather_kernel(const ParticleInput in, size_t n, const uint64_t* 
 			if (x == 0) lev = t.depth;
 			else {
 				int b = 63 - __clzll((long long)x);
-				lev = t.depth - 1 - b / DIM;
+				lev = max(0, t.depth - 1 - b / DIM);     // a new problem of a forest: a new root
 			}
 		}
 		newlev[s] = (uint8_t)lev;
@@ -183,6 +231,7 @@ __global__ void centres_kernel(DevTree t, int L, size_t off, size_t m)
 	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= m) return;
 	uint64_t v = t.code[off + c];
+	const double* geo = t.geo + (t.nprob > 1 ? 4 * (v >> (DIM * L)) : 0);
 	double step = 1.0 / (double)(1ull << (L + 1));
 	double x = step, y = step, z = step;
 	step *= 2;
@@ -192,10 +241,10 @@ __global__ void centres_kernel(DevTree t, int L, size_t off, size_t m)
 		x += step * (double)(v & 1); v >>= 1;
 		step *= 2;
 	}
-	double scale = t.geo[3];
-	t.cx[off + c] = __dadd_rn(__dmul_rn(x, scale), t.geo[0]);
-	t.cy[off + c] = __dadd_rn(__dmul_rn(y, scale), t.geo[1]);
-	if (DIM == 3) t.cz[off + c] = __dadd_rn(__dmul_rn(z, scale), t.geo[2]);
+	double scale = geo[3];
+	t.cx[off + c] = __dadd_rn(__dmul_rn(x, scale), geo[0]);
+	t.cy[off + c] = __dadd_rn(__dmul_rn(y, scale), geo[1]);
+	if (DIM == 3) t.cz[off + c] = __dadd_rn(__dmul_rn(z, scale), geo[2]);
 	t.tbeg[off + c] = 0; t.tend[off + c] = 0;
 }
 
@@ -265,8 +314,10 @@ __global__ void lists_kernel(DevTree t, int L, unsigned* flags)
 	int32_t* out = t.close_idx + (off + c) * t.close_stride;
 	int nc = 0, nf = 0;
 	if (L == 1) {
+		// the other children of the root (forest: of the same root)
+		const int32_t pc = t.parent[off + c];
 		for (size_t k = 0; k < m; ++k)
-			if (k != c) { if (nc < t.close_stride) out[nc] = (int32_t)k; nc++; }
+			if (k != c && t.parent[off + k] == pc) { if (nc < t.close_stride) out[nc] = (int32_t)k; nc++; }
 	} else {
 		int me[3];
 		cell_coords<DIM>(t.code[off + c], me);
@@ -335,15 +386,19 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, boo
 {
 	const int dim = in.dim;
 	const size_t n = in.ns + in.nt;
-	if (n == 0 || n > 0xffffffffull || depth < 1 || depth > MAX_LEVELS - 1 || dim * (depth - 1) > 62) {
-		ctx.last_error = "tree: unsupported particle count or depth";
+	const int nprob = std::max(in.nprob, 1);
+	int pbits = 0;
+	while ((1ll << pbits) < nprob) ++pbits;
+	if (n == 0 || n > 0xffffffffull || depth < 1 || depth > MAX_LEVELS - 1 || dim * (depth - 1) + pbits > 62 ||
+	    (nprob > 1 && (in.nt > 0 || !in.poff))) {
+		ctx.last_error = "tree: unsupported particle count, depth or problem count";
 		return ERR_ARG;
 	}
 	cudaStream_t s = ctx.stream;
 	t = DevTree();
-	t.dim = dim; t.depth = depth; t.n = n; t.nt = in.nt;
+	t.dim = dim; t.depth = depth; t.n = n; t.nt = in.nt; t.nprob = nprob;
 	t.close_stride = dim == 3 ? 26 : 8;
-	t.geo = take<double>(ctx, 4);
+	t.geo = take<double>(ctx, 4 * (size_t)nprob);
 	t.x = take<double>(ctx, n); t.y = take<double>(ctx, n); t.z = dim == 3 ? take<double>(ctx, n) : nullptr;
 	t.q = take<double>(ctx, n); t.orig = take<uint32_t>(ctx, n); t.pcode = take<uint64_t>(ctx, n);
 	uint64_t* keys = take<uint64_t>(ctx, n);
@@ -360,7 +415,10 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, boo
 
 	LFMM_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(unsigned) * (MAX_LEVELS + 2), s));
 	const unsigned TB = 256;
-	if (dim == 3) {
+	if (dim == 3 && nprob > 1) {
+		bbox_segment_kernel<3><<<nprob, BBOX_THREADS, 0, s>>>(in, t.geo);
+		codes_kernel<3><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
+	} else if (dim == 3) {
 		bbox_partial_kernel<3><<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(in, n, partial);
 		bbox_final_kernel<3><<<1, 32, 0, s>>>(partial, BBOX_BLOCKS, t.geo);
 		codes_kernel<3><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
@@ -369,7 +427,7 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, boo
 		bbox_final_kernel<2><<<1, 32, 0, s>>>(partial, BBOX_BLOCKS, t.geo);
 		codes_kernel<2><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
 	}
-	int which = radix_sort_pairs(keys, vals, keys2, vals2, n, 0, dim * (depth - 1), scratch, s);
+	int which = radix_sort_pairs(keys, vals, keys2, vals2, n, 0, dim * (depth - 1) + pbits, scratch, s);
 	uint64_t* sk = which ? keys2 : keys;
 	uint32_t* sv = which ? vals2 : vals;
 	if (dim == 3) gather_kernel<3><<<div_up(n, TB), TB, 0, s>>>(in, n, sk, sv, t, newlev, hist);
@@ -411,7 +469,7 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, boo
 		else parent_cells_kernel<2><<<div_up(m1, TB), TB, 0, s>>>(flags, excl, m1, t, t.loff[L + 1], t.loff[L]);
 		cell_ends_kernel<<<div_up(t.lsize[L], TB), TB, 0, s>>>(t, t.loff[L], t.lsize[L], (uint32_t)m1);
 	}
-	LFMM_CUDA(ctx, cudaMemsetAsync(t.parent, 0xff, sizeof(int32_t), s));   // root has no parent
+	LFMM_CUDA(ctx, cudaMemsetAsync(t.parent, 0xff, sizeof(int32_t) * t.lsize[0], s));   // roots have no parent
 	for (int L = 0; L < depth; ++L) {
 		if (dim == 3) centres_kernel<3><<<div_up(t.lsize[L], TB), TB, 0, s>>>(t, L, t.loff[L], t.lsize[L]);
 		else centres_kernel<2><<<div_up(t.lsize[L], TB), TB, 0, s>>>(t, L, t.loff[L], t.lsize[L]);

@@ -33,6 +33,9 @@ struct DevTree {
 	int32_t* far_cnt = nullptr;                 // per cell, for statistics
 	size_t n_far_pairs = 0, n_close_pairs = 0;
 	// adaptive form (tree_build_adaptive); global cell indices unless noted
+	// forest of nprob independent problems (batched solves): the problem index
+	// sits above the Morton bits of every code, geo holds 4 doubles per problem
+	int nprob = 1;
 	bool adaptive = false;
 	int max_leaf = 0;
 	uint32_t *pbeg = nullptr, *pend = nullptr;  // particles of every cell
@@ -49,13 +52,26 @@ struct DevTree {
 };
 
 // Input particles: targets (nt, q = 0) followed by sources (ns, with q).
+// nprob > 1: the sources are nprob independent problems, problem k at
+// [poff[k], poff[k + 1]) (device offsets; no separate targets).
 struct ParticleInput {
 	int dim = 3;
 	size_t ns = 0, nt = 0;
 	const double* src = nullptr;   // device, ns x dim interleaved
 	const double* srcq = nullptr;  // device, ns
 	const double* tgt = nullptr;   // device, nt x dim interleaved
+	const uint32_t* poff = nullptr;
+	int nprob = 1;
 };
+
+// Size of the box of cell g (level t.lev[g]) of an adaptive-form tree; the
+// scale is per problem in a forest.
+__device__ __forceinline__ double cell_size(const DevTree& t, size_t g)
+{
+	const int L = t.lev[g];
+	const double scale = t.nprob > 1 ? t.geo[4 * (t.code[g] >> (t.dim * L)) + 3] : t.geo_host[3];
+	return scale / (double)(1ull << L);
+}
 
 // partition: split each leaf into sources then q == 0 targets; lists: build
 // the close lists and far counts.

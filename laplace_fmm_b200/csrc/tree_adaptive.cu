@@ -284,6 +284,7 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	a = DevTree();
 	a.dim = 3; a.depth = depth; a.n = u.n; a.nt = u.nt; a.targets_num = u.targets_num;
 	a.geo = u.geo;
+	a.nprob = u.nprob;
 	for (int d = 0; d < 4; ++d) a.geo_host[d] = u.geo_host[d];
 	a.x = u.x; a.y = u.y; a.z = u.z; a.q = u.q; a.orig = u.orig; a.pcode = u.pcode;
 	a.close_stride = 26;

@@ -161,3 +161,25 @@ def cuda_copy_math_constants():
 
 def cuda_clear_math_constants():
     return None
+
+
+def solve_batch(problems, N: int = FMM_AUTO, tree_depth: int = FMM_AUTO, max_leaf: int = 64,
+                precision: str = "mixed", eps: float = 1.0e-8, ctx: Context | None = None):
+    """Independent 3D problems [(positions, charges), ...] solved together
+    (one forest of octrees, one launch per FMM pass); returns
+    [(potentials, forces), ...] in the same order."""
+    ctx = ctx or default_context()
+    parts = [_split(p, 3) for p in problems]
+    offs = np.zeros(len(parts) + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum([len(p[0]) for p in parts])
+    pos = np.ascontiguousarray(np.concatenate([p[0] for p in parts]))
+    q = np.ascontiguousarray(np.concatenate([p[1] for p in parts]))
+    n = len(pos)
+    pot = np.zeros(n)
+    fld = np.zeros((n, 3))
+    opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
+    stats = LfmmStats()
+    ctx.check(ctx.lib.lfmm3d_solve_batch(ctx.handle, len(parts), offs.ctypes.data_as(ctypes.c_void_p), _ptr(pos),
+                                         _ptr(q), ctypes.byref(opts), _ptr(pot), _ptr(fld), ctypes.byref(stats)),
+              "lfmm3d_solve_batch")
+    return [(pot[offs[k]:offs[k + 1]], fld[offs[k]:offs[k + 1]]) for k in range(len(parts))]

@@ -14,7 +14,7 @@ from pathlib import Path
 
 import numpy as np
 
-from ._lib import Context, LfmmError, default_context
+from ._lib import PRECISION, Context, LfmmError, LfmmLearnedInfo, LfmmSolveOpts, LfmmStats, default_context
 
 N_IN, N_HIDDEN, N_OUT = 16, 64, 6
 N_PARAMS = N_HIDDEN * N_IN + N_HIDDEN + N_HIDDEN * N_HIDDEN + N_HIDDEN + N_OUT * N_HIDDEN + N_OUT
@@ -122,12 +122,109 @@ class OrderMLP:
     def params_host(self) -> np.ndarray:
         return self.params.cpu().numpy()
 
+    def shift_outputs(self, delta: float):
+        """Add delta to every output (log10 error): the calibration offset."""
+        self.params[N_PARAMS - N_OUT:] += float(delta)
+
+    def predicted_log10(self, feats: np.ndarray) -> np.ndarray:
+        """log10 of the predicted rel-L2 of a problem at each of the six orders,
+        from its leaves' features (leaves weighted by their particles), as the
+        solver aggregates them."""
+        Y = self.forward(feats).astype(np.float64)
+        w = 10.0 ** feats[:, 0].astype(np.float64) - 1.0
+        return 0.5 * np.log10((w[:, None] * 10.0 ** (2.0 * Y)).sum(0) / max(w.sum(), 1.0))
+
+    def folded_params(self) -> np.ndarray:
+        """Parameters with the input normalisation folded into the first layer
+        (W1' = W1 / std, b1' = b1 - W1' mean): the network on raw features, as
+        the solver runs it."""
+        p = self.params_host().astype(np.float64)
+        nw1 = N_HIDDEN * N_IN
+        W1 = p[:nw1].reshape(N_HIDDEN, N_IN)
+        b1 = p[nw1:nw1 + N_HIDDEN]
+        W1f = W1 / self.x_std.astype(np.float64)
+        b1f = b1 - W1f @ self.x_mean.astype(np.float64)
+        out = p.copy()
+        out[:nw1] = W1f.ravel()
+        out[nw1:nw1 + N_HIDDEN] = b1f
+        return out.astype(np.float32)
+
+    def device_params(self, folded: bool = True):
+        """A device tensor holding the parameters the solver takes."""
+        torch = _torch()
+        if not folded:
+            return self.params
+        return torch.from_numpy(self.folded_params()).to(self._dev)
+
     # -- persistence ---------------------------------------------------------
     def save(self, path: Path | str = WEIGHTS, **meta):
-        np.savez(path, params=self.params_host(), x_mean=self.x_mean, x_std=self.x_std,
-                 **{k: np.asarray(v) for k, v in meta.items()})
+        np.savez(path, params=self.params_host(), folded=self.folded_params(), x_mean=self.x_mean,
+                 x_std=self.x_std, **{k: np.asarray(v) for k, v in meta.items()})
 
     @classmethod
     def load(cls, path: Path | str = WEIGHTS, ctx: Context | None = None) -> "OrderMLP":
         z = np.load(path)
         return cls(z["params"], ctx=ctx, x_mean=z["x_mean"], x_std=z["x_std"])
+
+
+def _f64(a, cols):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, cols)) if cols else \
+        np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def features(src, q, targets=None, tree_depth: int = 10, max_leaf: int = 64, ctx: Context | None = None):
+    """Per-leaf features [n_leaves][16] of the adaptive tree and the leaf of
+    every input particle (targets first, then sources)."""
+    ctx = ctx or default_context(0)
+    src, q = _f64(src, 3), _f64(q, 0)
+    tgt = None if targets is None else _f64(targets, 3)
+    nt = 0 if tgt is None else len(tgt)
+    opts = LfmmSolveOpts(0, tree_depth, max_leaf, 1, 1e-8)
+    cap = (len(src) + nt) + 1
+    feats = np.zeros((cap, N_IN), np.float32)
+    leaf_of = np.zeros(len(src) + nt, np.int32)
+    nl = ctypes.c_size_t()
+    ctx.check(ctx.lib.lfmm3d_features(ctx.handle, len(src), _p(src), _p(q), nt, _p(tgt), ctypes.byref(opts),
+                                      _p(feats), cap, _p(leaf_of), ctypes.byref(nl)), "lfmm3d_features")
+    return feats[:nl.value].copy(), leaf_of
+
+
+def load_params(path: Path | str = WEIGHTS) -> np.ndarray:
+    """The trained network (input normalisation folded in) shipped with the package."""
+    return np.load(path)["folded"].astype(np.float32)
+
+
+class LearnedSolver:
+    """3D solve at the order the network picks for a tolerance, with the
+    fixed-order fallback judged by a sampled FP64 direct-sum check."""
+
+    def __init__(self, params: np.ndarray | None = None, ctx: Context | None = None):
+        torch = _torch()
+        self.ctx = ctx or default_context(0)
+        p = load_params() if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        self.d_params = torch.from_numpy(p).to(torch.device("cuda", self.ctx.device))
+
+    def solve(self, src, q, targets=None, tol: float = 1e-6, tree_depth: int = 10, max_leaf: int = 64,
+              precision: str = "mixed", check_targets: int = 256, stats: bool = False):
+        src, q = _f64(src, 3), _f64(q, 0)
+        tgt = None if targets is None else _f64(targets, 3)
+        nt = 0 if tgt is None else len(tgt)
+        nout = nt if nt else len(src)
+        pot = np.zeros(nout)
+        fld = np.zeros((nout, 3))
+        opts = LfmmSolveOpts(0, tree_depth, max_leaf, PRECISION[precision], tol)
+        info = LfmmLearnedInfo()
+        st = LfmmStats()
+        _torch().cuda.synchronize(self.d_params.device)
+        self.ctx.check(self.ctx.lib.lfmm3d_solve_learned(
+            self.ctx.handle, len(src), _p(src), _p(q), nt, _p(tgt), ctypes.byref(opts),
+            ctypes.c_void_p(self.d_params.data_ptr()), tol, check_targets, _p(pot), _p(fld), ctypes.byref(info),
+            ctypes.byref(st) if stats else None), "lfmm3d_solve_learned")
+        out = {"potentials": pot, "forces": fld, "info": info.as_dict()}
+        if stats:
+            out["stats"] = st.as_dict()
+        return out

@@ -1,0 +1,200 @@
+"""Train the order-selection network on (feature, measured error) pairs that
+the FMM generates itself, on the GPU.
+
+    python -m laplace_fmm_b200.train_order [--train 512] [--heldout 64]
+
+Problems: 1-8 isotropic Gaussian clusters (sigma log-uniform in [0.005, 0.2],
+centres uniform in the unit cube), N log-uniform in [1e4, 1e6], charges
+uniform in [-1, 1]; plus larger ones (1e6-8e6 particles, Gaussian clusters or
+a Plummer sphere in a uniform background) so that the network covers
+millions of particles; adaptive octree (<= 10 levels, <= 64 per leaf).  Each
+problem is labelled by solving it (mixed form) at p = 4, 6, ..., 14 and
+comparing with the FP64 direct sum at 1024 sampled targets: the label of a
+leaf at order p is log10 of the RMS absolute potential error of its sampled
+targets, so that the leaves' labels, weighted by their particle counts and
+divided by the RMS potential (self term removed), give the problem's rel-L2.
+The solver gets that RMS potential from the same sampled direct sum that
+judges its result.  Leaves without a sampled target are masked out.
+
+Training: Adam (lr 1e-3), batches of 4096 leaves, masked mean-squared error,
+all in the library's CUDA kernels.  The held-out problems measure what the
+network gains over the fixed order: the order it picks for tolerance 1e-6,
+the error reached there, and the fastest fixed order that meets the
+tolerance on every training problem.  Writes ``order_mlp.npz`` beside this
+file (parameters with the input normalisation folded in, plus the
+normalisation, the loss curve and the held-out summary).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from ._lib import LfmmSolveOpts, default_context
+from .order import N_OUT, ORDERS, WEIGHTS, LearnedSolver, OrderMLP, features
+from .workloads import gaussian_mix3d, plummer_mix3d
+
+DEPTH, MAX_LEAF, SAMPLES = 10, 64, 1024
+
+
+def problem(i: int, kind: str):
+    """Seeded problem i of a set: 'train' / 'heldout' (1-8 Gaussian clusters,
+    N log-uniform in [1e4, 1e6]) or 'large' (N log-uniform in [1e6, 8e6]:
+    Gaussian clusters, or a Plummer sphere of scale radius log-uniform in
+    [0.02, 0.1] mixed 50/50 with a uniform background)."""
+    base = {"train": 10_000, "heldout": 90_000, "large": 50_000}[kind]
+    g = np.random.default_rng(base + i)
+    if kind != "large":
+        n = int(round(10 ** g.uniform(4.0, 6.0)))
+        return gaussian_mix3d(n, seed=base + i)
+    n = int(round(10 ** g.uniform(6.0, np.log10(8e6))))
+    if i % 2 == 0:
+        return gaussian_mix3d(n, seed=base + i)
+    a = float(10 ** g.uniform(np.log10(0.02), -1.0))
+    return plummer_mix3d(n, seed=base + i, a=a)
+
+
+def solve(ctx, pos, q, N):
+    import ctypes
+    pot = np.zeros(len(pos))
+    fld = np.zeros((len(pos), 3))
+    opts = LfmmSolveOpts(N, DEPTH, MAX_LEAF, 1, 1e-8)
+    vp = ctypes.c_void_p
+    ctx.check(ctx.lib.lfmm3d_solve_ex(ctx.handle, len(pos), pos.ctypes.data_as(vp), q.ctypes.data_as(vp), 0, None,
+                                      ctypes.byref(opts), pot.ctypes.data_as(vp), fld.ctypes.data_as(vp), None),
+              "solve")
+    return pot
+
+
+def direct(ctx, pos, q, idx):
+    import ctypes
+    tgt = np.ascontiguousarray(pos[idx])
+    pot = np.zeros(len(idx))
+    fld = np.zeros((len(idx), 3))
+    vp = ctypes.c_void_p
+    ctx.check(ctx.lib.lfmm3d_direct(ctx.handle, len(pos), pos.ctypes.data_as(vp), q.ctypes.data_as(vp), len(idx),
+                                    tgt.ctypes.data_as(vp), pot.ctypes.data_as(vp), fld.ctypes.data_as(vp)),
+              "direct")
+    return pot
+
+
+def label(ctx, pos, q, seed):
+    """Features, per-leaf labels [leaves][6], mask, and the sampled rel-L2 of
+    the whole problem at each order."""
+    feats, leaf_of = features(pos, q, tree_depth=DEPTH, max_leaf=MAX_LEAF, ctx=ctx)
+    g = np.random.default_rng(seed)
+    idx = np.sort(g.choice(len(pos), min(SAMPLES, len(pos)), replace=False))
+    self_term = q[idx] * 1e4
+    exact = direct(ctx, pos, q, idx) - self_term
+    scale = np.sqrt(np.mean(exact ** 2))           # RMS potential: rel-L2 = RMS error / scale
+    nl = len(feats)
+    T = np.zeros((nl, N_OUT), np.float32)
+    M = np.zeros((nl, N_OUT), np.float32)
+    leaves = leaf_of[idx]
+    counts = np.bincount(leaves, minlength=nl)
+    has = counts > 0
+    err = np.zeros(N_OUT)
+    for k, p in enumerate(ORDERS):
+        e = solve(ctx, pos, q, p + 1)[idx] - self_term - exact      # absolute error
+        err[k] = np.sqrt(np.mean(e ** 2)) / scale
+        ms = np.bincount(leaves, weights=e ** 2, minlength=nl)
+        T[has, k] = 0.5 * np.log10(ms[has] / counts[has] + 1e-30)
+        M[has, k] = 1.0
+    return feats, T, M, err, scale
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=512)
+    ap.add_argument("--heldout", type=int, default=64)
+    ap.add_argument("--large", type=int, default=32, help="extra training problems of 1e6-8e6 particles")
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--quantile", type=float, default=0.7,
+                    help="calibration: the quantile of the training problems' shortfall added to the outputs")
+    ap.add_argument("--data", default=None, help="save the labelled problems here (npz)")
+    ap.add_argument("--out", default=str(WEIGHTS))
+    a = ap.parse_args(argv)
+    ctx = default_context(0)
+    t0 = time.time()
+    data = {"train": [], "heldout": []}
+    for kind, count in (("train", a.train), ("large", a.large), ("heldout", a.heldout)):
+        for i in range(count):
+            pos, q = problem(i, kind)
+            data["heldout" if kind == "heldout" else "train"].append((len(pos),) + label(ctx, pos, q, seed=7 + i))
+    t_label = time.time() - t0
+    if a.data:
+        blob = {}
+        for kind in ("train", "heldout"):
+            for i, (n, feats, T_, M_, err, scale) in enumerate(data[kind]):
+                blob.update({f"{kind}{i}_feats": feats, f"{kind}{i}_T": T_, f"{kind}{i}_M": M_,
+                             f"{kind}{i}_err": err, f"{kind}{i}_scale": np.float64(scale), f"{kind}{i}_n": np.int64(n)})
+        np.savez_compressed(a.data, **blob)
+    X = np.concatenate([d[1] for d in data["train"]])
+    T = np.concatenate([d[2] for d in data["train"]])
+    M = np.concatenate([d[3] for d in data["train"]])
+    keep = M.sum(1) > 0
+    X, T, M = X[keep], T[keep], M[keep]
+    mean, std = X.mean(0), X.std(0) + 1e-6
+    net = OrderMLP(seed=1, ctx=ctx, x_mean=mean, x_std=std)
+    Xn = net.normalise(X)
+    g = np.random.default_rng(3)
+    losses = []
+    for ep in range(a.epochs):
+        perm = g.permutation(len(Xn))
+        tot = 0.0
+        for b in range(0, len(perm), a.batch):
+            j = perm[b:b + a.batch]
+            tot += net.train_step(Xn[j], T[j], M[j], lr=a.lr) * len(j)
+        losses.append(tot / len(perm))
+    t_train = time.time() - t0 - t_label
+    # calibration: the network's problem-level prediction against the measured
+    # rel-L2 of every training problem near the tolerance; the 90th percentile
+    # of the shortfall is added to the outputs (folded into their biases)
+    res = []
+    for n, feats, T_t, M_t, err, scale in data["train"]:
+        pred = net.predicted_log10(feats) - np.log10(scale)
+        for k in range(N_OUT):
+            if 1e-3 * a.tol <= err[k] <= 1e3 * a.tol:
+                res.append(np.log10(err[k]) - pred[k])
+    delta = float(np.quantile(res, a.quantile)) if res else 0.0
+    net.shift_outputs(delta)
+    # held-out: the learned solve (with its sampled check and fallback) against
+    # the fixed order that meets the tolerance on every training problem
+    fixed = next((p for k, p in enumerate(ORDERS) if all(d[4][k] <= a.tol for d in data["train"])), ORDERS[-1])
+    solver = LearnedSolver(net.folded_params(), ctx=ctx)
+    picked, first_ok, final_ok, best, t_learned, t_fixed = [], 0, 0, [], 0.0, 0.0
+    for i, (n, feats, T_h, M_h, err, scale) in enumerate(data["heldout"]):
+        pos, q = problem(i, "heldout")
+        solve(ctx, pos, q, fixed + 1)                        # warm the operator caches
+        s0 = time.perf_counter()
+        r = solver.solve(pos, q, tol=a.tol, tree_depth=DEPTH, max_leaf=MAX_LEAF, check_targets=256)
+        s1 = time.perf_counter()
+        solve(ctx, pos, q, fixed + 1)
+        s2 = time.perf_counter()
+        t_learned += s1 - s0
+        t_fixed += s2 - s1
+        info = r["info"]
+        picked.append(info["predicted_N"] - 1)
+        first_ok += int(not info["fallback"])
+        final_ok += int(info["checked_error"] <= a.tol)
+        best.append(next((pp for k, pp in enumerate(ORDERS) if err[k] <= a.tol), ORDERS[-1]))
+    summary = {"train_problems": a.train, "large_problems": a.large, "heldout_problems": a.heldout,
+               "leaves": int(len(X)),
+               "loss_first": losses[0], "loss_last": losses[-1], "label_s": t_label, "train_s": t_train,
+               "calibration_log10": delta, "calibration_residuals": len(res),
+               "fixed_p_all_train": fixed, "heldout_mean_p_picked": float(np.mean(picked)),
+               "heldout_mean_p_best_even": float(np.mean(best)), "heldout_no_fallback": first_ok,
+               "heldout_within_tol": final_ok, "heldout_s_learned": t_learned, "heldout_s_fixed": t_fixed}
+    net.save(a.out, losses=np.array(losses), summary=json.dumps(summary))
+    print(json.dumps(summary))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

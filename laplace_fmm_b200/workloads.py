@@ -99,3 +99,24 @@ def sample_targets(n: int, k: int = 4096, seed: int = 777):
 def rel_l2(x, ref):
     x = np.asarray(x); ref = np.asarray(ref)
     return float(np.linalg.norm((x - ref).ravel()) / np.linalg.norm(ref.ravel()))
+
+
+def batch3d(count: int = 1024, seed: int = 5150, nmin: int = 2048, nmax: int = 262144, sigma: float = 0.05):
+    """Uneven independent problems: sizes log-uniform in [nmin, nmax], each
+    uniform in its own unit cube or one Gaussian cluster (sigma) with equal
+    probability, charges uniform in [-1, 1].  Returns a list of (pos, q)."""
+    g = _rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(np.exp(g.uniform(np.log(nmin), np.log(nmax)))))
+        if g.random() < 0.5:
+            pos = g.random((n, 3))
+        else:
+            c = g.uniform(0.2, 0.8, 3)
+            pos = np.empty((0, 3))
+            while len(pos) < n:
+                p = c + sigma * g.standard_normal((2 * (n - len(pos)) + 16, 3))
+                pos = np.concatenate([pos, p[_in_open_cube(p, 3)]])
+            pos = pos[:n]
+        out.append((pos, g.uniform(-1.0, 1.0, n)))
+    return out

@@ -1,0 +1,57 @@
+"""Batched solves: a forest of independent problems (each its own box and
+root) solved together must give each problem the result it gets alone on
+the same tree, and match the FP64 direct sum."""
+import numpy as np
+import pytest
+
+from laplace_fmm_b200 import FastMultipole3d, compute_exact, InteractionType, solve_batch
+from laplace_fmm_b200.workloads import batch3d, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def noself(p, q):
+    return p - q * 1e4
+
+
+@pytest.fixture(scope="module")
+def problems():
+    ps = batch3d(10, seed=77, nmin=1500, nmax=60000)
+    g = np.random.default_rng(3)
+    # a single particle, an empty problem and a shifted, scaled copy
+    ps.insert(3, (g.random((1, 3)), np.array([0.5])))
+    ps.insert(5, (np.zeros((0, 3)), np.zeros(0)))
+    p, q = ps[0]
+    ps.append((p * 37.0 - 5.0, q))
+    return ps
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-6), ("fp64", 1e-12)])
+def test_batch_matches_single_solves(ctx, problems, precision, tol):
+    out = solve_batch(problems, N=11, tree_depth=8, max_leaf=64, precision=precision, ctx=ctx)
+    assert len(out) == len(problems)
+    for (pos, q), (pot, fld) in zip(problems, out):
+        assert len(pot) == len(pos)
+        if len(pos) < 2:
+            continue
+        f = FastMultipole3d((pos, q), N=11, tree_depth=8, max_leaf=64, precision=precision, ctx=ctx)
+        assert rel_l2(noself(pot, q), noself(f.potentials, q)) < tol
+        assert rel_l2(fld, f.forces) < tol
+
+
+def test_single_particle_gets_its_self_term(ctx, problems):
+    out = solve_batch(problems, N=9, tree_depth=8, max_leaf=64, ctx=ctx)
+    pot, fld = out[3]
+    assert pot[0] == pytest.approx(0.5 * 1e4) and np.all(fld == 0)
+
+
+def test_batch_accuracy_vs_direct(ctx, problems):
+    out = solve_batch(problems, N=13, tree_depth=8, max_leaf=64, ctx=ctx)
+    for k in (0, 2, 4):
+        pos, q = problems[k]
+        idx = np.arange(0, len(pos), max(1, len(pos) // 500))
+        pe = compute_exact(InteractionType.Potential3d, (pos, q), pos[idx], ctx=ctx)
+        fe = compute_exact(InteractionType.Force3d, (pos, q), pos[idx], ctx=ctx)
+        pot, fld = out[k]
+        assert rel_l2(noself(pot[idx], q[idx]), noself(pe, q[idx])) < 3e-6
+        assert rel_l2(fld[idx], fe) < 1e-5

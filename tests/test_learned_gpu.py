@@ -1,0 +1,95 @@
+"""Learned order selection end to end: per-leaf features, the shipped
+network's order choice, the sampled FP64 check with the fixed-order fallback,
+and what the network gains over the fixed order it falls back to."""
+import numpy as np
+import pytest
+
+from laplace_fmm_b200 import FastMultipole3d
+from laplace_fmm_b200.order import WEIGHTS, LearnedSolver, N_PARAMS, features, load_params
+from laplace_fmm_b200.workloads import gaussian_mix3d, rel_l2, uniform3d
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def noself(p, q):
+    return p - q * 1e4
+
+
+def test_features_and_leaf_map(ctx):
+    src, q = gaussian_mix3d(60000, seed=5)
+    feats, leaf_of = features(src, q, tree_depth=10, max_leaf=64, ctx=ctx)
+    nl = len(feats)
+    assert feats.shape == (nl, 16) and np.all(np.isfinite(feats))
+    assert leaf_of.min() >= 0 and leaf_of.max() < nl
+    counts = np.bincount(leaf_of, minlength=nl)
+    assert np.all(counts >= 1) and counts.max() <= 64
+    np.testing.assert_allclose(10.0 ** feats[:, 0] - 1.0, counts, rtol=1e-5)
+
+
+@pytest.fixture(scope="module")
+def solver(ctx):
+    if not WEIGHTS.exists():
+        pytest.skip("trained network not present")
+    return LearnedSolver(ctx=ctx)
+
+
+@pytest.mark.parametrize("seed", [90001, 90002, 90003])
+def test_learned_solve_within_tolerance(solver, ctx, seed):
+    src, q = gaussian_mix3d(120000, seed=seed)
+    r = solver.solve(src, q, tol=TOL, check_targets=2048)
+    info = r["info"]
+    assert 5 <= info["order_N"] <= 15
+    assert 0 <= info["checked_error"] <= TOL
+    # the same order through the plain entry point: identical arithmetic
+    f = FastMultipole3d((src, q), N=info["order_N"], tree_depth=10, max_leaf=64, precision="mixed", ctx=ctx)
+    assert rel_l2(noself(r["potentials"], q), noself(f.potentials, q)) < 1e-12
+    assert rel_l2(r["forces"], f.forces) < 1e-12
+
+
+def test_checked_error_is_the_sampled_rel_l2(solver, ctx):
+    """The reported check equals the rel-L2 at the evenly spaced sample
+    outputs recomputed with the exact FP64 direct sum."""
+    from laplace_fmm_b200 import InteractionType, compute_exact
+    src, q = gaussian_mix3d(50000, seed=90021)
+    m = 300
+    r = solver.solve(src, q, tol=TOL, check_targets=m)
+    idx = np.arange(m) * (len(src) // m)
+    pe = compute_exact(InteractionType.Potential3d, (src, q), src[idx], ctx=ctx) - q[idx] * 1e4
+    fe = compute_exact(InteractionType.Force3d, (src, q), src[idx], ctx=ctx)
+    ep = rel_l2(r["potentials"][idx] - q[idx] * 1e4, pe)
+    ef = rel_l2(r["forces"][idx], fe)
+    assert r["info"]["checked_error"] == pytest.approx(ep, rel=1e-6)
+    assert r["info"]["checked_error_field"] == pytest.approx(ef, rel=1e-6)
+
+
+def test_fallback_replaces_a_bad_prediction(ctx):
+    """A network that predicts negligible error at every order picks p = 4;
+    the sampled check catches it and the solve is rerun at N = 15."""
+    bad = np.zeros(N_PARAMS, np.float32)
+    bad[-6:] = -30.0                       # output biases: log10 error = -30 everywhere
+    s = LearnedSolver(bad, ctx=ctx)
+    src, q = uniform3d(80000, seed=11)
+    r = s.solve(src, q, tol=TOL, tree_depth=10, max_leaf=64, check_targets=1024)
+    info = r["info"]
+    assert info["predicted_N"] == 5 and info["fallback"] == 1 and info["order_N"] == 15
+    assert info["checked_error"] <= TOL
+
+
+def test_gain_over_fixed_order(solver, ctx):
+    """Held-out problems: the network's order stays within the tolerance (after
+    the check) at a lower order than the fixed fallback on average."""
+    picked = []
+    for seed in (90010, 90011, 90012, 90013):
+        src, q = gaussian_mix3d(150000, seed=seed)
+        r = solver.solve(src, q, tol=TOL, check_targets=1024)
+        assert r["info"]["checked_error"] <= TOL
+        picked.append(r["info"]["order_N"])
+    assert np.mean(picked) < 15
+
+
+def test_shipped_weights_have_the_kernel_layout():
+    if not WEIGHTS.exists():
+        pytest.skip("trained network not present")
+    p = load_params()
+    assert p.shape == (N_PARAMS,) and np.all(np.isfinite(p))
