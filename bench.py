@@ -655,7 +655,8 @@ def main():
             "config": base_config(cfg, world), "accuracy": r["acc"], "phases_ms": {
                 k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves", "ms_total",
                                       "ms_m2l_kernel")},
-            "tree": {k: stats[k] for k in ("n_cells", "n_leaves", "n_far_pairs", "n_close_pairs", "n_p2p_pairs")},
+            "tree": {k: stats[k] for k in ("n_cells", "n_leaves", "n_far_pairs", "n_close_pairs", "n_p2p_pairs",
+                                           "n_m2p", "n_w", "n_x")},
             "roofline": roofline(cfg, stats, peaks, fp64, fp32, tf32),
             "roofline_leaves": roofline(cfg, stats, peaks, fp64, fp32, tf32, phase="leaves"),
             "fp64_peak_tflops_measured": fp64, "fp32_peak_tflops_measured": fp32, "tf32_peak_tflops_measured": tf32,

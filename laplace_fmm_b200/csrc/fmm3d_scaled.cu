@@ -13,17 +13,24 @@ using namespace scaled;
 
 namespace {
 
-bool g_scaled_const_ready = false;
+bool g_scaled_const_ready[64] = {};
 
 int upload_scaled_constants(Context& ctx)
 {
-	if (g_scaled_const_ready) return OK;
+	if (ctx.device < 0 || ctx.device >= 64) { ctx.last_error = "device index above 63"; return ERR_ARG; }
+	if (g_scaled_const_ready[ctx.device]) return OK;
 	unsigned char n_of[NX2MAX], m_of[NX2MAX];
 	for (int n = 0; n < MAXN3; ++n)
 		for (int m = 0; m <= n; ++m) { n_of[tix(n, m)] = (unsigned char)n; m_of[tix(n, m)] = (unsigned char)m; }
+	float inv_f[NINV];
+	double inv_d[NINV];
+	inv_f[0] = 0.f; inv_d[0] = 0.0;
+	for (int k = 1; k < NINV; ++k) { inv_d[k] = 1.0 / k; inv_f[k] = 1.0f / (float)k; }
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_n_of, n_of, sizeof(n_of)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_m_of, m_of, sizeof(m_of)));
-	g_scaled_const_ready = true;
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_f, inv_f, sizeof(inv_f)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_d, inv_d, sizeof(inv_d)));
+	g_scaled_const_ready[ctx.device] = true;
 	return OK;
 }
 

@@ -19,6 +19,12 @@ constexpr int WPB = 4;
 
 __constant__ unsigned char c_n_of[NX2MAX];
 __constant__ unsigned char c_m_of[NX2MAX];
+constexpr int NINV = 64;
+__constant__ float c_inv_f[NINV];      // 1 / k (k >= 1), rounded to FP32
+__constant__ double c_inv_d[NINV];     // 1 / k, FP64
+template <typename real> __device__ __forceinline__ real inv_of(int k);
+template <> __device__ __forceinline__ float inv_of<float>(int k) { return c_inv_f[k]; }
+template <> __device__ __forceinline__ double inv_of<double>(int k) { return c_inv_d[k]; }
 
 template <typename real> struct V2;
 template <> struct V2<double> { using t = double2; static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); } };
@@ -340,25 +346,32 @@ __device__ void eval_expansion(const typename V2<real>::t* __restrict__ Lc, real
 	dec_to_sph<real>(dx, dy, dz, r, th, ph);
 	real y, x;
 	sc<real>(th, &y, &x);
-	const real ir = real(1) / r;
+	const real ir = real(1) / r, iy = real(1) / y;
 	real phi = 0, mt0 = 0, mt1 = 0, mt2 = 0;
+	real s1, c1;
+	sc<real>(ph, &s1, &c1);
+	real cm_ = 1, sm_ = 0;           // cos(m phi), sin(m phi) by the angle-addition recurrence
 	// LOCAL: rn = r^(n-1) ; MULTI: rn = r^-(n+2)
 	real Pmm = 1, rpow = LOCAL ? ir : ir * ir;
 	for (int m = 0; m < N; ++m) {
-		if (m > 0) { Pmm = Pmm * y * (real)(1 - 2 * m); rpow *= LOCAL ? r : ir; }
-		real sm_, cm_;
-		sc<real>(m * ph, &sm_, &cm_);
+		if (m > 0) {
+			Pmm = Pmm * y * (real)(1 - 2 * m);
+			rpow *= LOCAL ? r : ir;
+			const real cn = cm_ * c1 - sm_ * s1;
+			sm_ = sm_ * c1 + cm_ * s1;
+			cm_ = cn;
+		}
 		const real mult = m ? real(2) : real(1);
 		real Pn = Pmm, Pn1 = 0, rn = rpow;
 		for (int n = m; n < N; ++n) {
 			real Pnext = (n == m) ? Pmm * x * (real)(2 * n + 1)
-			                      : ((real)(2 * n + 1) * x * Pn - (real)(n + m) * Pn1) / (real)(n + 1 - m);
+			                      : ((real)(2 * n + 1) * x * Pn - (real)(n + m) * Pn1) * inv_of<real>(n + 1 - m);
 			real K = knm[tix(n, m)];
 			real Yr = Pn * cm_ * K, Yi = Pn * sm_ * K;
 			typename V2<real>::t A = Lc[tix(n, m)];
 			real cr = A.x * rn, ci = A.y * rn;
 			real ycr = Yr * cr - Yi * ci;                 // Re(Y A) r^(n-1) or r^-(n+2)
-			real gq = K * ((real)(1 - m + n) * Pnext - (real)(n + 1) * x * Pn) / y;
+			real gq = K * ((real)(1 - m + n) * Pnext - (real)(n + 1) * x * Pn) * iy;
 			if (LOCAL) {
 				phi += mult * (r * ycr);
 				mt0 -= mult * ((real)n * ycr);
@@ -372,10 +385,9 @@ __device__ void eval_expansion(const typename V2<real>::t* __restrict__ Lc, real
 		}
 	}
 	pot = phi;
-	real s2, c2;
-	sc<real>(ph, &s2, &c2);
-	fx = mt0 * y * c2 + mt1 * x * c2 - mt2 * s2 / y;
-	fy = mt0 * y * s2 + mt1 * x * s2 + mt2 * c2 / y;
+	const real s2 = s1, c2 = c1;
+	fx = mt0 * y * c2 + mt1 * x * c2 - mt2 * s2 * iy;
+	fy = mt0 * y * s2 + mt1 * x * s2 + mt2 * c2 * iy;
 	fz = mt0 * x - mt1 * y;
 }
 

@@ -77,15 +77,18 @@ def test_fallback_replaces_a_bad_prediction(ctx):
 
 
 def test_gain_over_fixed_order(solver, ctx):
-    """Held-out problems: the network's order stays within the tolerance (after
-    the check) at a lower order than the fixed fallback on average."""
+    """The first held-out problems of the training script (never trained on):
+    after the check every solve is within the tolerance, at a lower order on
+    average than the fixed order the network replaces (N = 15, the lowest
+    fixed order that meets 1e-6 on every training problem)."""
+    from laplace_fmm_b200.train_order import problem
     picked = []
-    for seed in (90010, 90011, 90012, 90013):
-        src, q = gaussian_mix3d(150000, seed=seed)
+    for i in range(8):
+        src, q = problem(i, "heldout")
         r = solver.solve(src, q, tol=TOL, check_targets=1024)
         assert r["info"]["checked_error"] <= TOL
         picked.append(r["info"]["order_N"])
-    assert np.mean(picked) < 15
+    assert np.mean(picked) < 15 and min(picked) <= 14
 
 
 def test_shipped_weights_have_the_kernel_layout():
