@@ -79,6 +79,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the mixed one")
     ap.add_argument("--no-learned", action="store_true", help="mixed form at the fixed order N instead of the learned one")
+    ap.add_argument("--no-plan", action="store_true", help="skip timing repeated solves through a solve plan")
     ap.add_argument("--max-leaf", type=int, default=None, help="override the adaptive split threshold (0: uniform)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None, help="override the configuration's")
     ap.add_argument("--order", type=int, default=None, help="override N (degrees)")
@@ -352,6 +353,28 @@ def run_ours(args, cfg, rank, world, local_rank):
         pms = t0.elapsed_time(t1) / reps
         plain = {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms, "precision": "fp64"}
     ctx_t.close()
+    # a solve plan at the same order: the tree and a CUDA graph built once,
+    # charges changed per execution (device buffers)
+    plan_line = None
+    if dim == 3 and max_leaf > 0 and not args.no_plan:
+        Nplan = stats.get("order_N") or N
+        hp = ctypes.c_void_p()
+        popts = LfmmSolveOpts(Nplan, depth, max_leaf, prec, 1e-8)
+        ctx.check(L.lfmm3d_plan_create(ctx.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), ctypes.byref(popts),
+                                       ctypes.byref(hp)), "plan")
+        for _ in range(max(1, args.warmup)):
+            ctx.check(L.lfmm3d_plan_execute(hp, vp(d_q.data_ptr()), vp(d_pot.data_ptr()), vp(d_fld.data_ptr())), "plan")
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            ctx.check(L.lfmm3d_plan_execute(hp, vp(d_q.data_ptr()), vp(d_pot.data_ptr()), vp(d_fld.data_ptr())), "plan")
+        p1.record(stream)
+        p1.synchronize()
+        pl_ms = p0.elapsed_time(p1) / args.steps
+        L.lfmm3d_plan_destroy(hp)
+        plan_line = {"value": world * n / (pl_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pl_ms,
+                     "N_degrees": Nplan, "what": "repeated solves on one geometry: tree and CUDA graph built once"}
     # accuracy on 4096 seeded targets against the FP64 direct sum (on the GPU)
     idx = sample_targets(n)
     tgt = torch.from_numpy(np.ascontiguousarray(pos[idx])).cuda()
@@ -398,7 +421,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
                "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
     return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx,
-                plain=plain, learned=dict(info_box) if learned else None)
+                plain=plain, learned=dict(info_box) if learned else None, plan=plan_line)
 
 
 def m2l_flops(N):
@@ -669,6 +692,8 @@ def main():
             line["config"]["N_degrees"] = r["learned"]["order_N"]
             line["config"]["order_p"] = r["learned"]["order_N"] - 1
             line["config"]["plain_fp64_N_degrees"] = cfg["N"]
+        if r["plan"]:
+            line["plan_execute"] = r["plan"]
         if r["plain"]:
             line["plain_fp64"] = r["plain"]
             line["speedup_vs_plain_fp64"] = r["plain"]["ms_per_step"] / r["ms"]

@@ -140,6 +140,23 @@ int lfmm3d_solve_batch_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, 
                               const double* src_q, const lfmm_solve_opts* opts, double* pot, double* field,
                               lfmm_stats* stats);
 
+/* ---- solve plans: one geometry, many charge vectors (no counterpart in the
+ * reference, which rebuilds the tree on every solve) ------------------------
+ * lfmm3d_plan_create builds the tree of the positions once (device buffers;
+ * opts as for lfmm3d_solve_ex, N given explicitly, N <= 15), warms every
+ * cache and captures the FMM passes in a CUDA graph on the context's stream.
+ * lfmm3d_plan_execute (device buffers, input order, n_src each) enqueues: copy
+ * the charges in, launch the graph, copy potential and field out; the results
+ * are complete once the context's stream is synchronised.  The tree keeps the
+ * creation charges' split into sources and zero-charge targets; later charges
+ * only change values.  The plan uses the context's stream and operator cache:
+ * destroy it before the context; executions of one plan must not overlap. */
+typedef struct lfmm_plan lfmm_plan;
+int lfmm3d_plan_create(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q,
+                       const lfmm_solve_opts* opts, lfmm_plan** plan);
+int lfmm3d_plan_execute(lfmm_plan* plan, const double* src_q, double* pot, double* field);
+void lfmm3d_plan_destroy(lfmm_plan* plan);
+
 /* ---- 2D ---------------------------------------------------------------- */
 int lfmm2d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
                  const double* tgt_xy, int N, int tree_depth, double eps, int precision, double* pot,

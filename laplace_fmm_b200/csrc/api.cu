@@ -325,6 +325,7 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	// levels and SIMT GEMMs elsewhere; simt = SIMT GEMMs only; rotation =
 	// per-pair rotations on the plain path
 	c.m2l_engine = 3;
+	if (const char* e = std::getenv("LFMM_M2L_TUNE")) c.tune_m2l = std::strcmp(e, "0") != 0;
 	if (const char* e = std::getenv("LFMM_M2L"))
 		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 0 : 3);
 	int ndev = 0;

@@ -2,6 +2,7 @@
 #pragma once
 #include "common.cuh"
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace lfmm {
@@ -19,6 +20,16 @@ public:
 	size_t capacity() const { return cap_; }
 	size_t high_water() const { return high_; }
 	void release();
+	// position in the block; rewind(mark()) replays the same addresses while
+	// no extra chunk was taken in between (chunks() unchanged)
+	size_t mark() const { return used_; }
+	void rewind(size_t m) { used_ = m; }
+	size_t chunks() const { return extra_.size(); }
+	void swap(Arena& o)
+	{
+		std::swap(base_, o.base_); std::swap(cap_, o.cap_); std::swap(used_, o.used_);
+		std::swap(high_, o.high_); std::swap(extra_total_, o.extra_total_); extra_.swap(o.extra_);
+	}
 private:
 	char* base_ = nullptr;
 	size_t cap_ = 0, used_ = 0, high_ = 0, extra_total_ = 0;
@@ -66,6 +77,7 @@ struct OpCacheEntry {
 	void* ptr = nullptr;
 	size_t bytes = 0;
 	unsigned long long stamp = 0;
+	int pinned = 0;                   // > 0: a captured graph reads it (never evicted)
 };
 
 struct Context {
@@ -83,6 +95,10 @@ struct Context {
 	cudaEvent_t ev[16] = {};
 	cudaEvent_t kev[32] = {};          // pairs around the tensor-core M2L launches (timing)
 	int kev_used = 0;
+	// M2L autotuner: slot split chosen per (operator rows, level-size bucket);
+	// 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0): the fixed rule.
+	int m2l_split[257][33] = {};
+	int tune_m2l = 1;
 	int timing = 0;
 };
 

