@@ -103,6 +103,23 @@ def parse():
     return a
 
 
+def max_over_ranks(value: float, dist, device="cuda") -> float:
+    """The largest value over the ranks (device time of the slowest rank);
+    the value itself on one process."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank: int, world: int, ms: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank
+    processes its own copy of the workload (replicas, weak scaling)."""
+    return world * units_per_rank / (ms * 1e-3) / 1e6
+
+
 def make_particles(cfg):
     from laplace_fmm_b200 import workloads as W
     return getattr(W, cfg["gen"])(cfg["n"], seed=cfg["seed"])
@@ -323,11 +340,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps, dist)
     # per-phase split (separate timed solve with phase events)
     ctx_t = Context(local_rank, timing=True)
     st = LfmmStats()
@@ -412,12 +425,8 @@ def run_ours(args, cfg, rank, world, local_rank):
             e.record(stream)
             e.synchronize()
             tot += s.elapsed_time(e)
-        e2e_ms = tot / args.steps
-        if dist:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        e2e = {"value": world * n / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": e2e_ms,
+        e2e_ms = max_over_ranks(tot / args.steps, dist)
+        e2e = {"value": aggregate_rate(n, world, e2e_ms), "unit": "Mparticles/s", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
                "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
     return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx,
@@ -671,7 +680,7 @@ def main():
         stats = r["stats"]
         radix_passes = (cfg["dim"] * (cfg["depth"] - 1) + 7) // 8
         line = {
-            "metric": METRIC, "value": world * cfg["n"] / (r["ms"] * 1e-3) / 1e6, "unit": "Mparticles/s",
+            "metric": METRIC, "value": aggregate_rate(cfg["n"], world, r["ms"]), "unit": "Mparticles/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if cfg["precision"] == "fp64" else "f32/tf32", "data": "synthetic (seeded PCG64)",
