@@ -59,10 +59,11 @@ CONFIGS = {
     # as one batch (mixed, N = 14); the plain FP64 form (p = 10, N = 11) one problem
     # at a time beside it
     "c5": dict(dim=3, batch=True, count=1024, seed=5150, N=14, plain_N=11, depth=10, max_leaf=64,
-               precision="mixed", n=0,
+               precision="mixed", n=0, learned=True, tol=1e-6, check_targets=32,
                workload="batched 3D: 1024 problems, N log-uniform in [2048, 262144], uniform or one Gaussian "
-                        "cluster (sigma 0.05) each, mixed precision p=13 (N=14), adaptive octrees (<=10 levels, "
-                        "<=64 per leaf); plain FP64 p=10 one problem at a time beside it"),
+                        "cluster (sigma 0.05) each, mixed precision at the learned order for rel-L2 <= 1e-6 "
+                        "(32 checked outputs per problem), adaptive octrees (<=10 levels, <=64 per leaf); "
+                        "plain FP64 p=10 one problem at a time beside it"),
 }
 DEFAULT_CONFIG = "c3"
 METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
@@ -241,9 +242,14 @@ def tf32_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def launches_per_solve(depth, dim, radix_passes, adaptive, precision):
+def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=False):
     """Kernels the library enqueues for one solve (tree + FMM passes), counted
-    from the launch sites."""
+    from the launch sites; the learned solve adds its features (far strength
+    per level, accumulation per level, leaf features), the network, the
+    prediction sums, the sampled direct sum (split kernel and reduction) and
+    the RMS and error sums.  An ncu launch list of the 16.8M-particle learned
+    solve shows 267-270 launches of the library's kernels per solve."""
+    extra = (1 + (depth - 2) + (depth - 1) + 1 + 1 + 1 + 2 + 1 + 1) if learned else 0
     scan = 3
     tree = 2 + 1 + radix_passes * (1 + scan + 1) + 1 + 1 + scan + 1 + 1
     tree += (depth - 1) * (1 + scan + 1 + 1) + depth + 1
@@ -252,7 +258,7 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision):
         tree += depth + depth * (1 + scan) + depth + 1 + scan + 1 + 1 + lists + 2 + 2 + 3 * scan
         m2l = max(0, depth - 2) * (3 + 1 + 1) + 2 * 2          # plan + GEMM (+ split reduce), FP64 coarse converts
         fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + 1
-        return tree + fmm
+        return tree + fmm + extra
     tree += lists
     if dim == 3:
         fmm = 1 + (depth - 1) + max(0, depth - 2) * 5 + max(0, depth - 3) + 1
@@ -554,7 +560,7 @@ def run_batch(args, cfg):
     plain FP64 form one problem at a time, per-problem accuracy."""
     import torch
     from laplace_fmm_b200 import Context
-    from laplace_fmm_b200._lib import PRECISION, LfmmSolveOpts, LfmmStats
+    from laplace_fmm_b200._lib import PRECISION, LfmmLearnedInfo, LfmmSolveOpts, LfmmStats
     from laplace_fmm_b200.workloads import batch3d, rel_l2
     probs = batch3d(cfg["count"], seed=cfg["seed"])
     sizes = np.array([len(p) for p, _ in probs], dtype=np.uint64)
@@ -571,11 +577,22 @@ def run_batch(args, cfg):
     d_fld = torch.empty(n, 3, dtype=torch.float64, device="cuda")
     stream = torch.cuda.ExternalStream(ctx.stream)
     opts = LfmmSolveOpts(cfg["N"], cfg["depth"], cfg["max_leaf"], PRECISION[cfg["precision"]], 1e-8)
+    learned = bool(cfg.get("learned")) and not args.no_learned
+    info = LfmmLearnedInfo()
+    if learned:
+        from laplace_fmm_b200.order import load_params
+        d_params = torch.from_numpy(load_params()).cuda()
 
     def step():
-        ctx.check(L.lfmm3d_solve_batch_device(ctx.handle, len(probs), offs.ctypes.data_as(vp), vp(d_src.data_ptr()),
-                                              vp(d_q.data_ptr()), ctypes.byref(opts), vp(d_pot.data_ptr()),
-                                              vp(d_fld.data_ptr()), None), "batch")
+        if learned:
+            ctx.check(L.lfmm3d_solve_batch_learned_device(
+                ctx.handle, len(probs), offs.ctypes.data_as(vp), vp(d_src.data_ptr()), vp(d_q.data_ptr()),
+                ctypes.byref(opts), vp(d_params.data_ptr()), cfg["tol"], cfg["check_targets"], vp(d_pot.data_ptr()),
+                vp(d_fld.data_ptr()), ctypes.byref(info), None), "learned batch")
+        else:
+            ctx.check(L.lfmm3d_solve_batch_device(ctx.handle, len(probs), offs.ctypes.data_as(vp),
+                                                  vp(d_src.data_ptr()), vp(d_q.data_ptr()), ctypes.byref(opts),
+                                                  vp(d_pot.data_ptr()), vp(d_fld.data_ptr()), None), "batch")
 
     for _ in range(args.warmup):
         step()
@@ -637,6 +654,9 @@ def run_batch(args, cfg):
             "plain_fp64_one_at_a_time": {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s",
                                          "ms": pms, "N_degrees": cfg["plain_N"]},
             "speedup_vs_plain_fp64": pms / ms, "clocks": clk.summary()}
+    if learned:
+        line["learned_order"] = dict(info.as_dict(), tol=cfg["tol"], check_targets_per_problem=cfg["check_targets"])
+        line["config"]["N_degrees"] = info.order_N
     ctx.close()
     print(json.dumps(line))
     return 0
@@ -694,7 +714,8 @@ def main():
             "fp64_peak_tflops_measured": fp64, "fp32_peak_tflops_measured": fp32, "tf32_peak_tflops_measured": tf32,
             "peaks_source": peaks["source"], "e2e": r["e2e"], "clocks": r["clocks"],
             "gpu_launches": args.steps * launches_per_solve(stats["depth"], cfg["dim"], radix_passes,
-                                                            cfg.get("max_leaf", 0) > 0, cfg["precision"]),
+                                                            cfg.get("max_leaf", 0) > 0, cfg["precision"],
+                                                            learned=bool(r["learned"])),
         }
         if r["learned"]:
             line["learned_order"] = dict(r["learned"], tol=cfg["tol"], check_targets=cfg["check_targets"])

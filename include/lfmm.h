@@ -276,6 +276,16 @@ int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_x
                                 size_t n_tgt, const double* tgt_xyz, const lfmm_solve_opts* opts,
                                 const float* params, double tol, int check_targets, double* pot, double* field,
                                 lfmm_learned_info* info, lfmm_stats* stats);
+/* The batch at the order the network picks for tolerance tol (as
+ * lfmm3d_solve_learned; device buffers): up to check_targets sampled outputs
+ * per problem normalise each problem's prediction and judge its result; the
+ * batch runs at the highest order any problem needs, and reruns at N = 15
+ * when a problem misses tol.  info: the order used, the largest predicted
+ * and checked errors over the problems. */
+int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
+                                      const double* src_q, const lfmm_solve_opts* opts, const float* params,
+                                      double tol, int check_targets, double* pot, double* field,
+                                      lfmm_learned_info* info, lfmm_stats* stats);
 
 /* ---- rotation tables (tests) --------------------------------------------
  * Wigner small-d matrix for table slot `slot` (layout n(n+1)(4n-1)/6 +

@@ -27,7 +27,7 @@ EXPORTS = [
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
     "lfmm3d_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
-    "lfmm3d_solve_batch", "lfmm3d_solve_batch_device",
+    "lfmm3d_solve_batch", "lfmm3d_solve_batch_device", "lfmm3d_solve_batch_learned_device",
     "lfmm3d_plan_create", "lfmm3d_plan_execute", "lfmm3d_plan_destroy",
 ]
 
@@ -115,6 +115,8 @@ def load(path: Path | str = LIB_PATH):
         for f in ("lfmm3d_solve_learned", "lfmm3d_solve_learned_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, D, I, P, P,
                                       ctypes.POINTER(LfmmLearnedInfo), ctypes.POINTER(LfmmStats)]
+        L.lfmm3d_solve_batch_learned_device.argtypes = [P, I, P, P, P, ctypes.POINTER(LfmmSolveOpts), P, D, I, P, P,
+                                                         ctypes.POINTER(LfmmLearnedInfo), ctypes.POINTER(LfmmStats)]
         L.lfmm3d_plan_create.argtypes = [P, SZ, P, P, ctypes.POINTER(LfmmSolveOpts), ctypes.POINTER(P)]
         L.lfmm3d_plan_execute.argtypes = [P, P, P, P]
         L.lfmm3d_plan_destroy.argtypes = [P]

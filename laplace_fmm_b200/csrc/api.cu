@@ -261,9 +261,18 @@ int learned_dev(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, si
 	return OK;
 }
 
+// The learned order for a batch (params == nullptr: the order of opts).
+struct BatchLearned {
+	const float* params = nullptr;
+	double tol = 0.0;
+	int check = 0;
+	lfmm_learned_info* info = nullptr;
+};
+
 // Batched solve on device buffers (see lfmm3d_solve_batch).
 int batch_dev(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src, const double* q,
-              const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+              const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats,
+              const BatchLearned& learned = BatchLearned())
 {
 	Context& c = ctx->c;
 	if (!o || !offsets || nprob < 1 || !pot || !field) { c.last_error = "batch: bad arguments"; return ERR_ARG; }
@@ -289,8 +298,12 @@ int batch_dev(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src
 	ParticleInput in;
 	in.dim = 3; in.ns = n; in.nt = 0; in.src = src; in.srcq = q; in.poff = poff; in.nprob = nprob;
 	SolveStats ss;
-	int st = fmm3d_solve_scaled(c, in, resolve_order(3, o->N, o->eps), resolve_depth(3, o->tree_depth, big),
-	                            o->max_leaf, o->precision, pot, field, stats ? &ss : nullptr);
+	int st = learned.params
+	             ? solve_learned_batch_device(c, in, offsets, resolve_depth(3, o->tree_depth, big), o->max_leaf,
+	                                          o->precision, learned.params, learned.tol, learned.check, pot, field,
+	                                          learned.info, stats ? &ss : nullptr)
+	             : fmm3d_solve_scaled(c, in, resolve_order(3, o->N, o->eps), resolve_depth(3, o->tree_depth, big),
+	                                  o->max_leaf, o->precision, pot, field, stats ? &ss : nullptr);
 	// the host copy of offsets must outlive the async copy
 	LFMM_CUDA(c, cudaStreamSynchronize(c.stream));
 	if (st) return st;
@@ -505,6 +518,23 @@ int lfmm3d_solve_batch(lfmm_ctx* ctx, int nprob, const size_t* offsets, const do
 		st = check_flags(c);
 	}
 	c.arena.settle();
+	return st;
+}
+
+int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int nprob, const size_t* offsets, const double* src,
+                                      const double* q, const lfmm_solve_opts* o, const float* params, double tol,
+                                      int check_targets, double* pot, double* field, lfmm_learned_info* info,
+                                      lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	if (!params) { ctx->c.last_error = "learned batch: null params"; return LFMM_ERR_ARG; }
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	ctx->c.arena.reset();
+	BatchLearned bl;
+	bl.params = params; bl.tol = tol; bl.check = check_targets; bl.info = info;
+	int st = batch_dev(ctx, nprob, offsets, src, q, o, pot, field, stats, bl);
+	if (st == OK) st = check_flags(ctx->c);
+	ctx->c.arena.settle();
 	return st;
 }
 

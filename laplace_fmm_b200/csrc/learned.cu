@@ -205,6 +205,51 @@ __global__ void rms_kernel(const double* __restrict__ ep, size_t stride, size_t 
 	if ((threadIdx.x & 31) == 0) atomicAdd(acc, a);
 }
 
+// Forest: acc[prob * (NO + 1) + k] += w 10^(2 y[k]) per leaf, by the leaf's problem
+__global__ void predict_reduce_forest_kernel(DevTree t, const float* __restrict__ Y, const float* __restrict__ w,
+                                             double* __restrict__ acc)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= t.nleaves) return;
+	const size_t g = (size_t)t.leaves[i];
+	const size_t prob = (size_t)(t.code[g] >> (3 * t.lev[g]));
+	const double wi = w[i];
+	for (int k = 0; k < NO; ++k) atomicAdd(&acc[prob * (NO + 1) + k], wi * exp10(2.0 * fmin((double)Y[i * NO + k], 10.0)));
+	atomicAdd(&acc[prob * (NO + 1) + NO], wi);
+}
+
+__global__ void gather_points_kernel(const double* __restrict__ pts, const uint32_t* __restrict__ idx, size_t m,
+                                     double* __restrict__ out)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= m) return;
+	for (int d = 0; d < 3; ++d) out[3 * i + d] = pts[3 * (size_t)idx[i] + d];
+}
+
+// Forest samples: acc[4 prob + 0..3] += (pot - direct)^2, (direct - self)^2,
+// |dfield|^2, |field|^2; pot == nullptr: only the reference sums (the RMS).
+__global__ void check_forest_kernel(const double* __restrict__ pot, const double* __restrict__ fld,
+                                    const uint32_t* __restrict__ idx, const int32_t* __restrict__ prob, size_t m,
+                                    const double* __restrict__ q, const double* __restrict__ ep,
+                                    const double* __restrict__ ef, double* __restrict__ acc)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= m) return;
+	const size_t j = idx[i];
+	double* a = acc + 4 * (size_t)prob[i];
+	const double r = ep[i] - q[j] / FORCE_EPS;
+	atomicAdd(&a[1], r * r);
+	double f2 = 0.0;
+	for (int k = 0; k < 3; ++k) f2 += ef[3 * i + k] * ef[3 * i + k];
+	atomicAdd(&a[3], f2);
+	if (!pot) return;
+	const double d = pot[j] - ep[i];
+	atomicAdd(&a[0], d * d);
+	double e2 = 0.0;
+	for (int k = 0; k < 3; ++k) { const double e = fld[3 * j + k] - ef[3 * i + k]; e2 += e * e; }
+	atomicAdd(&a[2], e2);
+}
+
 template <typename T>
 T* take(Context& ctx, size_t n) { return static_cast<T*>(ctx.arena.take(sizeof(T) * std::max<size_t>(n, 1))); }
 
@@ -363,6 +408,110 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	}
 	li.checked_error = e[0];
 	li.checked_error_field = e[1];
+	li.order_N = N;
+	if (info) *info = li;
+	return OK;
+}
+
+// Batched learned solve (forest of in.nprob problems, hoff: host offsets).
+int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size_t* hoff, int depth, int max_leaf,
+                               int precision, const float* params, double tol, int check_targets, double* pot,
+                               double* field, lfmm_learned_info* info, SolveStats* stats)
+{
+	if (!params || !(tol > 0.0) || check_targets < 1 || max_leaf < 0) {
+		ctx.last_error = "learned batch: params, tol > 0, check_targets >= 1 required";
+		return ERR_ARG;
+	}
+	const int P = in.nprob;
+	cudaStream_t s = ctx.stream;
+	DevTree t;
+	int st = tree_build_adaptive(ctx, in, depth, max_leaf, t);
+	if (st) return st;
+	// samples: up to check_targets outputs of every problem, evenly spaced
+	std::vector<uint32_t> hidx;
+	std::vector<int32_t> hprob;
+	std::vector<size_t> soff(P + 1, 0);
+	for (int k = 0; k < P; ++k) {
+		const size_t nk = hoff[k + 1] - hoff[k];
+		const size_t mk = std::min<size_t>((size_t)check_targets, nk);
+		for (size_t j = 0; j < mk; ++j) { hidx.push_back((uint32_t)(hoff[k] + j * (nk / mk))); hprob.push_back(k); }
+		soff[k + 1] = hidx.size();
+	}
+	const size_t m = hidx.size();
+	uint32_t* idx = take<uint32_t>(ctx, m);
+	int32_t* prob = take<int32_t>(ctx, m);
+	double* sp = take<double>(ctx, 3 * m);
+	double* ep = take<double>(ctx, m);
+	double* ef = take<double>(ctx, 3 * m);
+	double* acc = take<double>(ctx, 4 * (size_t)P);
+	double* accp = take<double>(ctx, (size_t)(NO + 1) * P);
+	if (!idx || !prob || !sp || !ep || !ef || !acc || !accp) { ctx.last_error = "learned batch: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemcpyAsync(idx, hidx.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice, s));
+	LFMM_CUDA(ctx, cudaMemcpyAsync(prob, hprob.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice, s));
+	gather_points_kernel<<<div_up(m, 256), 256, 0, s>>>(in.src, idx, m, sp);
+	for (int k = 0; k < P; ++k) {
+		const size_t mk = soff[k + 1] - soff[k];
+		if (!mk) continue;
+		if ((st = direct_device(ctx, 3, hoff[k + 1] - hoff[k], in.src + 3 * hoff[k], in.srcq + hoff[k], mk,
+		                        sp + 3 * soff[k], ep + soff[k], ef + 3 * soff[k], /*fast=*/true)))
+			return st;
+	}
+	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
+	check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(nullptr, nullptr, idx, prob, m, in.srcq, ep, ef, acc);
+	// per-problem predictions
+	const size_t nl = t.nleaves;
+	float* feats = take<float>(ctx, nl * NF);
+	float* w = take<float>(ctx, nl);
+	float* Y = take<float>(ctx, nl * NO);
+	if (!feats || !w || !Y) { ctx.last_error = "learned batch: allocation failed"; return ERR_OOM; }
+	if ((st = features_device(ctx, t, feats, w))) return st;
+	if ((st = mlp_forward_device(ctx, params, (int)nl, feats, Y))) return st;
+	LFMM_CUDA(ctx, cudaMemsetAsync(accp, 0, sizeof(double) * (NO + 1) * P, s));
+	predict_reduce_forest_kernel<<<div_up(std::max<size_t>(nl, 1), 256), 256, 0, s>>>(t, Y, w, accp);
+	std::vector<double> ha(4 * (size_t)P), hp((size_t)(NO + 1) * P);
+	LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
+	LFMM_CUDA(ctx, cudaMemcpyAsync(hp.data(), accp, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, s));
+	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+	int N = 5;
+	double pred = 0.0;
+	for (int k = 0; k < P; ++k) {
+		const size_t mk = soff[k + 1] - soff[k];
+		if (!mk || hp[(size_t)k * (NO + 1) + NO] <= 0.0) continue;
+		const double rms = std::sqrt(ha[4 * (size_t)k + 1] / (double)mk);
+		if (!(rms > 0.0)) continue;    // nothing but self terms (one particle): no far-field error
+		double e[NO];
+		for (int j = 0; j < NO; ++j)
+			e[j] = 0.5 * std::log10(std::max(hp[(size_t)k * (NO + 1) + j], 1e-300) / hp[(size_t)k * (NO + 1) + NO]) -
+			       std::log10(std::max(rms, 1e-300));
+		int Nk = FB_N;
+		double pk = std::pow(10.0, predicted_log10(e, 14));
+		for (int p = 4; p <= 14; ++p) {
+			const double lp = predicted_log10(e, p);
+			if (lp <= std::log10(tol * LEARNED_MARGIN)) { Nk = p + 1; pk = std::pow(10.0, lp); break; }
+		}
+		if (Nk > N || (Nk == N && pk > pred)) { N = Nk; pred = pk; }
+	}
+	lfmm_learned_info li{};
+	li.predicted_N = N;
+	li.predicted_error = pred;
+	for (int pass = 0; pass < 2; ++pass) {
+		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+		LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
+		check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
+		LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
+		LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+		double ep_max = 0.0, ef_max = 0.0;
+		for (int k = 0; k < P; ++k) {
+			if (soff[k + 1] == soff[k]) continue;
+			ep_max = std::max(ep_max, std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)));
+			ef_max = std::max(ef_max, std::sqrt(ha[4 * (size_t)k + 2] / std::max(ha[4 * (size_t)k + 3], 1e-300)));
+		}
+		li.checked_error = ep_max;
+		li.checked_error_field = ef_max;
+		if (ep_max <= tol || N >= FB_N) break;
+		N = FB_N;                      // the fixed-order fallback for the whole batch
+		li.fallback = 1;
+	}
 	li.order_N = N;
 	if (info) *info = li;
 	return OK;

@@ -17,6 +17,13 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
                          const float* params, double tol, int check_targets, double* pot, double* field,
                          lfmm_learned_info* info, SolveStats* stats);
 
+// The same for a forest of in.nprob problems (hoff: host offsets): one order
+// for the batch (the highest any problem needs), samples and check per
+// problem (checked errors: the largest over the problems).
+int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size_t* hoff, int depth, int max_leaf,
+                               int precision, const float* params, double tol, int check_targets, double* pot,
+                               double* field, lfmm_learned_info* info, SolveStats* stats);
+
 // Per-leaf features [n_leaves][16] and the leaf of every input particle
 // (host buffers; either may be null).
 int features_tree(Context& ctx, const ParticleInput& in, int depth, int max_leaf, float* feats_host, size_t cap,

@@ -228,3 +228,30 @@ class LearnedSolver:
         if stats:
             out["stats"] = st.as_dict()
         return out
+
+    def solve_batch(self, problems, tol: float = 1e-6, tree_depth: int = 10, max_leaf: int = 64,
+                    precision: str = "mixed", check_targets: int = 64):
+        """Independent problems [(positions, charges), ...] as one batch at the
+        order the network picks (the highest any problem needs), each problem
+        judged on its own samples.  Returns ([(pot, forces), ...], info)."""
+        torch = _torch()
+        dev = self.d_params.device
+        parts = [(_f64(p, 3), _f64(c, 0)) for p, c in problems]
+        offs = np.zeros(len(parts) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(p) for p, _ in parts])
+        d_pos = torch.from_numpy(np.concatenate([p for p, _ in parts])).to(dev)
+        d_q = torch.from_numpy(np.concatenate([c for _, c in parts])).to(dev)
+        n = int(offs[-1])
+        d_pot = torch.empty(n, dtype=torch.float64, device=dev)
+        d_fld = torch.empty(n, 3, dtype=torch.float64, device=dev)
+        opts = LfmmSolveOpts(0, tree_depth, max_leaf, PRECISION[precision], tol)
+        info = LfmmLearnedInfo()
+        vp = ctypes.c_void_p
+        torch.cuda.synchronize(dev)
+        self.ctx.check(self.ctx.lib.lfmm3d_solve_batch_learned_device(
+            self.ctx.handle, len(parts), offs.ctypes.data_as(vp), vp(d_pos.data_ptr()), vp(d_q.data_ptr()),
+            ctypes.byref(opts), vp(self.d_params.data_ptr()), tol, check_targets, vp(d_pot.data_ptr()),
+            vp(d_fld.data_ptr()), ctypes.byref(info), None), "lfmm3d_solve_batch_learned_device")
+        torch.cuda.ExternalStream(self.ctx.stream, device=dev).synchronize()
+        pot, fld = d_pot.cpu().numpy(), d_fld.cpu().numpy()
+        return [(pot[offs[k]:offs[k + 1]], fld[offs[k]:offs[k + 1]]) for k in range(len(parts))], info.as_dict()

@@ -55,3 +55,21 @@ def test_batch_accuracy_vs_direct(ctx, problems):
         pot, fld = out[k]
         assert rel_l2(noself(pot[idx], q[idx]), noself(pe, q[idx])) < 3e-6
         assert rel_l2(fld[idx], fe) < 1e-5
+
+
+def test_learned_batch_within_tolerance(ctx, problems):
+    """The batch at the network's order: every problem within the tolerance
+    on its own samples, and the same result as the fixed-order batch at that
+    order."""
+    from laplace_fmm_b200.order import WEIGHTS, LearnedSolver
+    if not WEIGHTS.exists():
+        pytest.skip("trained network not present")
+    solver = LearnedSolver(ctx=ctx)
+    out, info = solver.solve_batch(problems, tol=1e-6, tree_depth=8, check_targets=64)
+    assert 5 <= info["order_N"] <= 15 and info["checked_error"] <= 1e-6
+    ref = solve_batch(problems, N=info["order_N"], tree_depth=8, max_leaf=64, ctx=ctx)
+    for (pos, q), (pot, fld), (rp, rf) in zip(problems, out, ref):
+        if len(pos) < 2:
+            continue
+        assert rel_l2(noself(pot, q), noself(rp, q)) < 1e-12
+        assert rel_l2(fld, rf) < 1e-12
