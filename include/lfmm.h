@@ -78,8 +78,9 @@ typedef struct {
 	size_t n_m2p;           /* adaptive tree: target-particle x W-cell evaluations */
 	size_t n_w, n_x;        /* adaptive tree: W and X list entries */
 	float ms_tree, ms_upward, ms_m2l, ms_l2l, ms_leaves, ms_total; /* device time, when timing */
-	float ms_m2l_kernel;    /* device time inside the tensor-core M2L kernel launches, when timing */
-	int n_m2l_kernel;       /* tensor-core M2L kernel launches timed */
+	float ms_m2l_kernel;    /* device time inside the M2L GEMMs, when timing (3D: the tensor-core
+	                           launches of the mixed form; 2D: the FP64 GEMM of every level) */
+	int n_m2l_kernel;       /* M2L GEMMs timed */
 } lfmm_stats;
 
 int lfmm_create(lfmm_ctx** ctx, const lfmm_options* opt);

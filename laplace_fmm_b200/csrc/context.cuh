@@ -102,6 +102,20 @@ struct Context {
 	int timing = 0;
 };
 
+// With 24 entries cached, evict the least recently used one no graph reads.
+inline void opcache_make_room(Context& ctx)
+{
+	if (ctx.opcache.size() < 24) return;
+	auto it = ctx.opcache.end();
+	for (auto j = ctx.opcache.begin(); j != ctx.opcache.end(); ++j)
+		if (!j->pinned && (it == ctx.opcache.end() || j->stamp < it->stamp)) it = j;
+	if (it != ctx.opcache.end()) {
+		cudaStreamSynchronize(ctx.stream);
+		cudaFree(it->ptr);
+		ctx.opcache.erase(it);
+	}
+}
+
 int tables_build(Context& ctx);
 void tables_free(Tables& t);
 

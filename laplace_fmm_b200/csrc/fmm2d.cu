@@ -5,6 +5,8 @@
 // Warp per box with one expansion coefficient per lane (N <= 30), block per
 // leaf for the near field.
 #include "fmm2d.cuh"
+#include "m2l_gemm.cuh"
+#include "primitives.cuh"
 
 namespace lfmm {
 
@@ -184,67 +186,131 @@ __global__ void __launch_bounds__(WPB2 * 32) down2d_kernel(DevTree t, Exp2 E, in
 	if (lane < N) E.inner[g * N + lane] = acc;
 }
 
-constexpr int LT2 = 128;
-
-__global__ void __launch_bounds__(LT2) leaves2d_kernel(DevTree t, Exp2 E, double* __restrict__ pot_out,
-                                                       double* __restrict__ fld_out)
+// L2L for L >= 3 added onto the M2L result of the level's GEMM:
+// b_k += sum_{n>=k} a_n C(n,k) (-z0)^(n-k), z0 = parent - child.
+__global__ void __launch_bounds__(WPB2 * 32) l2l2d_add_kernel(DevTree t, Exp2 E, int L)
 {
-	__shared__ double sx[LT2], sy[LT2], sq[LT2];
-	__shared__ double2 sL[32];
-	const int LL = t.depth - 1;
-	size_t leaf = blockIdx.x;
-	if (leaf >= t.lsize[LL]) return;
-	size_t off = t.loff[LL], g = off + leaf;
-	const bool tmode = t.targets_num > 0;
-	const uint32_t tb = tmode ? t.tbeg[g] : t.beg[g];
-	const uint32_t te = tmode ? t.tend[g] : t.end[g];
-	if (tb >= te) return;
+	__shared__ double2 sa[WPB2][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	size_t c = (size_t)blockIdx.x * WPB2 + w;
+	if (c >= t.lsize[L]) return;
 	const int N = E.N;
-	if (threadIdx.x < N) sL[threadIdx.x] = E.inner[g * N + threadIdx.x];
+	const size_t g = t.loff[L] + c, gp = t.loff[L - 1] + t.parent[g];
+	const double2 mz = make_double2(-(t.cx[gp] - t.cx[g]), -(t.cy[gp] - t.cy[g]));
+	if (lane < N) sa[w][lane] = E.inner[gp * N + lane];
+	__syncwarp();
+	if (lane >= N) return;
+	double2 acc = E.inner[g * N + lane];
+	double2 pw = make_double2(1.0, 0.0);
+	for (int n = lane; n < N; ++n) {
+		const double2 v = cmul(sa[w][n], pw);
+		const double bc = c_binom[n * BINOM_N + lane];
+		acc.x += v.x * bc; acc.y += v.y * bc;
+		pw = cmul(pw, mz);
+	}
+	E.inner[g * N + lane] = acc;
+}
+
+// Leaves: P2P over the close list (the leaf itself first) and L2P
+// (reference cpu/multipole.cpp:233-449).  One warp per work unit, a leaf's
+// targets in chunks of 32 (so a crowded leaf of a clustered set spreads over
+// many warps); a leaf of nt <= 16 targets is one unit whose warp runs TP = nt
+// rounded up to a power of two targets at once and splits the sources into
+// 32 / TP phases, summed by shuffles at the end.
+constexpr int LW2 = 4;
+
+__device__ __forceinline__ void leaf_targets(const DevTree& t, size_t g, uint32_t& tb, uint32_t& te)
+{
+	const bool tmode = t.targets_num > 0;
+	tb = tmode ? t.tbeg[g] : t.beg[g];
+	te = tmode ? t.tend[g] : t.end[g];
+}
+
+__global__ void leaf_units_kernel(DevTree t, uint32_t* __restrict__ units)
+{
+	const int LL = t.depth - 1;
+	const size_t leaf = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (leaf >= t.lsize[LL]) return;
+	uint32_t tb, te;
+	leaf_targets(t, t.loff[LL] + leaf, tb, te);
+	const uint32_t nt = te > tb ? te - tb : 0;
+	units[leaf] = nt == 0 ? 0 : (nt <= 16 ? 1 : (nt + 31) / 32);
+}
+
+__global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, const uint32_t* __restrict__ ubeg,
+                                                            const uint32_t* __restrict__ total,
+                                                            double* __restrict__ pot_out, double* __restrict__ fld_out)
+{
+	__shared__ double sx[LW2][32], sy[LW2][32], sq[LW2][32];
+	__shared__ double2 sL[LW2][32];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int LL = t.depth - 1;
+	const uint32_t u = blockIdx.x * LW2 + w;
+	if (u >= *total) return;
+	// the leaf of unit u: the last leaf whose first unit is <= u
+	uint32_t lo = 0, hi = (uint32_t)t.lsize[LL] - 1;
+	while (lo < hi) {
+		const uint32_t mid = (lo + hi + 1) >> 1;
+		if (ubeg[mid] <= u) lo = mid; else hi = mid - 1;
+	}
+	const size_t off = t.loff[LL], g = off + lo;
+	uint32_t tb, te;
+	leaf_targets(t, g, tb, te);
+	const int N = E.N;
+	if (lane < N) sL[w][lane] = E.inner[g * N + lane];
+	const int nt = (int)(te - tb);
+	int lt = 5;                                        // log2 of the targets per pass
+	if (nt <= 16) { lt = 0; while ((1 << lt) < nt) ++lt; }
+	const int TP = 1 << lt, G = 32 >> lt, ti = lane & (TP - 1), ph = lane >> lt;
 	const int ncl = t.close_cnt[g];
 	const int32_t* cl = t.close_idx + g * t.close_stride;
 	const double cx = t.cx[g], cy = t.cy[g];
-	for (uint32_t t0 = tb; t0 < te; t0 += LT2) {
-		uint32_t i = t0 + threadIdx.x;
+	{
+		const uint32_t t0 = tb + 32u * (u - ubeg[lo]);
+		const uint32_t i = t0 + ti;
 		const bool valid = i < te;
 		double xi = 0.0, yi = 0.0;
 		if (valid) { xi = t.x[i]; yi = t.y[i]; }
 		double pot = 0.0, fr = 0.0, fi = 0.0;
 		for (int e = -1; e < ncl; ++e) {
-			size_t sc = e < 0 ? g : off + cl[e];
+			const size_t sc = e < 0 ? g : off + cl[e];
 			const uint32_t sb = t.beg[sc], se = t.end[sc];
-			for (uint32_t s0 = sb; s0 < se; s0 += LT2) {
-				const int cnt = min((uint32_t)LT2, se - s0);
-				__syncthreads();
-				if (threadIdx.x < cnt) {
-					uint32_t j = s0 + threadIdx.x;
-					sx[threadIdx.x] = t.x[j]; sy[threadIdx.x] = t.y[j]; sq[threadIdx.x] = t.q[j];
+			for (uint32_t s0 = sb; s0 < se; s0 += 32) {
+				const int cnt = min(32u, se - s0);
+				__syncwarp();
+				if (lane < cnt) {
+					const uint32_t j = s0 + lane;
+					sx[w][lane] = t.x[j]; sy[w][lane] = t.y[j]; sq[w][lane] = t.q[j];
 				}
-				__syncthreads();
+				__syncwarp();
 				if (valid) {
-					for (int j = 0; j < cnt; ++j) {
-						double dx = xi - sx[j], dy = yi - sy[j];
-						double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
-						pot += sq[j] * 0.5 * log(r2);
-						double qr = sq[j] / r2;
+					for (int j = ph; j < cnt; j += G) {
+						const double dx = xi - sx[w][j], dy = yi - sy[w][j];
+						const double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
+						pot += sq[w][j] * 0.5 * log(r2);
+						const double qr = sq[w][j] / r2;
 						fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
 					}
 				}
 			}
 		}
-		__syncthreads();
-		if (valid) {
+		for (int o = TP; o < 32; o <<= 1) {
+			pot += __shfl_xor_sync(0xffffffffu, pot, o);
+			fr += __shfl_xor_sync(0xffffffffu, fr, o);
+			fi += __shfl_xor_sync(0xffffffffu, fi, o);
+		}
+		if (valid && ph == 0) {
 			double2 dz = make_double2(xi - cx, yi - cy), pw = make_double2(1.0, 0.0);
 			for (int k = 0; k < N; ++k) {
-				double2 Lk = sL[k];
+				const double2 Lk = sL[w][k];
 				pot += Lk.x * pw.x - Lk.y * pw.y;
 				if (k + 1 < N) {
-					double2 v = cmul(sL[k + 1], pw);
+					const double2 v = cmul(sL[w][k + 1], pw);
 					fr += (k + 1) * v.x; fi += (k + 1) * v.y;
 				}
 				pw = cmul(pw, dz);
 			}
-			uint32_t o = t.orig[i];
+			const uint32_t o = t.orig[i];
 			pot_out[o] = pot;
 			fld_out[2 * (size_t)o] = fr; fld_out[2 * (size_t)o + 1] = fi;
 		}
@@ -272,6 +338,7 @@ int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 	}
 	cudaStream_t s = ctx.stream;
 	const bool timing = ctx.timing != 0;
+	ctx.kev_used = 0;
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
 	DevTree t;
 	int st = tree_build(ctx, in, depth, t);
@@ -290,9 +357,42 @@ int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 	p2m2d_kernel<<<div_up(t.lsize[LL], WPB2), WPB2 * 32, 0, s>>>(t, E);
 	for (int L = depth - 2; L >= 0; --L) m2m2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
-	for (int L = 2; L < depth; ++L) down2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
+	if (ctx.m2l_engine == 1) {
+		// one warp per target cell over its far list
+		for (int L = 2; L < depth; ++L) down2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
+	} else {
+		// M2L as dense GEMMs grouped by (quadrant class, offset), all levels,
+		// then the L2L passes top-down
+		const size_t mark = ctx.arena.mark();
+		for (int L = 2; L < depth; ++L) {
+			if (t.lsize[L] == 0) continue;
+			M2LPlan plan;
+			if ((st = m2l_plan_build2d(ctx, t, L, plan))) return st;
+			const double* ops = m2l_ops2d(ctx, N, t.geo_host[3] / (double)(1ull << L));
+			if (!ops) return ERR_OOM;
+			double* outer = reinterpret_cast<double*>(E.outer + t.loff[L] * N);
+			double* inner = reinterpret_cast<double*>(E.inner + t.loff[L] * N);
+			const bool timed = timing && ctx.kev_used + 2 <= 32;
+			if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], s));
+			if ((st = m2l_gemm2d(ctx, plan, ops, outer, inner, N))) return st;
+			if (timed) { LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], s)); ctx.kev_used += 2; }
+			ctx.arena.rewind(mark);
+		}
+		for (int L = 3; L < depth; ++L)
+			if (t.lsize[L]) l2l2d_add_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
+	}
 	if (timing) { LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s)); LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s)); }
-	leaves2d_kernel<<<(unsigned)t.lsize[LL], LT2, 0, s>>>(t, E, pot, field);
+	if (t.lsize[LL]) {
+		const size_t nl = t.lsize[LL];
+		uint32_t* units = static_cast<uint32_t*>(ctx.arena.take(sizeof(uint32_t) * (2 * nl + 1)));
+		uint32_t* scr = static_cast<uint32_t*>(ctx.arena.take(sizeof(uint32_t) * scan_scratch_words(nl)));
+		if (!units || !scr) { ctx.last_error = "fmm2d: device allocation failed"; return ERR_OOM; }
+		leaf_units_kernel<<<div_up(nl, 256), 256, 0, s>>>(t, units);
+		scan_exclusive_u32(units, units + nl, nl, units + 2 * nl, scr, s);
+		// at most one unit per leaf plus one per 32 targets
+		const size_t max_units = nl + (n_out + 31) / 32;
+		leaves2d_kernel<<<div_up(max_units, LW2), LW2 * 32, 0, s>>>(t, E, units + nl, units + 2 * nl, pot, field);
+	}
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[5], s));
 	LFMM_CUDA(ctx, cudaGetLastError());
 	if (stats) {
@@ -310,6 +410,13 @@ int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 			cudaEventElapsedTime(&stats->ms_m2l, ctx.ev[2], ctx.ev[3]);
 			cudaEventElapsedTime(&stats->ms_leaves, ctx.ev[4], ctx.ev[5]);
 			cudaEventElapsedTime(&stats->ms_total, ctx.ev[0], ctx.ev[5]);
+			stats->ms_m2l_kernel = 0.f;
+			for (int k = 0; k + 1 < ctx.kev_used; k += 2) {
+				float ms = 0.f;
+				cudaEventElapsedTime(&ms, ctx.kev[k], ctx.kev[k + 1]);
+				stats->ms_m2l_kernel += ms;
+			}
+			stats->n_m2l_kernel = ctx.kev_used / 2;
 		}
 	}
 	return OK;

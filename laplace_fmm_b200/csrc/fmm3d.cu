@@ -467,16 +467,7 @@ double* m2l_ops_fp64(Context& ctx, int N, double h)
 	if (upload_constants(ctx)) return nullptr;
 	const int MT = m2l_padded(N), R = N * (N + 1);
 	size_t bytes = sizeof(double) * 343 * (size_t)MT * MT;
-	if (ctx.opcache.size() >= 24) {     // evict the least recently used entry no graph reads
-		auto it = ctx.opcache.end();
-		for (auto j = ctx.opcache.begin(); j != ctx.opcache.end(); ++j)
-			if (!j->pinned && (it == ctx.opcache.end() || j->stamp < it->stamp)) it = j;
-		if (it != ctx.opcache.end()) {
-			cudaStreamSynchronize(ctx.stream);
-			cudaFree(it->ptr);
-			ctx.opcache.erase(it);
-		}
-	}
+	opcache_make_room(ctx);
 	OpCacheEntry e;
 	e.N = N; e.prec = 0; e.h = h; e.bytes = bytes; e.stamp = ++ctx.opcache_clock;
 	if (cudaMalloc(&e.ptr, bytes) != cudaSuccess) { cudaGetLastError(); ctx.last_error = "m2l operators: out of memory"; return nullptr; }

@@ -10,7 +10,7 @@ struct SolveStats {
 	size_t n_far_pairs = 0, n_close_pairs = 0, n_p2p_pairs = 0;
 	size_t n_m2p = 0, n_w = 0, n_x = 0;
 	float ms_tree = 0, ms_upward = 0, ms_m2l = 0, ms_l2l = 0, ms_leaves = 0, ms_total = 0;
-	float ms_m2l_kernel = 0;     // inside the tensor-core M2L kernel launches
+	float ms_m2l_kernel = 0;     // inside the M2L GEMMs (3D: tensor-core launches; 2D: every level's)
 	int n_m2l_kernel = 0;        // those launches
 };
 

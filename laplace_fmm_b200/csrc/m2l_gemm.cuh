@@ -15,6 +15,7 @@
 namespace lfmm {
 
 constexpr int M2L_SLOTS = 189;    // far offsets per octant class
+constexpr int M2L_SLOTS2 = 27;    // 2D: far offsets per quadrant class
 constexpr int M2L_TILE = 64;      // targets per GEMM tile
 
 // Offsets of each octant class: slot -> direction id (dx+3)*49+(dy+3)*7+(dz+3)
@@ -42,5 +43,12 @@ int m2l_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan);
 // (real = double: plain form; float: mixed form).  ops: [343][MT][MT].
 template <typename real>
 int m2l_gemm(Context& ctx, const M2LPlan& plan, const real* ops, const real* mult, real* loc, int N);
+
+// 2D (FP64, expansions [cell][N] complex): the quadrant classes' 27 far
+// slots, the dense operators [49][MT][MT] (MT = 2N rounded up to 16) of cell
+// size h, and the GEMM.
+int m2l_plan_build2d(Context& ctx, const DevTree& t, int L, M2LPlan& plan);
+double* m2l_ops2d(Context& ctx, int N, double h);
+int m2l_gemm2d(Context& ctx, const M2LPlan& plan, const double* ops, const double* mult, double* loc, int N);
 
 } // namespace lfmm

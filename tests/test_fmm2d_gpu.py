@@ -80,3 +80,23 @@ def test_direct_matches_oracle(ctx, oracle, ns, nt):
     po, fo = oracle.direct2d(src, q, tgt)
     assert rel_l2(pe, po) < 1e-13
     assert rel_l2(np.stack([fe.real, fe.imag], 1), fo) < 1e-13
+
+
+@pytest.mark.parametrize("n,N,depth", [(400000, 20, 9), (50000, 30, 6), (20000, 3, 5)])
+def test_gemm_m2l_matches_per_pair(ctx, n, N, depth):
+    """The default 2D M2L (dense operators grouped by quadrant class and
+    offset, one GEMM per level) against the per-pair warp kernel: the same
+    sums in another order."""
+    import os
+    from laplace_fmm_b200 import Context
+    os.environ["LFMM_M2L"] = "rotation"
+    try:
+        pair = Context(0)
+    finally:
+        del os.environ["LFMM_M2L"]
+    src, q = clustered2d(n, seed=N)
+    a = FastMultipole((src, q), N=N, tree_depth=depth, ctx=ctx)
+    b = FastMultipole((src, q), N=N, tree_depth=depth, ctx=pair)
+    pair.close()
+    assert rel_l2(a.potentials, b.potentials) < 1e-13
+    assert rel_l2(a.forces, b.forces) < 1e-13
