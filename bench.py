@@ -43,10 +43,10 @@ CONFIGS = {
                metric="3D FMM Mparticles/s, plain FP64 form at p=8",
                workload="3D uniform 131,072 particles, FP64, p=8 (N=9), uniform octree depth 5"),
     # 2D clustered, 4,194,304 particles, p = 20 (N = 21), FP64
-    "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=9, precision="fp64",
+    "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=11, precision="fp64",
                metric="2D FMM Mparticles/s, FP64 at p=20",
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
-                        "p=20 (N=21), uniform quadtree depth 9"),
+                        "p=20 (N=21), uniform quadtree depth 11"),
     # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
     # mixed form at the order the network picks for rel-L2 <= 1e-6 (sampled
     # check of 256 outputs, fixed-order fallback); the plain FP64 form beside it

@@ -7,6 +7,8 @@
 #include "fmm2d.cuh"
 #include "m2l_gemm.cuh"
 #include "primitives.cuh"
+#include <cmath>
+#include <mutex>
 
 namespace lfmm {
 
@@ -14,7 +16,41 @@ namespace {
 
 constexpr int WPB2 = 4;
 constexpr int BINOM_N = 2 * MAXN2;
-__constant__ double c_binom[BINOM_N * BINOM_N];   // Pascal triangle, C(n,k) at n*60+k
+// Pascal triangle in global memory (lanes read different entries, which
+// constant memory would serialise): C(n,k) at n*60+k, and transposed,
+// C(n,k) at k*60+n.
+__device__ double c_binom[BINOM_N * BINOM_N];
+__device__ double c_binomT[BINOM_N * BINOM_N];
+
+// Natural logarithm of a normal, finite x > 0, table-driven after P. T. P.
+// Tang, "Table-driven implementation of the logarithm function in IEEE
+// floating-point arithmetic", ACM TOMS 16(4), 1990: x = 2^e m, m in [1, 2),
+// c = 1 + i/256 the table point nearest m, t = m/c - 1 (|t| <= 2^-9) from the
+// stored 1/c, log x = e ln2 + log c + log1p(t), log1p by its Taylor series to
+// t^5 (truncation below 1e-17).  The table and the split ln2 = hi + lo (hi
+// with 24 bits, so e hi is exact) are computed on the host in long double.
+struct LogTable {
+	double2 e[257];                    // (log c_i, 1 / c_i)
+	double ln2_hi, ln2_lo;
+};
+__device__ LogTable c_logtab;
+
+__device__ __forceinline__ double log_table(double x, const double2* __restrict__ tab, double ln2_hi, double ln2_lo)
+{
+	const int hi = __double2hiint(x);
+	const int e = (hi >> 20) - 1023;
+	const int mh = hi & 0xFFFFF;
+	const int i = (mh + (1 << 11)) >> 12;
+	const double m = __hiloint2double(mh | 0x3FF00000, __double2loint(x));
+	const double2 c = tab[i];
+	const double t = fma(m, c.y, -1.0);
+	double q = fma(t, 0.2, -0.25);
+	q = fma(t, q, 1.0 / 3.0);
+	q = fma(t, q, -0.5);
+	q = fma(t, q, 1.0);
+	const double de = (double)e;
+	return fma(de, ln2_hi, c.x + fma(de, ln2_lo, t * q));
+}
 
 struct Exp2 {
 	int N;
@@ -37,37 +73,39 @@ __device__ __forceinline__ double2 cpow_u(double2 b, int e)
 }
 __device__ __forceinline__ void coords2(uint64_t code, int* c) { c[0] = (int)compact2(code >> 1); c[1] = (int)compact2(code); }
 
-// a_k = -sum q (z - z0)^k / k, a_0 = sum q
+// a_k = -sum q (z - z0)^k / k, a_0 = sum q.  Lane k accumulates coefficient
+// k over the leaf's particles, staged 32 at a time.
 __global__ void __launch_bounds__(WPB2 * 32) p2m2d_kernel(DevTree t, Exp2 E)
 {
-	__shared__ double2 sacc[WPB2][32];
+	__shared__ double2 sz[WPB2][32];
+	__shared__ double sq[WPB2][32];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int LL = t.depth - 1;
 	size_t leaf = (size_t)blockIdx.x * WPB2 + w;
 	if (leaf >= t.lsize[LL]) return;
 	size_t g = t.loff[LL] + leaf;
 	const int N = E.N;
-	sacc[w][lane] = make_double2(0.0, 0.0);
-	__syncwarp();
 	const double cx = t.cx[g], cy = t.cy[g];
-	for (uint32_t base = t.beg[g]; base < t.end[g]; base += 32) {
-		uint32_t i = base + lane;
-		double q = 0.0;
-		double2 z = make_double2(0.0, 0.0);
-		if (i < t.end[g]) { q = t.q[i]; z = make_double2(t.x[i] - cx, t.y[i] - cy); }
-		for (int k = 0; k < N; ++k) {
-			double vr, vi;
-			if (k == 0) { vr = q; vi = 0.0; }
-			else { double2 p = cpow_u(z, k); vr = q * p.x; vi = q * p.y; }
-			vr = warp_sum(vr); vi = warp_sum(vi);
-			if (lane == 0) { sacc[w][k].x += vr; sacc[w][k].y += vi; }
+	const uint32_t pb = t.beg[g], pe = t.end[g];
+	double2 acc = make_double2(0.0, 0.0);
+	for (uint32_t base = pb; base < pe; base += 32) {
+		const int cnt = (int)min(32u, pe - base);
+		__syncwarp();
+		if (lane < cnt) {
+			const uint32_t i = base + lane;
+			sq[w][lane] = t.q[i];
+			sz[w][lane] = make_double2(t.x[i] - cx, t.y[i] - cy);
 		}
+		__syncwarp();
+		if (lane < N)
+			for (int j = 0; j < cnt; ++j) {
+				const double2 p = cpow_u(sz[w][j], lane);
+				acc.x = fma(sq[w][j], p.x, acc.x); acc.y = fma(sq[w][j], p.y, acc.y);
+			}
 	}
-	__syncwarp();
 	if (lane < N) {
-		double2 a = sacc[w][lane];
-		if (lane > 0) a = make_double2(-a.x / lane, -a.y / lane);
-		E.outer[g * N + lane] = a;
+		if (lane > 0) acc = make_double2(-acc.x / lane, -acc.y / lane);
+		E.outer[g * N + lane] = acc;
 	}
 }
 
@@ -95,7 +133,7 @@ __global__ void __launch_bounds__(WPB2 * 32) m2m2d_kernel(DevTree t, Exp2 E, int
 				double2 s = make_double2(0.0, 0.0);
 				for (int i = 1; i <= j; ++i) {
 					double2 v = cmul(sa[w][i], sp[w][j - i]);
-					double bc = c_binom[(j - 1) * BINOM_N + (i - 1)];
+					double bc = c_binomT[(i - 1) * BINOM_N + (j - 1)];
 					s.x += v.x * bc; s.y += v.y * bc;
 				}
 				double2 a0z = cmul(sa[w][0], sp[w][j]);
@@ -243,6 +281,10 @@ __global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, c
 {
 	__shared__ double sx[LW2][32], sy[LW2][32], sq[LW2][32];
 	__shared__ double2 sL[LW2][32];
+	__shared__ double2 slog[257];
+	for (int k = threadIdx.x; k < 257; k += LW2 * 32) slog[k] = c_logtab.e[k];
+	const double ln2_hi = c_logtab.ln2_hi, ln2_lo = c_logtab.ln2_lo;
+	__syncthreads();
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int LL = t.depth - 1;
 	const uint32_t u = blockIdx.x * LW2 + w;
@@ -287,7 +329,7 @@ __global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, c
 					for (int j = ph; j < cnt; j += G) {
 						const double dx = xi - sx[w][j], dy = yi - sy[w][j];
 						const double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
-						pot += sq[w][j] * 0.5 * log(r2);
+						pot = fma(sq[w][j], log_table(r2, slog, ln2_hi, ln2_lo), pot);     // halved below
 						const double qr = sq[w][j] / r2;
 						fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
 					}
@@ -299,6 +341,7 @@ __global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, c
 			fr += __shfl_xor_sync(0xffffffffu, fr, o);
 			fi += __shfl_xor_sync(0xffffffffu, fi, o);
 		}
+		pot *= 0.5;                                    // sum q log r2 -> sum q log r
 		if (valid && ph == 0) {
 			double2 dz = make_double2(xi - cx, yi - cy), pw = make_double2(1.0, 0.0);
 			for (int k = 0; k < N; ++k) {
@@ -317,7 +360,8 @@ __global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, c
 	}
 }
 
-bool g_binom_ready = false;
+std::mutex g_binom_mu;
+bool g_binom_ready[64] = {};
 
 } // namespace
 
@@ -325,17 +369,32 @@ int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
                        SolveStats* stats)
 {
 	if (N < 1 || N > MAXN2) { ctx.last_error = "order out of range (1 <= N <= 30)"; return ERR_ARG; }
-	if (!g_binom_ready) {
-		static double b[BINOM_N * BINOM_N];
+	if (ctx.device < 0 || ctx.device >= 64) { ctx.last_error = "device index above 63"; return ERR_ARG; }
+	std::unique_lock<std::mutex> lock(g_binom_mu);
+	if (!g_binom_ready[ctx.device]) {
+		static double b[BINOM_N * BINOM_N], bt[BINOM_N * BINOM_N];
 		for (int i = 0; i < BINOM_N * BINOM_N; ++i) b[i] = 0.0;
 		b[0] = 1.0;
 		for (int i = 1; i < BINOM_N; ++i) {
 			b[i * BINOM_N] = 1.0; b[i * BINOM_N + i] = 1.0;
 			for (int j = 1; j < i; ++j) b[i * BINOM_N + j] = b[(i - 1) * BINOM_N + j] + b[(i - 1) * BINOM_N + j - 1];
 		}
+		for (int n = 0; n < BINOM_N; ++n)
+			for (int k = 0; k < BINOM_N; ++k) bt[k * BINOM_N + n] = b[n * BINOM_N + k];
 		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_binom, b, sizeof(b)));
-		g_binom_ready = true;
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_binomT, bt, sizeof(bt)));
+		LogTable lt;
+		for (int i = 0; i <= 256; ++i) {
+			const long double c = 1.0L + (long double)i / 256.0L;
+			lt.e[i] = make_double2((double)logl(c), (double)(1.0L / c));
+		}
+		const long double ln2 = logl(2.0L);
+		lt.ln2_hi = (double)(float)ln2;
+		lt.ln2_lo = (double)(ln2 - (long double)lt.ln2_hi);
+		LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_logtab, &lt, sizeof(lt)));
+		g_binom_ready[ctx.device] = true;
 	}
+	lock.unlock();
 	cudaStream_t s = ctx.stream;
 	const bool timing = ctx.timing != 0;
 	ctx.kev_used = 0;
@@ -361,20 +420,26 @@ int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 		// one warp per target cell over its far list
 		for (int L = 2; L < depth; ++L) down2d_kernel<<<div_up(t.lsize[L], WPB2), WPB2 * 32, 0, s>>>(t, E, L);
 	} else {
-		// M2L as dense GEMMs grouped by (quadrant class, offset), all levels,
-		// then the L2L passes top-down
+		// M2L grouped by (quadrant class, offset), all levels: the Hankel
+		// factorisation (default) or dense operators (simt); then the L2L
+		// passes top-down
 		const size_t mark = ctx.arena.mark();
 		for (int L = 2; L < depth; ++L) {
 			if (t.lsize[L] == 0) continue;
 			M2LPlan plan;
 			if ((st = m2l_plan_build2d(ctx, t, L, plan))) return st;
-			const double* ops = m2l_ops2d(ctx, N, t.geo_host[3] / (double)(1ull << L));
-			if (!ops) return ERR_OOM;
-			double* outer = reinterpret_cast<double*>(E.outer + t.loff[L] * N);
-			double* inner = reinterpret_cast<double*>(E.inner + t.loff[L] * N);
+			const double h = t.geo_host[3] / (double)(1ull << L);
+			const double* ops = nullptr;
+			const double2* tab = nullptr;
+			if (ctx.m2l_engine == 0) ops = m2l_ops2d(ctx, N, h);
+			else tab = m2l_tab2d(ctx, N, h);
+			if (!ops && !tab) return ERR_OOM;
 			const bool timed = timing && ctx.kev_used + 2 <= 32;
 			if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], s));
-			if ((st = m2l_gemm2d(ctx, plan, ops, outer, inner, N))) return st;
+			if (ops) st = m2l_gemm2d(ctx, plan, ops, reinterpret_cast<double*>(E.outer + t.loff[L] * N),
+			                         reinterpret_cast<double*>(E.inner + t.loff[L] * N), N);
+			else st = m2l_hankel2d(ctx, plan, tab, E.outer + t.loff[L] * N, E.inner + t.loff[L] * N, N);
+			if (st) return st;
 			if (timed) { LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], s)); ctx.kev_used += 2; }
 			ctx.arena.rewind(mark);
 		}

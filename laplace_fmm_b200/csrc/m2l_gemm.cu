@@ -187,6 +187,138 @@ __global__ void m2l_ops2d_kernel(int N, int MT, double h, double* __restrict__ o
 	T[(size_t)(2 * i + 1) * MT + 2 * j + 1] = cr;
 }
 
+// The same operator factored through one real Hankel matrix shared by every
+// offset and level: T = diag(post) H diag(pre) plus the log term, with
+// H[i][j] = (i+j-1)! (H[0][0] = 0), pre_0 = -1, pre_j = (-1)^j / ((j-1)! z0^j),
+// post_i = 1 / (i! z0^i) and b_0 += a_0 conj(log(-z0)).  The per-offset
+// vectors of one level: tab[d] = pre[0..N), post[0..N), log term.
+__constant__ double c_fact[64];        // k!
+
+__global__ void m2l2d_tab_kernel(int N, double h, double2* __restrict__ tab)
+{
+	const int W = 2 * N + 1;
+	const int e = blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= 49 * W) return;
+	const int d = e / W, k = e - d * W;
+	const int dx = d / 7 - 3, dy = d % 7 - 3;
+	if (max(abs(dx), abs(dy)) <= 1) { tab[e] = make_double2(0.0, 0.0); return; }
+	const double zx = dx * h, zy = dy * h;
+	if (k == 2 * N) { tab[e] = make_double2(log(sqrt(zx * zx + zy * zy)), -atan2(-zy, -zx)); return; }
+	const int p = k < N ? k : k - N;           // power of 1 / z0
+	if (k == 0) { tab[e] = make_double2(-1.0, 0.0); return; }
+	const double r2 = zx * zx + zy * zy;
+	const double ix = zx / r2, iy = -zy / r2;
+	double px = 1.0, py = 0.0;
+	for (int q = 0; q < p; ++q) { const double nx = px * ix - py * iy; py = px * iy + py * ix; px = nx; }
+	const double f = k < N ? ((p & 1) ? -1.0 : 1.0) / c_fact[p - 1] : 1.0 / c_fact[p];
+	tab[e] = make_double2(f * px, f * py);
+}
+
+// Block of 128 threads per (quadrant class, tile of 64 targets) and slot
+// range; thread (ty, tx) owns rows ty + 4 r (r < TM) of targets tx and tx + 32.
+// Per slot: W = pre (.) a (gathered sources), S = H W, b += post (.) S.
+template <int TM>
+__global__ void __launch_bounds__(128) m2l2d_hankel_kernel(const double2* __restrict__ tab,
+                                                           const double2* __restrict__ mult, double2* __restrict__ loc,
+                                                           const int32_t* __restrict__ vtab,
+                                                           const int32_t* __restrict__ order,
+                                                           const uint32_t* __restrict__ cls_count, int N,
+                                                           double2* __restrict__ part, size_t cells)
+{
+	const int S = gridDim.y, sidx = blockIdx.y;
+	const int slot0 = sidx * M2L_SLOTS2 / S, slot1 = (sidx + 1) * M2L_SLOTS2 / S;
+	if (S > 1) loc = part + (size_t)sidx * cells * N;
+	__shared__ double Wr[32][65], Wi[32][65];
+	__shared__ double sH[64];
+	__shared__ double2 spost[32];
+	__shared__ double2 slg;
+	__shared__ int32_t src[64], tgt[64];
+	__shared__ int s_cls, s_n;
+	__shared__ uint32_t s_start;
+	const int tid = threadIdx.x, ty = tid >> 5, tx = tid & 31;
+	if (tid == 0) {
+		uint32_t b = blockIdx.x, start = 0;
+		int cls = -1, nn = 0;
+		for (int o = 0; o < 4; ++o) {
+			const uint32_t cnt = cls_count[o], tiles = (cnt + 63) / 64;
+			if (b < tiles) { cls = o; start += b * 64; nn = (int)min(64u, cnt - b * 64); break; }
+			b -= tiles; start += cnt;
+		}
+		s_cls = cls; s_n = nn; s_start = start;
+	}
+	if (tid < 64) sH[tid] = tid == 0 ? 0.0 : c_fact[tid - 1];
+	__syncthreads();
+	const int cls = s_cls;
+	if (cls < 0) return;
+	if (tid < 64) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
+	double ar[TM][2], ai[TM][2];
+#pragma unroll
+	for (int r = 0; r < TM; ++r) { ar[r][0] = ar[r][1] = ai[r][0] = ai[r][1] = 0.0; }
+	__syncthreads();
+	for (int slot = slot0; slot < slot1; ++slot) {
+		int mine = -1;
+		if (tid < 64 && tgt[tid] >= 0) mine = vtab[(size_t)tgt[tid] * M2L_SLOTS2 + slot];
+		if (tid < 64) src[tid] = mine;
+		if (!__syncthreads_or(mine >= 0)) continue;
+		const double2* T = tab + (size_t)c_slot_dir2[cls][slot] * (2 * N + 1);
+		if (tid < N) spost[tid] = T[N + tid];
+		if (tid == 0) slg = T[2 * N];
+		for (int idx = tid; idx < 64 * N; idx += 128) {
+			const int c = idx / N, k = idx - c * N;
+			const int s = src[c];
+			const double2 a = s >= 0 ? mult[(size_t)s * N + k] : make_double2(0.0, 0.0);
+			const double2 p = T[k];
+			Wr[k][c] = a.x * p.x - a.y * p.y;
+			Wi[k][c] = a.x * p.y + a.y * p.x;
+		}
+		__syncthreads();
+		double sr[TM][2], si[TM][2];
+#pragma unroll
+		for (int r = 0; r < TM; ++r) { sr[r][0] = sr[r][1] = si[r][0] = si[r][1] = 0.0; }
+		for (int k = 0; k < N; ++k) {
+			const double br0 = Wr[k][tx], br1 = Wr[k][tx + 32], bi0 = Wi[k][tx], bi1 = Wi[k][tx + 32];
+#pragma unroll
+			for (int r = 0; r < TM; ++r) {
+				const double hk = sH[ty + 4 * r + k];
+				sr[r][0] = fma(hk, br0, sr[r][0]); sr[r][1] = fma(hk, br1, sr[r][1]);
+				si[r][0] = fma(hk, bi0, si[r][0]); si[r][1] = fma(hk, bi1, si[r][1]);
+			}
+		}
+#pragma unroll
+		for (int r = 0; r < TM; ++r) {
+			const int i = ty + 4 * r;
+			if (i < N) {
+				const double2 p = spost[i];
+#pragma unroll
+				for (int j = 0; j < 2; ++j) {
+					ar[r][j] += p.x * sr[r][j] - p.y * si[r][j];
+					ai[r][j] += p.x * si[r][j] + p.y * sr[r][j];
+				}
+			}
+		}
+		if (ty == 0) {                         // b_0 += a_0 lg, a_0 = -W[0]
+			const double2 lg = slg;
+#pragma unroll
+			for (int j = 0; j < 2; ++j) {
+				const double a0r = -Wr[0][tx + 32 * j], a0i = -Wi[0][tx + 32 * j];
+				ar[0][j] += a0r * lg.x - a0i * lg.y;
+				ai[0][j] += a0r * lg.y + a0i * lg.x;
+			}
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int j = 0; j < 2; ++j) {
+		const int tg = tgt[tx + 32 * j];
+		if (tg < 0) continue;
+#pragma unroll
+		for (int r = 0; r < TM; ++r) {
+			const int i = ty + 4 * r;
+			if (i < N) loc[(size_t)tg * N + i] = make_double2(ar[r][j], ai[r][j]);
+		}
+	}
+}
+
 // C[MT x 64] = sum over the octant's offsets of T_dir[MT x MT] * B[MT x 64];
 // 256 threads, thread (ty, tx) owns rows ty + 16 i and columns tx + 16 j.
 // blockIdx.y = split s of S: slots [s*189/S, (s+1)*189/S); with S > 1 the
@@ -372,6 +504,10 @@ int upload_slots(Context& ctx)
 	}
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_slot_dir2, sd, sizeof(sd)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_dir_slot2, ds, sizeof(ds)));
+	double fact[64];
+	fact[0] = 1.0;
+	for (int k = 1; k < 64; ++k) fact[k] = fact[k - 1] * k;
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_fact, fact, sizeof(fact)));
 	g_slots_uploaded[ctx.device] = true;
 	return OK;
 }
@@ -412,6 +548,51 @@ double* m2l_ops2d(Context& ctx, int N, double h)
 	if (cudaGetLastError() != cudaSuccess) { cudaFree(e.ptr); ctx.last_error = "2D m2l operators: launch failed"; return nullptr; }
 	ctx.opcache.push_back(e);
 	return static_cast<double*>(e.ptr);
+}
+
+double2* m2l_tab2d(Context& ctx, int N, double h)
+{
+	for (auto& e : ctx.opcache)
+		if (e.N == N && e.prec == 21 && e.h == h) { e.stamp = ++ctx.opcache_clock; return static_cast<double2*>(e.ptr); }
+	if (upload_slots(ctx)) return nullptr;
+	opcache_make_room(ctx);
+	OpCacheEntry e;
+	e.N = N; e.prec = 21; e.h = h; e.bytes = sizeof(double2) * 49 * (size_t)(2 * N + 1); e.stamp = ++ctx.opcache_clock;
+	if (cudaMalloc(&e.ptr, e.bytes) != cudaSuccess) { cudaGetLastError(); ctx.last_error = "2D m2l tables: out of memory"; return nullptr; }
+	const int cnt = 49 * (2 * N + 1);
+	m2l2d_tab_kernel<<<div_up(cnt, 128), 128, 0, ctx.stream>>>(N, h, static_cast<double2*>(e.ptr));
+	if (cudaGetLastError() != cudaSuccess) { cudaFree(e.ptr); ctx.last_error = "2D m2l tables: launch failed"; return nullptr; }
+	ctx.opcache.push_back(e);
+	return static_cast<double2*>(e.ptr);
+}
+
+int m2l_hankel2d(Context& ctx, const M2LPlan& plan, const double2* tab, const double2* mult, double2* loc, int N)
+{
+	if (N < 1 || N > 32) { ctx.last_error = "2D m2l: order too large"; return ERR_UNSUPPORTED; }
+	const unsigned tiles = (unsigned)(plan.cells / 64 + 4);
+	int S = 1;
+	while (S < 8 && tiles * S < 4u * (unsigned)ctx.num_sms) S *= 2;
+	double2* part = nullptr;
+	if (S > 1) {
+		part = static_cast<double2*>(ctx.arena.take(sizeof(double2) * (size_t)S * plan.cells * N));
+		if (!part) S = 1;
+	}
+	const dim3 grid(tiles, S);
+	cudaStream_t s = ctx.stream;
+	const int TM = N <= 8 ? 2 : N <= 16 ? 4 : N <= 24 ? 6 : 8;
+	switch (TM) {
+	case 2: m2l2d_hankel_kernel<2><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
+	case 4: m2l2d_hankel_kernel<4><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
+	case 6: m2l2d_hankel_kernel<6><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
+	default: m2l2d_hankel_kernel<8><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
+	}
+	if (S > 1) {
+		const size_t nel = plan.cells * (size_t)N * 2;
+		split_reduce_kernel<double><<<div_up(nel, 256), 256, 0, s>>>(reinterpret_cast<const double*>(part),
+		                                                             reinterpret_cast<double*>(loc), nel, S);
+	}
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
 }
 
 int m2l_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan)

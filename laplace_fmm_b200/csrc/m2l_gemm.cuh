@@ -50,5 +50,9 @@ int m2l_gemm(Context& ctx, const M2LPlan& plan, const real* ops, const real* mul
 int m2l_plan_build2d(Context& ctx, const DevTree& t, int L, M2LPlan& plan);
 double* m2l_ops2d(Context& ctx, int N, double h);
 int m2l_gemm2d(Context& ctx, const M2LPlan& plan, const double* ops, const double* mult, double* loc, int N);
+// The same M2L through the Hankel factorisation (the default 2D engine):
+// the per-offset tables of cell size h and the launch (N <= 32).
+double2* m2l_tab2d(Context& ctx, int N, double h);
+int m2l_hankel2d(Context& ctx, const M2LPlan& plan, const double2* tab, const double2* mult, double2* loc, int N);
 
 } // namespace lfmm

@@ -82,21 +82,29 @@ def test_direct_matches_oracle(ctx, oracle, ns, nt):
     assert rel_l2(np.stack([fe.real, fe.imag], 1), fo) < 1e-13
 
 
-@pytest.mark.parametrize("n,N,depth", [(400000, 20, 9), (50000, 30, 6), (20000, 3, 5)])
-def test_gemm_m2l_matches_per_pair(ctx, n, N, depth):
-    """The default 2D M2L (dense operators grouped by quadrant class and
-    offset, one GEMM per level) against the per-pair warp kernel: the same
-    sums in another order."""
+def engine_context(name):
     import os
     from laplace_fmm_b200 import Context
-    os.environ["LFMM_M2L"] = "rotation"
+    os.environ["LFMM_M2L"] = name
     try:
-        pair = Context(0)
+        return Context(0)
     finally:
         del os.environ["LFMM_M2L"]
+
+
+@pytest.mark.parametrize("n,N,depth", [(400000, 20, 9), (50000, 30, 6), (20000, 3, 5), (30000, 9, 6),
+                                       (30000, 17, 6), (30000, 25, 6), (200000, 21, 11)])
+def test_m2l_engines_agree(ctx, n, N, depth):
+    """The default 2D M2L (the Hankel factorisation, grouped by quadrant class
+    and offset), the dense-operator GEMMs and the per-pair warp kernel: the
+    same sums in other orders."""
+    pair, dense = engine_context("rotation"), engine_context("simt")
     src, q = clustered2d(n, seed=N)
     a = FastMultipole((src, q), N=N, tree_depth=depth, ctx=ctx)
     b = FastMultipole((src, q), N=N, tree_depth=depth, ctx=pair)
+    c = FastMultipole((src, q), N=N, tree_depth=depth, ctx=dense)
     pair.close()
-    assert rel_l2(a.potentials, b.potentials) < 1e-13
-    assert rel_l2(a.forces, b.forces) < 1e-13
+    dense.close()
+    for other in (b, c):
+        assert rel_l2(a.potentials, other.potentials) < 1e-13
+        assert rel_l2(a.forces, other.forces) < 1e-13
