@@ -314,25 +314,40 @@ __global__ void __launch_bounds__(LW2 * 32) leaves2d_kernel(DevTree t, Exp2 E, c
 		double xi = 0.0, yi = 0.0;
 		if (valid) { xi = t.x[i]; yi = t.y[i]; }
 		double pot = 0.0, fr = 0.0, fi = 0.0;
-		for (int e = -1; e < ncl; ++e) {
-			const size_t sc = e < 0 ? g : off + cl[e];
-			const uint32_t sb = t.beg[sc], se = t.end[sc];
-			for (uint32_t s0 = sb; s0 < se; s0 += 32) {
-				const int cnt = min(32u, se - s0);
-				__syncwarp();
-				if (lane < cnt) {
-					const uint32_t j = s0 + lane;
-					sx[w][lane] = t.x[j]; sy[w][lane] = t.y[j]; sq[w][lane] = t.q[j];
-				}
-				__syncwarp();
-				if (valid) {
-					for (int j = ph; j < cnt; j += G) {
-						const double dx = xi - sx[w][j], dy = yi - sy[w][j];
-						const double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
-						pot = fma(sq[w][j], log_table(r2, slog, ln2_hi, ln2_lo), pot);     // halved below
-						const double qr = sq[w][j] / r2;
-						fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
-					}
+		// the close cells' particles as one stream (the leaf first): lane e
+		// holds cell e's first particle and its inclusive end in the stream
+		uint32_t cbeg = 0, cinc = 0;
+		if (lane <= ncl) {
+			const size_t sc = lane == 0 ? g : off + cl[lane - 1];
+			cbeg = t.beg[sc];
+			cinc = t.end[sc] - cbeg;
+		}
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, cinc, o);
+			if (lane >= o) cinc += v;
+		}
+		const uint32_t total = __shfl_sync(0xffffffffu, cinc, ncl);
+		for (uint32_t s0 = 0; s0 < total; s0 += 32) {
+			const int cnt = (int)min(32u, total - s0);
+			const uint32_t pos = s0 + lane;
+			uint32_t j = 0;
+			for (int e = 0; e <= ncl; ++e) {        // the cell holding stream position pos
+				const uint32_t inc = __shfl_sync(0xffffffffu, cinc, e);
+				const uint32_t bg = __shfl_sync(0xffffffffu, cbeg, e);
+				const uint32_t ex = e ? __shfl_sync(0xffffffffu, cinc, e - 1) : 0u;
+				if (pos >= ex && pos < inc) j = bg + (pos - ex);
+			}
+			__syncwarp();
+			if (lane < cnt) { sx[w][lane] = t.x[j]; sy[w][lane] = t.y[j]; sq[w][lane] = t.q[j]; }
+			__syncwarp();
+			if (valid) {
+				for (int k = ph; k < cnt; k += G) {
+					const double dx = xi - sx[w][k], dy = yi - sy[w][k];
+					const double r2 = fmax(dx * dx + dy * dy, FORCE_EPS2);
+					pot = fma(sq[w][k], log_table(r2, slog, ln2_hi, ln2_lo), pot);     // halved below
+					const double qr = sq[w][k] / r2;
+					fr = fma(dx, qr, fr); fi = fma(-dy, qr, fi);
 				}
 			}
 		}

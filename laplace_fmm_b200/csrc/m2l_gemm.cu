@@ -214,11 +214,44 @@ __global__ void m2l2d_tab_kernel(int N, double h, double2* __restrict__ tab)
 	tab[e] = make_double2(f * px, f * py);
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int bytes)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory"); }
+
+// FP64 tensor-core MMA (mma.sync m8n8k4, the FP64 path of sm_100): D = A B + C
+// with A 8x4 row-major (lane: A[lane/4][lane%4]), B 4x8 column-major
+// (lane: B[lane%4][lane/4]) and C, D 8x8 (lane: C[lane/4][2 (lane%4) + 0, 1]).
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b)
+{
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+	             : "+d"(d0), "+d"(d1)
+	             : "d"(a), "d"(b));
+}
+
+constexpr int H2_LD = 136;             // row stride (doubles) of the staged W: conflict-free B fragments
+
+// Dynamic shared memory of the Hankel kernel for order N (bytes).
+inline size_t hankel_smem(int N)
+{
+	const int R4 = (N + 3) / 4 * 4, RS = N | 1;
+	return sizeof(double2) * (64 * (size_t)RS + 2 * (size_t)N + 1) + sizeof(double) * (size_t)R4 * H2_LD +
+	       sizeof(int32_t) * M2L_SLOTS2 * 65;
+}
+
 // Block of 128 threads per (quadrant class, tile of 64 targets) and slot
-// range; thread (ty, tx) owns rows ty + 4 r (r < TM) of targets tx and tx + 32.
-// Per slot: W = pre (.) a (gathered sources), S = H W, b += post (.) S.
-template <int TM>
-__global__ void __launch_bounds__(128) m2l2d_hankel_kernel(const double2* __restrict__ tab,
+// range.  Per slot: W = pre (.) a (gathered sources, stored as columns
+// 2c + re/im), S = H W on the FP64 tensor cores (warp w: columns
+// [32w, 32w + 32), all rows in MTL tiles of 8), b += post (.) S on the
+// accumulator fragments, which hold the re and im of one target side by side.
+// The next non-empty slot's sources and tables are staged by cp.async
+// (zero-filled where a target has no source) while the current one computes.
+template <int MTL>
+__global__ void __launch_bounds__(128, MTL < 4 ? 4 : 3) m2l2d_hankel_kernel(const double2* __restrict__ tab,
                                                            const double2* __restrict__ mult, double2* __restrict__ loc,
                                                            const int32_t* __restrict__ vtab,
                                                            const int32_t* __restrict__ order,
@@ -228,14 +261,21 @@ __global__ void __launch_bounds__(128) m2l2d_hankel_kernel(const double2* __rest
 	const int S = gridDim.y, sidx = blockIdx.y;
 	const int slot0 = sidx * M2L_SLOTS2 / S, slot1 = (sidx + 1) * M2L_SLOTS2 / S;
 	if (S > 1) loc = part + (size_t)sidx * cells * N;
-	__shared__ double Wr[32][65], Wi[32][65];
-	__shared__ double sH[64];
+	const int R4 = (N + 3) / 4 * 4, W2 = 2 * N + 1;
+	const int RS = N | 1;                  // odd row stride: conflict-free reads by source
+	extern __shared__ __align__(16) unsigned char dsm[];
+	double2* raw = reinterpret_cast<double2*>(dsm);                 // [64][RS] sources of a slot
+	double2* sT = raw + 64 * RS;                                     // [2N+1] pre, post, log term
+	double* Wc = reinterpret_cast<double*>(sT + W2);                 // [R4][H2_LD]
+	int32_t* srcs = reinterpret_cast<int32_t*>(Wc + R4 * H2_LD);     // [27][65]
+	__shared__ double sH[72];              // (k-1)!, read up to index 8 MTL + R4 - 2 <= 62
 	__shared__ double2 spost[32];
 	__shared__ double2 slg;
-	__shared__ int32_t src[64], tgt[64];
-	__shared__ int s_cls, s_n;
-	__shared__ uint32_t s_start;
-	const int tid = threadIdx.x, ty = tid >> 5, tx = tid & 31;
+	__shared__ int32_t tgt[64];
+	__shared__ int s_cls, s_n, s_cnt;
+	__shared__ int s_list[M2L_SLOTS2];
+	__shared__ uint32_t s_start, s_mask;
+	const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
 	if (tid == 0) {
 		uint32_t b = blockIdx.x, start = 0;
 		int cls = -1, nn = 0;
@@ -244,77 +284,111 @@ __global__ void __launch_bounds__(128) m2l2d_hankel_kernel(const double2* __rest
 			if (b < tiles) { cls = o; start += b * 64; nn = (int)min(64u, cnt - b * 64); break; }
 			b -= tiles; start += cnt;
 		}
-		s_cls = cls; s_n = nn; s_start = start;
+		s_cls = cls; s_n = nn; s_start = start; s_mask = 0;
 	}
-	if (tid < 64) sH[tid] = tid == 0 ? 0.0 : c_fact[tid - 1];
+	if (tid < 72) sH[tid] = tid == 0 || tid > 63 ? 0.0 : c_fact[tid - 1];
 	__syncthreads();
 	const int cls = s_cls;
 	if (cls < 0) return;
 	if (tid < 64) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
-	double ar[TM][2], ai[TM][2];
-#pragma unroll
-	for (int r = 0; r < TM; ++r) { ar[r][0] = ar[r][1] = ai[r][0] = ai[r][1] = 0.0; }
+	for (int e = N * H2_LD + tid; e < R4 * H2_LD; e += 128) Wc[e] = 0.0;   // rows N..R4-1 stay 0
 	__syncthreads();
-	for (int slot = slot0; slot < slot1; ++slot) {
-		int mine = -1;
-		if (tid < 64 && tgt[tid] >= 0) mine = vtab[(size_t)tgt[tid] * M2L_SLOTS2 + slot];
-		if (tid < 64) src[tid] = mine;
-		if (!__syncthreads_or(mine >= 0)) continue;
-		const double2* T = tab + (size_t)c_slot_dir2[cls][slot] * (2 * N + 1);
-		if (tid < N) spost[tid] = T[N + tid];
-		if (tid == 0) slg = T[2 * N];
-		for (int idx = tid; idx < 64 * N; idx += 128) {
-			const int c = idx / N, k = idx - c * N;
-			const int s = src[c];
-			const double2 a = s >= 0 ? mult[(size_t)s * N + k] : make_double2(0.0, 0.0);
-			const double2 p = T[k];
-			Wr[k][c] = a.x * p.x - a.y * p.y;
-			Wi[k][c] = a.x * p.y + a.y * p.x;
-		}
+	// every target's slot row (contiguous in vtab), and which slots are used
+	for (int idx = tid; idx < 64 * M2L_SLOTS2; idx += 128) {
+		const int c = idx / M2L_SLOTS2, sl = idx - c * M2L_SLOTS2;
+		const int32_t v = tgt[c] >= 0 ? vtab[(size_t)tgt[c] * M2L_SLOTS2 + sl] : -1;
+		srcs[sl * 65 + c] = v;
+		if (v >= 0 && sl >= slot0 && sl < slot1) atomicOr(&s_mask, 1u << sl);
+	}
+	__syncthreads();
+	if (tid == 0) {
+		int n = 0;
+		for (int sl = slot0; sl < slot1; ++sl)
+			if (s_mask >> sl & 1u) s_list[n++] = sl;
+		s_cnt = n;
+	}
+	__syncthreads();
+	const int nl = s_cnt;
+	auto issue = [&](int j) {
+		const int sl = s_list[j];
+		const int32_t* sr = srcs + sl * 65;
+		if (lane < N)                          // warp w: sources w, w + 4, ...; lane: coefficient
+			for (int c = w; c < 64; c += 4) {
+				const int32_t s = sr[c];
+				cp_async16(raw + c * RS + lane, s >= 0 ? mult + (size_t)s * N + lane : mult, s >= 0 ? 16 : 0);
+			}
+		if (tid < W2) cp_async16(sT + tid, tab + (size_t)c_slot_dir2[cls][sl] * W2 + tid, 16);
+		cp_async_commit();
+	};
+	double ar[MTL][4][2];                  // b of rows 8 mt + g, target 16 w + 4 nt + t4 (re, im)
+#pragma unroll
+	for (int mt = 0; mt < MTL; ++mt)
+#pragma unroll
+		for (int nt = 0; nt < 4; ++nt) ar[mt][nt][0] = ar[mt][nt][1] = 0.0;
+	if (nl > 0) issue(0);
+	for (int j = 0; j < nl; ++j) {
+		cp_async_wait<0>();
 		__syncthreads();
-		double sr[TM][2], si[TM][2];
+		{
+			const int c = tid & 63;            // source c, coefficients k = tid / 64 + 2 m
+			for (int k = tid >> 6; k < N; k += 2) {
+				const double2 a = raw[c * RS + k], p = sT[k];
+				*reinterpret_cast<double2*>(Wc + k * H2_LD + 2 * c) =
+				    make_double2(a.x * p.x - a.y * p.y, a.x * p.y + a.y * p.x);
+			}
+		}
+		if (tid < N) spost[tid] = sT[N + tid];
+		if (tid == N) slg = sT[2 * N];
+		__syncthreads();
+		if (j + 1 < nl) issue(j + 1);          // lands while the MMAs run
+		double sacc[MTL][4][2];
 #pragma unroll
-		for (int r = 0; r < TM; ++r) { sr[r][0] = sr[r][1] = si[r][0] = si[r][1] = 0.0; }
-		for (int k = 0; k < N; ++k) {
-			const double br0 = Wr[k][tx], br1 = Wr[k][tx + 32], bi0 = Wi[k][tx], bi1 = Wi[k][tx + 32];
+		for (int mt = 0; mt < MTL; ++mt)
 #pragma unroll
-			for (int r = 0; r < TM; ++r) {
-				const double hk = sH[ty + 4 * r + k];
-				sr[r][0] = fma(hk, br0, sr[r][0]); sr[r][1] = fma(hk, br1, sr[r][1]);
-				si[r][0] = fma(hk, bi0, si[r][0]); si[r][1] = fma(hk, bi1, si[r][1]);
+			for (int nt = 0; nt < 4; ++nt) sacc[mt][nt][0] = sacc[mt][nt][1] = 0.0;
+		for (int k0 = 0; k0 < R4; k0 += 4) {
+			double bf[4];
+#pragma unroll
+			for (int nt = 0; nt < 4; ++nt) bf[nt] = Wc[(k0 + t4) * H2_LD + 32 * w + 8 * nt + g];
+#pragma unroll
+			for (int mt = 0; mt < MTL; ++mt) {
+				const double af = sH[8 * mt + g + k0 + t4];
+#pragma unroll
+				for (int nt = 0; nt < 4; ++nt) dmma_8x8x4(sacc[mt][nt][0], sacc[mt][nt][1], af, bf[nt]);
 			}
 		}
 #pragma unroll
-		for (int r = 0; r < TM; ++r) {
-			const int i = ty + 4 * r;
+		for (int mt = 0; mt < MTL; ++mt) {
+			const int i = 8 * mt + g;
 			if (i < N) {
 				const double2 p = spost[i];
 #pragma unroll
-				for (int j = 0; j < 2; ++j) {
-					ar[r][j] += p.x * sr[r][j] - p.y * si[r][j];
-					ai[r][j] += p.x * si[r][j] + p.y * sr[r][j];
+				for (int nt = 0; nt < 4; ++nt) {
+					const double sr_ = sacc[mt][nt][0], si_ = sacc[mt][nt][1];
+					ar[mt][nt][0] += p.x * sr_ - p.y * si_;
+					ar[mt][nt][1] += p.x * si_ + p.y * sr_;
 				}
 			}
 		}
-		if (ty == 0) {                         // b_0 += a_0 lg, a_0 = -W[0]
+		if (g == 0) {                          // row 0: b_0 += a_0 lg, a_0 = -W[0]
 			const double2 lg = slg;
 #pragma unroll
-			for (int j = 0; j < 2; ++j) {
-				const double a0r = -Wr[0][tx + 32 * j], a0i = -Wi[0][tx + 32 * j];
-				ar[0][j] += a0r * lg.x - a0i * lg.y;
-				ai[0][j] += a0r * lg.y + a0i * lg.x;
+			for (int nt = 0; nt < 4; ++nt) {
+				const int c = 16 * w + 4 * nt + t4;
+				const double a0r = -Wc[2 * c], a0i = -Wc[2 * c + 1];
+				ar[0][nt][0] += a0r * lg.x - a0i * lg.y;
+				ar[0][nt][1] += a0r * lg.y + a0i * lg.x;
 			}
 		}
-		__syncthreads();
 	}
 #pragma unroll
-	for (int j = 0; j < 2; ++j) {
-		const int tg = tgt[tx + 32 * j];
+	for (int nt = 0; nt < 4; ++nt) {
+		const int tg = tgt[16 * w + 4 * nt + t4];
 		if (tg < 0) continue;
 #pragma unroll
-		for (int r = 0; r < TM; ++r) {
-			const int i = ty + 4 * r;
-			if (i < N) loc[(size_t)tg * N + i] = make_double2(ar[r][j], ai[r][j]);
+		for (int mt = 0; mt < MTL; ++mt) {
+			const int i = 8 * mt + g;
+			if (i < N) loc[(size_t)tg * N + i] = make_double2(ar[mt][nt][0], ar[mt][nt][1]);
 		}
 	}
 }
@@ -579,13 +653,22 @@ int m2l_hankel2d(Context& ctx, const M2LPlan& plan, const double2* tab, const do
 	}
 	const dim3 grid(tiles, S);
 	cudaStream_t s = ctx.stream;
-	const int TM = N <= 8 ? 2 : N <= 16 ? 4 : N <= 24 ? 6 : 8;
-	switch (TM) {
-	case 2: m2l2d_hankel_kernel<2><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
-	case 4: m2l2d_hankel_kernel<4><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
-	case 6: m2l2d_hankel_kernel<6><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
-	default: m2l2d_hankel_kernel<8><<<grid, 128, 0, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells); break;
+	const int MTL = (N + 7) / 8;           // row tiles of 8
+	const size_t smem = hankel_smem(N);
+	auto go = [&](auto kern) -> cudaError_t {
+		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		if (e != cudaSuccess) return e;
+		kern<<<grid, 128, smem, s>>>(tab, mult, loc, plan.vtab, plan.order, plan.oct_count, N, part, plan.cells);
+		return cudaGetLastError();
+	};
+	cudaError_t e;
+	switch (MTL) {
+	case 1: e = go(m2l2d_hankel_kernel<1>); break;
+	case 2: e = go(m2l2d_hankel_kernel<2>); break;
+	case 3: e = go(m2l2d_hankel_kernel<3>); break;
+	default: e = go(m2l2d_hankel_kernel<4>); break;
 	}
+	if (e != cudaSuccess) return cuda_fail(ctx, e, "m2l2d_hankel_kernel");
 	if (S > 1) {
 		const size_t nel = plan.cells * (size_t)N * 2;
 		split_reduce_kernel<double><<<div_up(nel, 256), 256, 0, s>>>(reinterpret_cast<const double*>(part),
