@@ -505,6 +505,139 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const real* __restrict__ 
 	}
 }
 
+// 3D FP64 M2L on the FP64 tensor cores: C[MT x 64] = sum over the octant
+// class's non-empty slots of T_dir[MT x MT] B[MT x 64], B the gathered
+// source multipoles.  256 threads: warp (wm, wn) = (w & 3, w >> 2) owns row
+// tiles wm + 4 i (i < MTW) and target tiles 4 wn .. 4 wn + 3 (8 x 8 each),
+// FP64 accumulators in registers across all slots.  The operator columns
+// and source rows of the next 16-wide K chunk are staged by cp.async
+// (double buffered, zero-filled past R and where a target has no source);
+// both staged tiles are row-major with a row stride of 20 doubles, which
+// keeps the fragment reads conflict-free.
+constexpr int DG_LD = 20;
+
+inline size_t dmma_gemm_smem(int MT) { return sizeof(double) * 2 * (size_t)(MT + 64) * DG_LD; }
+
+template <int MTW>
+__global__ void __launch_bounds__(256, 1) m2l_gemm_dmma_kernel(const double* __restrict__ ops,
+                                                               const double* __restrict__ mult,
+                                                               double* __restrict__ loc,
+                                                               const int32_t* __restrict__ vtab,
+                                                               const int32_t* __restrict__ order,
+                                                               const uint32_t* __restrict__ oct_count, int R,
+                                                               int MT, double* __restrict__ part, size_t cells)
+{
+	const int S = gridDim.y, sidx = blockIdx.y;
+	const int slot0 = sidx * M2L_SLOTS / S, slot1 = (sidx + 1) * M2L_SLOTS / S;
+	if (S > 1) loc = part + (size_t)sidx * cells * R;
+	extern __shared__ __align__(16) double dsm_d[];
+	double* As = dsm_d;                                  // [2][MT][DG_LD]
+	double* Bs = dsm_d + 2 * MT * DG_LD;                 // [2][64][DG_LD]
+	__shared__ int32_t tgt[64];
+	__shared__ int16_t s_list[M2L_SLOTS];
+	__shared__ uint32_t s_mask[6];
+	__shared__ int s_oct, s_n, s_cnt;
+	__shared__ uint32_t s_start;
+	const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+	const int wm = w & 3, wn = w >> 2;
+	if (tid == 0) {
+		uint32_t b = blockIdx.x, start = 0;
+		int oct = -1, nn = 0;
+		for (int o = 0; o < 8; ++o) {
+			const uint32_t cnt = oct_count[o], tiles = (cnt + 63) / 64;
+			if (b < tiles) { oct = o; start += b * 64; nn = (int)min(64u, cnt - b * 64); break; }
+			b -= tiles; start += cnt;
+		}
+		s_oct = oct; s_n = nn; s_start = start;
+	}
+	if (tid < 6) s_mask[tid] = 0;
+	__syncthreads();
+	const int oct = s_oct;
+	if (oct < 0) return;
+	if (tid < 64) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
+	__syncthreads();
+	for (int idx = tid; idx < 64 * M2L_SLOTS; idx += 256) {
+		const int c = idx / M2L_SLOTS, sl = idx - c * M2L_SLOTS;
+		if (sl < slot0 || sl >= slot1 || tgt[c] < 0) continue;
+		if (vtab[(size_t)tgt[c] * M2L_SLOTS + sl] >= 0) atomicOr(&s_mask[sl >> 5], 1u << (sl & 31));
+	}
+	__syncthreads();
+	if (tid == 0) {
+		int n = 0;
+		for (int sl = slot0; sl < slot1; ++sl)
+			if (s_mask[sl >> 5] >> (sl & 31) & 1u) s_list[n++] = (int16_t)sl;
+		s_cnt = n;
+	}
+	__syncthreads();
+	const int KC = MT / 16;
+	const int iters = s_cnt * KC;
+	// B staging: thread (c, quarter) copies k = 16 kc + 4 quarter + {0..3} of target c's source
+	const int bc = tid & 63, bq = tid >> 6;
+	const int32_t my_tgt = tgt[bc];
+	auto issue = [&](int it, int buf) {
+		const int j = it / KC, kc = it - j * KC;
+		const int sl = s_list[j];
+		const double* A = ops + (size_t)c_slot_dir[oct][sl] * MT * MT + 16 * kc;
+		double* ad = As + (size_t)buf * MT * DG_LD;
+		for (int e = tid; e < MT * 8; e += 256) {
+			const int r = e >> 3, q = e & 7;
+			cp_async16(ad + r * DG_LD + 2 * q, A + (size_t)r * MT + 2 * q, 16);
+		}
+		const int32_t s = my_tgt >= 0 ? vtab[(size_t)my_tgt * M2L_SLOTS + sl] : -1;
+		double* bd = Bs + (size_t)buf * 64 * DG_LD + bc * DG_LD + 4 * bq;
+#pragma unroll
+		for (int h = 0; h < 2; ++h) {
+			const int k = 16 * kc + 4 * bq + 2 * h;
+			const bool ok = s >= 0 && k < R;
+			cp_async16(bd + 2 * h, ok ? mult + (size_t)s * R + k : mult, ok ? 16 : 0);
+		}
+		cp_async_commit();
+	};
+	double acc[MTW][4][2];
+#pragma unroll
+	for (int i = 0; i < MTW; ++i)
+#pragma unroll
+		for (int n = 0; n < 4; ++n) acc[i][n][0] = acc[i][n][1] = 0.0;
+	const int MTT = MT / 8;                    // row tiles
+	if (iters > 0) issue(0, 0);
+	for (int it = 0; it < iters; ++it) {
+		const int cur = it & 1;
+		if (it + 1 < iters) { issue(it + 1, cur ^ 1); cp_async_wait<1>(); }
+		else cp_async_wait<0>();
+		__syncthreads();
+		const double* a_ = As + (size_t)cur * MT * DG_LD;
+		const double* b_ = Bs + (size_t)cur * 64 * DG_LD;
+#pragma unroll
+		for (int ks = 0; ks < 4; ++ks) {
+			double bf[4];
+#pragma unroll
+			for (int n = 0; n < 4; ++n) bf[n] = b_[(8 * (4 * wn + n) + g) * DG_LD + 4 * ks + t4];
+#pragma unroll
+			for (int i = 0; i < MTW; ++i) {
+				const int mt = wm + 4 * i;
+				if (mt < MTT) {
+					const double af = a_[(8 * mt + g) * DG_LD + 4 * ks + t4];
+#pragma unroll
+					for (int n = 0; n < 4; ++n) dmma_8x8x4(acc[i][n][0], acc[i][n][1], af, bf[n]);
+				}
+			}
+		}
+		__syncthreads();                       // the buffer is refilled two iterations on
+	}
+#pragma unroll
+	for (int n = 0; n < 4; ++n)
+#pragma unroll
+		for (int h = 0; h < 2; ++h) {
+			const int tg = tgt[8 * (4 * wn + n) + 2 * t4 + h];
+			if (tg < 0) continue;
+#pragma unroll
+			for (int i = 0; i < MTW; ++i) {
+				const int r = 8 * (wm + 4 * i) + g;
+				if (r < R) loc[(size_t)tg * R + r] = acc[i][n][h];
+			}
+		}
+}
+
 template <typename real>
 __global__ void split_reduce_kernel(const real* __restrict__ part, real* __restrict__ loc, size_t n, int S)
 {
@@ -713,7 +846,31 @@ int gemm_rt(Context& ctx, const M2LPlan& plan, const real* ops, const real* mult
 	}
 	dim3 grid(tiles, S);
 	cudaStream_t s = ctx.stream;
-	if constexpr (DIM == 2) {
+	if constexpr (DIM == 3 && sizeof(real) == sizeof(double)) {
+		const size_t smem = dmma_gemm_smem(MT);
+		const int mtw = (MT / 8 + 3) / 4;
+		auto go = [&](auto kern) -> cudaError_t {
+			cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+			if (e != cudaSuccess) return e;
+			kern<<<grid, 256, smem, s>>>(reinterpret_cast<const double*>(ops), reinterpret_cast<const double*>(mult),
+			                             reinterpret_cast<double*>(loc), plan.vtab, plan.order, plan.oct_count, R, MT,
+			                             reinterpret_cast<double*>(part), plan.cells);
+			return cudaGetLastError();
+		};
+		cudaError_t e;
+		switch (mtw) {
+		case 1: e = go(m2l_gemm_dmma_kernel<1>); break;
+		case 2: e = go(m2l_gemm_dmma_kernel<2>); break;
+		case 3: e = go(m2l_gemm_dmma_kernel<3>); break;
+		case 4: e = go(m2l_gemm_dmma_kernel<4>); break;
+		case 5: e = go(m2l_gemm_dmma_kernel<5>); break;
+		case 6: e = go(m2l_gemm_dmma_kernel<6>); break;
+		case 7: e = go(m2l_gemm_dmma_kernel<7>); break;
+		case 8: e = go(m2l_gemm_dmma_kernel<8>); break;
+		default: ctx.last_error = "m2l gemm: order too large"; return ERR_UNSUPPORTED;
+		}
+		if (e != cudaSuccess) return cuda_fail(ctx, e, "m2l_gemm_dmma_kernel");
+	} else if constexpr (DIM == 2) {
 		switch (MT / 16) {
 		case 1: launch_gemm<real, 1, 2>(grid, s, ops, mult, loc, plan, R, part); break;
 		case 2: launch_gemm<real, 2, 2>(grid, s, ops, mult, loc, plan, R, part); break;
