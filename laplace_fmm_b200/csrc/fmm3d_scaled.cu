@@ -115,8 +115,16 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 			l2l_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, inner + t.loff[L - 1] * Nx2,
 			                                                                     inner + t.loff[L] * Nx2, N, T, ctx.dev_flags);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s));
-	constexpr int LW = leaf_warps<real>();
-	leaves_scaled_kernel<real><<<div_up(nl, LW), LW * 32, 0, s>>>(t, qr, outer, inner, N, knm, pot, field);
+	if constexpr (sizeof(real) == sizeof(float)) {
+		// near field and expansions as two kernels (the near field's few
+		// registers keep many warps resident)
+		constexpr int LWP = 8, LWE = leaf_warps<real>();
+		p2p_f32_kernel<LWP><<<div_up(nl, LWP), LWP * 32, 0, s>>>(t, qr, pot, field);
+		eval_scaled_kernel<real, LWE><<<div_up(nl, LWE), LWE * 32, 0, s>>>(t, outer, inner, N, knm, pot, field);
+	} else {
+		constexpr int LW = leaf_warps<real>();
+		leaves_scaled_kernel<real><<<div_up(nl, LW), LW * 32, 0, s>>>(t, qr, outer, inner, N, knm, pot, field);
+	}
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[5], s));
 	LFMM_CUDA(ctx, cudaGetLastError());
 	(void)stats;

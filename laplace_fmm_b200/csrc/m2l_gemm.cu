@@ -31,22 +31,28 @@ __device__ __forceinline__ void coords3(uint64_t code, int* c)
 
 // Fill the V table of level L: slot of each far source in the target's
 // octant class; the candidates are the children of the parent's close cells
-// and of the parent (reference cpu/morton_tree.cpp:147-208).
+// and of the parent (reference cpu/morton_tree.cpp:147-208).  A warp per
+// target cell: the row is first set to -1, then lane e places the far
+// children of the parent's e-th close cell (the parent itself last), so
+// every store of the warp lands in the same row.
 __global__ void vtab_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsigned* flags)
 {
-	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-	size_t m = t.lsize[L];
+	const int lane = threadIdx.x & 31;
+	const size_t c = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const size_t m = t.lsize[L];
 	if (c >= m) return;
-	size_t off = t.loff[L], poff = t.loff[L - 1];
+	int32_t* row = vtab + c * M2L_SLOTS;
+	for (int sl = lane; sl < M2L_SLOTS; sl += 32) row[sl] = -1;
+	__syncwarp();
+	const size_t off = t.loff[L], poff = t.loff[L - 1];
 	int me[3];
 	coords3(t.code[off + c], me);
-	int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
-	int32_t* row = vtab + c * M2L_SLOTS;
-	int32_t p = t.parent[off + c];
-	int npc = t.close_cnt[poff + p];
+	const int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
+	const int32_t p = t.parent[off + c];
+	const int npc = t.close_cnt[poff + p];
 	const int32_t* pl = t.close_idx + (poff + p) * t.close_stride;
-	for (int e = 0; e <= npc; ++e) {
-		int32_t pn = e < npc ? pl[e] : p;
+	for (int e = lane; e <= npc; e += 32) {
+		const int32_t pn = e < npc ? pl[e] : p;
 		for (uint32_t k = t.beg[poff + pn]; k < t.end[poff + pn]; ++k) {
 			if (k == c) continue;
 			int o[3];
@@ -821,11 +827,11 @@ int m2l_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan)
 	plan.oct_count = static_cast<uint32_t*>(ctx.arena.take(sizeof(uint32_t) * 16));
 	if (!plan.vtab || !plan.order || !plan.oct_count) { ctx.last_error = "m2l plan: allocation failed"; return ERR_OOM; }
 	cudaStream_t s = ctx.stream;
-	LFMM_CUDA(ctx, cudaMemsetAsync(plan.vtab, 0xff, sizeof(int32_t) * m * M2L_SLOTS, s));
 	LFMM_CUDA(ctx, cudaMemsetAsync(plan.oct_count, 0, sizeof(uint32_t) * 16, s));
+	if (m == 0) return OK;
 	count_oct_kernel<<<div_up(m, 256), 256, 0, s>>>(t, L, plan.oct_count);
 	scatter_oct_kernel<<<div_up(m, 256), 256, 0, s>>>(t, L, plan.oct_count, plan.order);
-	vtab_kernel<<<div_up(m, 128), 128, 0, s>>>(t, L, plan.vtab, ctx.dev_flags);
+	vtab_kernel<<<div_up(m * 32, 256), 256, 0, s>>>(t, L, plan.vtab, ctx.dev_flags);   // warp per cell
 	LFMM_CUDA(ctx, cudaGetLastError());
 	return OK;
 }

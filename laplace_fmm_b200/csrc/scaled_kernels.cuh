@@ -517,5 +517,190 @@ __global__ void __launch_bounds__(LW * 32) leaves_scaled_kernel(DevTree t, const
 	}
 }
 
+// FP32 near field on its own (few registers, high occupancy): one warp per
+// leaf, targets in passes of up to 32; a pass of np <= 16 targets runs
+// TP = np rounded up to a power of two targets at once and splits the
+// sources into 32 / TP phases (groups of 4), summed by shuffles.  Sources of
+// the leaf and its U list are staged 32 at a time as hi + lo offsets in the
+// target leaf's frame, padded with zero charges to a multiple of 4 and read
+// as float4; the self pair is only tested for in the leaf's own chunks.
+// Partial sums over 16 sources in FP32, carried in FP64; 1/r from the
+// hardware approximation (relative error below 2^-22.9; r^2 >= 1e-8 is never
+// subnormal).  Writes pot (with the reference's self term) and field in
+// input order; the expansions are added by eval_scaled_kernel.
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+	float y;
+	asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+	return y;
+}
+
+template <bool SELF>
+__device__ __forceinline__ void p2p_f32_chunk(const float* __restrict__ sx, const float* __restrict__ sy,
+                                              const float* __restrict__ sz, const float* __restrict__ lx,
+                                              const float* __restrict__ ly, const float* __restrict__ lz,
+                                              const float* __restrict__ sq, int cnt4, int jb, int js, int self,
+                                              float xi, float yi, float zi, float xl, float yl, float zl,
+                                              double& pot, double& fx, double& fy, double& fz)
+{
+	for (int j0 = jb; j0 < cnt4; j0 += 4 * js) {
+		float p = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+		for (int h = 0; h < 4; ++h) {
+			const int j = j0 + js * h;
+			if (j < cnt4) {
+				const float4 X = *reinterpret_cast<const float4*>(sx + j), Y = *reinterpret_cast<const float4*>(sy + j);
+				const float4 Z = *reinterpret_cast<const float4*>(sz + j), XL = *reinterpret_cast<const float4*>(lx + j);
+				const float4 YL = *reinterpret_cast<const float4*>(ly + j), ZL = *reinterpret_cast<const float4*>(lz + j);
+				const float4 Q = *reinterpret_cast<const float4*>(sq + j);
+				const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w}, zs[4] = {Z.x, Z.y, Z.z, Z.w};
+				const float xls[4] = {XL.x, XL.y, XL.z, XL.w}, yls[4] = {YL.x, YL.y, YL.z, YL.w};
+				const float zls[4] = {ZL.x, ZL.y, ZL.z, ZL.w}, qs[4] = {Q.x, Q.y, Q.z, Q.w};
+#pragma unroll
+				for (int k = 0; k < 4; ++k) {
+					const float dx = (xi - xs[k]) + (xl - xls[k]);
+					const float dy = (yi - ys[k]) + (yl - yls[k]);
+					const float dz = (zi - zs[k]) + (zl - zls[k]);
+					const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), (float)FORCE_EPS2);
+					const float inv = rsqrt_approx(r2);
+					const float qi = (SELF && j + k == self) ? 0.f : qs[k] * inv;
+					const float qi3 = qi * (inv * inv);
+					p += qi;
+					ax = fmaf(dx, qi3, ax); ay = fmaf(dy, qi3, ay); az = fmaf(dz, qi3, az);
+				}
+			}
+		}
+		pot += p; fx += ax; fy += ay; fz += az;
+	}
+}
+
+template <int LW>
+__global__ void __launch_bounds__(LW * 32, 768 / (LW * 32)) p2p_f32_kernel(DevTree t, const float* __restrict__ qr,
+                                                         double* __restrict__ pot_out, double* __restrict__ fld_out)
+{
+	__shared__ __align__(16) float sx[LW][32], sy[LW][32], sz[LW][32], sq[LW][32];
+	__shared__ __align__(16) float lx[LW][32], ly[LW][32], lz[LW][32];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const size_t li = (size_t)blockIdx.x * LW + w;
+	if (li >= t.nleaves) return;
+	const size_t g = t.leaves[li];
+	const uint32_t tb = t.tbeg[g], te = t.tend[g];
+	if (tb >= te) return;
+	const bool tmode = t.targets_num > 0;
+	const uint32_t ub = t.u_off[li], ue = t.u_off[li + 1];
+	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
+		const int np = (int)min(32u, te - t0);
+		int lt = 0;                            // log2 of the targets run at once
+		while ((1 << lt) < np) ++lt;
+		const int ti = lane & ((1 << lt) - 1), ph = lane >> lt, G = 32 >> lt;
+		const uint32_t i = t0 + ti;
+		const bool valid = ti < np;
+		float xi = 0.f, yi = 0.f, zi = 0.f, xl = 0.f, yl = 0.f, zl = 0.f;
+		if (valid) {
+			const double ax_ = t.x[i] - cx, ay_ = t.y[i] - cy, az_ = t.z[i] - cz;
+			xi = (float)ax_; yi = (float)ay_; zi = (float)az_;
+			xl = (float)(ax_ - (double)xi); yl = (float)(ay_ - (double)yi); zl = (float)(az_ - (double)zi);
+		}
+		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+		for (int64_t e = (int64_t)ub - 1; e < (int64_t)ue; ++e) {
+			const bool own = e < (int64_t)ub;
+			const size_t sc_ = own ? g : (size_t)t.u_idx[e];
+			const uint32_t sb = t.pbeg[sc_], se = t.send[sc_];
+			for (uint32_t s0 = sb; s0 < se; s0 += 32) {
+				const int cnt = min(32u, se - s0), cnt4 = (cnt + 3) & ~3;
+				__syncwarp();
+				if (lane < cnt) {
+					const uint32_t j = s0 + lane;
+					const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
+					const float hx = (float)dx_, hy = (float)dy_, hz = (float)dz_;
+					sx[w][lane] = hx; sy[w][lane] = hy; sz[w][lane] = hz;
+					lx[w][lane] = (float)(dx_ - (double)hx); ly[w][lane] = (float)(dy_ - (double)hy);
+					lz[w][lane] = (float)(dz_ - (double)hz);
+					sq[w][lane] = qr[j];
+				} else if (lane < cnt4) {
+					sx[w][lane] = sy[w][lane] = sz[w][lane] = 0.f;
+					lx[w][lane] = ly[w][lane] = lz[w][lane] = 0.f;
+					sq[w][lane] = 0.f;
+				}
+				__syncwarp();
+				if (valid) {
+					if (own)
+						p2p_f32_chunk<true>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G,
+						                    (int)(i - s0), xi, yi, zi, xl, yl, zl, pot, fx, fy, fz);
+					else
+						p2p_f32_chunk<false>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G, -1, xi,
+						                     yi, zi, xl, yl, zl, pot, fx, fy, fz);
+				}
+			}
+		}
+		for (int o = 1 << lt; o < 32; o <<= 1) {
+			pot += __shfl_xor_sync(0xffffffffu, pot, o);
+			fx += __shfl_xor_sync(0xffffffffu, fx, o);
+			fy += __shfl_xor_sync(0xffffffffu, fy, o);
+			fz += __shfl_xor_sync(0xffffffffu, fz, o);
+		}
+		if (valid && ph == 0) {
+			if (!tmode) pot += t.q[i] * (1.0 / FORCE_EPS);
+			const uint32_t o = t.orig[i];
+			pot_out[o] = pot;
+			fld_out[3 * (size_t)o] = fx; fld_out[3 * (size_t)o + 1] = fy; fld_out[3 * (size_t)o + 2] = fz;
+		}
+	}
+}
+
+// M2P over the W list and L2P of the leaf's local expansion, added onto the
+// near field already in the outputs: one warp per leaf, lane = target.
+template <typename real, int LW>
+__global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const typename V2<real>::t* __restrict__ outer,
+                                                             const typename V2<real>::t* __restrict__ inner, int N,
+                                                             const real* __restrict__ knm, double* __restrict__ pot_out,
+                                                             double* __restrict__ fld_out)
+{
+	using v2 = typename V2<real>::t;
+	__shared__ v2 sL[LW][NX2MAX], sM[LW][NX2MAX];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const size_t li = (size_t)blockIdx.x * LW + w;
+	if (li >= t.nleaves) return;
+	const size_t g = t.leaves[li];
+	const uint32_t tb = t.tbeg[g], te = t.tend[g];
+	if (tb >= te) return;
+	const int Nx2 = N * (N + 1) / 2;
+	const double ihg = 1.0 / cell_size(t, g);
+	for (int c = lane; c < Nx2; c += 32) sL[w][c] = inner[g * Nx2 + c];
+	const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
+	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+	__syncwarp();
+	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
+		const uint32_t i = t0 + lane;
+		const bool valid = i < te;
+		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+		for (uint32_t e = wb; e < we; ++e) {
+			const size_t D = t.w_idx[e];
+			__syncwarp();
+			for (int c = lane; c < Nx2; c += 32) sM[w][c] = outer[D * Nx2 + c];
+			__syncwarp();
+			if (valid) {
+				const double ihd = 1.0 / cell_size(t, D);
+				real mp, mx_, my_, mz_;
+				eval_expansion<false, real>(sM[w], (real)((t.x[i] - t.cx[D]) * ihd), (real)((t.y[i] - t.cy[D]) * ihd),
+				                            (real)((t.z[i] - t.cz[D]) * ihd), N, knm, mp, mx_, my_, mz_);
+				pot += (double)mp * ihd;
+				fx += (double)mx_ * ihd * ihd; fy += (double)my_ * ihd * ihd; fz += (double)mz_ * ihd * ihd;
+			}
+		}
+		if (valid) {
+			real lp, lx_, ly_, lz_;
+			eval_expansion<true, real>(sL[w], (real)((t.x[i] - cx) * ihg), (real)((t.y[i] - cy) * ihg),
+			                           (real)((t.z[i] - cz) * ihg), N, knm, lp, lx_, ly_, lz_);
+			pot += (double)lp * ihg;
+			fx += (double)lx_ * ihg * ihg; fy += (double)ly_ * ihg * ihg; fz += (double)lz_ * ihg * ihg;
+			const uint32_t o = t.orig[i];
+			pot_out[o] += pot;
+			fld_out[3 * (size_t)o] += fx; fld_out[3 * (size_t)o + 1] += fy; fld_out[3 * (size_t)o + 2] += fz;
+		}
+	}
+}
+
 } // namespace scaled
 } // namespace lfmm
