@@ -356,6 +356,14 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	}
 	for (auto& e : c.ev) cudaEventCreate(&e);
 	for (auto& e : c.kev) cudaEventCreate(&e);
+	int prio_lo = 0, prio_hi = 0;
+	if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
+	    cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming) != cudaSuccess) {
+		lfmm_destroy(ctx);
+		return LFMM_ERR_CUDA;
+	}
 	cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
 	if (tables_build(c) != OK) {
 		lfmm_destroy(ctx);
@@ -371,13 +379,17 @@ void lfmm_destroy(lfmm_ctx* ctx)
 	Context& c = ctx->c;
 	cudaSetDevice(c.device);
 	if (c.stream) cudaStreamSynchronize(c.stream);
+	if (c.side) cudaStreamSynchronize(c.side);
 	c.arena.release();
 	for (auto& e : c.opcache) cudaFree(e.ptr);
 	c.opcache.clear();
 	tables_free(c.tables);
 	for (auto& e : c.ev) if (e) cudaEventDestroy(e);
 	for (auto& e : c.kev) if (e) cudaEventDestroy(e);
+	if (c.fork_ev) cudaEventDestroy(c.fork_ev);
+	if (c.join_ev) cudaEventDestroy(c.join_ev);
 	if (c.dev_flags) cudaFree(c.dev_flags);
+	if (c.side) cudaStreamDestroy(c.side);
 	if (c.stream) cudaStreamDestroy(c.stream);
 	delete ctx;
 }

@@ -93,6 +93,8 @@ struct Context {
 	std::string last_error;
 	int verbose = 0;
 	cudaEvent_t ev[16] = {};
+	cudaStream_t side = nullptr;        // lowest-priority stream for work that overlaps a solve
+	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 	cudaEvent_t kev[32] = {};          // pairs around the tensor-core M2L launches (timing)
 	int kev_used = 0;
 	// M2L autotuner: slot split chosen per (operator rows, level-size bucket);

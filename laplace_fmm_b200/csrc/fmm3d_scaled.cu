@@ -3,6 +3,7 @@
 // M2L accumulation on levels 2-3, FP64 tile sums and self term).
 // Passes: P2M (every leaf, any level) -> M2M -> M2L (V, direction GEMMs) ->
 // P2L (X) -> L2L -> leaves: P2P (self + U), M2P (W), L2P.
+#include <cmath>
 #include "scaled_kernels.cuh"
 #include "m2l_tc.cuh"
 #include <algorithm>
@@ -19,9 +20,22 @@ int upload_scaled_constants(Context& ctx)
 {
 	if (ctx.device < 0 || ctx.device >= 64) { ctx.last_error = "device index above 63"; return ERR_ARG; }
 	if (g_scaled_const_ready[ctx.device]) return OK;
-	unsigned char n_of[NX2MAX], m_of[NX2MAX];
-	for (int n = 0; n < MAXN3; ++n)
-		for (int m = 0; m <= n; ++m) { n_of[tix(n, m)] = (unsigned char)n; m_of[tix(n, m)] = (unsigned char)m; }
+	unsigned char n_of[NXD], m_of[NXD];
+	float2 rec_f[NXD];
+	double2 rec_d[NXD];
+	float sig_f[MAXN3 + 2];
+	double sig_d[MAXN3 + 2];
+	for (int n = 0; n <= MAXN3; ++n)
+		for (int m = 0; m <= n; ++m) {
+			const int i = tix(n, m);
+			n_of[i] = (unsigned char)n; m_of[i] = (unsigned char)m;
+			const double d1 = (double)(n + 1) * (n + 1) - (double)m * m;
+			rec_d[i] = make_double2((2.0 * n + 1.0) / std::sqrt(d1), std::sqrt(((double)n * n - (double)m * m) / d1));
+			rec_f[i] = make_float2((float)rec_d[i].x, (float)rec_d[i].y);
+		}
+	sig_d[0] = 0.0;
+	for (int m = 1; m <= MAXN3 + 1; ++m) sig_d[m] = -std::sqrt((2.0 * m - 1.0) / (2.0 * m));
+	for (int m = 0; m <= MAXN3 + 1; ++m) sig_f[m] = (float)sig_d[m];
 	float inv_f[NINV];
 	double inv_d[NINV];
 	inv_f[0] = 0.f; inv_d[0] = 0.0;
@@ -30,6 +44,10 @@ int upload_scaled_constants(Context& ctx)
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_m_of, m_of, sizeof(m_of)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_f, inv_f, sizeof(inv_f)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_d, inv_d, sizeof(inv_d)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_rec_f, rec_f, sizeof(rec_f)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_rec_d, rec_d, sizeof(rec_d)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_sig_f, sig_f, sizeof(sig_f)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_sig_d, sig_d, sizeof(sig_d)));
 	g_scaled_const_ready[ctx.device] = true;
 	return OK;
 }
@@ -118,9 +136,9 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 	if constexpr (sizeof(real) == sizeof(float)) {
 		// near field and expansions as two kernels (the near field's few
 		// registers keep many warps resident)
-		constexpr int LWP = 8, LWE = leaf_warps<real>();
+		constexpr int LWP = 8, LWE = eval_warps<real>();
 		p2p_f32_kernel<LWP><<<div_up(nl, LWP), LWP * 32, 0, s>>>(t, qr, pot, field);
-		eval_scaled_kernel<real, LWE><<<div_up(nl, LWE), LWE * 32, 0, s>>>(t, outer, inner, N, knm, pot, field);
+		eval_scaled_kernel<real, LWE><<<div_up(nl, LWE), LWE * 32, 0, s>>>(t, outer, inner, N, pot, field);
 	} else {
 		constexpr int LW = leaf_warps<real>();
 		leaves_scaled_kernel<real><<<div_up(nl, LW), LW * 32, 0, s>>>(t, qr, outer, inner, N, knm, pot, field);

@@ -286,13 +286,15 @@ double predicted_log10(const double* e, int p)
 // per-leaf errors aggregated over the leaves, divided by the RMS potential
 // rms) is within tol * margin (N = p + 1), or the fallback order when none
 // is.  Synchronises (reads six sums).
-int learned_order(Context& ctx, const DevTree& t, const float* params, double tol, double rms, int& N, double& pred)
+// The network's per-order error sums over the leaves (device, NO + 1
+// doubles): features, forward pass and reduction, launched on the stream.
+int learned_predict_launch(Context& ctx, const DevTree& t, const float* params, double*& acc)
 {
 	const size_t nl = t.nleaves;
 	float* feats = take<float>(ctx, nl * NF);
 	float* w = take<float>(ctx, nl);
 	float* Y = take<float>(ctx, nl * NO);
-	double* acc = take<double>(ctx, NO + 1);
+	acc = take<double>(ctx, NO + 1);
 	if (!feats || !w || !Y || !acc) { ctx.last_error = "learned order: allocation failed"; return ERR_OOM; }
 	int st = features_device(ctx, t, feats, w);
 	if (st) return st;
@@ -300,6 +302,14 @@ int learned_order(Context& ctx, const DevTree& t, const float* params, double to
 	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * (NO + 1), ctx.stream));
 	const unsigned blocks = (unsigned)std::min<size_t>(div_up(std::max<size_t>(nl, 1), 256), 4 * (size_t)ctx.num_sms);
 	predict_reduce_kernel<<<blocks, 256, 0, ctx.stream>>>(Y, w, nl, acc);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+// The order from the sums of learned_predict_launch and the RMS of the
+// sampled potential.  Synchronises.
+int learned_pick(Context& ctx, const double* acc, double tol, double rms, int& N, double& pred)
+{
 	double h[NO + 1];
 	LFMM_CUDA(ctx, cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
@@ -317,14 +327,25 @@ int learned_order(Context& ctx, const DevTree& t, const float* params, double to
 }
 
 // The FP64 direct sum at m outputs spread evenly through the output range:
-// positions sp, potential ep and field ef at them; *rms = RMS of the
-// potential without the self term.  Synchronises.
+// positions sp, potential ep and field ef at them, and the sum of squares of
+// the potential without the self term in acc[0].  Launched on the context's
+// lowest-priority side stream, forked from the main stream, so that it runs
+// beside the tree build and the order prediction; samples_join makes the
+// main stream wait for it and returns the RMS.
 struct Samples {
 	size_t m = 0, stride = 1;
 	double *sp = nullptr, *ep = nullptr, *ef = nullptr, *acc = nullptr;
 };
 
-int direct_samples(Context& ctx, const ParticleInput& in, size_t m, Samples& S, double* rms)
+// Swaps the context's stream for the side stream while in scope.
+struct OnSideStream {
+	Context& c;
+	cudaStream_t main;
+	explicit OnSideStream(Context& c_) : c(c_), main(c_.stream) { c.stream = c.side; }
+	~OnSideStream() { c.stream = main; }
+};
+
+int direct_samples_launch(Context& ctx, const ParticleInput& in, size_t m, Samples& S)
 {
 	const size_t n_out = in.nt ? in.nt : in.ns;
 	S.m = std::min(m, n_out);
@@ -335,17 +356,36 @@ int direct_samples(Context& ctx, const ParticleInput& in, size_t m, Samples& S, 
 	S.ef = take<double>(ctx, 3 * S.m);
 	S.acc = take<double>(ctx, 4);
 	if (!S.sp || !S.ep || !S.ef || !S.acc) { ctx.last_error = "sampled check: allocation failed"; return ERR_OOM; }
-	cudaStream_t s = ctx.stream;
-	sample_points_kernel<<<div_up(S.m, 256), 256, 0, s>>>(pts, S.stride, S.m, S.sp);
-	int st = direct_device(ctx, 3, in.ns, in.src, in.srcq, S.m, S.sp, S.ep, S.ef, /*fast=*/true);
-	if (st) return st;
-	// the RMS: the check against the direct sum itself (pot = direct, zero error)
-	LFMM_CUDA(ctx, cudaMemsetAsync(S.acc, 0, sizeof(double) * 4, s));
-	rms_kernel<<<(unsigned)std::min<size_t>(div_up(S.m, 256), 64), 256, 0, s>>>(S.ep, S.stride, S.m,
-	                                                                              in.nt ? nullptr : in.srcq, S.acc);
+	LFMM_CUDA(ctx, cudaEventRecord(ctx.fork_ev, ctx.stream));
+	LFMM_CUDA(ctx, cudaStreamWaitEvent(ctx.side, ctx.fork_ev, 0));
+	int st = OK;
+	{
+		OnSideStream on_side(ctx);
+		cudaStream_t s = ctx.stream;
+		sample_points_kernel<<<div_up(S.m, 256), 256, 0, s>>>(pts, S.stride, S.m, S.sp);
+		st = direct_device(ctx, 3, in.ns, in.src, in.srcq, S.m, S.sp, S.ep, S.ef, /*fast=*/true);
+		if (st == OK) {
+			// the RMS: the check against the direct sum itself (pot = direct, zero error)
+			cudaError_t e = cudaMemsetAsync(S.acc, 0, sizeof(double) * 4, s);
+			if (e == cudaSuccess) {
+				rms_kernel<<<(unsigned)std::min<size_t>(div_up(S.m, 256), 64), 256, 0, s>>>(
+					S.ep, S.stride, S.m, in.nt ? nullptr : in.srcq, S.acc);
+				e = cudaGetLastError();
+			}
+			if (e == cudaSuccess) e = cudaEventRecord(ctx.join_ev, s);
+			if (e != cudaSuccess) st = cuda_fail(ctx, e, "sampled direct sums");
+		}
+	}
+	if (st) cudaStreamSynchronize(ctx.side);   // nothing of it outlives the failed solve
+	return st;
+}
+
+int samples_join(Context& ctx, const Samples& S, double* rms)
+{
+	LFMM_CUDA(ctx, cudaStreamWaitEvent(ctx.stream, ctx.join_ev, 0));
 	double h;
-	LFMM_CUDA(ctx, cudaMemcpyAsync(&h, S.acc, sizeof(double), cudaMemcpyDeviceToHost, s));
-	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+	LFMM_CUDA(ctx, cudaMemcpyAsync(&h, S.acc, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+	LFMM_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
 	*rms = std::sqrt(h / (double)S.m);
 	return OK;
 }
@@ -383,16 +423,21 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	const bool timing = ctx.timing != 0;
 	ctx.kev_used = 0;
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
-	DevTree t;
-	int st = tree_build_adaptive(ctx, in, depth, max_leaf, t);
-	if (st) return st;
-	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
 	Samples S;
+	int st = direct_samples_launch(ctx, in, (size_t)check_targets, S);
+	if (st) return st;
+	DevTree t;
+	double* pacc = nullptr;
 	double rms = 0.0;
-	if ((st = direct_samples(ctx, in, (size_t)check_targets, S, &rms))) return st;
+	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t)) ||
+	    (timing && (st = cudaEventRecord(ctx.ev[1], s) == cudaSuccess ? OK : ERR_CUDA)) ||
+	    (st = learned_predict_launch(ctx, t, params, pacc)) || (st = samples_join(ctx, S, &rms))) {
+		cudaStreamSynchronize(ctx.side);
+		return st;
+	}
 	int N = FB_N;
 	double pred = 0.0;
-	if ((st = learned_order(ctx, t, params, tol, rms, N, pred))) return st;
+	if ((st = learned_pick(ctx, pacc, tol, rms, N, pred))) return st;
 	lfmm_learned_info li{};
 	li.predicted_N = N;
 	li.predicted_error = pred;

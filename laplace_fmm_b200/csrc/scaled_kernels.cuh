@@ -17,8 +17,31 @@ constexpr int CMAX = (MAXN3 * (MAXN3 + 1) / 2 + 31) / 32;
 constexpr int NX2MAX = MAXN3 * (MAXN3 + 1) / 2;
 constexpr int WPB = 4;
 
-__constant__ unsigned char c_n_of[NX2MAX];
-__constant__ unsigned char c_m_of[NX2MAX];
+template <typename real> struct V2;
+template <> struct V2<double> { using t = double2; static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); } };
+template <> struct V2<float> { using t = float2; static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); } };
+
+constexpr int NXD = (MAXN3 + 1) * (MAXN3 + 2) / 2;   // coefficients of degree <= MAXN3
+__constant__ unsigned char c_n_of[NXD];
+__constant__ unsigned char c_m_of[NXD];
+// Solid harmonics in Cartesian form, orthonormal basis B_nm = r^n Y_nm
+// (regular) and r^-(n+1) Y_nm (irregular), Y_nm = sqrt((n-m)!/(n+m)!)
+// P_n^m(cos t) e^{i m phi} with the Condon-Shortley phase:
+//   B_00 = 1 (or 1/r), B_mm = s_m w B_{m-1,m-1}, w = x + iy (or w / r^2),
+//   s_m = -sqrt((2m - 1) / (2m)),
+//   B_{n+1,m} = a_nm z B_nm - b_nm r^2 B_{n-1,m}   (or (a z B_nm - b B_{n-1,m}) / r^2)
+// with (a_nm, b_nm) = ((2n + 1) / sqrt((n+1)^2 - m^2), sqrt((n^2 - m^2) / ((n+1)^2 - m^2)))
+// stored at tix(n, m).
+__constant__ float2 c_rec_f[NXD];
+__constant__ double2 c_rec_d[NXD];
+__constant__ float c_sig_f[MAXN3 + 2];
+__constant__ double c_sig_d[MAXN3 + 2];
+template <typename real> __device__ __forceinline__ typename V2<real>::t rec_c(int i);
+template <> __device__ __forceinline__ float2 rec_c<float>(int i) { return c_rec_f[i]; }
+template <> __device__ __forceinline__ double2 rec_c<double>(int i) { return c_rec_d[i]; }
+template <typename real> __device__ __forceinline__ real sig_c(int m);
+template <> __device__ __forceinline__ float sig_c<float>(int m) { return c_sig_f[m]; }
+template <> __device__ __forceinline__ double sig_c<double>(int m) { return c_sig_d[m]; }
 constexpr int NINV = 64;
 __constant__ float c_inv_f[NINV];      // 1 / k (k >= 1), rounded to FP32
 __constant__ double c_inv_d[NINV];     // 1 / k, FP64
@@ -26,9 +49,6 @@ template <typename real> __device__ __forceinline__ real inv_of(int k);
 template <> __device__ __forceinline__ float inv_of<float>(int k) { return c_inv_f[k]; }
 template <> __device__ __forceinline__ double inv_of<double>(int k) { return c_inv_d[k]; }
 
-template <typename real> struct V2;
-template <> struct V2<double> { using t = double2; static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); } };
-template <> struct V2<float> { using t = float2; static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); } };
 
 template <typename real>
 struct Tab {
@@ -517,6 +537,119 @@ __global__ void __launch_bounds__(LW * 32) leaves_scaled_kernel(DevTree t, const
 	}
 }
 
+// Expansion evaluation through Cartesian solid harmonics.  A real field
+// phi = sum_{n, m >= 0} (2 - d_m0) Re(E_nm B_nm) (E stored for m >= 0; the
+// m < 0 coefficients are (-1)^m conj(E_n|m|)) has, with the derivative rules
+//   regular:   d_z B_nm = sqrt((n-m)(n+m)) B_{n-1,m},
+//              (d_x + i d_y) B_nm = sqrt((n-m)(n-m-1)) B_{n-1,m+1},
+//              (d_x - i d_y) B_nm = -sqrt((n+m)(n+m-1)) B_{n-1,m-1},
+//   irregular: d_z B_nm = -sqrt((n+1-m)(n+1+m)) B_{n+1,m},
+//              (d_x + i d_y) B_nm = sqrt((n+m+1)(n+m+2)) B_{n+1,m+1},
+//              (d_x - i d_y) B_nm = -sqrt((n-m+1)(n-m+2)) B_{n+1,m-1},
+// a gradient that is again a real field in the same basis, of degree one
+// less (local) or one more (multipole).  derive_coefs turns E into the
+// potential's and the three gradient components' coefficients, the weight
+// (2 - d_m0) folded in; eval_cart streams one target's harmonics through the
+// recurrences and takes the four dot products.
+template <typename real>
+__device__ __forceinline__ typename V2<real>::t coef_full(const typename V2<real>::t* __restrict__ E, int N, int n, int m)
+{
+	using v2 = typename V2<real>::t;
+	if (n < 0 || n >= N || m > n || -m > n) return V2<real>::make(0, 0);
+	if (m == 0) return V2<real>::make(E[tix(n, 0)].x, 0);
+	if (m > 0) return E[tix(n, m)];
+	const v2 e = E[tix(n, -m)];
+	return (m & 1) ? V2<real>::make(-e.x, e.y) : V2<real>::make(e.x, -e.y);
+}
+
+// The four coefficient sets of one (n, m): potential, d/dx, d/dy, d/dz.
+template <typename real> struct Coef4 {
+	typename V2<real>::t f, gx, gy, gz;
+};
+
+template <bool IRR, typename real>
+__device__ void derive_coefs(const typename V2<real>::t* __restrict__ E, int N, Coef4<real>* C, int lane)
+{
+	using v2 = typename V2<real>::t;
+	const int NB = IRR ? N + 1 : N, NG = IRR ? N + 1 : N - 1;
+	for (int e = lane; e < NB * (NB + 1) / 2; e += 32) {
+		const int n = c_n_of[e], k = c_m_of[e];
+		Coef4<real> o;
+		if (n < N) {
+			const v2 c = E[e];
+			o.f = k ? V2<real>::make(2 * c.x, 2 * c.y) : V2<real>::make(c.x, 0);
+		} else {
+			o.f = V2<real>::make(0, 0);
+		}
+		if (n < NG) {
+			v2 Z, P, M;
+			if (!IRR) {
+				const v2 c0 = coef_full<real>(E, N, n + 1, k), cm = coef_full<real>(E, N, n + 1, k - 1);
+				const v2 cp = coef_full<real>(E, N, n + 1, k + 1);
+				const real fz = sqrt((real)((n + 1 - k) * (n + 1 + k))), fp = sqrt((real)((n + 2 - k) * (n + 1 - k)));
+				const real fm = sqrt((real)((n + 2 + k) * (n + 1 + k)));
+				Z = V2<real>::make(c0.x * fz, c0.y * fz);
+				P = V2<real>::make(cm.x * fp, cm.y * fp);
+				M = V2<real>::make(-cp.x * fm, -cp.y * fm);
+			} else {
+				const v2 c0 = coef_full<real>(E, N, n - 1, k), cm = coef_full<real>(E, N, n - 1, k - 1);
+				const v2 cp = coef_full<real>(E, N, n - 1, k + 1);
+				const real fz = sqrt((real)max((n - k) * (n + k), 0)), fp = sqrt((real)max((n + k - 1) * (n + k), 0));
+				const real fm = sqrt((real)max((n - k - 1) * (n - k), 0));
+				Z = V2<real>::make(-c0.x * fz, -c0.y * fz);
+				P = V2<real>::make(cm.x * fp, cm.y * fp);
+				M = V2<real>::make(-cp.x * fm, -cp.y * fm);
+			}
+			// d_x = (P + M) / 2, d_y = (P - M) / 2i; weight 2 for k > 0
+			const real w = k ? real(1) : real(0.5);
+			o.gx = V2<real>::make(w * (P.x + M.x), w * (P.y + M.y));
+			o.gy = V2<real>::make(w * (P.y - M.y), -w * (P.x - M.x));
+			o.gz = V2<real>::make(2 * w * Z.x, 2 * w * Z.y);
+		} else {
+			o.gx = o.gy = o.gz = V2<real>::make(0, 0);
+		}
+		C[e] = o;
+	}
+}
+
+// phi and grad phi at (x, y, z) (the expansion's scaled frame) from the
+// coefficients of derive_coefs (zero where a set has no such degree).
+template <bool IRR, typename real>
+__device__ void eval_cart(const Coef4<real>* C, real x, real y, real z, int N, real& pot, real& gx, real& gy,
+                          real& gz)
+{
+	using v2 = typename V2<real>::t;
+	const int NB = IRR ? N + 1 : N;
+	const real r2 = x * x + y * y + z * z;
+	const real ir2 = IRR ? real(1) / r2 : real(0);
+	const real wx = IRR ? x * ir2 : x, wy = IRR ? y * ir2 : y;
+	real bx = IRR ? rsq<real>(r2) : real(1), by = 0;
+	real p = 0, ex = 0, ey = 0, ez = 0;
+	for (int m = 0; m < NB; ++m) {
+		if (m > 0) {
+			const real sgm = sig_c<real>(m);
+			const real nx = sgm * (wx * bx - wy * by), ny = sgm * (wx * by + wy * bx);
+			bx = nx; by = ny;
+		}
+		real px = 0, py = 0, cx = bx, cy = by;
+		int i = tix(m, m);
+		for (int n = m; n < NB; ++n) {
+			const Coef4<real> c = C[i];
+			p = fma(c.f.x, cx, fma(-c.f.y, cy, p));
+			ex = fma(c.gx.x, cx, fma(-c.gx.y, cy, ex));
+			ey = fma(c.gy.x, cx, fma(-c.gy.y, cy, ey));
+			ez = fma(c.gz.x, cx, fma(-c.gz.y, cy, ez));
+			const v2 ab = rec_c<real>(i);
+			const real az = ab.x * z, bb = IRR ? ab.y : ab.y * r2;
+			real nx = fma(az, cx, -bb * px), ny = fma(az, cy, -bb * py);
+			if (IRR) { nx *= ir2; ny *= ir2; }
+			px = cx; py = cy; cx = nx; cy = ny;
+			i += n + 1;                        // tix(n + 1, m)
+		}
+	}
+	pot = p; gx = ex; gy = ey; gz = ez;
+}
+
 // FP32 near field on its own (few registers, high occupancy): one warp per
 // leaf, targets in passes of up to 32; a pass of np <= 16 targets runs
 // TP = np rounded up to a power of two targets at once and splits the
@@ -650,15 +783,18 @@ __global__ void __launch_bounds__(LW * 32, 768 / (LW * 32)) p2p_f32_kernel(DevTr
 }
 
 // M2P over the W list and L2P of the leaf's local expansion, added onto the
-// near field already in the outputs: one warp per leaf, lane = target.
+// near field already in the outputs: one warp per leaf, lane = target; each
+// expansion's coefficients derived once per 32 targets (derive_coefs), the
+// targets evaluated by eval_cart.
+template <typename real> constexpr int eval_warps() { return sizeof(real) == sizeof(float) ? 4 : 2; }
+
 template <typename real, int LW>
 __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const typename V2<real>::t* __restrict__ outer,
                                                              const typename V2<real>::t* __restrict__ inner, int N,
-                                                             const real* __restrict__ knm, double* __restrict__ pot_out,
-                                                             double* __restrict__ fld_out)
+                                                             double* __restrict__ pot_out, double* __restrict__ fld_out)
 {
 	using v2 = typename V2<real>::t;
-	__shared__ v2 sL[LW][NX2MAX], sM[LW][NX2MAX];
+	__shared__ Coef4<real> sC[LW][NXD];
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const size_t li = (size_t)blockIdx.x * LW + w;
 	if (li >= t.nleaves) return;
@@ -667,34 +803,37 @@ __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const t
 	if (tb >= te) return;
 	const int Nx2 = N * (N + 1) / 2;
 	const double ihg = 1.0 / cell_size(t, g);
-	for (int c = lane; c < Nx2; c += 32) sL[w][c] = inner[g * Nx2 + c];
 	const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
 	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
-	__syncwarp();
 	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
 		const uint32_t i = t0 + lane;
 		const bool valid = i < te;
+		double xi = 0, yi = 0, zi = 0;
+		if (valid) { xi = t.x[i]; yi = t.y[i]; zi = t.z[i]; }
 		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
 		for (uint32_t e = wb; e < we; ++e) {
 			const size_t D = t.w_idx[e];
 			__syncwarp();
-			for (int c = lane; c < Nx2; c += 32) sM[w][c] = outer[D * Nx2 + c];
+			derive_coefs<true, real>(outer + D * Nx2, N, sC[w], lane);
 			__syncwarp();
 			if (valid) {
 				const double ihd = 1.0 / cell_size(t, D);
-				real mp, mx_, my_, mz_;
-				eval_expansion<false, real>(sM[w], (real)((t.x[i] - t.cx[D]) * ihd), (real)((t.y[i] - t.cy[D]) * ihd),
-				                            (real)((t.z[i] - t.cz[D]) * ihd), N, knm, mp, mx_, my_, mz_);
+				real mp, gx, gy, gz;
+				eval_cart<true, real>(sC[w], (real)((xi - t.cx[D]) * ihd), (real)((yi - t.cy[D]) * ihd),
+				                      (real)((zi - t.cz[D]) * ihd), N, mp, gx, gy, gz);
 				pot += (double)mp * ihd;
-				fx += (double)mx_ * ihd * ihd; fy += (double)my_ * ihd * ihd; fz += (double)mz_ * ihd * ihd;
+				fx -= (double)gx * ihd * ihd; fy -= (double)gy * ihd * ihd; fz -= (double)gz * ihd * ihd;
 			}
 		}
+		__syncwarp();
+		derive_coefs<false, real>(inner + g * Nx2, N, sC[w], lane);
+		__syncwarp();
 		if (valid) {
-			real lp, lx_, ly_, lz_;
-			eval_expansion<true, real>(sL[w], (real)((t.x[i] - cx) * ihg), (real)((t.y[i] - cy) * ihg),
-			                           (real)((t.z[i] - cz) * ihg), N, knm, lp, lx_, ly_, lz_);
+			real lp, gx, gy, gz;
+			eval_cart<false, real>(sC[w], (real)((xi - cx) * ihg), (real)((yi - cy) * ihg),
+			                       (real)((zi - cz) * ihg), N, lp, gx, gy, gz);
 			pot += (double)lp * ihg;
-			fx += (double)lx_ * ihg * ihg; fy += (double)ly_ * ihg * ihg; fz += (double)lz_ * ihg * ihg;
+			fx -= (double)gx * ihg * ihg; fy -= (double)gy * ihg * ihg; fz -= (double)gz * ihg * ihg;
 			const uint32_t o = t.orig[i];
 			pot_out[o] += pot;
 			fld_out[3 * (size_t)o] += fx; fld_out[3 * (size_t)o + 1] += fy; fld_out[3 * (size_t)o + 2] += fz;
