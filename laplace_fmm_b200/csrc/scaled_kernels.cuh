@@ -287,6 +287,68 @@ __device__ __forceinline__ void accumulate_harmonics(real q, real r, real th, re
 	}
 }
 
+// One warp's particles (lane = particle, q = 0 for none) summed into the
+// coefficients q conj(B_nm) (regular: P2M; irregular: P2L) through the
+// Cartesian recurrences of eval_cart: for each order m the lanes write their
+// N - m values to a row of buf (stride 2 MAXN3 + 1, odd: conflict-free
+// columns), then lane c adds up column c (in FP64 for orders 0 and 1, else
+// in a tree of FP32 partial sums).
+constexpr int ACC_LD = 2 * MAXN3 + 1;
+
+template <bool IRR, typename real>
+__device__ __forceinline__ void accumulate_cart(real q, real x, real y, real z, int N, typename V2<real>::t* sacc,
+                                                real* buf, int lane)
+{
+	using v2 = typename V2<real>::t;
+	const real r2 = x * x + y * y + z * z;
+	const real ir2 = IRR ? real(1) / r2 : real(0);
+	const real wx = IRR ? x * ir2 : x, wy = IRR ? y * ir2 : y;
+	real bx = IRR ? rsq<real>(r2) : real(1), by = 0;
+	real* row = buf + lane * ACC_LD;
+	for (int m = 0; m < N; ++m) {
+		if (m > 0) {
+			const real sgm = sig_c<real>(m);
+			const real nx = sgm * (wx * bx - wy * by), ny = sgm * (wx * by + wy * bx);
+			bx = nx; by = ny;
+		}
+		real px = 0, py = 0, cx = bx, cy = by;
+		int i = tix(m, m);
+		for (int n = m; n < N; ++n) {
+			row[2 * (n - m)] = q * cx;
+			row[2 * (n - m) + 1] = -q * cy;
+			const v2 ab = rec_c<real>(i);
+			const real az = ab.x * z, bb = IRR ? ab.y : ab.y * r2;
+			real nx = fma(az, cx, -bb * px), ny = fma(az, cy, -bb * py);
+			if (IRR) { nx *= ir2; ny *= ir2; }
+			px = cx; py = cy; cx = nx; cy = ny;
+			i += n + 1;
+		}
+		__syncwarp();
+		if (lane < 2 * (N - m)) {
+			real* a = reinterpret_cast<real*>(sacc + tix(m + (lane >> 1), m)) + (lane & 1);
+			if (m < 2) {
+				// orders 0 and 1 in FP64: the leaves' monopole and dipole rounding
+				// errors add up over the whole far field
+				double sum = 0.0;
+#pragma unroll 8
+				for (int r = 0; r < 32; ++r) sum += (double)buf[r * ACC_LD + lane];
+				*a += (real)sum;
+			} else {
+				// eight interleaved partial sums, then a tree
+				real p[8];
+#pragma unroll
+				for (int k = 0; k < 8; ++k) p[k] = buf[k * ACC_LD + lane];
+#pragma unroll
+				for (int r = 8; r < 32; r += 8)
+#pragma unroll
+					for (int k = 0; k < 8; ++k) p[k] += buf[(r + k) * ACC_LD + lane];
+				*a += ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
+			}
+		}
+		__syncwarp();
+	}
+}
+
 // P2M, warp per leaf, in the leaf's scaled frame
 template <typename real>
 __global__ void __launch_bounds__(WPB * 32) p2m_scaled_kernel(DevTree t, const real* __restrict__ xr, const real* __restrict__ yr,
@@ -295,6 +357,7 @@ __global__ void __launch_bounds__(WPB * 32) p2m_scaled_kernel(DevTree t, const r
                                                               typename V2<real>::t* __restrict__ outer)
 {
 	__shared__ typename V2<real>::t sacc[WPB][NX2MAX];
+	__shared__ real sbuf[WPB][32 * ACC_LD];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	size_t li = (size_t)blockIdx.x * WPB + w;
 	if (li >= t.nleaves) return;
@@ -306,9 +369,9 @@ __global__ void __launch_bounds__(WPB * 32) p2m_scaled_kernel(DevTree t, const r
 	const uint32_t b = t.pbeg[g], e = t.send[g];
 	for (uint32_t base = b; base < e; base += 32) {
 		uint32_t i = base + lane;
-		real q = 0, r = 1, th = 1, ph = 0;
-		if (i < e) { q = qr[i]; dec_to_sph<real>(xr[i] * ih, yr[i] * ih, zr[i] * ih, r, th, ph); }
-		accumulate_harmonics<false, real>(q, r, th, ph, N, knm, sacc[w]);
+		real q = 0, x = 0, y = 0, z = 0;
+		if (i < e) { q = qr[i]; x = xr[i] * ih; y = yr[i] * ih; z = zr[i] * ih; }
+		accumulate_cart<false, real>(q, x, y, z, N, sacc[w], sbuf[w], lane);
 	}
 	__syncwarp();
 	typename V2<real>::t* out = outer + g * Nx2;
@@ -322,6 +385,7 @@ __global__ void __launch_bounds__(WPB * 32) p2l_kernel(DevTree t, int N, const r
                                                        typename V2<real>::t* __restrict__ inner)
 {
 	__shared__ typename V2<real>::t sacc[WPB][NX2MAX];
+	__shared__ real sbuf[WPB][32 * ACC_LD];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	size_t g = (size_t)blockIdx.x * WPB + w;
 	if (g >= t.ncells) return;
@@ -337,12 +401,12 @@ __global__ void __launch_bounds__(WPB * 32) p2l_kernel(DevTree t, int N, const r
 		const uint32_t b = t.pbeg[C], en = t.send[C];
 		for (uint32_t base = b; base < en; base += 32) {
 			uint32_t i = base + lane;
-			real q = 0, r = 1, th = 1, ph = 0;
+			real q = 0, x = 0, y = 0, z = 1;              // an empty lane: q = 0 at a finite point
 			if (i < en) {
 				q = (real)t.q[i];
-				dec_to_sph<real>((real)((t.x[i] - cx) * ih), (real)((t.y[i] - cy) * ih), (real)((t.z[i] - cz) * ih), r, th, ph);
+				x = (real)((t.x[i] - cx) * ih); y = (real)((t.y[i] - cy) * ih); z = (real)((t.z[i] - cz) * ih);
 			}
-			accumulate_harmonics<true, real>(q, r, th, ph, N, knm, sacc[w]);
+			accumulate_cart<true, real>(q, x, y, z, N, sacc[w], sbuf[w], lane);
 		}
 	}
 	__syncwarp();
