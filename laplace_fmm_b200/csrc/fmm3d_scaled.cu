@@ -134,10 +134,13 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 			                                                                     inner + t.loff[L] * Nx2, N, T, ctx.dev_flags);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s));
 	if constexpr (sizeof(real) == sizeof(float)) {
-		// near field and expansions as two kernels (the near field's few
-		// registers keep many warps resident)
-		constexpr int LWP = 8, LWE = eval_warps<real>();
-		p2p_f32_kernel<LWP><<<div_up(nl, LWP), LWP * 32, 0, s>>>(t, qr, pot, field);
+		// the near field (a resident grid taking leaves from a counter), then
+		// the expansions added onto it
+		constexpr int LWP = 4, LWE = eval_warps<real>();
+		unsigned* next_leaf = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
+		if (!next_leaf) { ctx.last_error = "scaled solve: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(ctx, cudaMemsetAsync(next_leaf, 0, sizeof(unsigned), s));
+		p2p_f32_kernel<LWP><<<6 * ctx.num_sms, LWP * 32, 0, s>>>(t, qr, pot, field, next_leaf);
 		eval_scaled_kernel<real, LWE><<<div_up(nl, LWE), LWE * 32, 0, s>>>(t, outer, inner, N, pot, field);
 	} else {
 		constexpr int LW = leaf_warps<real>();

@@ -773,75 +773,81 @@ __device__ __forceinline__ void p2p_f32_chunk(const float* __restrict__ sx, cons
 
 template <int LW>
 __global__ void __launch_bounds__(LW * 32, 768 / (LW * 32)) p2p_f32_kernel(DevTree t, const float* __restrict__ qr,
-                                                         double* __restrict__ pot_out, double* __restrict__ fld_out)
+                                                         double* __restrict__ pot_out, double* __restrict__ fld_out,
+                                                         unsigned* __restrict__ next_leaf)
 {
 	__shared__ __align__(16) float sx[LW][32], sy[LW][32], sz[LW][32], sq[LW][32];
 	__shared__ __align__(16) float lx[LW][32], ly[LW][32], lz[LW][32];
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const size_t li = (size_t)blockIdx.x * LW + w;
-	if (li >= t.nleaves) return;
-	const size_t g = t.leaves[li];
-	const uint32_t tb = t.tbeg[g], te = t.tend[g];
-	if (tb >= te) return;
 	const bool tmode = t.targets_num > 0;
-	const uint32_t ub = t.u_off[li], ue = t.u_off[li + 1];
-	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
-	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
-		const int np = (int)min(32u, te - t0);
-		int lt = 0;                            // log2 of the targets run at once
-		while ((1 << lt) < np) ++lt;
-		const int ti = lane & ((1 << lt) - 1), ph = lane >> lt, G = 32 >> lt;
-		const uint32_t i = t0 + ti;
-		const bool valid = ti < np;
-		float xi = 0.f, yi = 0.f, zi = 0.f, xl = 0.f, yl = 0.f, zl = 0.f;
-		if (valid) {
-			const double ax_ = t.x[i] - cx, ay_ = t.y[i] - cy, az_ = t.z[i] - cz;
-			xi = (float)ax_; yi = (float)ay_; zi = (float)az_;
-			xl = (float)(ax_ - (double)xi); yl = (float)(ay_ - (double)yi); zl = (float)(az_ - (double)zi);
-		}
-		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
-		for (int64_t e = (int64_t)ub - 1; e < (int64_t)ue; ++e) {
-			const bool own = e < (int64_t)ub;
-			const size_t sc_ = own ? g : (size_t)t.u_idx[e];
-			const uint32_t sb = t.pbeg[sc_], se = t.send[sc_];
-			for (uint32_t s0 = sb; s0 < se; s0 += 32) {
-				const int cnt = min(32u, se - s0), cnt4 = (cnt + 3) & ~3;
-				__syncwarp();
-				if (lane < cnt) {
-					const uint32_t j = s0 + lane;
-					const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
-					const float hx = (float)dx_, hy = (float)dy_, hz = (float)dz_;
-					sx[w][lane] = hx; sy[w][lane] = hy; sz[w][lane] = hz;
-					lx[w][lane] = (float)(dx_ - (double)hx); ly[w][lane] = (float)(dy_ - (double)hy);
-					lz[w][lane] = (float)(dz_ - (double)hz);
-					sq[w][lane] = qr[j];
-				} else if (lane < cnt4) {
-					sx[w][lane] = sy[w][lane] = sz[w][lane] = 0.f;
-					lx[w][lane] = ly[w][lane] = lz[w][lane] = 0.f;
-					sq[w][lane] = 0.f;
-				}
-				__syncwarp();
-				if (valid) {
-					if (own)
-						p2p_f32_chunk<true>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G,
-						                    (int)(i - s0), xi, yi, zi, xl, yl, zl, pot, fx, fy, fz);
-					else
-						p2p_f32_chunk<false>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G, -1, xi,
-						                     yi, zi, xl, yl, zl, pot, fx, fy, fz);
+	// a resident grid: each warp takes the next leaf from a counter
+	for (;;) {
+		unsigned lid = 0;
+		if (lane == 0) lid = atomicAdd(next_leaf, 1u);
+		const size_t li = __shfl_sync(0xffffffffu, lid, 0);
+		if (li >= t.nleaves) return;
+		const size_t g = t.leaves[li];
+		const uint32_t tb = t.tbeg[g], te = t.tend[g];
+		if (tb >= te) continue;
+		const uint32_t ub = t.u_off[li], ue = t.u_off[li + 1];
+		const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+		for (uint32_t t0 = tb; t0 < te; t0 += 32) {
+			const int np = (int)min(32u, te - t0);
+			int lt = 0;                            // log2 of the targets run at once
+			while ((1 << lt) < np) ++lt;
+			const int ti = lane & ((1 << lt) - 1), ph = lane >> lt, G = 32 >> lt;
+			const uint32_t i = t0 + ti;
+			const bool valid = ti < np;
+			float xi = 0.f, yi = 0.f, zi = 0.f, xl = 0.f, yl = 0.f, zl = 0.f;
+			if (valid) {
+				const double ax_ = t.x[i] - cx, ay_ = t.y[i] - cy, az_ = t.z[i] - cz;
+				xi = (float)ax_; yi = (float)ay_; zi = (float)az_;
+				xl = (float)(ax_ - (double)xi); yl = (float)(ay_ - (double)yi); zl = (float)(az_ - (double)zi);
+			}
+			double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+			for (int64_t e = (int64_t)ub - 1; e < (int64_t)ue; ++e) {
+				const bool own = e < (int64_t)ub;
+				const size_t sc_ = own ? g : (size_t)t.u_idx[e];
+				const uint32_t sb = t.pbeg[sc_], se = t.send[sc_];
+				for (uint32_t s0 = sb; s0 < se; s0 += 32) {
+					const int cnt = min(32u, se - s0), cnt4 = (cnt + 3) & ~3;
+					__syncwarp();
+					if (lane < cnt) {
+						const uint32_t j = s0 + lane;
+						const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
+						const float hx = (float)dx_, hy = (float)dy_, hz = (float)dz_;
+						sx[w][lane] = hx; sy[w][lane] = hy; sz[w][lane] = hz;
+						lx[w][lane] = (float)(dx_ - (double)hx); ly[w][lane] = (float)(dy_ - (double)hy);
+						lz[w][lane] = (float)(dz_ - (double)hz);
+						sq[w][lane] = qr[j];
+					} else if (lane < cnt4) {
+						sx[w][lane] = sy[w][lane] = sz[w][lane] = 0.f;
+						lx[w][lane] = ly[w][lane] = lz[w][lane] = 0.f;
+						sq[w][lane] = 0.f;
+					}
+					__syncwarp();
+					if (valid) {
+						if (own)
+							p2p_f32_chunk<true>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G,
+							                    (int)(i - s0), xi, yi, zi, xl, yl, zl, pot, fx, fy, fz);
+						else
+							p2p_f32_chunk<false>(sx[w], sy[w], sz[w], lx[w], ly[w], lz[w], sq[w], cnt4, 4 * ph, 4 * G, -1, xi,
+							                     yi, zi, xl, yl, zl, pot, fx, fy, fz);
+					}
 				}
 			}
-		}
-		for (int o = 1 << lt; o < 32; o <<= 1) {
-			pot += __shfl_xor_sync(0xffffffffu, pot, o);
-			fx += __shfl_xor_sync(0xffffffffu, fx, o);
-			fy += __shfl_xor_sync(0xffffffffu, fy, o);
-			fz += __shfl_xor_sync(0xffffffffu, fz, o);
-		}
-		if (valid && ph == 0) {
-			if (!tmode) pot += t.q[i] * (1.0 / FORCE_EPS);
-			const uint32_t o = t.orig[i];
-			pot_out[o] = pot;
-			fld_out[3 * (size_t)o] = fx; fld_out[3 * (size_t)o + 1] = fy; fld_out[3 * (size_t)o + 2] = fz;
+			for (int o = 1 << lt; o < 32; o <<= 1) {
+				pot += __shfl_xor_sync(0xffffffffu, pot, o);
+				fx += __shfl_xor_sync(0xffffffffu, fx, o);
+				fy += __shfl_xor_sync(0xffffffffu, fy, o);
+				fz += __shfl_xor_sync(0xffffffffu, fz, o);
+			}
+			if (valid && ph == 0) {
+				if (!tmode) pot += t.q[i] * (1.0 / FORCE_EPS);
+				const uint32_t o = t.orig[i];
+				pot_out[o] = pot;
+				fld_out[3 * (size_t)o] = fx; fld_out[3 * (size_t)o + 1] = fy; fld_out[3 * (size_t)o + 2] = fz;
+			}
 		}
 	}
 }
