@@ -268,13 +268,20 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=Fa
     if adaptive or precision != "fp64":
         tree += depth + depth * (1 + scan) + depth + 1 + scan + 1 + 1 + lists + 2 + 2 + 3 * scan
         m2l = max(0, depth - 2) * (3 + 1 + 1) + 2 * 2          # plan + GEMM (+ split reduce), FP64 coarse converts
-        fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + 1
+        leaves = 2 if precision == "mixed" else 1               # FP32: near field, then the expansions
+        fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + leaves
         return tree + fmm + extra
     tree += lists
     if dim == 3:
         fmm = 1 + (depth - 1) + max(0, depth - 2) * 5 + max(0, depth - 3) + 1
     else:
-        fmm = 1 + (depth - 1) + max(0, depth - 2) + 1
+        # per level 2..depth-1: class count, scatter, slot table, Hankel M2L,
+        # and a split reduction on the levels too small to fill the GPU
+        # (fewer than ~37k cells: levels up to 7); L2L adds; leaf work units
+        # (count + scan) and the leaves
+        levels = max(0, depth - 2)
+        split = sum(1 for L in range(2, depth) if 4 ** L < 37000)
+        fmm = 1 + (depth - 1) + 4 * levels + split + max(0, depth - 3) + 1 + scan + 1
     return tree + fmm
 
 

@@ -257,6 +257,8 @@ typedef struct {
 	double predicted_error;     /* the network's rel-L2 estimate of the potential at predicted_N */
 	double checked_error;       /* sampled rel-L2 of the potential, self term removed (-1: no check) */
 	double checked_error_field; /* the same for the field */
+	int fp64_resolved;          /* problems rerun in the FP64 form at N = 15 because the mixed form
+	                               missed tol even there (0 or 1 for a single solve) */
 } lfmm_learned_info;
 
 /* 3D solve at the order the network picks for tolerance tol (rel-L2 of the
@@ -266,7 +268,8 @@ typedef struct {
  * leaves' errors over the samples' RMS potential give the predicted rel-L2,
  * and the lowest p in 4..14 within tol is solved (else N = 15).  The same
  * samples then judge the result: a solve above tol is rerun at the fixed
- * order N = 15 (the fallback).  params: device pointer to the network
+ * order N = 15 (the fallback), and a mixed-precision solve still above tol
+ * there is rerun in the FP64 form (fp64_resolved).  params: device pointer to the network
  * (LFMM_MLP_PARAMS floats, inputs unnormalised).  opts gives the tree
  * (tree_depth, max_leaf) and precision; opts->N and opts->eps are ignored.
  * Synchronises.  Host and device-buffer variants. */
@@ -281,8 +284,10 @@ int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_x
  * lfmm3d_solve_learned; device buffers): up to check_targets sampled outputs
  * per problem normalise each problem's prediction and judge its result; the
  * batch runs at the highest order any problem needs, and reruns at N = 15
- * when a problem misses tol.  info: the order used, the largest predicted
- * and checked errors over the problems. */
+ * when a problem misses tol; a problem still above tol there (mixed form) is
+ * rerun alone in the FP64 form into its slice of the outputs.  info: the
+ * order used, the largest predicted and checked errors over the problems,
+ * the number of FP64 reruns. */
 int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
                                       const double* src_q, const lfmm_solve_opts* opts, const float* params,
                                       double tol, int check_targets, double* pot, double* field,

@@ -451,6 +451,13 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
 		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
 	}
+	if (e[0] > tol && precision == LFMM_PRECISION_MIXED) {
+		// the mixed form cannot reach tol even at N = 15: the FP64 form
+		if ((st = fmm3d_scaled_on_tree(ctx, t, FB_N, LFMM_PRECISION_FP64, pot, field, stats))) return st;
+		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+		N = FB_N;
+		li.fp64_resolved = 1;
+	}
 	li.checked_error = e[0];
 	li.checked_error_field = e[1];
 	li.order_N = N;
@@ -556,6 +563,37 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 		if (ep_max <= tol || N >= FB_N) break;
 		N = FB_N;                      // the fixed-order fallback for the whole batch
 		li.fallback = 1;
+	}
+	if (precision == LFMM_PRECISION_MIXED && li.checked_error > tol) {
+		// problems the mixed form cannot bring within tol even at N = 15:
+		// each rerun alone in the FP64 form, into its slice of the outputs
+		for (int k = 0; k < P; ++k) {
+			if (soff[k + 1] == soff[k]) continue;
+			if (std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)) <= tol) continue;
+			ParticleInput pk;
+			pk.dim = 3; pk.ns = hoff[k + 1] - hoff[k]; pk.nt = 0;
+			pk.src = in.src + 3 * hoff[k]; pk.srcq = in.srcq + hoff[k];
+			const size_t mark = ctx.arena.mark();
+			st = fmm3d_solve_scaled(ctx, pk, FB_N, depth, max_leaf, LFMM_PRECISION_FP64, pot + hoff[k], field + 3 * hoff[k],
+			                        nullptr, nullptr);
+			ctx.arena.rewind(mark);
+			if (st) return st;
+			++li.fp64_resolved;
+		}
+		if (li.fp64_resolved) {
+			LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
+			check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
+			LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
+			LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+			double ep_max = 0.0, ef_max = 0.0;
+			for (int k = 0; k < P; ++k) {
+				if (soff[k + 1] == soff[k]) continue;
+				ep_max = std::max(ep_max, std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)));
+				ef_max = std::max(ef_max, std::sqrt(ha[4 * (size_t)k + 2] / std::max(ha[4 * (size_t)k + 3], 1e-300)));
+			}
+			li.checked_error = ep_max;
+			li.checked_error_field = ef_max;
+		}
 	}
 	li.order_N = N;
 	if (info) *info = li;

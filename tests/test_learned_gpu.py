@@ -76,6 +76,24 @@ def test_fallback_replaces_a_bad_prediction(ctx):
     assert info["checked_error"] <= TOL
 
 
+def test_fp64_rerun_below_the_mixed_floor(solver, ctx):
+    """A tolerance the mixed form cannot reach even at N = 15 (1e-7; the FP64
+    form reaches ~1.6e-7 here): after the fallback misses, the solve is rerun
+    in the FP64 form at N = 15, the result is that solve's and the reported
+    check is its sampled error."""
+    src, q = uniform3d(60000, seed=12)
+    r = solver.solve(src, q, tol=1e-7, tree_depth=10, max_leaf=64, check_targets=1024)
+    info = r["info"]
+    assert info["fp64_resolved"] == 1 and info["order_N"] == 15
+    f = FastMultipole3d((src, q), N=15, tree_depth=10, max_leaf=64, precision="fp64", ctx=ctx)
+    assert rel_l2(noself(r["potentials"], q), noself(f.potentials, q)) < 1e-12
+    assert rel_l2(r["forces"], f.forces) < 1e-12
+    idx = np.arange(1024) * (len(src) // 1024)
+    from laplace_fmm_b200 import InteractionType, compute_exact
+    pe = compute_exact(InteractionType.Potential3d, (src, q), src[idx], ctx=ctx) - q[idx] * 1e4
+    assert info["checked_error"] == pytest.approx(rel_l2(f.potentials[idx] - q[idx] * 1e4, pe), rel=1e-6)
+
+
 def test_gain_over_fixed_order(solver, ctx):
     """The first held-out problems of the training script (never trained on):
     after the check every solve is within the tolerance, at a lower order on
