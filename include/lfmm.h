@@ -250,6 +250,21 @@ int lfmm3d_features(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const do
                     const double* tgt_xyz, const lfmm_solve_opts* opts, float* feats, size_t cap, int* leaf_of,
                     size_t* n_leaves);
 
+/* Vector charges: the reference's fmm::FastMultipole3d<Vector3d>
+ * (cpu/multipole3d.h:10-24 with value = Vector3d; cpu/multipole3d.cpp:414-853):
+ * field[3 i + c] = (sum_j q_j x (x_i - x_j) / max(r, 1e-4)^3)_c at every
+ * target, q_j = (src_q3[3 j], src_q3[3 j + 1], src_q3[3 j + 2]).  No
+ * potential (the reference computes none for vector charges).  Sources are
+ * the particles with q != 0 (the reference's zero-charge rule); one tree,
+ * three scalar passes combined by a cross product.  opts as lfmm3d_solve_ex
+ * (max_leaf 0: the uniform tree; N <= 15).  Host and device-buffer variants;
+ * the host one synchronises. */
+int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q3, size_t n_tgt,
+                        const double* tgt_xyz, const lfmm_solve_opts* opts, double* field, lfmm_stats* stats);
+int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q3,
+                               size_t n_tgt, const double* tgt_xyz, const lfmm_solve_opts* opts, double* field,
+                               lfmm_stats* stats);
+
 typedef struct {
 	int order_N;                /* degrees of the final solve */
 	int predicted_N;            /* degrees the network chose */

@@ -20,6 +20,7 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_DEVICE
 EXPORTS = [
     "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream",
     "lfmm3d_solve", "lfmm3d_solve_device", "lfmm3d_solve_ex", "lfmm3d_solve_ex_device",
+    "lfmm3d_solve_vector", "lfmm3d_solve_vector_device",
     "lfmm2d_solve", "lfmm2d_solve_device",
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
     "lfmm3d_direct_device_noalloc",
@@ -96,6 +97,9 @@ def load(path: Path | str = LIB_PATH):
             getattr(L, f).argtypes = solve
         for f in ("lfmm3d_solve_ex", "lfmm3d_solve_ex_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, P,
+                                      ctypes.POINTER(LfmmStats)]
+        for f in ("lfmm3d_solve_vector", "lfmm3d_solve_vector_device"):
+            getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P,
                                       ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
                   "lfmm3d_direct_device_noalloc"):

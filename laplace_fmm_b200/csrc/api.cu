@@ -436,6 +436,72 @@ int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t ns, const double* src, const do
 	return st;
 }
 
+int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt,
+                               const double* tgt, const lfmm_solve_opts* o, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return LFMM_ERR_ARG; }
+	if ((ns && (!src || !q3)) || (nt && !tgt) || !field) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
+	if (o->precision != LFMM_PRECISION_FP64 && o->precision != LFMM_PRECISION_MIXED) {
+		c.last_error = "unknown precision";
+		return LFMM_ERR_ARG;
+	}
+	const int Nr = resolve_order(3, o->N, o->eps), Dr = resolve_depth(3, o->tree_depth, ns + nt);
+	if (Nr < 1 || Dr < 1) { c.last_error = "order and tree depth must be >= 1"; return LFMM_ERR_ARG; }
+	c.arena.reset();
+	ctx->has_tree = false;
+	ParticleInput in;
+	in.dim = 3; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q3; in.tgt = tgt;
+	SolveStats ss;
+	int st = fmm3d_solve_vector(c, in, Nr, Dr, o->max_leaf, o->precision, field, stats ? &ss : nullptr);
+	if (st == OK) {
+		fill_stats(stats, ss);
+		st = check_flags(c);
+	}
+	c.arena.settle();
+	return st;
+}
+
+int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt, const double* tgt,
+                        const lfmm_solve_opts* o, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if ((ns && (!src || !q3)) || (nt && !tgt) || !field) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
+	const size_t nout = nt ? nt : ns;
+	// the device copies live outside the solve's arena (it resets it)
+	double *dsrc = nullptr, *dq = nullptr, *dtgt = nullptr, *dfld = nullptr;
+	auto release = [&] { cudaFree(dsrc); cudaFree(dq); cudaFree(dtgt); cudaFree(dfld); };
+	if ((ns && (cudaMalloc(&dsrc, sizeof(double) * 3 * ns) != cudaSuccess ||
+	            cudaMalloc(&dq, sizeof(double) * 3 * ns) != cudaSuccess)) ||
+	    (nt && cudaMalloc(&dtgt, sizeof(double) * 3 * nt) != cudaSuccess) ||
+	    (nout && cudaMalloc(&dfld, sizeof(double) * 3 * nout) != cudaSuccess)) {
+		cudaGetLastError();
+		release();
+		c.last_error = "device allocation failed";
+		return LFMM_ERR_OOM;
+	}
+	cudaStream_t s = c.stream;
+	int st = OK;
+	cudaError_t e = cudaSuccess;
+	if (ns) e = cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
+	if (e == cudaSuccess && ns) e = cudaMemcpyAsync(dq, q3, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
+	if (e == cudaSuccess && nt) e = cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s);
+	if (e != cudaSuccess) st = cuda_fail(c, e, "vector solve: copy in");
+	if (st == OK) st = lfmm3d_solve_vector_device(ctx, ns, dsrc, dq, nt, dtgt, o, dfld, stats);
+	if (st == OK) {
+		e = cudaMemcpyAsync(field, dfld, sizeof(double) * 3 * nout, cudaMemcpyDeviceToHost, s);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+		if (e != cudaSuccess) st = cuda_fail(c, e, "vector solve: copy out");
+	}
+	cudaStreamSynchronize(s);
+	release();
+	return st;
+}
+
 int lfmm2d_solve(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt, int N,
                  int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
 {

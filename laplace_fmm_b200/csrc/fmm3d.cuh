@@ -25,6 +25,9 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 // depth `depth`; > 0: adaptive, at most `depth` levels): precision 0 = FP64,
 // 1 = mixed (FP32 expansions / near field, FP64 M2L on levels 2-3, FP64 tile
 // sums and self term).  N <= 15.
+// Vector charges (in.srcq: 3 doubles per source): field = sum q x d / r^3.
+int fmm3d_solve_vector(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
+                       double* field, SolveStats* stats);
 int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
                        double* pot, double* field, SolveStats* stats, DevTree* tree_out = nullptr);
 // The same on a tree built by tree_build_adaptive (phase events 0 and 1, the

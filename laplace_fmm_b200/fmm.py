@@ -46,7 +46,8 @@ class InteractionType(Enum):
 
 
 def _split(particles, dim):
-    """(positions (n, dim) float64 C-contiguous, charges (n,) float64)."""
+    """(positions (n, dim) float64 C-contiguous, charges (n,) float64; vector
+    charges of a 3D solve stay (n, 3))."""
     if isinstance(particles, np.ndarray) and particles.dtype.names:
         c = particles["center"]
         if dim == 2 and np.iscomplexobj(c):
@@ -54,13 +55,17 @@ def _split(particles, dim):
         else:
             pos = np.asarray(c, dtype=np.float64).reshape(-1, dim)
         q = np.asarray(particles["q"], dtype=np.float64)
+        if not (dim == 3 and q.ndim == 2 and q.shape[1] == 3):
+            q = q.reshape(-1)
     else:
         pos, q = particles
         pos = np.asarray(pos)
         if dim == 2 and np.iscomplexobj(pos):
             pos = np.stack([pos.real, pos.imag], axis=1)
         pos = pos.reshape(-1, dim)
-        q = np.asarray(q, dtype=np.float64).reshape(-1)
+        q = np.asarray(q, dtype=np.float64)
+        if not (dim == 3 and q.ndim == 2 and q.shape[1] == 3):
+            q = q.reshape(-1)
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     q = np.ascontiguousarray(q, dtype=np.float64)
     if len(pos) != len(q):
@@ -103,6 +108,18 @@ class _Solver:
         pot = np.zeros(nout)
         fld = np.zeros((nout, dim))
         stats = LfmmStats()
+        if sq.ndim == 2:
+            # vector charges (reference FastMultipole3d<Vector3d>): field only
+            opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
+            ctx.check(ctx.lib.lfmm3d_solve_vector(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos),
+                                                  ctypes.byref(opts), _ptr(fld), ctypes.byref(stats)),
+                      "lfmm3d_solve_vector")
+            self.potentials = np.zeros(0)
+            self.forces = fld
+            self.stats = stats.as_dict()
+            self.N = stats.order_N
+            self.tree_depth = stats.depth
+            return
         if dim == 3 and max_leaf:
             opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
             st = ctx.lib.lfmm3d_solve_ex(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos),
@@ -120,7 +137,9 @@ class _Solver:
 
 
 class FastMultipole3d(_Solver):
-    """3D rotation-based Laplace FMM (reference fmm::gpu::FastMultipole3d<double>)."""
+    """3D rotation-based Laplace FMM (reference fmm::gpu::FastMultipole3d<double>;
+    with charges of shape (n, 3), fmm::FastMultipole3d<Vector3d>: forces =
+    sum q x d / r^3, no potentials)."""
     dim = 3
 
 

@@ -99,6 +99,22 @@ class Oracle:
             raise RuntimeError(f"oracle fmm3d failed with status {st}")
         return pot, fld
 
+    def fmm3d_vec(self, src, q3, targets=None, N=AUTO, depth=AUTO, eps=1e-8):
+        """Vector charges (reference FastMultipole3d<Vector3d>,
+        cpu/multipole3d.cpp:414-853): the field sum q x d / r^3 written as
+        e_x x E^(x) + e_y x E^(y) + e_z x E^(z), E^(c) the field of this
+        oracle's scalar FMM for the charges' component c (the reference sums
+        the same cross products pairwise in the near field and from its three
+        expansions' gradients in the far field).  Each particle's charge must
+        be zero in all components or in none, so that the three scalar solves
+        split sources and targets alike (the reference's zero rule)."""
+        q3 = _f64(q3).reshape(-1, 3)
+        z = q3 == 0
+        if np.any(z.any(axis=1) != z.all(axis=1)):
+            raise ValueError("a charge with some zero components: the scalar solves would split it differently")
+        E = [self.fmm3d(src, np.ascontiguousarray(q3[:, c]), targets, N, depth, eps)[1] for c in range(3)]
+        return np.stack([E[1][:, 2] - E[2][:, 1], E[2][:, 0] - E[0][:, 2], E[0][:, 1] - E[1][:, 0]], axis=1)
+
     def fmm2d(self, src, q, targets=None, N=AUTO, depth=AUTO, eps=1e-8):
         src = _f64(src).reshape(-1, 2); q = _f64(q)
         nt = 0 if targets is None else len(targets)
@@ -237,6 +253,8 @@ class Reference:
         self.lib = L
         L.ref_fmm3d.argtypes = [_SZ, _P, _P, _I, _I, _D, _P, _P]
         L.ref_fmm3d_st.argtypes = [_SZ, _P, _P, _SZ, _P, _I, _I, _D, _P, _P]
+        L.ref_fmm3d_vec.argtypes = [_SZ, _P, _P, _I, _I, _D, _P]
+        L.ref_fmm3d_vec_st.argtypes = [_SZ, _P, _P, _SZ, _P, _I, _I, _D, _P]
         L.ref_fmm2d.argtypes = [_SZ, _P, _P, _I, _I, _D, _P, _P]
         L.ref_fmm2d_st.argtypes = [_SZ, _P, _P, _SZ, _P, _I, _I, _D, _P, _P]
         L.ref_wignerd.argtypes = [_I, _D, _P]
@@ -268,6 +286,18 @@ class Reference:
             self.lib.ref_fmm3d_st(len(src), _ptr(src), _ptr(q), len(tgt), _ptr(tgt), int(N), int(depth), float(eps),
                                   _ptr(pot), _ptr(fld))
         return pot, fld
+
+    def fmm3d_vec(self, src, q3, targets=None, N=AUTO, depth=AUTO, eps=1e-8):
+        src = _f64(src).reshape(-1, 3); q3 = _f64(q3).reshape(-1, 3)
+        if targets is None:
+            fld = np.zeros((len(src), 3))
+            self.lib.ref_fmm3d_vec(len(src), _ptr(src), _ptr(q3), int(N), int(depth), float(eps), _ptr(fld))
+        else:
+            tgt = _f64(targets).reshape(-1, 3)
+            fld = np.zeros((len(tgt), 3))
+            self.lib.ref_fmm3d_vec_st(len(src), _ptr(src), _ptr(q3), len(tgt), _ptr(tgt), int(N), int(depth),
+                                      float(eps), _ptr(fld))
+        return fld
 
     def fmm2d(self, src, q, targets=None, N=AUTO, depth=AUTO, eps=1e-8):
         src = _f64(src).reshape(-1, 2); q = _f64(q)

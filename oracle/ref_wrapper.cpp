@@ -5,6 +5,8 @@
 // tests, the fixture generator and bench.py's reference arm load it, as the
 // checker and the CPU baseline.  Entry points:
 //   * ref_fmm3d / ref_fmm3d_st : fmm::FastMultipole3d<double> (cpu/multipole3d.cpp:1296-1374)
+//   * ref_fmm3d_vec / ref_fmm3d_vec_st : fmm::FastMultipole3d<Vector3d> (vector charges,
+//                                cpu/multipole3d.cpp:414-853, instantiated at :1397)
 //   * ref_fmm2d / ref_fmm2d_st : fmm::FastMultipole            (cpu/multipole.cpp:451-522)
 //   * ref_tree3d_* / ref_tree2d_* : fmm::MortonTree<dim,...>    (cpu/morton_tree.cpp:286-493)
 //   * ref_wignerd              : fmm::ComputeWignerD            (common/special_functions.cpp:211-351)
@@ -43,6 +45,17 @@ std::vector<fmm::particle3d> make3d(const double* xyz, const double* q, size_t n
 	std::vector<fmm::particle3d> p(n);
 	for (size_t i = 0; i < n; ++i)
 		p[i] = { fmm::Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]), q ? q[i] : 0.0, 0 };
+	return p;
+}
+
+using vparticle = fmm::FastMultipole3d<fmm::Vector3d>::particle_t;
+
+std::vector<vparticle> make3v(const double* xyz, const double* q3, size_t n)
+{
+	std::vector<vparticle> p(n);
+	for (size_t i = 0; i < n; ++i)
+		p[i] = { fmm::Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]),
+		         q3 ? fmm::Vector3d(q3[3 * i], q3[3 * i + 1], q3[3 * i + 2]) : fmm::Vector3d(0, 0, 0), 0 };
 	return p;
 }
 
@@ -98,6 +111,30 @@ int ref_fmm3d_st(size_t ns, const double* sxyz, const double* sq, size_t nt, con
 		pot[i] = f.potentials[i];
 		for (int c = 0; c < 3; ++c) field[3 * i + c] = f.forces[i][c];
 	}
+	return 0;
+}
+
+int ref_fmm3d_vec(size_t n, const double* xyz, const double* q3, int N, int depth, double eps, double* field)
+{
+	ensure_tables();
+	Quiet quiet(!g_verbose);
+	auto p = make3v(xyz, q3, n);
+	fmm::FastMultipole3d<fmm::Vector3d> f(p, eps, N, depth);
+	for (size_t i = 0; i < n; ++i)
+		for (int c = 0; c < 3; ++c) field[3 * i + c] = f.forces[i][c];
+	return 0;
+}
+
+int ref_fmm3d_vec_st(size_t ns, const double* sxyz, const double* sq3, size_t nt, const double* txyz, int N,
+                     int depth, double eps, double* field)
+{
+	ensure_tables();
+	Quiet quiet(!g_verbose);
+	auto s = make3v(sxyz, sq3, ns);
+	auto t = make3v(txyz, nullptr, nt);
+	fmm::FastMultipole3d<fmm::Vector3d> f(s, t, eps, N, depth);
+	for (size_t i = 0; i < nt; ++i)
+		for (int c = 0; c < 3; ++c) field[3 * i + c] = f.forces[i][c];
 	return 0;
 }
 

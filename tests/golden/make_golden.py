@@ -6,7 +6,7 @@ Runs the UNMODIFIED reference CPU path (built from its sources by
 inputs, outputs, trees and Wigner-d tables as ``tests/golden/*.npz``.  The
 fixtures pin the C oracle in the CPU tests and travel with the repository.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [vector]
 """
 import sys
 from pathlib import Path
@@ -40,6 +40,14 @@ CASES_3D = [
     ("c3d_n18", 1200, 0, 18, 3, 13),
     ("c3d_deep", 600, 0, 5, 6, 14),
 ]
+CASES_VEC = [
+    # vector charges (reference FastMultipole3d<Vector3d>); zero_frac: share of
+    # particles with q = 0 (the reference then makes them the targets)
+    # name, n_src, n_tgt, N, depth, seed, zero_frac
+    ("c3d_vec", 2000, 0, 9, 4, 31, 0.0),
+    ("c3d_vec_st", 1500, 600, 8, 4, 32, 0.0),
+    ("c3d_vec_zero", 1200, 0, 7, 4, 33, 0.1),
+]
 CASES_2D = [
     ("c2d_src", 2000, 0, 21, 5, 21),
     ("c2d_st", 1500, 600, 12, 5, 22),
@@ -47,9 +55,28 @@ CASES_2D = [
 ]
 
 
+def vector_cases(R):
+    for name, ns, nt, N, D, seed, zf in CASES_VEC:
+        g = rng(seed)
+        src = g.random((ns, 3)); q = g.uniform(-1, 1, (ns, 3))
+        if zf:
+            q[g.random(ns) < zf] = 0.0
+        tgt = g.random((nt, 3)) * 1.2 - 0.1 if nt else None
+        fld = R.fmm3d_vec(src, q, targets=tgt, N=N, depth=D)
+        d = dict(src=src, q=q, field=fld, N=np.int64(N), depth=np.int64(D))
+        if tgt is not None:
+            d["tgt"] = tgt
+        np.savez_compressed(HERE / f"{name}.npz", **d)
+
+
 def main():
     R = Reference()
     R.set_threads(1)
+    if sys.argv[1:] == ["vector"]:          # the vector-charge fixtures alone
+        vector_cases(R)
+        print("wrote", sorted(p.name for p in HERE.glob("c3d_vec*.npz")))
+        return
+    vector_cases(R)
     for name, ns, nt, N, D, seed in CASES_3D:
         g = rng(seed)
         src = g.random((ns, 3)); q = g.uniform(-1, 1, ns)
