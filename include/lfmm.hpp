@@ -107,7 +107,7 @@ inline void split(const std::vector<P>& ps, std::vector<double>& xyz, std::vecto
 template <typename value>
 class FastMultipole3d;
 
-// Scalar charges (the vector-charge variant of the reference is not provided).
+// Scalar charges.
 template <>
 class FastMultipole3d<double> {
 public:
@@ -144,6 +144,53 @@ private:
 		c.check(lfmm3d_solve_ex(c.h, src.size(), sx.data(), sq.data(), tgt ? tgt->size() : 0,
 		                        tgt ? tx.data() : nullptr, &o, potentials.data(), field.data(), &stats),
 		        "lfmm3d_solve_ex");
+		forces.resize(nout);
+		for (size_t i = 0; i < nout; ++i) forces[i] = Vector3d(field[3 * i], field[3 * i + 1], field[3 * i + 2]);
+	}
+};
+
+// Vector charges (reference FastMultipole3d<Vector3d>): forces = sum q x d / r^3
+// at every target; potentials stays empty, as in the reference.
+template <>
+class FastMultipole3d<Vector3d> {
+public:
+	using particle_t = particle<point3d, Vector3d>;
+
+	FastMultipole3d(const std::vector<particle_t>& particles, double eps = 1.e-8, int N = FMM_AUTO,
+	                int tree_depth = FMM_AUTO, int max_leaf = 0, int precision = LFMM_PRECISION_FP64)
+	{
+		solve(particles, nullptr, eps, N, tree_depth, max_leaf, precision);
+	}
+	FastMultipole3d(const std::vector<particle_t>& source_particles, const std::vector<particle_t>& target_particles,
+	                double eps = 1.e-8, int N = FMM_AUTO, int tree_depth = FMM_AUTO, int max_leaf = 0,
+	                int precision = LFMM_PRECISION_FP64)
+	{
+		solve(source_particles, &target_particles, eps, N, tree_depth, max_leaf, precision);
+	}
+
+	std::vector<Vector3d> forces;
+	std::vector<double> potentials;
+	lfmm_stats stats{};
+
+private:
+	void solve(const std::vector<particle_t>& src, const std::vector<particle_t>* tgt, double eps, int N, int depth,
+	           int max_leaf, int precision)
+	{
+		std::vector<double> sx(3 * src.size()), sq(3 * src.size()), tx;
+		for (size_t i = 0; i < src.size(); ++i)
+			for (int c = 0; c < 3; ++c) { sx[3 * i + c] = src[i].center[c]; sq[3 * i + c] = src[i].q[c]; }
+		if (tgt) {
+			tx.resize(3 * tgt->size());
+			for (size_t i = 0; i < tgt->size(); ++i)
+				for (int c = 0; c < 3; ++c) tx[3 * i + c] = (*tgt)[i].center[c];
+		}
+		const size_t nout = tgt ? tgt->size() : src.size();
+		std::vector<double> field(3 * nout);
+		lfmm_solve_opts o{N, depth, max_leaf, precision, eps};
+		auto& c = detail::ctx();
+		c.check(lfmm3d_solve_vector(c.h, src.size(), sx.data(), sq.data(), tgt ? tgt->size() : 0,
+		                            tgt ? tx.data() : nullptr, &o, field.data(), &stats),
+		        "lfmm3d_solve_vector");
 		forces.resize(nout);
 		for (size_t i = 0; i < nout; ++i) forces[i] = Vector3d(field[3 * i], field[3 * i + 1], field[3 * i + 2]);
 	}

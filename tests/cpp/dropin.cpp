@@ -1,6 +1,6 @@
 // A reference-style caller compiled against the drop-in header: 3D solve in
-// source-only and source/target mode, 2D solve, and the direct sum; prints
-// the results as text for the test to compare.
+// source-only and source/target mode, vector charges, 2D solve, and the
+// direct sum; prints the results as text for the test to compare.
 #include "lfmm.hpp"
 
 #include <cstdio>
@@ -14,6 +14,8 @@ int main()
 	for (auto& p : p3) { p.center = fmm::Vector3d(u(g), u(g), u(g)); p.q = c(g); }
 	std::vector<fmm::particle3d> t3(300);
 	for (auto& p : t3) { p.center = fmm::Vector3d(u(g), u(g), u(g)); p.q = 0.0; }
+	std::vector<fmm::particle<fmm::point3d, fmm::Vector3d>> pv(2500);
+	for (auto& p : pv) { p.center = fmm::Vector3d(u(g), u(g), u(g)); p.q = fmm::Vector3d(c(g), c(g), c(g)); }
 	std::vector<fmm::particle2d> p2(3000);
 	for (auto& p : p2) { p.center = {u(g), u(g)}; p.q = c(g); }
 
@@ -21,6 +23,7 @@ int main()
 	fmm::gpu::cudaCopyMathConstants();
 	fmm::gpu::FastMultipole3d<double> a(p3, 1e-8, 9, 4);
 	fmm::gpu::FastMultipole3d<double> b(p3, t3, 1e-8, 9, 4);
+	fmm::gpu::FastMultipole3d<fmm::Vector3d> v(pv, 1e-8, 8, 4);
 	fmm::gpu::FastMultipole f2(p2, 1e-8, 16, 5);
 	auto e3 = fmm::gpu::ComputeExact<fmm::InteractionType::Potential3d>(p3, t3);
 	fmm::gpu::cudaClearMathConstants();
@@ -35,5 +38,9 @@ int main()
 		            b.forces[i][2], e3[i]);
 	for (size_t i = 0; i < p2.size(); ++i)
 		std::printf("c %.17g %.17g %.17g\n", f2.potentials[i], f2.forces[i].real(), f2.forces[i].imag());
+	for (size_t i = 0; i < pv.size(); ++i)
+		std::printf("v %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", pv[i].center[0], pv[i].center[1],
+		            pv[i].center[2], pv[i].q[0], pv[i].q[1], pv[i].q[2], v.forces[i][0], v.forces[i][1], v.forces[i][2]);
+	if (!v.potentials.empty()) return 1;
 	return 0;
 }

@@ -42,3 +42,5 @@ def test_dropin_matches_oracle(dropin_bin, oracle):
     assert rel_l2(b[:, 4], pe) < 1e-13
     pot, fld = oracle.fmm2d(p2[:, :2], p2[:, 2], N=16, depth=5)
     assert rel_l2(c[:, 0], pot) < 1e-12 and rel_l2(c[:, 1:], fld) < 1e-12
+    v = np.array(rows["v"])                  # vector charges: position, q, field
+    assert rel_l2(v[:, 6:], oracle.fmm3d_vec(v[:, :3], v[:, 3:6], N=8, depth=4)) < 5e-12
