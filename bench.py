@@ -66,6 +66,13 @@ CONFIGS = {
                         "cluster (sigma 0.05) each, mixed precision at the learned order for rel-L2 <= 1e-6 "
                         "(32 checked outputs per problem), adaptive octrees (<=10 levels, <=64 per leaf); "
                         "plain FP64 p=10 one problem at a time beside it"),
+    # vector charges (the reference's FastMultipole3d<Vector3d>): 4,194,304 particles of the
+    # clustered mixture, charges U(-1, 1)^3, mixed precision, N = 12, adaptive octree;
+    # the FP64 form beside it
+    "c6": dict(dim=3, vector=True, n=4194304, gen="plummer_mix3d", seed=606, N=12, depth=10, max_leaf=64,
+               precision="mixed", metric="3D vector-charge FMM Mparticles/s (field q x r / r^3)",
+               workload="3D vector charges: Plummer (a=0.05) + uniform 4,194,304 particles, charges U(-1,1)^3, "
+                        "adaptive octree (<=10 levels, <=64 per leaf), mixed precision, p=11 (N=12)"),
 }
 DEFAULT_CONFIG = "c3"
 METRIC = "3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: mixed+learned-p vs plain"
@@ -253,7 +260,7 @@ def tf32_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=False):
+def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=False, parts=False):
     """Kernels the library enqueues for one solve (tree + FMM passes), counted
     from the launch sites; the learned solve adds its features (far strength
     per level, accumulation per level, leaf features), the network, the
@@ -270,7 +277,7 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=Fa
         m2l = max(0, depth - 2) * (3 + 1 + 1) + 2 * 2          # plan + GEMM (+ split reduce), FP64 coarse converts
         leaves = 2 if precision == "mixed" else 1               # FP32: near field, then the expansions
         fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + leaves
-        return tree + fmm + extra
+        return (tree, fmm) if parts else tree + fmm + extra
     tree += lists
     if dim == 3:
         fmm = 1 + (depth - 1) + max(0, depth - 2) * 5 + max(0, depth - 3) + 1
@@ -695,11 +702,128 @@ def run_batch(args, cfg):
     return 0
 
 
+def vector_launches(depth, precision):
+    """One tree, three scalar passes, the nonzero-charge, three component and
+    one cross-product kernels."""
+    tree, fmm = launches_per_solve(depth, 3, (3 * (depth - 1) + 7) // 8, True, precision, parts=True)
+    return tree + 3 * fmm + 1 + 3 + 1
+
+
+def run_vector(args, cfg):
+    """Vector charges: the solve on device buffers, end to end through the
+    host entry point, accuracy at 4096 targets against the FP64 direct sum
+    (three scalar direct sums combined by the cross product), the FP64 form
+    beside it and the reference's own vector FMM on the host cores."""
+    import torch
+    from laplace_fmm_b200 import Context
+    from laplace_fmm_b200._lib import PRECISION, LfmmSolveOpts, LfmmStats
+    from laplace_fmm_b200.workloads import rel_l2, sample_targets
+    n, N, depth, ml = cfg["n"], cfg["N"], cfg["depth"], cfg["max_leaf"]
+    pos, _ = make_particles(cfg)
+    q3 = np.random.Generator(np.random.PCG64(cfg["seed"] + 1)).uniform(-1, 1, (n, 3))
+    ctx = Context(0)
+    L = ctx.lib
+    vp = ctypes.c_void_p
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    d_src, d_q = torch.from_numpy(pos).cuda(), torch.from_numpy(q3).cuda()
+    d_fld = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+
+    def solve(precision, stats=None, host=None, c=None):
+        c = c or ctx
+        opts = LfmmSolveOpts(N, depth, ml, PRECISION[precision], 1e-8)
+        sp = ctypes.byref(stats) if stats is not None else None
+        if host:
+            hs, hq, hf = host
+            c.check(L.lfmm3d_solve_vector(c.handle, n, vp(hs.data_ptr()), vp(hq.data_ptr()), 0, None,
+                                          ctypes.byref(opts), vp(hf.data_ptr()), sp), "vector solve")
+        else:
+            c.check(L.lfmm3d_solve_vector_device(c.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), 0, None,
+                                                 ctypes.byref(opts), vp(d_fld.data_ptr()), sp), "vector solve")
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for k in range(steps):
+            starts[k].record(stream)
+            fn()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / steps
+
+    for _ in range(args.warmup):
+        solve(cfg["precision"])
+    with ClockSampler(0) as clk:
+        ms = timed(lambda: solve(cfg["precision"]), args.steps)
+    st = LfmmStats()
+    ctx_t = Context(0, timing=True)
+    solve(cfg["precision"], c=ctx_t)                  # warms this context's caches
+    solve(cfg["precision"], stats=st, c=ctx_t)
+    torch.cuda.synchronize()
+    ctx_t.close()
+    field = d_fld.cpu().numpy()
+    # accuracy: B = sum_c e_c x E^(c) from three FP64 direct sums at the sampled targets
+    idx = sample_targets(n)
+    tgt = torch.from_numpy(np.ascontiguousarray(pos[idx])).cuda()
+    E = []
+    for c in range(3):
+        qc = torch.from_numpy(np.ascontiguousarray(q3[:, c])).cuda()
+        ep = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+        ef = torch.empty((len(idx), 3), dtype=torch.float64, device="cuda")
+        ctx.check(L.lfmm3d_direct_device(ctx.handle, n, vp(d_src.data_ptr()), vp(qc.data_ptr()), len(idx),
+                                         vp(tgt.data_ptr()), vp(ep.data_ptr()), vp(ef.data_ptr())), "direct")
+        stream.synchronize()
+        E.append(ef.cpu().numpy())
+    Bd = np.stack([E[1][:, 2] - E[2][:, 1], E[2][:, 0] - E[0][:, 2], E[0][:, 1] - E[1][:, 0]], axis=1)
+    acc = {"rel_l2_field": rel_l2(field[idx], Bd), "targets": len(idx)}
+    # the FP64 form
+    solve("fp64")
+    pms = timed(lambda: solve("fp64"), max(1, min(args.steps, 3)))
+    # end to end through the host entry point (pinned buffers)
+    hs, hq = torch.from_numpy(pos).pin_memory(), torch.from_numpy(q3).pin_memory()
+    hf = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    solve(cfg["precision"], host=(hs, hq, hf))
+    e2e_ms = timed(lambda: solve(cfg["precision"], host=(hs, hq, hf)), max(1, min(args.steps, 3)))
+    # the reference's own vector FMM (host cores) on every 64th particle, uniform depth 7
+    cpu = None
+    if not args.no_cpu_baseline:
+        solver, kind = cpu_solver()
+        if kind == "reference":
+            cores = os.cpu_count() or 1
+            solver.set_threads(cores)
+            p, qq = np.ascontiguousarray(pos[::64]), np.ascontiguousarray(q3[::64])
+            t0 = time.perf_counter()
+            solver.fmm3d_vec(p, qq, N=N, depth=7)
+            s = time.perf_counter() - t0
+            cpu = {"value": len(p) / s / 1e6, "unit": "Mparticles/s", "cores": cores, "kind": kind,
+                   "sample": f"every 64th particle of the seeded set ({len(p)}), uniform depth 7"}
+    peaks = measured_peaks()
+    stats = st.as_dict()
+    tf32 = tf32_peak_tflops(torch)
+    line = {"metric": cfg["metric"], "value": n / (ms * 1e-3) / 1e6, "unit": "Mparticles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32", "data": "synthetic (seeded PCG64)",
+            "config": base_config(cfg, 1), "accuracy": acc,
+            "phases_ms_last_pass": {k: stats[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_l2l", "ms_leaves",
+                                                          "ms_total", "ms_m2l_kernel")},
+            "roofline_last_pass": roofline(cfg, stats, peaks, fp64_peak_tflops(torch), fp32_peak_tflops(torch), tf32),
+            "e2e": {"value": n / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(hs.numel() * 8 + hq.numel() * 8), "d2h_bytes_per_step": int(hf.numel() * 8)},
+            "plain_fp64": {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms},
+            "speedup_vs_plain_fp64": pms / ms, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": args.steps * vector_launches(depth, cfg["precision"])}
+    ctx.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     cfg = args.cfg
     if cfg.get("batch"):
         return run_batch(args, cfg)
+    if cfg.get("vector") and args.impl == "ours":
+        return run_vector(args, cfg)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -709,6 +833,35 @@ def main():
         if rank != 0:
             return 0
         pos, q = make_particles(cfg)
+        if cfg.get("vector"):
+            # the reference's vector FMM on the same particles and charges (sample as run_vector's)
+            q = np.random.Generator(np.random.PCG64(cfg["seed"] + 1)).uniform(-1, 1, (cfg["n"], 3))
+            solver, kind = cpu_solver()
+            if kind != "reference":
+                print(json.dumps({"impl": "reference", "unavailable": "the reference build (oracle/_ref) is absent"}))
+                return 0
+            cores = os.cpu_count() or 1
+            solver.set_threads(cores)
+            p, qq = np.ascontiguousarray(pos[::64]), np.ascontiguousarray(q[::64])
+            times = []
+            for k in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                solver.fmm3d_vec(p, qq, N=cfg["N"], depth=7)
+                if k >= args.warmup:
+                    times.append(time.perf_counter() - t0)
+            s = float(np.median(times))
+            v = len(p) / s / 1e6
+            sample = f"every 64th particle of the seeded set ({len(p)}), uniform depth 7"
+            print(json.dumps({"impl": "reference", "metric": cfg["metric"], "value": v, "unit": "Mparticles/s",
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
+                              "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+                              "config": base_config(cfg, 1),
+                              "cpu_baseline": {"value": v, "unit": "Mparticles/s", "cores": cores, "kind": kind,
+                                               "sample": sample},
+                              "e2e": {"value": v, "unit": "Mparticles/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+            return 0
         for _ in range(max(0, min(args.warmup, 1))):
             run_cpu(cfg, pos, q, 1)
         cb = run_cpu(cfg, pos, q, args.steps)

@@ -257,8 +257,9 @@ int lfmm3d_features(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const do
  * potential (the reference computes none for vector charges).  Sources are
  * the particles with q != 0 (the reference's zero-charge rule); one tree,
  * three scalar passes combined by a cross product.  opts as lfmm3d_solve_ex
- * (max_leaf 0: the uniform tree; N <= 15).  Host and device-buffer variants;
- * the host one synchronises. */
+ * (max_leaf 0: the uniform tree; N <= 15); stats describe the tree and the
+ * last of the three passes.  Host and device-buffer variants; the host one
+ * synchronises. */
 int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q3, size_t n_tgt,
                         const double* tgt_xyz, const lfmm_solve_opts* opts, double* field, lfmm_stats* stats);
 int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q3,

@@ -68,6 +68,12 @@ int fmm3d_solve_vector(Context& ctx, const ParticleInput& in, int N, int depth, 
 	int st = tree_build_adaptive(ctx, split, depth, max_leaf, t);
 	if (st) return st;
 	for (int c = 0; c < 3; ++c) {
+		if (c == 2 && stats && ctx.timing) {
+			// the statistics' phases and kernel times describe the last pass
+			ctx.kev_used = 0;
+			LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[0], s));
+			LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
+		}
 		component_kernel<<<div_up(t.n, 256), 256, 0, s>>>(t, in.nt, in.srcq, c);
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, E + 3 * n_out * c, c == 2 ? stats : nullptr)))
 			return st;
