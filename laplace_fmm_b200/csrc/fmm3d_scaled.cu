@@ -141,7 +141,10 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 		if (!next_leaf) { ctx.last_error = "scaled solve: allocation failed"; return ERR_OOM; }
 		LFMM_CUDA(ctx, cudaMemsetAsync(next_leaf, 0, sizeof(unsigned), s));
 		p2p_f32_kernel<LWP><<<6 * ctx.num_sms, LWP * 32, 0, s>>>(t, qr, pot, field, next_leaf);
-		eval_scaled_kernel<real, LWE><<<div_up(nl, LWE), LWE * 32, 0, s>>>(t, outer, inner, N, pot, field);
+		unsigned* next_eval = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
+		if (!next_eval) { ctx.last_error = "scaled solve: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(ctx, cudaMemsetAsync(next_eval, 0, sizeof(unsigned), s));
+		eval_scaled_kernel<real, LWE><<<8 * ctx.num_sms, LWE * 32, 0, s>>>(t, outer, inner, N, pot, field, next_eval);
 	} else {
 		constexpr int LW = leaf_warps<real>();
 		leaves_scaled_kernel<real><<<div_up(nl, LW), LW * 32, 0, s>>>(t, qr, outer, inner, N, knm, pot, field);

@@ -853,7 +853,8 @@ __global__ void __launch_bounds__(LW * 32, 768 / (LW * 32)) p2p_f32_kernel(DevTr
 }
 
 // M2P over the W list and L2P of the leaf's local expansion, added onto the
-// near field already in the outputs: one warp per leaf, lane = target; each
+// near field already in the outputs: one warp per leaf at a time, lane =
+// target; each
 // expansion's coefficients derived once per 32 targets (derive_coefs), the
 // targets evaluated by eval_cart.
 template <typename real> constexpr int eval_warps() { return sizeof(real) == sizeof(float) ? 4 : 2; }
@@ -861,52 +862,59 @@ template <typename real> constexpr int eval_warps() { return sizeof(real) == siz
 template <typename real, int LW>
 __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const typename V2<real>::t* __restrict__ outer,
                                                              const typename V2<real>::t* __restrict__ inner, int N,
-                                                             double* __restrict__ pot_out, double* __restrict__ fld_out)
+                                                             double* __restrict__ pot_out, double* __restrict__ fld_out,
+                                                             unsigned* __restrict__ next_leaf)
 {
 	using v2 = typename V2<real>::t;
 	__shared__ Coef4<real> sC[LW][NXD];
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const size_t li = (size_t)blockIdx.x * LW + w;
-	if (li >= t.nleaves) return;
-	const size_t g = t.leaves[li];
-	const uint32_t tb = t.tbeg[g], te = t.tend[g];
-	if (tb >= te) return;
-	const int Nx2 = N * (N + 1) / 2;
-	const double ihg = 1.0 / cell_size(t, g);
-	const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
-	const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
-	for (uint32_t t0 = tb; t0 < te; t0 += 32) {
-		const uint32_t i = t0 + lane;
-		const bool valid = i < te;
-		double xi = 0, yi = 0, zi = 0;
-		if (valid) { xi = t.x[i]; yi = t.y[i]; zi = t.z[i]; }
-		double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
-		for (uint32_t e = wb; e < we; ++e) {
-			const size_t D = t.w_idx[e];
+	// a resident grid: each warp takes the next leaf from a counter (leaves'
+	// W lists differ in length, so fixed blocks of leaves finish unevenly)
+	for (;;) {
+		unsigned lid = 0;
+		if (lane == 0) lid = atomicAdd(next_leaf, 1u);
+		const size_t li = __shfl_sync(0xffffffffu, lid, 0);
+		if (li >= t.nleaves) return;
+		const size_t g = t.leaves[li];
+		const uint32_t tb = t.tbeg[g], te = t.tend[g];
+		if (tb >= te) continue;
+		const int Nx2 = N * (N + 1) / 2;
+		const double ihg = 1.0 / cell_size(t, g);
+		const uint32_t wb = t.w_off[li], we = t.w_off[li + 1];
+		const double cx = t.cx[g], cy = t.cy[g], cz = t.cz[g];
+		for (uint32_t t0 = tb; t0 < te; t0 += 32) {
+			const uint32_t i = t0 + lane;
+			const bool valid = i < te;
+			double xi = 0, yi = 0, zi = 0;
+			if (valid) { xi = t.x[i]; yi = t.y[i]; zi = t.z[i]; }
+			double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+			for (uint32_t e = wb; e < we; ++e) {
+				const size_t D = t.w_idx[e];
+				__syncwarp();
+				derive_coefs<true, real>(outer + D * Nx2, N, sC[w], lane);
+				__syncwarp();
+				if (valid) {
+					const double ihd = 1.0 / cell_size(t, D);
+					real mp, gx, gy, gz;
+					eval_cart<true, real>(sC[w], (real)((xi - t.cx[D]) * ihd), (real)((yi - t.cy[D]) * ihd),
+					                      (real)((zi - t.cz[D]) * ihd), N, mp, gx, gy, gz);
+					pot += (double)mp * ihd;
+					fx -= (double)gx * ihd * ihd; fy -= (double)gy * ihd * ihd; fz -= (double)gz * ihd * ihd;
+				}
+			}
 			__syncwarp();
-			derive_coefs<true, real>(outer + D * Nx2, N, sC[w], lane);
+			derive_coefs<false, real>(inner + g * Nx2, N, sC[w], lane);
 			__syncwarp();
 			if (valid) {
-				const double ihd = 1.0 / cell_size(t, D);
-				real mp, gx, gy, gz;
-				eval_cart<true, real>(sC[w], (real)((xi - t.cx[D]) * ihd), (real)((yi - t.cy[D]) * ihd),
-				                      (real)((zi - t.cz[D]) * ihd), N, mp, gx, gy, gz);
-				pot += (double)mp * ihd;
-				fx -= (double)gx * ihd * ihd; fy -= (double)gy * ihd * ihd; fz -= (double)gz * ihd * ihd;
+				real lp, gx, gy, gz;
+				eval_cart<false, real>(sC[w], (real)((xi - cx) * ihg), (real)((yi - cy) * ihg),
+				                       (real)((zi - cz) * ihg), N, lp, gx, gy, gz);
+				pot += (double)lp * ihg;
+				fx -= (double)gx * ihg * ihg; fy -= (double)gy * ihg * ihg; fz -= (double)gz * ihg * ihg;
+				const uint32_t o = t.orig[i];
+				pot_out[o] += pot;
+				fld_out[3 * (size_t)o] += fx; fld_out[3 * (size_t)o + 1] += fy; fld_out[3 * (size_t)o + 2] += fz;
 			}
-		}
-		__syncwarp();
-		derive_coefs<false, real>(inner + g * Nx2, N, sC[w], lane);
-		__syncwarp();
-		if (valid) {
-			real lp, gx, gy, gz;
-			eval_cart<false, real>(sC[w], (real)((xi - cx) * ihg), (real)((yi - cy) * ihg),
-			                       (real)((zi - cz) * ihg), N, lp, gx, gy, gz);
-			pot += (double)lp * ihg;
-			fx -= (double)gx * ihg * ihg; fy -= (double)gy * ihg * ihg; fz -= (double)gz * ihg * ihg;
-			const uint32_t o = t.orig[i];
-			pot_out[o] += pot;
-			fld_out[3 * (size_t)o] += fx; fld_out[3 * (size_t)o + 1] += fy; fld_out[3 * (size_t)o + 2] += fz;
 		}
 	}
 }
