@@ -718,7 +718,7 @@ __device__ void eval_cart(const Coef4<real>* C, real x, real y, real z, int N, r
 // leaf, targets in passes of up to 32; a pass of np <= 16 targets runs
 // TP = np rounded up to a power of two targets at once and splits the
 // sources into 32 / TP phases (groups of 4), summed by shuffles.  Sources of
-// the leaf and its U list are staged 32 at a time as hi + lo offsets in the
+// the leaf and its U list are staged 32 at a time as negated hi + lo offsets in the
 // target leaf's frame, padded with zero charges to a multiple of 4 and read
 // as float4; the self pair is only tested for in the leaf's own chunks.
 // Partial sums over 16 sources in FP32, carried in FP64; 1/r from the
@@ -732,6 +732,12 @@ __device__ __forceinline__ float rsqrt_approx(float x)
 	return y;
 }
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// Sources are staged NEGATED (leaf centre minus source, hi and lo), so each
+// offset is a packed add: dx = (xi + sx) + (xl + lx), the same value as the
+// difference.  Two sources per packed FP32 instruction (add / mul / fma
+// .f32x2, sm_100); the clamp and 1/r stay scalar.
 template <bool SELF>
 __device__ __forceinline__ void p2p_f32_chunk(const float* __restrict__ sx, const float* __restrict__ sy,
                                               const float* __restrict__ sz, const float* __restrict__ lx,
@@ -740,8 +746,11 @@ __device__ __forceinline__ void p2p_f32_chunk(const float* __restrict__ sx, cons
                                               float xi, float yi, float zi, float xl, float yl, float zl,
                                               double& pot, double& fx, double& fy, double& fz)
 {
+	const float2 xi2 = f2(xi, xi), yi2 = f2(yi, yi), zi2 = f2(zi, zi);
+	const float2 xl2 = f2(xl, xl), yl2 = f2(yl, yl), zl2 = f2(zl, zl);
+	const float eps2 = (float)FORCE_EPS2;
 	for (int j0 = jb; j0 < cnt4; j0 += 4 * js) {
-		float p = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+		float2 p = f2(0.f, 0.f), ax = p, ay = p, az = p;
 #pragma unroll
 		for (int h = 0; h < 4; ++h) {
 			const int j = j0 + js * h;
@@ -750,24 +759,30 @@ __device__ __forceinline__ void p2p_f32_chunk(const float* __restrict__ sx, cons
 				const float4 Z = *reinterpret_cast<const float4*>(sz + j), XL = *reinterpret_cast<const float4*>(lx + j);
 				const float4 YL = *reinterpret_cast<const float4*>(ly + j), ZL = *reinterpret_cast<const float4*>(lz + j);
 				const float4 Q = *reinterpret_cast<const float4*>(sq + j);
-				const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w}, zs[4] = {Z.x, Z.y, Z.z, Z.w};
-				const float xls[4] = {XL.x, XL.y, XL.z, XL.w}, yls[4] = {YL.x, YL.y, YL.z, YL.w};
-				const float zls[4] = {ZL.x, ZL.y, ZL.z, ZL.w}, qs[4] = {Q.x, Q.y, Q.z, Q.w};
+				const float2 xs[2] = {f2(X.x, X.y), f2(X.z, X.w)}, ys[2] = {f2(Y.x, Y.y), f2(Y.z, Y.w)};
+				const float2 zs[2] = {f2(Z.x, Z.y), f2(Z.z, Z.w)}, xls[2] = {f2(XL.x, XL.y), f2(XL.z, XL.w)};
+				const float2 yls[2] = {f2(YL.x, YL.y), f2(YL.z, YL.w)}, zls[2] = {f2(ZL.x, ZL.y), f2(ZL.z, ZL.w)};
+				const float2 qs[2] = {f2(Q.x, Q.y), f2(Q.z, Q.w)};
 #pragma unroll
-				for (int k = 0; k < 4; ++k) {
-					const float dx = (xi - xs[k]) + (xl - xls[k]);
-					const float dy = (yi - ys[k]) + (yl - yls[k]);
-					const float dz = (zi - zs[k]) + (zl - zls[k]);
-					const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), (float)FORCE_EPS2);
-					const float inv = rsqrt_approx(r2);
-					const float qi = (SELF && j + k == self) ? 0.f : qs[k] * inv;
-					const float qi3 = qi * (inv * inv);
-					p += qi;
-					ax = fmaf(dx, qi3, ax); ay = fmaf(dy, qi3, ay); az = fmaf(dz, qi3, az);
+				for (int k = 0; k < 2; ++k) {
+					const float2 dx = __fadd2_rn(__fadd2_rn(xi2, xs[k]), __fadd2_rn(xl2, xls[k]));
+					const float2 dy = __fadd2_rn(__fadd2_rn(yi2, ys[k]), __fadd2_rn(yl2, yls[k]));
+					const float2 dz = __fadd2_rn(__fadd2_rn(zi2, zs[k]), __fadd2_rn(zl2, zls[k]));
+					const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+					const float2 inv = f2(rsqrt_approx(fmaxf(r2.x, eps2)), rsqrt_approx(fmaxf(r2.y, eps2)));
+					float2 qi = __fmul2_rn(qs[k], inv);
+					if (SELF) {
+						if (j + 2 * k == self) qi.x = 0.f;
+						if (j + 2 * k + 1 == self) qi.y = 0.f;
+					}
+					const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
+					p = __fadd2_rn(p, qi);
+					ax = __ffma2_rn(dx, qi3, ax); ay = __ffma2_rn(dy, qi3, ay); az = __ffma2_rn(dz, qi3, az);
 				}
 			}
 		}
-		pot += p; fx += ax; fy += ay; fz += az;
+		pot += (double)p.x + (double)p.y; fx += (double)ax.x + (double)ax.y;
+		fy += (double)ay.x + (double)ay.y; fz += (double)az.x + (double)az.y;
 	}
 }
 
@@ -814,7 +829,7 @@ __global__ void __launch_bounds__(LW * 32, 768 / (LW * 32)) p2p_f32_kernel(DevTr
 					__syncwarp();
 					if (lane < cnt) {
 						const uint32_t j = s0 + lane;
-						const double dx_ = t.x[j] - cx, dy_ = t.y[j] - cy, dz_ = t.z[j] - cz;
+						const double dx_ = cx - t.x[j], dy_ = cy - t.y[j], dz_ = cz - t.z[j];   // negated
 						const float hx = (float)dx_, hy = (float)dy_, hz = (float)dz_;
 						sx[w][lane] = hx; sy[w][lane] = hy; sz[w][lane] = hz;
 						lx[w][lane] = (float)(dx_ - (double)hx); ly[w][lane] = (float)(dy_ - (double)hy);
