@@ -60,6 +60,127 @@ template <typename real> const real* ops_of(Context& ctx, int N);
 template <> const double* ops_of<double>(Context& ctx, int N) { return m2l_ops_fp64(ctx, N, 1.0); }
 template <> const float* ops_of<float>(Context& ctx, int N) { return m2l_ops_fp32(ctx, N); }
 
+// Dense FP64 scaled M2M (OP = SOP_M2M) or L2L operators, one per child octant
+// o (the octant bits of the child's code): column r is translate_scaled, the
+// rotation-based shift of the SIMT kernels, applied to the r-th unit vector.
+// out: [8][MT][MT], pre-zeroed.
+template <int OP>
+__global__ void __launch_bounds__(WPB * 32) shift_ops_kernel(int N, int MT, Tab<double> T, double* __restrict__ out,
+                                                             unsigned* flags)
+{
+	__shared__ SmemT<double> sm[WPB];
+	__shared__ double2 unit[WPB][NX2MAX];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int Nx2 = N * (N + 1) / 2, R = 2 * Nx2;
+	const size_t task = (size_t)blockIdx.x * WPB + w;
+	const int o = (int)(task / R), r = (int)(task % R);
+	if (o >= 8) return;
+	const int bx = (o >> 2) & 1, by = (o >> 1) & 1, bz = o & 1;
+	const int d = OP == SOP_M2M ? dir_id(2 * bx - 1, 2 * by - 1, 2 * bz - 1) : dir_id(1 - 2 * bx, 1 - 2 * by, 1 - 2 * bz);
+	for (int c = lane; c < Nx2; c += 32)
+		unit[w][c] = make_double2(c == r / 2 && !(r & 1) ? 1.0 : 0.0, c == r / 2 && (r & 1) ? 1.0 : 0.0);
+	__syncwarp();
+	double2 acc[CMAX];
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) acc[k] = make_double2(0.0, 0.0);
+	translate_scaled<OP, double>(unit[w], d, acc, N, Nx2, sm[w], T, flags);
+	double* op = out + (size_t)o * MT * MT;
+#pragma unroll
+	for (int k = 0; k < CMAX; ++k) {
+		const int c = lane + 32 * k;
+		if (c < Nx2) {
+			op[(size_t)(2 * c) * MT + r] = acc[k].x;
+			op[(size_t)(2 * c + 1) * MT + r] = acc[k].y;
+		}
+	}
+}
+
+// Moves the diagonal of the 8 FP64 operators [8][MT][MT] into diag [8][MT]
+// (FP32; zero past R) and zeroes it in the operators.
+__global__ void split_diag_kernel(double* __restrict__ ops64, int MT, int R, float* __restrict__ diag)
+{
+	const int e = blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= 8 * MT) return;
+	const int o = e / MT, c = e % MT;
+	double* p = ops64 + ((size_t)o * MT + c) * MT + c;
+	diag[e] = c < R ? (float)*p : 0.f;
+	*p = 0.0;
+}
+
+// The tensor-core M2M (op 0) or L2L (op 1, followed by its diagonal) operators
+// of order N, cached in the context (built once; the plan's warm solves build
+// them before capture).
+const uint4* shift_ops_tc(Context& ctx, int N, int op)
+{
+	const int tag = 30 + op;
+	for (auto& e : ctx.opcache)
+		if (e.N == N && e.prec == tag) { e.stamp = ++ctx.opcache_clock; return static_cast<const uint4*>(e.ptr); }
+	const int MT = m2l_padded(N), R = N * (N + 1);
+	const size_t bytes64 = sizeof(double) * 8 * (size_t)MT * MT;
+	const size_t bytes_tc = tc_ops_bytes(8, N) + (op == 1 ? sizeof(float) * 8 * MT : 0);
+	opcache_make_room(ctx);
+	double* d = nullptr;
+	void* tc = nullptr;
+	if (cudaMalloc(&d, bytes64) != cudaSuccess || cudaMalloc(&tc, bytes_tc) != cudaSuccess) {
+		cudaGetLastError();
+		if (d) cudaFree(d);
+		ctx.last_error = "shift operators: out of memory";
+		return nullptr;
+	}
+	const Tab<double> T = tables_of<double>(ctx.tables.d);
+	const size_t tasks = (size_t)8 * R;
+	cudaMemsetAsync(d, 0, bytes64, ctx.stream);
+	if (op == 0) {
+		shift_ops_kernel<SOP_M2M><<<div_up(tasks, WPB), WPB * 32, 0, ctx.stream>>>(N, MT, T, d, ctx.dev_flags);
+	} else {
+		shift_ops_kernel<SOP_L2L><<<div_up(tasks, WPB), WPB * 32, 0, ctx.stream>>>(N, MT, T, d, ctx.dev_flags);
+		split_diag_kernel<<<div_up(8 * MT, 256), 256, 0, ctx.stream>>>(
+			d, MT, R, reinterpret_cast<float*>(static_cast<uint8_t*>(tc) + tc_ops_bytes(8, N)));
+	}
+	int st = cudaGetLastError() == cudaSuccess ? tc_ops_convert(ctx, d, 8, N, tc) : ERR_CUDA;
+	if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) st = ERR_CUDA;
+	cudaFree(d);
+	if (st != OK) {
+		cudaFree(tc);
+		ctx.last_error = "shift operators: build failed";
+		return nullptr;
+	}
+	OpCacheEntry e;
+	e.N = N; e.prec = tag; e.h = 1.0; e.bytes = bytes_tc;
+	e.stamp = ++ctx.opcache_clock; e.ptr = tc;
+	ctx.opcache.push_back(e);
+	return static_cast<const uint4*>(tc);
+}
+
+// M2M plan of level L for the tensor-core engine: the non-leaf cells (order,
+// one class; a leaf keeps its P2M expansion) and their children by octant
+// (vtab[cell][8]: level-local index at L + 1, or -1).
+__global__ void m2m_plan_kernel(DevTree t, int L, int32_t* __restrict__ vtab, int32_t* __restrict__ order,
+                                uint32_t* __restrict__ count)
+{
+	const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= t.lsize[L]) return;
+	const size_t g = t.loff[L] + c, cb = t.loff[L + 1];
+	if (t.beg[g] >= t.end[g]) return;
+	for (uint32_t k = t.beg[g]; k < t.end[g]; ++k) vtab[c * 8 + (size_t)(t.code[cb + k] & 7ull)] = (int32_t)k;
+	order[atomicAdd(count, 1u)] = (int32_t)c;
+}
+
+int m2m_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan)
+{
+	const size_t m = t.lsize[L];
+	plan.cells = m;
+	plan.vtab = static_cast<int32_t*>(ctx.arena.take(sizeof(int32_t) * 8 * m));
+	plan.order = static_cast<int32_t*>(ctx.arena.take(sizeof(int32_t) * m));
+	plan.oct_count = static_cast<uint32_t*>(ctx.arena.take(sizeof(uint32_t) * 8));
+	if (!plan.vtab || !plan.order || !plan.oct_count) { ctx.last_error = "m2m plan: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemsetAsync(plan.vtab, 0xff, sizeof(int32_t) * 8 * m, ctx.stream));
+	LFMM_CUDA(ctx, cudaMemsetAsync(plan.oct_count, 0, sizeof(uint32_t) * 8, ctx.stream));
+	m2m_plan_kernel<<<div_up(m, 256), 256, 0, ctx.stream>>>(t, L, plan.vtab, plan.order, plan.oct_count);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
 template <typename real>
 int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, SolveStats* stats)
 {
@@ -93,18 +214,36 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 	const unsigned nl = (unsigned)t.nleaves;
 	relcoords_kernel<real><<<nl, 128, 0, s>>>(t, xr, yr, zr, qr);
 	p2m_scaled_kernel<real><<<div_up(nl, WPB), WPB * 32, 0, s>>>(t, xr, yr, zr, qr, N, knm, outer);
-	for (int L = t.depth - 2; L >= 0; --L)
-		m2m_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, outer + t.loff[L + 1] * Nx2,
-		                                                                     outer + t.loff[L] * Nx2, N, T, ctx.dev_flags);
-	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
 	int st;
+	// the FP32 levels' shifts on the tensor-core engine (dense scaled operators,
+	// one per child octant), else the rotation-based SIMT kernels
+	const bool tc_shift = sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N);
+	if (tc_shift) {
+		const uint4* mops = shift_ops_tc(ctx, N, 0);
+		if (!mops) return ERR_OOM;
+		for (int L = t.depth - 2; L >= 0; --L) {
+			if (t.lsize[L] == 0) continue;
+			M2LPlan mp;
+			if ((st = m2m_plan_build(ctx, t, L, mp))) return st;
+			if ((st = shift_gemm_tc(ctx, TC_M2M, mp, mops, reinterpret_cast<const float*>(outer + t.loff[L + 1] * Nx2),
+			                        reinterpret_cast<float*>(outer + t.loff[L] * Nx2), N)))
+				return st;
+		}
+	} else {
+		for (int L = t.depth - 2; L >= 0; --L)
+			m2m_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, outer + t.loff[L + 1] * Nx2,
+			                                                                     outer + t.loff[L] * Nx2, N, T,
+			                                                                     ctx.dev_flags);
+	}
+	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[2], s));
+	std::vector<M2LPlan> plans(t.depth);
 	if (t.depth > 2) {
 		const real* ops = ops_of<real>(ctx, N);
 		const double* opd = coarse64 ? m2l_ops_fp64(ctx, N, 1.0) : nullptr;
 		if (!ops || (coarse64 && !opd)) return ERR_OOM;
 		for (int L = 2; L < t.depth; ++L) {
 			if (t.lsize[L] == 0) continue;
-			M2LPlan plan;
+			M2LPlan& plan = plans[L];
 			if ((st = m2l_plan_build(ctx, t, L, plan))) return st;
 			const real* mL = reinterpret_cast<const real*>(outer + t.loff[L] * Nx2);
 			real* lL = reinterpret_cast<real*>(inner + t.loff[L] * Nx2);
@@ -128,10 +267,25 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 	if (t.adaptive && t.n_x > 0)
 		p2l_kernel<real><<<div_up(C, WPB), WPB * 32, 0, s>>>(t, N, knm, inner);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s));
-	for (int L = 3; L < t.depth; ++L)
-		if (t.lsize[L])
-			l2l_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, inner + t.loff[L - 1] * Nx2,
-			                                                                     inner + t.loff[L] * Nx2, N, T, ctx.dev_flags);
+	if (tc_shift && t.depth > 3) {
+		const uint4* lops = shift_ops_tc(ctx, N, 1);
+		if (!lops) return ERR_OOM;
+		for (int L = 3; L < t.depth; ++L) {
+			if (t.lsize[L] == 0) continue;
+			// the level's cells grouped by octant (its M2L plan), one slot: the parent
+			M2LPlan lp = plans[L];
+			lp.vtab = t.parent + t.loff[L];
+			if ((st = shift_gemm_tc(ctx, TC_L2L, lp, lops, reinterpret_cast<const float*>(inner + t.loff[L - 1] * Nx2),
+			                        reinterpret_cast<float*>(inner + t.loff[L] * Nx2), N)))
+				return st;
+		}
+	} else {
+		for (int L = 3; L < t.depth; ++L)
+			if (t.lsize[L])
+				l2l_scaled_kernel<real><<<div_up(t.lsize[L], WPB), WPB * 32, 0, s>>>(t, L, inner + t.loff[L - 1] * Nx2,
+				                                                                     inner + t.loff[L] * Nx2, N, T,
+				                                                                     ctx.dev_flags);
+	}
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[4], s));
 	if constexpr (sizeof(real) == sizeof(float)) {
 		// the near field (a resident grid taking leaves from a counter), then

@@ -165,13 +165,20 @@ struct TcCfg {
 };
 
 // grid (tiles, slot splits).  With S = gridDim.y > 1 split s handles slots
-// [s*189/S, (s+1)*189/S) and writes part[s][cell][R]; else loc[cell][R].
-template <int NC>
+// [s*SLOTS/S, (s+1)*SLOTS/S) and writes part[s][cell][R]; else loc[cell][R].
+// MODE picks the operator of a (class, slot) and the store:
+//   TC_M2L    189 far slots, operator c_tc_slot_dir[class][slot], loc = sum;
+//   TC_M2M    8 slots (child octants), operator = slot, loc = sum;
+//   TC_L2L    1 slot (the parent), operator = class (the child's octant)
+//             without its diagonal, loc += sum + diag[class] * parent (the
+//             diagonal, 2^-(n+1) on degree n, applied exactly in FP32: through
+//             the TF32 split the dominant coefficients would lose 2^-22 per level).
+template <int NC, int SLOTS, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
-              unsigned* flags)
+              const float* __restrict__ diag, unsigned* flags)
 {
 	using C = TcCfg<NC>;
 	extern __shared__ uint8_t dsm[];
@@ -179,14 +186,14 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	__shared__ uint64_t tfull_bar, tempty_bar, drain_bar;
 	__shared__ uint32_t tmem_sh;
 	__shared__ int32_t tgt[TC_M];
-	__shared__ uint32_t active_mask[(M2L_SLOTS + 31) / 32];
-	__shared__ int16_t active[M2L_SLOTS];
+	__shared__ uint32_t active_mask[(SLOTS + 31) / 32];
+	__shared__ int16_t active[SLOTS];
 	__shared__ int s_nactive, s_oct, s_n, s_abort;
 	__shared__ uint32_t s_start;
 
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 	const int S = gridDim.y, sidx = blockIdx.y;
-	const int slot0 = sidx * M2L_SLOTS / S, slot1 = (sidx + 1) * M2L_SLOTS / S;
+	const int slot0 = sidx * SLOTS / S, slot1 = (sidx + 1) * SLOTS / S;
 	float* out = S > 1 ? part + (size_t)sidx * cells * R : loc;
 	uint8_t* base = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
 	volatile int* abort = &s_abort;
@@ -203,7 +210,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		}
 		s_oct = oct; s_n = nn; s_start = start; s_abort = 0; s_nactive = 0;
 	}
-	if (tid < (M2L_SLOTS + 31) / 32) active_mask[tid] = 0u;
+	if (tid < (SLOTS + 31) / 32) active_mask[tid] = 0u;
 	__syncthreads();
 	if (s_oct < 0) return;
 	const int oct = s_oct;
@@ -227,7 +234,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	// slots in which at least one target of the tile has a source
 	if (warp < 4) {
 		const int myt = tgt[tid];
-		const int32_t* row = vtab + (size_t)(myt >= 0 ? myt : 0) * M2L_SLOTS;
+		const int32_t* row = vtab + (size_t)(myt >= 0 ? myt : 0) * SLOTS;
 		for (int s = slot0; s < slot1; ++s) {
 			const unsigned any = __ballot_sync(0xffffffffu, myt >= 0 && row[s] >= 0);
 			if (lane == 0 && any) atomicOr(&active_mask[s >> 5], 1u << (s & 31));
@@ -252,8 +259,8 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		uint32_t it = 0;
 		for (int j = 0; j < nact; ++j) {
 			const int slot = active[j];
-			const int dir = c_tc_slot_dir[oct][slot];
-			const int src = myt >= 0 ? vtab[(size_t)myt * M2L_SLOTS + slot] : -1;
+			const int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
+			const int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
 			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
 			bool ok = true;
 			for (int kb = 0; kb < C::KB; ++kb, ++it) {
@@ -364,9 +371,17 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			if (tg >= 0 && !*abort) {
 				float* o = out + (size_t)tg * R + half * W;
 				const int lim = R - half * W;
+				if (MODE == TC_L2L) {
+					const float* xs = mult + (size_t)vtab[tg] * R + half * W;
+					const float* dg = diag + oct * NC + half * W;
 #pragma unroll
-				for (int c = 0; c < W; ++c)
-					if (c < lim) o[c] = acc[c];
+					for (int c = 0; c < W; ++c)
+						if (c < lim) o[c] += acc[c] + dg[c] * xs[c];
+				} else {
+#pragma unroll
+					for (int c = 0; c < W; ++c)
+						if (c < lim) o[c] = acc[c];
+				}
 			}
 		}
 	}
@@ -386,11 +401,12 @@ __global__ void tc_split_reduce_kernel(const float* __restrict__ part, float* __
 	loc[i] = s;
 }
 
-// FP64 scaled operators [343][NC][NC] -> per (direction, K block): hi rows then
-// lo rows, NC rows of 32 TF32 values, 16-byte chunk c of row r at c ^ (r & 7).
-__global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int NC, int R, int KB, uint32_t* __restrict__ out)
+// FP64 scaled operators [ndir][NC][NC] -> per (direction, K block): hi rows
+// then lo rows, NC rows of 32 TF32 values, 16-byte chunk c of row r at c ^ (r & 7).
+__global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, int NC, int R, int KB,
+                                    uint32_t* __restrict__ out)
 {
-	const size_t total = (size_t)343 * KB * 2 * NC * 32;
+	const size_t total = (size_t)ndir * KB * 2 * NC * 32;
 	const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (e >= total) return;
 	const int j = (int)(e % 32);
@@ -408,18 +424,18 @@ __global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int NC, in
 	out[word] = x == 0 ? hi : lo;
 }
 
-template <int NC>
+template <int NC, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
-           bool timed)
+           bool timed, const float* diag = nullptr)
 {
 	using C = TcCfg<NC>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	dim3 grid(tiles, S);
 	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
-	m2l_tc_kernel<NC><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(reinterpret_cast<const uint8_t*>(ops), mult, loc,
-	                                                            plan.vtab, plan.order, plan.oct_count, R, part,
-	                                                            plan.cells, ctx.dev_flags);
+	m2l_tc_kernel<NC, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+		reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part, plan.cells,
+		diag, ctx.dev_flags);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
 		ctx.kev_used += 2;
@@ -442,7 +458,8 @@ template <int NC>
 int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
 {
 	using C = TcCfg<NC>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, M2L_SLOTS, TC_M2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                    C::SMEM));
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	int S = 1;
 	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
@@ -483,6 +500,23 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 	return run_tc<NC>(ctx, plan, ops, mult, loc, R, S, part, true);
 }
 
+// M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
+template <int NC>
+int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int R)
+{
+	using C = TcCfg<NC>;
+	if (mode == TC_M2M) {
+		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 8, TC_M2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                    C::SMEM));
+		return run_tc<NC, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false);
+	}
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 1, TC_L2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                    C::SMEM));
+	// the diagonal [8][NC] follows the 8 operators
+	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + (size_t)8 * C::KB * C::OP_BYTES);
+	return run_tc<NC, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, diag);
+}
+
 std::mutex g_upload_mu;
 bool g_uploaded[64] = {};
 
@@ -515,7 +549,7 @@ const uint4* m2l_ops_tc(Context& ctx, int N)
 		ctx.last_error = "tensor-core operators: out of memory";
 		return nullptr;
 	}
-	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(d, NC, R, KB, static_cast<uint32_t*>(e.ptr));
+	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(d, 343, NC, R, KB, static_cast<uint32_t*>(e.ptr));
 	if (cudaGetLastError() != cudaSuccess) {
 		cudaFree(e.ptr);
 		ctx.last_error = "tensor-core operators: launch failed";
@@ -523,6 +557,37 @@ const uint4* m2l_ops_tc(Context& ctx, int N)
 	}
 	ctx.opcache.push_back(e);
 	return static_cast<const uint4*>(e.ptr);
+}
+
+size_t tc_ops_bytes(int ndir, int N) { return (size_t)ndir * m2l_tc_kblocks(N) * 2 * m2l_padded(N) * 128; }
+
+int tc_ops_convert(Context& ctx, const double* ops64, int ndir, int N, void* out)
+{
+	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N);
+	const size_t words = tc_ops_bytes(ndir, N) / 4;
+	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(ops64, ndir, NC, R, KB, static_cast<uint32_t*>(out));
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N)
+{
+	if (mode != TC_M2M && mode != TC_L2L) { ctx.last_error = "tensor-core shift: bad mode"; return ERR_ARG; }
+	const int R = N * (N + 1);
+	switch (m2l_padded(N)) {
+	case 64: return launch_shift_tc<64>(ctx, mode, plan, ops, src, dst, R);
+	case 80: return launch_shift_tc<80>(ctx, mode, plan, ops, src, dst, R);
+	case 96: return launch_shift_tc<96>(ctx, mode, plan, ops, src, dst, R);
+	case 112: return launch_shift_tc<112>(ctx, mode, plan, ops, src, dst, R);
+	case 144: return launch_shift_tc<144>(ctx, mode, plan, ops, src, dst, R);
+	case 160: return launch_shift_tc<160>(ctx, mode, plan, ops, src, dst, R);
+	case 192: return launch_shift_tc<192>(ctx, mode, plan, ops, src, dst, R);
+	case 224: return launch_shift_tc<224>(ctx, mode, plan, ops, src, dst, R);
+	case 240: return launch_shift_tc<240>(ctx, mode, plan, ops, src, dst, R);
+	default:
+		ctx.last_error = "tensor-core shift: unsupported order";
+		return ERR_UNSUPPORTED;
+	}
 }
 
 int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N)

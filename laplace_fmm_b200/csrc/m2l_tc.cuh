@@ -27,4 +27,21 @@ const uint4* m2l_ops_tc(Context& ctx, int N);
 // loc = sum over slots of T_dir mult[src] for every cell of the level (FP32).
 int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N);
 
+// The same engine for the level-to-level shifts, whose scaled operators are
+// one per child octant:
+//   TC_M2M  targets = the level's non-leaf cells (one class), 8 slots = the
+//           child octants, vtab[cell][8] = child (next level) or -1, and
+//           dst[cell] = sum_o T_o src[child_o];
+//   TC_L2L  targets = the level's cells grouped by octant (class = octant),
+//           1 slot = the parent (previous level), dst[cell] += T_class src[parent]
+//           with T's diagonal taken out of the operators and applied in FP32:
+//           ops holds the 8 operators (tc_ops_bytes(8, N)) and then the
+//           diagonal as float [8][m2l_padded(N)].
+enum { TC_M2L = 0, TC_M2M = 1, TC_L2L = 2 };
+int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N);
+// FP64 operators [ndir][m2l_padded(N)][m2l_padded(N)] -> the tensor-core layout
+// at out (tc_ops_bytes(ndir, N) bytes, 16-byte aligned).
+size_t tc_ops_bytes(int ndir, int N);
+int tc_ops_convert(Context& ctx, const double* ops64, int ndir, int N, void* out);
+
 } // namespace lfmm

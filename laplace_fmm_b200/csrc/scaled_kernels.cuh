@@ -630,9 +630,23 @@ __device__ __forceinline__ typename V2<real>::t coef_full(const typename V2<real
 template <typename real> struct Coef4 {
 	typename V2<real>::t f, gx, gy, gz;
 };
+// FP32 form as stored for eval_cart: the real parts of the four sets, then
+// their negated imaginary parts, so one float4 load feeds two packed FMAs.
+struct CoefP {
+	float4 re, im;
+};
+template <typename real> struct CoefStore { using t = Coef4<real>; };
+template <> struct CoefStore<float> { using t = CoefP; };
+__device__ __forceinline__ void put_coef(Coef4<double>* C, int e, const Coef4<double>& o) { C[e] = o; }
+__device__ __forceinline__ void put_coef(CoefP* C, int e, const Coef4<float>& o)
+{
+	C[e].re = make_float4(o.f.x, o.gx.x, o.gy.x, o.gz.x);
+	C[e].im = make_float4(-o.f.y, -o.gx.y, -o.gy.y, -o.gz.y);
+}
 
 template <bool IRR, typename real>
-__device__ void derive_coefs(const typename V2<real>::t* __restrict__ E, int N, Coef4<real>* C, int lane)
+__device__ void derive_coefs(const typename V2<real>::t* __restrict__ E, int N, typename CoefStore<real>::t* C,
+                             int lane)
 {
 	using v2 = typename V2<real>::t;
 	const int NB = IRR ? N + 1 : N, NG = IRR ? N + 1 : N - 1;
@@ -672,7 +686,7 @@ __device__ void derive_coefs(const typename V2<real>::t* __restrict__ E, int N, 
 		} else {
 			o.gx = o.gy = o.gz = V2<real>::make(0, 0);
 		}
-		C[e] = o;
+		put_coef(C, e, o);
 	}
 }
 
@@ -712,6 +726,45 @@ __device__ void eval_cart(const Coef4<real>* C, real x, real y, real z, int N, r
 		}
 	}
 	pot = p; gx = ex; gy = ey; gz = ez;
+}
+
+// The FP32 evaluation on packed f32x2 arithmetic (sm_100): the potential and
+// d/dx sums in one float2, d/dy and d/dz in another, the harmonic's real and
+// imaginary parts in a third; the same operations in the same order as the
+// scalar form, so the same results.
+template <bool IRR>
+__device__ void eval_cart(const CoefP* C, float x, float y, float z, int N, float& pot, float& gx, float& gy,
+                          float& gz)
+{
+	const int NB = IRR ? N + 1 : N;
+	const float r2 = x * x + y * y + z * z;
+	const float ir2 = IRR ? 1.f / r2 : 0.f;
+	const float wx = IRR ? x * ir2 : x, wy = IRR ? y * ir2 : y;
+	float bx = IRR ? rsq<float>(r2) : 1.f, by = 0.f;
+	float2 pe = make_float2(0.f, 0.f), yz = pe;
+	const float2 ir22 = make_float2(ir2, ir2);
+	for (int m = 0; m < NB; ++m) {
+		if (m > 0) {
+			const float sgm = sig_c<float>(m);
+			const float nx = sgm * (wx * bx - wy * by), ny = sgm * (wx * by + wy * bx);
+			bx = nx; by = ny;
+		}
+		float2 pv = make_float2(0.f, 0.f), cv = make_float2(bx, by);
+		int i = tix(m, m);
+		for (int n = m; n < NB; ++n) {
+			const float4 re = C[i].re, im = C[i].im;
+			const float2 cxx = make_float2(cv.x, cv.x), cyy = make_float2(cv.y, cv.y);
+			pe = __ffma2_rn(make_float2(re.x, re.y), cxx, __ffma2_rn(make_float2(im.x, im.y), cyy, pe));
+			yz = __ffma2_rn(make_float2(re.z, re.w), cxx, __ffma2_rn(make_float2(im.z, im.w), cyy, yz));
+			const float2 ab = c_rec_f[i];
+			const float az = ab.x * z, bb = IRR ? ab.y : ab.y * r2;
+			float2 nv = __ffma2_rn(make_float2(az, az), cv, __fmul2_rn(make_float2(-bb, -bb), pv));
+			if (IRR) nv = __fmul2_rn(nv, ir22);
+			pv = cv; cv = nv;
+			i += n + 1;                        // tix(n + 1, m)
+		}
+	}
+	pot = pe.x; gx = pe.y; gy = yz.x; gz = yz.y;
 }
 
 // FP32 near field on its own (few registers, high occupancy): one warp per
@@ -880,8 +933,7 @@ __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const t
                                                              double* __restrict__ pot_out, double* __restrict__ fld_out,
                                                              unsigned* __restrict__ next_leaf)
 {
-	using v2 = typename V2<real>::t;
-	__shared__ Coef4<real> sC[LW][NXD];
+	__shared__ typename CoefStore<real>::t sC[LW][NXD];
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	// a resident grid: each warp takes the next leaf from a counter (leaves'
 	// W lists differ in length, so fixed blocks of leaves finish unevenly)
@@ -911,7 +963,7 @@ __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const t
 				if (valid) {
 					const double ihd = 1.0 / cell_size(t, D);
 					real mp, gx, gy, gz;
-					eval_cart<true, real>(sC[w], (real)((xi - t.cx[D]) * ihd), (real)((yi - t.cy[D]) * ihd),
+					eval_cart<true>(sC[w], (real)((xi - t.cx[D]) * ihd), (real)((yi - t.cy[D]) * ihd),
 					                      (real)((zi - t.cz[D]) * ihd), N, mp, gx, gy, gz);
 					pot += (double)mp * ihd;
 					fx -= (double)gx * ihd * ihd; fy -= (double)gy * ihd * ihd; fz -= (double)gz * ihd * ihd;
@@ -922,7 +974,7 @@ __global__ void __launch_bounds__(LW * 32) eval_scaled_kernel(DevTree t, const t
 			__syncwarp();
 			if (valid) {
 				real lp, gx, gy, gz;
-				eval_cart<false, real>(sC[w], (real)((xi - cx) * ihg), (real)((yi - cy) * ihg),
+				eval_cart<false>(sC[w], (real)((xi - cx) * ihg), (real)((yi - cy) * ihg),
 				                       (real)((zi - cz) * ihg), N, lp, gx, gy, gz);
 				pot += (double)lp * ihg;
 				fx -= (double)gx * ihg * ihg; fy -= (double)gy * ihg * ihg; fz -= (double)gz * ihg * ihg;
