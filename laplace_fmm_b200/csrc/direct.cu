@@ -16,17 +16,19 @@ namespace {
 
 constexpr int DT = 128;
 
-// 1 / sqrt(x) for the sampled checks: an FP32 seed refined by two Newton
-// steps in FP64 (relative error ~1e-16); the FP64 square root and divide
-// where the seed's range does not reach.
+// 1 / sqrt(x) for the sampled checks (x = the clamped r^2 >= 1e-8): the
+// hardware's FP64 reciprocal square root approximation (rsqrt.approx.ftz.f64,
+// no FP32 round trip) refined by one third-order step of the binomial series
+// (1 - r)^(-1/2) = 1 + r/2 + 3r^2/8 + ..., r = 1 - x y^2: a seed error e
+// leaves ~(5/16)(2e)^3, below FP64 rounding for e < 2^-18.  The FP64 square
+// root and divide above 1e300.
 __device__ __forceinline__ double rsqrt_refined(double x)
 {
-	if (!(x > 1e-30 && x < 1e30)) return 1.0 / sqrt(x);
-	double y = (double)rsqrtf((float)x);
-	const double hx = 0.5 * x;
-	y = y * fma(-hx * y, y, 1.5);
-	y = y * fma(-hx * y, y, 1.5);
-	return y;
+	if (!(x < 1e300)) return 1.0 / sqrt(x);
+	double y;
+	asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+	const double r = fma(-x * y, y, 1.0);
+	return fma(y * r, fma(r, 0.375, 0.5), y);
 }
 
 // Sums of target i over sources [s_lo, s_hi): out[0] = potential, out[1..dim] = field.

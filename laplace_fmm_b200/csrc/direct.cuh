@@ -8,8 +8,9 @@ namespace lfmm {
 int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks);
 // Enqueue with S source chunks; part: scratch of 4 * nt * S doubles (written
 // before it is read; nothing needs to start at zero), unused when S == 1.
-// fast: 3D 1/r from an FP32 seed refined by two FP64 Newton steps (the
-// sampled checks); otherwise an FP64 square root and divide per pair.
+// fast: 3D 1/r from the FP64 reciprocal square root approximation refined
+// by one third-order series step (the sampled checks); otherwise an FP64
+// square root and divide per pair.
 int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
                   const double* tgt, double* pot, double* fld, double* part, int S, bool fast = false);
 // Enqueue on ctx.stream, scratch from the arena; all pointers are device pointers.
