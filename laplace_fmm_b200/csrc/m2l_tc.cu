@@ -1,16 +1,23 @@
 // tcgen05 M2L engine (m2l_tc.cuh).  One CTA per tile of 128 targets of one
 // octant class; D[128 targets][NC coefficients] in TMEM.  Warp roles:
 //   warps 0-3  producers: thread t gathers target t's source multipole for
-//              the K block, splits it into TF32 hi / lo and writes both rows
-//              128-byte swizzled; thread 0 also starts the bulk copy of the
-//              operator block (hi and lo, stored pre-swizzled) into the stage.
+//              the K block and splits it into TF32 hi / lo: hi into TMEM lane
+//              t (read by two MMAs straight from tensor memory), lo into the
+//              stage's shared memory as a 128-byte swizzled row (read by
+//              one); thread 0 also starts the bulk copy of the operator block
+//              (hi and lo, stored pre-swizzled) into the stage.
 //   warp 4     TMEM owner; lane 0 issues the MMAs (M=128, N=NC, K=8):
 //              main = B_hi T_hi (fresh per slot), corr += B_hi T_lo + B_lo T_hi.
 //   warps 5-12 epilogue: after each slot, add main to FP32 registers (warp w
 //              reads TMEM lanes 32 (w % 4) .. +31, half of the columns each).
-// Two smem stages (full: 128 arrivals + operator bytes; empty: MMA commit),
-// one main accumulator (full: MMA commit after the slot; empty: 256 epilogue
-// arrivals).  Every wait is bounded; on expiry the kernel sets
+// TMEM: main at columns [0, NC), corr at [256, 256 + NC), the stages' B_hi
+// (32 columns each) in the gaps [NC, 256) and [256 + NC, 512).  The two
+// accumulators stay apart: each tensor-core accumulate rounds at its
+// accumulator's ulp, and the corrections summed into main (measured) doubled
+// the mixed form's error on clustered sets.  With no 32-column gap (NC = 240)
+// B_hi goes to shared memory beside B_lo.  Stages (full: 128 arrivals +
+// operator bytes; empty: MMA commit): up to three; one main accumulator
+// (full: MMA commit after the slot; empty: 256 epilogue arrivals).  Every wait is bounded; on expiry the kernel sets
 // DEV_ERR_TIMEOUT, waits (bounded) for its copies and MMAs in flight, frees
 // TMEM and returns.
 #include "m2l_tc.cuh"
@@ -24,11 +31,10 @@ namespace {
 __constant__ int16_t c_tc_slot_dir[8][M2L_SLOTS];
 
 constexpr int TC_M = 128;                 // targets per tile
-constexpr int NSTAGE = 2;
+constexpr int NSTAGE_MAX = 3;
 constexpr int EPI_WARP0 = 5, EPI_WARPS = 8;
 constexpr int TC_THREADS = (EPI_WARP0 + EPI_WARPS) * 32;
 constexpr uint32_t TMEM_COLS = 512;
-constexpr uint32_t CORR_COL = 256;
 constexpr int WAIT_LIMIT = 1 << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -51,6 +57,20 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
 	d |= (uint64_t)1u << 46;
 	d |= (uint64_t)2u << 61;
 	return d;
+}
+
+// D (+)= A B^T with A read from tensor memory (M lanes x K columns of TF32)
+template <int NC>
+__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate)
+{
+	constexpr uint32_t IDESC = (1u << 4)                     // D: FP32
+	                         | (2u << 7)                     // A: TF32
+	                         | (2u << 10)                    // B: TF32
+	                         | ((uint32_t)(NC >> 3) << 17)   // N
+	                         | ((uint32_t)(TC_M >> 4) << 24); // M
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+	             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(IDESC), "r"(accumulate));
 }
 
 template <int NC>
@@ -132,6 +152,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
 	for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// registers -> TMEM, 32 lanes x 16 consecutive columns (the thread's own lane)
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r)
+{
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+	                "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+	             : "memory");
+}
+
 // acc[0 .. W) += TMEM columns [col, col + W) of this warp's 32 lanes
 template <int W>
 __device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
@@ -156,11 +185,19 @@ template <int NC>
 struct TcCfg {
 	static constexpr int KB = (NC + 31) / 32;           // K blocks of 32 inputs
 	static constexpr int OP_BYTES = 2 * NC * 128;       // operator block: hi rows, then lo rows
-	static constexpr int A_BYTES = TC_M * 128;          // multipole block, one of hi / lo
-	static constexpr int STAGE = OP_BYTES + 2 * A_BYTES;
+	static constexpr int A_BYTES = TC_M * 128;          // one 32-wide K block of the multipoles (hi or lo)
+	static constexpr uint32_t CORR_COL = 256;
+	static constexpr int GAP = (256 - NC) / 32;         // B_hi stages per TMEM gap
+	static constexpr bool HI_TMEM = GAP >= 1;           // B_hi in TMEM (else in shared memory)
+	static constexpr int STAGE = OP_BYTES + (HI_TMEM ? 1 : 2) * A_BYTES;
+	static constexpr int NSTAGE = HI_TMEM ? (2 * GAP < NSTAGE_MAX ? 2 * GAP : NSTAGE_MAX) : 2;
 	static constexpr int HALF = NC / 2;                 // columns per epilogue warp
 	static constexpr int SMEM = NSTAGE * STAGE + 1024;
+	// TMEM column of stage s's B_hi: the gap after main, then the gap after corr
+	static __device__ __forceinline__ uint32_t hi_col(uint32_t s)
+	{ return s < (uint32_t)GAP ? NC + 32u * s : CORR_COL + NC + 32u * (s - GAP); }
 	static_assert(NC % 16 == 0 && NC >= 16 && NC <= 256, "MMA N");
+	static_assert(CORR_COL + NC <= TMEM_COLS, "TMEM columns");
 	static_assert(HALF % 8 == 0, "epilogue column split");
 };
 
@@ -182,7 +219,8 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 {
 	using C = TcCfg<NC>;
 	extern __shared__ uint8_t dsm[];
-	__shared__ uint64_t full_bar[NSTAGE], empty_bar[NSTAGE];
+	constexpr int NSTAGE = C::NSTAGE;
+	__shared__ uint64_t full_bar[NSTAGE_MAX], empty_bar[NSTAGE_MAX];
 	__shared__ uint64_t tfull_bar, tempty_bar, drain_bar;
 	__shared__ uint32_t tmem_sh;
 	__shared__ int32_t tgt[TC_M];
@@ -272,32 +310,48 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 					const float2 w = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
 					v[2 * q] = w.x; v[2 * q + 1] = w.y;
 				}
-				if (it >= NSTAGE && !mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort)) {
+				// the TMEM stores below are warp-collective: the warp gives up as one
+				const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
+				if (!__all_sync(0xffffffffu, got)) {
 					ok = false;
 					break;
 				}
+				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 				uint8_t* stage = base + st * C::STAGE;
 				if (tid == 0) {
 					mbar_expect_tx(smem_u32(&full_bar[st]), C::OP_BYTES);
 					bulk_g2s(smem_u32(stage), ops + ((size_t)dir * C::KB + kb) * C::OP_BYTES, C::OP_BYTES,
 					         smem_u32(&full_bar[st]));
 				}
-				uint8_t* rh = stage + C::OP_BYTES + tid * 128;
-				uint8_t* rl = rh + C::A_BYTES;
+				// lo to the stage's swizzled row tid; hi to TMEM columns
+				// [hi_col(st), +32) of lane tid (or to the row after lo's)
+				const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + C::hi_col(st);
+				uint8_t* rl = stage + C::OP_BYTES + tid * 128;
+				uint8_t* rh = rl + C::A_BYTES;
 #pragma unroll
-				for (int c = 0; c < 8; ++c) {
-					uint32_t h[4], l[4];
+				for (int hf = 0; hf < 2; ++hf) {
+					uint32_t h[16], l[16];
 #pragma unroll
-					for (int e = 0; e < 4; ++e) {
-						const float x = v[4 * c + e];
+					for (int e = 0; e < 16; ++e) {
+						const float x = v[16 * hf + e];
 						h[e] = tf32_rna(x);
 						l[e] = tf32_rna(x - __uint_as_float(h[e]));
 					}
-					const int pc = c ^ (tid & 7);
-					*reinterpret_cast<uint4*>(rh + pc * 16) = make_uint4(h[0], h[1], h[2], h[3]);
-					*reinterpret_cast<uint4*>(rl + pc * 16) = make_uint4(l[0], l[1], l[2], l[3]);
+					if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * hf, h);
+#pragma unroll
+					for (int c = 0; c < 4; ++c) {
+						const int pc = (4 * hf + c) ^ (tid & 7);
+						*reinterpret_cast<uint4*>(rl + pc * 16) = make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
+						if constexpr (!C::HI_TMEM)
+							*reinterpret_cast<uint4*>(rh + pc * 16) =
+								make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+					}
 				}
 				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				if constexpr (C::HI_TMEM) {
+					asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+					asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+				}
 				mbar_arrive(smem_u32(&full_bar[st]));
 			}
 			if (!ok) {
@@ -323,15 +377,21 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 					if (!mbar_wait(smem_u32(&full_bar[st]), (it / NSTAGE) & 1u, abort)) { ok = false; break; }
 					asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 					const uint32_t sb = smem_u32(base + st * C::STAGE);
-					const uint32_t op_hi = sb, op_lo = sb + NC * 128;
-					const uint32_t a_hi = sb + C::OP_BYTES, a_lo = a_hi + C::A_BYTES;
+					const uint32_t op_hi = sb, op_lo = sb + NC * 128, a_lo = sb + C::OP_BYTES;
+					const uint32_t a_hi_t = tmem + C::hi_col(st), a_hi_s = a_lo + C::A_BYTES;
 #pragma unroll
 					for (int ks = 0; ks < 4; ++ks) {
-						const uint64_t ah = desc_sw128(a_hi + ks * 32), al = desc_sw128(a_lo + ks * 32);
 						const uint64_t bh = desc_sw128(op_hi + ks * 32), bl = desc_sw128(op_lo + ks * 32);
-						mma_tf32<NC>(tmem, ah, bh, (kb | ks) != 0);
-						mma_tf32<NC>(tmem + CORR_COL, ah, bl, (j | kb | ks) != 0);
-						mma_tf32<NC>(tmem + CORR_COL, al, bh, 1u);
+						const uint64_t al = desc_sw128(a_lo + ks * 32);
+						if constexpr (C::HI_TMEM) {
+							mma_tf32_ta<NC>(tmem, a_hi_t + 8u * ks, bh, (kb | ks) != 0);
+							mma_tf32_ta<NC>(tmem + C::CORR_COL, a_hi_t + 8u * ks, bl, (j | kb | ks) != 0);
+						} else {
+							const uint64_t ah = desc_sw128(a_hi_s + ks * 32);
+							mma_tf32<NC>(tmem, ah, bh, (kb | ks) != 0);
+							mma_tf32<NC>(tmem + C::CORR_COL, ah, bl, (j | kb | ks) != 0);
+						}
+						mma_tf32<NC>(tmem + C::CORR_COL, al, bh, 1u);
 					}
 					mma_commit(smem_u32(&empty_bar[st]));
 				}
@@ -366,7 +426,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			*abort = 1;
 			atomicOr(flags, DEV_ERR_TIMEOUT);
 		} else {
-			if (nact > 0) tmem_accumulate<W>(taddr + CORR_COL, acc);
+			if (nact > 0) tmem_accumulate<W>(taddr + C::CORR_COL, acc);
 			const int tg = tgt[quarter * 32 + lane];
 			if (tg >= 0 && !*abort) {
 				float* o = out + (size_t)tg * R + half * W;

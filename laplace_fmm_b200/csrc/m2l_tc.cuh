@@ -2,10 +2,11 @@
 // GEMM for the FP32 levels, TF32 with a hi + lo split of both operands:
 //   D = B T^T ~= B_hi T_hi + (B_hi T_lo + B_lo T_hi)
 // with D[targets][output coefficients], B the gathered source multipoles and
-// T the offset's operator.  The hi x hi product of each far slot is summed in
-// a fresh TMEM accumulator and added to FP32 registers after the slot (one
-// FP32 chain across 189 slots would keep only ~1e-5 relative accuracy); the
-// two small correction products accumulate in TMEM across all slots.
+// T the offset's operator.  The three products of each far slot are summed
+// in a fresh TMEM accumulator and added to FP32 registers after the slot (one
+// tensor-core FP32 chain across 189 slots would keep only ~1e-5 relative
+// accuracy).  B is stored by the producers into tensor memory and read from
+// there by the MMAs; shared memory holds only the operator stages.
 #pragma once
 #include "m2l_gemm.cuh"
 
