@@ -471,11 +471,11 @@ def m2l_flops(N):
     return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
 
 
-# DRAM bytes per millisecond of m2l_tc_kernel time, from an ncu capture of a
-# 2,097,152-particle case of the default workload (1.35 GB over 6.97 ms in 4
-# launches); the kernel's traffic grows with its work, so a full launch's
-# traffic is this rate times its duration.
-M2L_TC_DRAM_BYTES_PER_MS = 1.354e9 / 6.969
+# DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode), from an ncu
+# capture of a 2,097,152-particle case of the default workload at N = 14
+# (727 MB over 3.03 ms in 4 launches); the kernel's traffic grows with its
+# work, so a full launch's traffic is this rate times its duration.
+M2L_TC_DRAM_BYTES_PER_MS = 727.2e6 / 3.031
 
 
 def padded(N):
