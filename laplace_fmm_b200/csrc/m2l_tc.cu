@@ -181,14 +181,16 @@ __device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
 	}
 }
 
-template <int NC>
+// TMEM_HI = false keeps the sources' hi parts in shared memory (the L2L
+// mode: one slot of 7 K blocks per tile leaves the TMEM stores' waits exposed)
+template <int NC, bool TMEM_HI = true>
 struct TcCfg {
 	static constexpr int KB = (NC + 31) / 32;           // K blocks of 32 inputs
 	static constexpr int OP_BYTES = 2 * NC * 128;       // operator block: hi rows, then lo rows
 	static constexpr int A_BYTES = TC_M * 128;          // one 32-wide K block of the multipoles (hi or lo)
 	static constexpr uint32_t CORR_COL = 256;
 	static constexpr int GAP = (256 - NC) / 32;         // B_hi stages per TMEM gap
-	static constexpr bool HI_TMEM = GAP >= 1;           // B_hi in TMEM (else in shared memory)
+	static constexpr bool HI_TMEM = TMEM_HI && GAP >= 1; // B_hi in TMEM (else in shared memory)
 	static constexpr int STAGE = OP_BYTES + (HI_TMEM ? 1 : 2) * A_BYTES;
 	static constexpr int NSTAGE = HI_TMEM ? (2 * GAP < NSTAGE_MAX ? 2 * GAP : NSTAGE_MAX) : 2;
 	static constexpr int HALF = NC / 2;                 // columns per epilogue warp
@@ -217,7 +219,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
               const float* __restrict__ diag, unsigned* flags)
 {
-	using C = TcCfg<NC>;
+	using C = TcCfg<NC, MODE != TC_L2L>;
 	extern __shared__ uint8_t dsm[];
 	constexpr int NSTAGE = C::NSTAGE;
 	__shared__ uint64_t full_bar[NSTAGE_MAX], empty_bar[NSTAGE_MAX];
@@ -488,7 +490,7 @@ template <int NC, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
            bool timed, const float* diag = nullptr)
 {
-	using C = TcCfg<NC>;
+	using C = TcCfg<NC, MODE != TC_L2L>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	dim3 grid(tiles, S);
 	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
@@ -565,13 +567,14 @@ template <int NC>
 int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int R)
 {
 	using C = TcCfg<NC>;
+	using CL = TcCfg<NC, false>;
 	if (mode == TC_M2M) {
 		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 8, TC_M2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		                                    C::SMEM));
 		return run_tc<NC, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false);
 	}
 	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 1, TC_L2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                                    C::SMEM));
+	                                    CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
 	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + (size_t)8 * C::KB * C::OP_BYTES);
 	return run_tc<NC, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, diag);

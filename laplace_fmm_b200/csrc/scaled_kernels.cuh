@@ -731,7 +731,7 @@ __device__ void eval_cart(const Coef4<real>* C, real x, real y, real z, int N, r
 // The FP32 evaluation on packed f32x2 arithmetic (sm_100): the potential and
 // d/dx sums in one float2, d/dy and d/dz in another, the harmonic's real and
 // imaginary parts in a third; the same operations in the same order as the
-// scalar form, so the same results.
+// scalar form.
 template <bool IRR>
 __device__ void eval_cart(const CoefP* C, float x, float y, float z, int N, float& pot, float& gx, float& gy,
                           float& gz)
