@@ -11,7 +11,7 @@ namespace lfmm {
 namespace {
 
 __constant__ int16_t c_slot_dir[8][M2L_SLOTS];
-__constant__ int16_t c_dir_slot[8][343];
+__device__ int16_t g_dir_slot[8][343];    // global: vtab_kernel stages it in shared memory
 // 2D: 4 child classes x 27 far offsets, direction id (dx + 3) * 7 + (dy + 3)
 __constant__ int16_t c_slot_dir2[4][M2L_SLOTS2];
 __constant__ int16_t c_dir_slot2[4][49];
@@ -37,6 +37,11 @@ __device__ __forceinline__ void coords3(uint64_t code, int* c)
 // every store of the warp lands in the same row.
 __global__ void vtab_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsigned* flags)
 {
+	// the direction -> slot table in shared memory: the lanes look up
+	// different entries, which constant memory would serialise
+	__shared__ int16_t s_dir_slot[8 * 343];
+	for (int i = threadIdx.x; i < 8 * 343; i += blockDim.x) s_dir_slot[i] = (&g_dir_slot[0][0])[i];
+	__syncthreads();
 	const int lane = threadIdx.x & 31;
 	const size_t c = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const size_t m = t.lsize[L];
@@ -48,18 +53,22 @@ __global__ void vtab_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsign
 	int me[3];
 	coords3(t.code[off + c], me);
 	const int oct = ((me[0] & 1) << 2) | ((me[1] & 1) << 1) | (me[2] & 1);
+	const int16_t* ds = s_dir_slot + oct * 343;
 	const int32_t p = t.parent[off + c];
 	const int npc = t.close_cnt[poff + p];
 	const int32_t* pl = t.close_idx + (poff + p) * t.close_stride;
 	for (int e = lane; e <= npc; e += 32) {
 		const int32_t pn = e < npc ? pl[e] : p;
+		// a child of pn sits at 2 coords(pn) + its octant bits (code = pn's code << 3 | octant)
+		int q[3];
+		coords3(t.code[poff + pn], q);
+		const int bx = 2 * q[0] - me[0], by = 2 * q[1] - me[1], bz = 2 * q[2] - me[2];
 		for (uint32_t k = t.beg[poff + pn]; k < t.end[poff + pn]; ++k) {
 			if (k == c) continue;
-			int o[3];
-			coords3(t.code[off + k], o);
-			int dx = o[0] - me[0], dy = o[1] - me[1], dz = o[2] - me[2];
+			const int ko = (int)(t.code[off + k] & 7ull);
+			const int dx = bx + ((ko >> 2) & 1), dy = by + ((ko >> 1) & 1), dz = bz + (ko & 1);
 			if (max(max(abs(dx), abs(dy)), abs(dz)) <= 1) continue;
-			int slot = c_dir_slot[oct][(dx + 3) * 49 + (dy + 3) * 7 + (dz + 3)];
+			const int slot = ds[(dx + 3) * 49 + (dy + 3) * 7 + (dz + 3)];
 			if (slot < 0) { atomicOr(flags, DEV_ERR_DIRECTION); continue; }
 			row[slot] = (int32_t)k;
 		}
@@ -700,7 +709,7 @@ int upload_slots(Context& ctx)
 	if (g_slots_uploaded[ctx.device]) return OK;
 	const M2LSlots& S = m2l_slots();
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_slot_dir, S.slot_dir, sizeof(S.slot_dir)));
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_dir_slot, S.dir_slot, sizeof(S.dir_slot)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(g_dir_slot, S.dir_slot, sizeof(S.dir_slot)));
 	int16_t sd[4][M2L_SLOTS2], ds[4][49];
 	for (int o = 0; o < 4; ++o) {
 		for (int d = 0; d < 49; ++d) ds[o][d] = -1;
