@@ -16,6 +16,19 @@ constexpr double PI = 3.14159265358979323846;
 
 // Triangular (n,m) index, 0 <= m <= n (reference common/utils.h:130-147).
 __host__ __device__ constexpr inline int tix(int n, int m) { return n * (n + 1) / 2 + m; }
+// The degree n of triangular index c = tix(n, m) (m = c - tix(n, 0)), computed
+// rather than looked up: lanes of a warp ask for different c, which a
+// constant-memory table would serialise.
+__device__ __forceinline__ int tri_row(int c)
+{
+	// n = (sqrt(8c + 1) - 1) / 2 from the hardware reciprocal square root
+	// (r >= 1); the estimate is within one of n, which the two steps correct
+	const float r = 8.f * (float)c + 1.f;
+	int n = (int)((r * rsqrtf(r) - 1.f) * 0.5f);
+	if (tix(n + 1, 0) <= c) ++n;
+	if (tix(n, 0) > c) --n;
+	return n;
+}
 // Wigner-d (n,m,k) index, |k| <= n (reference common/special_functions.cpp:216-221).
 __host__ __device__ constexpr inline int dix(int n, int m, int k)
 { return n * (n + 1) * (4 * n - 1) / 6 + m * (2 * n + 1) + (k + n); }

@@ -18,8 +18,6 @@ constexpr int CMAX = (MAXN3 * (MAXN3 + 1) / 2 + 31) / 32;   // coefficients per 
 constexpr int NX2MAX = MAXN3 * (MAXN3 + 1) / 2;             // 171
 constexpr int WPB = 4;                                      // warps per block, box kernels
 
-__constant__ unsigned char c_n_of[NX2MAX];
-__constant__ unsigned char c_m_of[NX2MAX];
 
 enum { OP_M2M = 0, OP_M2L = 1, OP_L2L = 2 };
 
@@ -46,7 +44,7 @@ __device__ __forceinline__ void rotate_y_warp(const double2* __restrict__ in, do
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			int n = c_n_of[c], m = c_m_of[c];
+			const int n = tri_row(c), m = c - tix(n, 0);
 			const double* Dr = D + dix(n, m, 0);
 			double vr = 0.0, vi = 0.0;
 			const double2* row = in + tix(n, 0);
@@ -103,7 +101,7 @@ __device__ void translate_warp(const double2* __restrict__ src, double px, doubl
 #pragma unroll
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
-		if (c < Nx2) sm.a[c] = cmul(src[c], E1[c_m_of[c]]);
+		if (c < Nx2) sm.a[c] = cmul(src[c], E1[c - tix(tri_row(c), 0)]);
 	}
 	__syncwarp();
 	rotate_y_warp(sm.a, sm.b, D1, Nx2);
@@ -113,7 +111,7 @@ __device__ void translate_warp(const double2* __restrict__ src, double px, doubl
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			int j = c_n_of[c], k = c_m_of[c];
+			const int j = tri_row(c), k = c - tix(j, 0);
 			const double* cf = cube + (j * MAXN3 + k) * MAXN3;
 			double sr = 0.0, si = 0.0;
 			if (OP == OP_M2L) {
@@ -145,7 +143,7 @@ __device__ void translate_warp(const double2* __restrict__ src, double px, doubl
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			double2 v = cmul(sm.b[c], E2[c_m_of[c]]);
+			double2 v = cmul(sm.b[c], E2[c - tix(tri_row(c), 0)]);
 			acc[t].x += v.x; acc[t].y += v.y;
 		}
 	}
@@ -443,17 +441,12 @@ __global__ void __launch_bounds__(WPB * 32) m2l_ops_kernel(int N, int MT, double
 	}
 }
 
-bool g_const_ready = false;
 
+// The plain form's kernels need no constant tables (the (n, m) of a
+// triangular index is computed: tri_row); kept as the solvers' setup hook.
 int upload_constants(Context& ctx)
 {
-	if (g_const_ready) return OK;
-	unsigned char n_of[NX2MAX], m_of[NX2MAX];
-	for (int n = 0; n < MAXN3; ++n)
-		for (int m = 0; m <= n; ++m) { n_of[tix(n, m)] = (unsigned char)n; m_of[tix(n, m)] = (unsigned char)m; }
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_n_of, n_of, sizeof(n_of)));
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_m_of, m_of, sizeof(m_of)));
-	g_const_ready = true;
+	(void)ctx;
 	return OK;
 }
 

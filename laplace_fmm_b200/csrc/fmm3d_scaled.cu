@@ -20,7 +20,6 @@ int upload_scaled_constants(Context& ctx)
 {
 	if (ctx.device < 0 || ctx.device >= 64) { ctx.last_error = "device index above 63"; return ERR_ARG; }
 	if (g_scaled_const_ready[ctx.device]) return OK;
-	unsigned char n_of[NXD], m_of[NXD];
 	float2 rec_f[NXD];
 	double2 rec_d[NXD];
 	float sig_f[MAXN3 + 2];
@@ -28,7 +27,6 @@ int upload_scaled_constants(Context& ctx)
 	for (int n = 0; n <= MAXN3; ++n)
 		for (int m = 0; m <= n; ++m) {
 			const int i = tix(n, m);
-			n_of[i] = (unsigned char)n; m_of[i] = (unsigned char)m;
 			const double d1 = (double)(n + 1) * (n + 1) - (double)m * m;
 			rec_d[i] = make_double2((2.0 * n + 1.0) / std::sqrt(d1), std::sqrt(((double)n * n - (double)m * m) / d1));
 			rec_f[i] = make_float2((float)rec_d[i].x, (float)rec_d[i].y);
@@ -40,8 +38,6 @@ int upload_scaled_constants(Context& ctx)
 	double inv_d[NINV];
 	inv_f[0] = 0.f; inv_d[0] = 0.0;
 	for (int k = 1; k < NINV; ++k) { inv_d[k] = 1.0 / k; inv_f[k] = 1.0f / (float)k; }
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_n_of, n_of, sizeof(n_of)));
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_m_of, m_of, sizeof(m_of)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_f, inv_f, sizeof(inv_f)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_inv_d, inv_d, sizeof(inv_d)));
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_rec_f, rec_f, sizeof(rec_f)));

@@ -22,8 +22,6 @@ template <> struct V2<double> { using t = double2; static __device__ __forceinli
 template <> struct V2<float> { using t = float2; static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); } };
 
 constexpr int NXD = (MAXN3 + 1) * (MAXN3 + 2) / 2;   // coefficients of degree <= MAXN3
-__constant__ unsigned char c_n_of[NXD];
-__constant__ unsigned char c_m_of[NXD];
 // Solid harmonics in Cartesian form, orthonormal basis B_nm = r^n Y_nm
 // (regular) and r^-(n+1) Y_nm (irregular), Y_nm = sqrt((n-m)!/(n+m)!)
 // P_n^m(cos t) e^{i m phi} with the Condon-Shortley phase:
@@ -84,7 +82,7 @@ __device__ __forceinline__ void rotate_y_t(const typename V2<real>::t* __restric
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			int n = c_n_of[c], m = c_m_of[c];
+			const int n = tri_row(c), m = c - tix(n, 0);
 			const real* Dr = D + dix(n, m, 0);
 			real vr = 0, vi = 0;
 			const typename V2<real>::t* row = in + tix(n, 0);
@@ -130,7 +128,7 @@ __device__ void translate_scaled(const typename V2<real>::t* __restrict__ src, i
 #pragma unroll
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
-		if (c < Nx2) sm.a[c] = cmulv<real>(src[c], E1[c_m_of[c]]);
+		if (c < Nx2) sm.a[c] = cmulv<real>(src[c], E1[c - tix(tri_row(c), 0)]);
 	}
 	__syncwarp();
 	rotate_y_t<real>(sm.a, sm.b, D1, Nx2);
@@ -140,7 +138,7 @@ __device__ void translate_scaled(const typename V2<real>::t* __restrict__ src, i
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			int j = c_n_of[c], k = c_m_of[c];
+			const int j = tri_row(c), k = c - tix(j, 0);
 			const real* cf = cube + (j * MAXN3 + k) * MAXN3;
 			real sr = 0, si = 0;
 			if (OP == SOP_M2M) {
@@ -170,7 +168,7 @@ __device__ void translate_scaled(const typename V2<real>::t* __restrict__ src, i
 	for (int t = 0; t < CMAX; ++t) {
 		int c = lane + 32 * t;
 		if (c < Nx2) {
-			typename V2<real>::t v = cmulv<real>(sm.b[c], E2[c_m_of[c]]);
+			typename V2<real>::t v = cmulv<real>(sm.b[c], E2[c - tix(tri_row(c), 0)]);
 			acc[t].x += v.x; acc[t].y += v.y;
 		}
 	}
@@ -651,7 +649,7 @@ __device__ void derive_coefs(const typename V2<real>::t* __restrict__ E, int N, 
 	using v2 = typename V2<real>::t;
 	const int NB = IRR ? N + 1 : N, NG = IRR ? N + 1 : N - 1;
 	for (int e = lane; e < NB * (NB + 1) / 2; e += 32) {
-		const int n = c_n_of[e], k = c_m_of[e];
+		const int n = tri_row(e), k = e - tix(n, 0);
 		Coef4<real> o;
 		if (n < N) {
 			const v2 c = E[e];
