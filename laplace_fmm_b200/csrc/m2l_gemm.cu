@@ -14,7 +14,7 @@ __constant__ int16_t c_slot_dir[8][M2L_SLOTS];
 __device__ int16_t g_dir_slot[8][343];    // global: vtab_kernel stages it in shared memory
 // 2D: 4 child classes x 27 far offsets, direction id (dx + 3) * 7 + (dy + 3)
 __constant__ int16_t c_slot_dir2[4][M2L_SLOTS2];
-__constant__ int16_t c_dir_slot2[4][49];
+__device__ int16_t g_dir_slot2[4][49];    // global: vtab2_kernel stages it in shared memory
 
 template <int DIM> struct GemmDim;
 template <> struct GemmDim<3> {
@@ -137,6 +137,11 @@ __global__ void scatter_cls2_kernel(DevTree t, int L, uint32_t* __restrict__ cnt
 // that are not adjacent, reference cpu/morton_tree.cpp:147-208) as slots.
 __global__ void vtab2_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsigned* flags)
 {
+	// the direction -> slot table in shared memory: the threads look up
+	// different entries, which constant memory would serialise
+	__shared__ int16_t s_dir_slot2[4 * 49];
+	for (int i = threadIdx.x; i < 4 * 49; i += blockDim.x) s_dir_slot2[i] = (&g_dir_slot2[0][0])[i];
+	__syncthreads();
 	size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	size_t m = t.lsize[L];
 	if (c >= m) return;
@@ -144,19 +149,23 @@ __global__ void vtab2_kernel(DevTree t, int L, int32_t* __restrict__ vtab, unsig
 	int me[2];
 	coords2g(t.code[off + c], me);
 	const int cls = ((me[0] & 1) << 1) | (me[1] & 1);
+	const int16_t* ds = s_dir_slot2 + cls * 49;
 	int32_t* row = vtab + c * M2L_SLOTS2;
 	int32_t p = t.parent[off + c];
 	int npc = t.close_cnt[poff + p];
 	const int32_t* pl = t.close_idx + (poff + p) * t.close_stride;
 	for (int e = 0; e <= npc; ++e) {
 		int32_t pn = e < npc ? pl[e] : p;
+		// a child of pn sits at 2 coords(pn) + its quadrant bits (code = pn's code << 2 | quadrant)
+		int q[2];
+		coords2g(t.code[poff + pn], q);
+		const int bx = 2 * q[0] - me[0], by = 2 * q[1] - me[1];
 		for (uint32_t k = t.beg[poff + pn]; k < t.end[poff + pn]; ++k) {
 			if (k == c) continue;
-			int o[2];
-			coords2g(t.code[off + k], o);
-			int dx = o[0] - me[0], dy = o[1] - me[1];
+			const int ko = (int)(t.code[off + k] & 3ull);
+			const int dx = bx + ((ko >> 1) & 1), dy = by + (ko & 1);
 			if (max(abs(dx), abs(dy)) <= 1) continue;
-			int slot = (abs(dx) <= 3 && abs(dy) <= 3) ? c_dir_slot2[cls][(dx + 3) * 7 + (dy + 3)] : -1;
+			int slot = (abs(dx) <= 3 && abs(dy) <= 3) ? ds[(dx + 3) * 7 + (dy + 3)] : -1;
 			if (slot < 0) { atomicOr(flags, DEV_ERR_DIRECTION); continue; }
 			row[slot] = (int32_t)k;
 		}
@@ -725,7 +734,7 @@ int upload_slots(Context& ctx)
 			}
 	}
 	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_slot_dir2, sd, sizeof(sd)));
-	LFMM_CUDA(ctx, cudaMemcpyToSymbol(c_dir_slot2, ds, sizeof(ds)));
+	LFMM_CUDA(ctx, cudaMemcpyToSymbol(g_dir_slot2, ds, sizeof(ds)));
 	double fact[64];
 	fact[0] = 1.0;
 	for (int k = 1; k < 64; ++k) fact[k] = fact[k - 1] * k;
