@@ -105,9 +105,10 @@ __global__ void split_diag_kernel(double* __restrict__ ops64, int MT, int R, flo
 
 // The tensor-core M2M (op 0) or L2L (op 1, followed by its diagonal) operators
 // of order N, cached in the context (built once; the plan's warm solves build
-// them before capture).
-const uint4* shift_ops_tc(Context& ctx, int N, int op)
+// them before capture).  nullptr on failure, with st = ERR_OOM or ERR_CUDA.
+const uint4* shift_ops_tc(Context& ctx, int N, int op, int& st)
 {
+	st = OK;
 	const int tag = 30 + op;
 	for (auto& e : ctx.opcache)
 		if (e.N == N && e.prec == tag) { e.stamp = ++ctx.opcache_clock; return static_cast<const uint4*>(e.ptr); }
@@ -121,6 +122,7 @@ const uint4* shift_ops_tc(Context& ctx, int N, int op)
 		cudaGetLastError();
 		if (d) cudaFree(d);
 		ctx.last_error = "shift operators: out of memory";
+		st = ERR_OOM;
 		return nullptr;
 	}
 	const Tab<double> T = tables_of<double>(ctx.tables.d);
@@ -133,7 +135,7 @@ const uint4* shift_ops_tc(Context& ctx, int N, int op)
 		split_diag_kernel<<<div_up(8 * MT, 256), 256, 0, ctx.stream>>>(
 			d, MT, R, reinterpret_cast<float*>(static_cast<uint8_t*>(tc) + tc_ops_bytes(8, N)));
 	}
-	int st = cudaGetLastError() == cudaSuccess ? tc_ops_convert(ctx, d, 8, N, tc) : ERR_CUDA;
+	st = cudaGetLastError() == cudaSuccess ? tc_ops_convert(ctx, d, 8, N, tc) : ERR_CUDA;
 	if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) st = ERR_CUDA;
 	cudaFree(d);
 	if (st != OK) {
@@ -215,8 +217,8 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 	// one per child octant), else the rotation-based SIMT kernels
 	const bool tc_shift = sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N);
 	if (tc_shift) {
-		const uint4* mops = shift_ops_tc(ctx, N, 0);
-		if (!mops) return ERR_OOM;
+		const uint4* mops = shift_ops_tc(ctx, N, 0, st);
+		if (!mops) return st;
 		for (int L = t.depth - 2; L >= 0; --L) {
 			if (t.lsize[L] == 0) continue;
 			M2LPlan mp;
@@ -264,8 +266,8 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 		p2l_kernel<real><<<div_up(C, WPB), WPB * 32, 0, s>>>(t, N, knm, inner);
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[3], s));
 	if (tc_shift && t.depth > 3) {
-		const uint4* lops = shift_ops_tc(ctx, N, 1);
-		if (!lops) return ERR_OOM;
+		const uint4* lops = shift_ops_tc(ctx, N, 1, st);
+		if (!lops) return st;
 		for (int L = 3; L < t.depth; ++L) {
 			if (t.lsize[L] == 0) continue;
 			// the level's cells grouped by octant (its M2L plan), one slot: the parent
