@@ -266,7 +266,8 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=Fa
     per level, accumulation per level, leaf features), the network, the
     prediction sums, the sampled direct sum (split kernel and reduction) and
     the RMS and error sums.  An ncu launch list of the 16.8M-particle learned
-    solve shows 267-270 launches of the library's kernels per solve."""
+    solve shows 277 launches per solve: these 276 and the statistics pass of
+    a timing context."""
     extra = (1 + (depth - 2) + (depth - 1) + 1 + 1 + 1 + 2 + 1 + 1) if learned else 0
     scan = 3
     tree = 2 + 1 + radix_passes * (1 + scan + 1) + 1 + 1 + scan + 1 + 1
@@ -274,9 +275,12 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=Fa
     lists = depth - 1
     if adaptive or precision != "fp64":
         tree += depth + depth * (1 + scan) + depth + 1 + scan + 1 + 1 + lists + 2 + 2 + 3 * scan
-        m2l = max(0, depth - 2) * (3 + 1 + 1) + 2 * 2          # plan + GEMM (+ split reduce), FP64 coarse converts
+        # plan (class count, scatter, slot table) + GEMM per level; split
+        # reductions and FP64 converts on the coarse levels 2-3
+        m2l = max(0, depth - 2) * (3 + 1) + 2 + 2 * 2
+        m2m = (depth - 1) * (2 if precision == "mixed" else 1)  # mixed: plan + tensor-core GEMM per level
         leaves = 2 if precision == "mixed" else 1               # FP32: near field, then the expansions
-        fmm = 1 + 1 + (depth - 1) + m2l + 1 + max(0, depth - 3) + leaves
+        fmm = 1 + 1 + m2m + m2l + 1 + max(0, depth - 3) + leaves
         return (tree, fmm) if parts else tree + fmm + extra
     tree += lists
     if dim == 3:
