@@ -90,6 +90,23 @@ int lfmm_version(void);
 /* the context's CUDA stream (cudaStream_t), for callers that order work on it */
 void* lfmm_stream(lfmm_ctx* ctx);
 
+/* Device-side checks (a list that overflowed its bound, a tensor-core wait
+ * that gave up, an offset outside the operator set) set flags on the device.
+ * A call that synchronises (host buffers, or device buffers with stats)
+ * reports them itself as LFMM_ERR_DEVICE.  An asynchronous call (device
+ * buffers without stats, lfmm3d_plan_execute) cannot: it latches its flags
+ * into the context's pinned host memory when its work ends on the stream and
+ * clears them on the device, so the next solve starts clean.  lfmm_check
+ * synchronises the context's stream and returns LFMM_ERR_DEVICE (message in
+ * lfmm_last_error) if any asynchronous call since the previous lfmm_check set
+ * a flag; the results of that call are then incomplete.  No counterpart in
+ * the reference, which checks nothing. */
+int lfmm_check(lfmm_ctx* ctx);
+/* Sets device error flags on the context's stream as a failing device-side
+ * check would (flags: bit mask, nonzero), so that callers can test their
+ * handling of LFMM_ERR_DEVICE without a real failure. */
+int lfmm_debug_raise_flags(lfmm_ctx* ctx, unsigned flags);
+
 /* ---- 3D ----------------------------------------------------------------
  * Host buffers.  src_xyz: n_src x 3, src_q: n_src, tgt_xyz: n_tgt x 3 (or
  * NULL with n_tgt = 0).  pot: n_out, field: n_out x 3, n_out = n_tgt ? n_tgt
@@ -99,7 +116,9 @@ int lfmm3d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const doubl
                  double* field, lfmm_stats* stats);
 /* Same with device buffers; enqueued on the context's stream, returns after
  * the solve has been issued and its host-side sizing syncs are done (the
- * results are complete once the stream is synchronised). */
+ * results are complete once the stream is synchronised).  With stats the call
+ * synchronises and reports device-side check failures; without, they are
+ * reported by lfmm_check. */
 int lfmm3d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                         const double* tgt_xyz, int N, int tree_depth, double eps, int precision, double* pot,
                         double* field, lfmm_stats* stats);
@@ -202,8 +221,10 @@ int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
  * callers that must not allocate inside their step (an allocator that has
  * reserved the device's memory, or a loop where cudaMalloc / cudaFree would
  * synchronise the device).  The first call on each device looks up the
- * array's address (and may load the module): make it before any stream
- * capture.  The array is shared by every context on the device, so calls
+ * array's address and loads the kernels a call can launch (either may load
+ * the module): make it before any stream capture.  The address is cached per
+ * device for the life of the process; a cudaDeviceReset invalidates it.  The
+ * caller's current device is unchanged on return.  The array is shared by every context on the device, so calls
  * that overlap in time on one device race; serialise them.  Nothing in the
  * scratch needs to start at zero.  All pointers are device pointers. */
 #define LFMM_DIRECT_NOALLOC_MAX_TARGETS 65536

@@ -18,7 +18,8 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_DEVICE
 
 # Every symbol include/lfmm.h declares (checked by the CPU tests).
 EXPORTS = [
-    "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream",
+    "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream", "lfmm_check",
+    "lfmm_debug_raise_flags",
     "lfmm3d_solve", "lfmm3d_solve_device", "lfmm3d_solve_ex", "lfmm3d_solve_ex_device",
     "lfmm3d_solve_vector", "lfmm3d_solve_vector_device",
     "lfmm2d_solve", "lfmm2d_solve_device",
@@ -92,6 +93,8 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_last_error.restype = ctypes.c_char_p
         L.lfmm_stream.argtypes = [P]
         L.lfmm_stream.restype = P
+        L.lfmm_check.argtypes = [P]
+        L.lfmm_debug_raise_flags.argtypes = [P, ctypes.c_uint]
         solve = [P, SZ, P, P, SZ, P, I, I, D, I, P, P, ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device"):
             getattr(L, f).argtypes = solve

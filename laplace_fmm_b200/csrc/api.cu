@@ -70,6 +70,25 @@ int cuda_fail(Context& ctx, cudaError_t e, const char* where)
 
 Context& ctx_of(lfmm_ctx* c) { return c->c; }
 
+__global__ void latch_flags_kernel(unsigned* dev, volatile unsigned* host)
+{
+	const unsigned f = *dev;
+	if (f) {
+		*host |= f;
+		*dev = 0u;
+	}
+}
+
+// Stream-ordered: at the end of an asynchronous solve, move its device error
+// flags into the context's pinned host word (cleared on the device, so the
+// next solve starts clean); lfmm_check reports them.
+int latch_flags(Context& c)
+{
+	latch_flags_kernel<<<1, 1, 0, c.stream>>>(c.dev_flags, c.host_flags_dev);
+	LFMM_CUDA(c, cudaGetLastError());
+	return OK;
+}
+
 } // namespace lfmm
 
 using namespace lfmm;
@@ -350,10 +369,17 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	if (c.device < 0 || c.device >= ndev || cudaSetDevice(c.device) != cudaSuccess) { delete ctx; return LFMM_ERR_ARG; }
 	if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    cudaMalloc(&c.dev_flags, sizeof(unsigned)) != cudaSuccess ||
-	    cudaMemset(c.dev_flags, 0, sizeof(unsigned)) != cudaSuccess) {
+	    cudaMemset(c.dev_flags, 0, sizeof(unsigned)) != cudaSuccess ||
+	    cudaHostAlloc(&c.host_flags, sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess ||
+	    cudaHostGetDevicePointer(&c.host_flags_dev, c.host_flags, 0) != cudaSuccess) {
+		cudaGetLastError();
+		if (c.host_flags) cudaFreeHost(c.host_flags);
+		if (c.dev_flags) cudaFree(c.dev_flags);
+		if (c.stream) cudaStreamDestroy(c.stream);
 		delete ctx;
 		return LFMM_ERR_CUDA;
 	}
+	*c.host_flags = 0u;
 	for (auto& e : c.ev) cudaEventCreate(&e);
 	for (auto& e : c.kev) cudaEventCreate(&e);
 	int prio_lo = 0, prio_hi = 0;
@@ -389,6 +415,7 @@ void lfmm_destroy(lfmm_ctx* ctx)
 	if (c.fork_ev) cudaEventDestroy(c.fork_ev);
 	if (c.join_ev) cudaEventDestroy(c.join_ev);
 	if (c.dev_flags) cudaFree(c.dev_flags);
+	if (c.host_flags) cudaFreeHost(c.host_flags);
 	if (c.side) cudaStreamDestroy(c.side);
 	if (c.stream) cudaStreamDestroy(c.stream);
 	delete ctx;
@@ -397,6 +424,33 @@ void lfmm_destroy(lfmm_ctx* ctx)
 const char* lfmm_last_error(const lfmm_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "null context"; }
 
 void* lfmm_stream(lfmm_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+__global__ void raise_flags_kernel(unsigned* dev, unsigned f) { atomicOr(dev, f); }
+
+int lfmm_debug_raise_flags(lfmm_ctx* ctx, unsigned flags)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	raise_flags_kernel<<<1, 1, 0, c.stream>>>(c.dev_flags, flags);
+	LFMM_CUDA(c, cudaGetLastError());
+	return LFMM_OK;
+}
+
+int lfmm_check(lfmm_ctx* ctx)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	LFMM_CUDA(c, cudaStreamSynchronize(c.stream));
+	const unsigned f = *(volatile unsigned*)c.host_flags;
+	if (f) {
+		*(volatile unsigned*)c.host_flags = 0u;
+		c.last_error = "device-side check failed in an earlier solve (flags " + std::to_string(f) + ")";
+		return LFMM_ERR_DEVICE;
+	}
+	return LFMM_OK;
+}
 
 int lfmm3d_solve(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt, int N,
                  int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats)
@@ -411,7 +465,7 @@ int lfmm3d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const doubl
 	if (!ctx) return LFMM_ERR_ARG;
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats, true);
-	if (st == OK && stats) st = check_flags(ctx->c);
+	if (st == OK) st = stats ? check_flags(ctx->c) : latch_flags(ctx->c);
 	ctx->c.arena.settle();
 	return st;
 }
@@ -431,7 +485,7 @@ int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t ns, const double* src, const do
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
 	                      true, o->max_leaf);
-	if (st == OK && stats) st = check_flags(ctx->c);
+	if (st == OK) st = stats ? check_flags(ctx->c) : latch_flags(ctx->c);
 	ctx->c.arena.settle();
 	return st;
 }
@@ -515,7 +569,7 @@ int lfmm2d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const doubl
 	if (!ctx) return LFMM_ERR_ARG;
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	int st = solve_device(ctx, 2, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats, true);
-	if (st == OK && stats) st = check_flags(ctx->c);
+	if (st == OK) st = stats ? check_flags(ctx->c) : latch_flags(ctx->c);
 	ctx->c.arena.settle();
 	return st;
 }

@@ -90,6 +90,11 @@ struct Context {
 	unsigned long long opcache_clock = 0;
 	int m2l_engine = 3;               // 0: dense SIMT GEMMs, 1: per-pair rotations (plain path), 3: tcgen05 on FP32 levels
 	unsigned* dev_flags = nullptr;      // device error flags
+	// Device errors of asynchronous solves (device buffers, no stats): latched
+	// at the end of each such solve into this mapped pinned word (host view,
+	// device view) and read by lfmm_check.
+	unsigned* host_flags = nullptr;
+	unsigned* host_flags_dev = nullptr;
 	std::string last_error;
 	int verbose = 0;
 	cudaEvent_t ev[16] = {};

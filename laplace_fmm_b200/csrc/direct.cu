@@ -160,6 +160,14 @@ int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const dou
 	return OK;
 }
 
+int direct_preload3(Context& ctx)
+{
+	cudaFuncAttributes a;
+	LFMM_CUDA(ctx, cudaFuncGetAttributes(&a, direct_kernel<3>));
+	LFMM_CUDA(ctx, cudaFuncGetAttributes(&a, direct_reduce_kernel<3>));
+	return OK;
+}
+
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                   double* pot, double* fld, bool fast)
 {

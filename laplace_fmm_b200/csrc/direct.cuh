@@ -13,6 +13,10 @@ int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks);
 // square root and divide per pair.
 int direct_launch(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
                   const double* tgt, double* pot, double* fld, double* part, int S, bool fast = false);
+// Load the 3D FP64 kernels that direct_launch may use (fast = false) into the
+// current device's context now rather than at their first launch (under lazy
+// module loading a first launch may allocate device memory).
+int direct_preload3(Context& ctx);
 // Enqueue on ctx.stream, scratch from the arena; all pointers are device pointers.
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                   double* pot, double* fld, bool fast = false);

@@ -6,7 +6,10 @@
 // device: calls that overlap in time on one device race on it.  Nothing in it
 // needs to start at zero (each partial is written before it is read).  Its
 // address is looked up once per device (cudaGetSymbolAddress, which may load
-// the module) on the first call with that device current.
+// the module) on the first call with that device current; the same first call
+// also loads both kernels a call can launch (the chunk reduction runs only
+// when the sources are split), so that no later call loads code, which can
+// allocate.  A cudaDeviceReset invalidates the cached address.
 #include "../../include/lfmm.h"
 #include "direct.cuh"
 #include <mutex>
@@ -36,6 +39,7 @@ double* scratch_of(lfmm::Context& c)
 			lfmm::cuda_fail(c, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(g_direct_scratch)");
 			return nullptr;
 		}
+		if (lfmm::direct_preload3(c) != lfmm::OK) return nullptr;
 		g_scratch_ptr[c.device] = static_cast<double*>(p);
 	}
 	return g_scratch_ptr[c.device];
@@ -60,11 +64,17 @@ extern "C" int lfmm3d_direct_device_noalloc(lfmm_ctx* h, size_t ns, const double
 		c.last_error = "null buffer";
 		return LFMM_ERR_ARG;
 	}
-	cudaError_t e = cudaSetDevice(c.device);
-	if (e != cudaSuccess) return lfmm::cuda_fail(c, e, "cudaSetDevice");
 	if (nt == 0) return LFMM_OK;
-	double* scratch = scratch_of(c);
-	if (!scratch) return LFMM_ERR_CUDA;
-	const int S = lfmm::direct_chunks(ns, nt, c.num_sms, SCRATCH_DOUBLES / (4 * nt));
-	return lfmm::direct_launch(c, 3, ns, src, q, nt, tgt, pot, field, scratch, S);
+	// the caller's current device is put back on every return
+	int prev = -1;
+	cudaError_t e = cudaGetDevice(&prev);
+	if (e != cudaSuccess) return lfmm::cuda_fail(c, e, "cudaGetDevice");
+	if (prev != c.device && (e = cudaSetDevice(c.device)) != cudaSuccess) return lfmm::cuda_fail(c, e, "cudaSetDevice");
+	int st = LFMM_ERR_CUDA;
+	if (double* scratch = scratch_of(c)) {
+		const int S = lfmm::direct_chunks(ns, nt, c.num_sms, SCRATCH_DOUBLES / (4 * nt));
+		st = lfmm::direct_launch(c, 3, ns, src, q, nt, tgt, pot, field, scratch, S);
+	}
+	if (prev != c.device) cudaSetDevice(prev);
+	return st;
 }

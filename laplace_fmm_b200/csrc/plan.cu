@@ -13,7 +13,7 @@
 #include <new>
 
 struct lfmm_ctx;
-namespace lfmm { Context& ctx_of(lfmm_ctx* c); }
+namespace lfmm { Context& ctx_of(lfmm_ctx* c); int latch_flags(Context& c); }
 
 struct lfmm_plan {
 	lfmm_ctx* ctx = nullptr;
@@ -157,7 +157,7 @@ int lfmm3d_plan_execute(lfmm_plan* p, const double* src_q, double* pot, double* 
 	LFMM_CUDA(c, cudaGraphLaunch(p->exec, c.stream));
 	LFMM_CUDA(c, cudaMemcpyAsync(pot, p->pot, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, c.stream));
 	LFMM_CUDA(c, cudaMemcpyAsync(field, p->fld, sizeof(double) * 3 * p->n, cudaMemcpyDeviceToDevice, c.stream));
-	return LFMM_OK;
+	return latch_flags(c);
 }
 
 void lfmm3d_plan_destroy(lfmm_plan* p)
