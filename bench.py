@@ -48,14 +48,16 @@ CONFIGS = {
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
                         "p=20 (N=21), uniform quadtree depth 11"),
     # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
-    # mixed form at the order the network picks for rel-L2 <= 1e-6 (sampled
-    # check of 256 outputs, fixed-order fallback); the plain FP64 form beside it
-    # at p = 13 (N = 14), the lowest fixed order that reaches 1e-6 here
-    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=14, depth=10, max_leaf=64, precision="mixed",
+    # mixed form at the order the network picks for rel-L2 <= 1e-6 on potential
+    # and field (sampled check of 256 outputs judged on its upper confidence
+    # bound, fixed-order fallback); the plain FP64 form beside it at p = 15
+    # (N = 16), the lowest fixed order at which both outputs reach 1e-6 here
+    # (N = 15: field 1.007e-6)
+    "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=16, depth=10, max_leaf=64, precision="mixed",
                learned=True, tol=1e-6, check_targets=256,
                workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels, "
-                        "<=64 per leaf), mixed precision at the learned order for rel-L2 <= 1e-6 "
-                        "(plain FP64 form at p=13, N=14)"),
+                        "<=64 per leaf), mixed precision at the learned order for rel-L2 <= 1e-6 on potential and "
+                        "field (plain FP64 form at p=15, N=16)"),
     # 1024 independent problems, N log-uniform in [2048, 262144] (about 60M particles),
     # each uniform in its own unit cube or one Gaussian cluster (sigma 0.05), solved
     # as one batch (mixed, N = 14); the plain FP64 form (p = 10, N = 11) one problem
@@ -476,10 +478,11 @@ def m2l_flops(N):
 
 
 # DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode), from an ncu
-# capture of a 2,097,152-particle case of the default workload at N = 14
-# (727 MB over 3.03 ms in 4 launches); the kernel's traffic grows with its
-# work, so a full launch's traffic is this rate times its duration.
-M2L_TC_DRAM_BYTES_PER_MS = 727.2e6 / 3.031
+# capture of a 2,097,152-particle case of the default workload at N = 16
+# (788.5 MB read + written over 4.365 ms in 4 launches); the kernel's traffic
+# grows with its work, so a full launch's traffic is this rate times its
+# duration.
+M2L_TC_DRAM_BYTES_PER_MS = 788.5e6 / 4.365
 
 
 def padded(N):
@@ -515,15 +518,23 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
         ms = stats["ms_m2l_kernel"]
         N = stats.get("order_N") or cfg["N"]
         nc = padded(N)
+        na = nc if nc <= 160 else 160                  # columns with the hi/lo corrections (degrees < 12)
         kpad = (nc + 31) // 32 * 32
+        kcorr = (na + 31) // 32 * 32
         flops = float(m2l_flops(N)) * stats["n_far_pairs"]
-        tensor = 3.0 * 2.0 * nc * kpad * stats["n_far_pairs"]     # hi x hi + two corrections, per V pair
+        # per V pair: B_hi T_hi over every column and K block, and the two
+        # corrections over the drained columns and their source degrees
+        tensor = (2.0 * nc * kpad + 2 * 2.0 * na * kcorr) * stats["n_far_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
+        bf16 = peaks["bf16_tflops"]
         return {"kernel": "m2l_tc_kernel (tcgen05 TF32 hi/lo, direction-grouped)", "bound": "tensor",
-                "achieved": achieved, "peak": tf32_tflops, "unit": "TFLOP/s", "frac": achieved / tf32_tflops,
-                "peak_source": "measured cuBLAS FP32 GEMM with TF32 (8192^3)", "algorithmic_flops": flops,
+                "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({peaks['source']}); the kernel runs TF32 MMAs, "
+                               "whose dense rate is half of bf16's: frac_tf32 uses the TF32 cuBLAS GEMM peak "
+                               "measured in this run",
+                "frac_tf32": achieved / tf32_tflops, "tf32_peak": tf32_tflops, "algorithmic_flops": flops,
                 "executed_tensor_flops": tensor, "executed_tensor_tflops": tensor / (ms * 1e-3) / 1e12,
-                "executed_frac": tensor / (ms * 1e-3) / 1e12 / tf32_tflops,
+                "executed_frac_tf32": tensor / (ms * 1e-3) / 1e12 / tf32_tflops,
                 "kernel_ms": ms, "kernel_launches": stats["n_m2l_kernel"], "phase_ms": phases["m2l"],
                 "traffic": M2L_TC_DRAM_BYTES_PER_MS * ms / stats["n_m2l_kernel"],
                 "traffic_unit": "bytes per launch (ncu capture of a 2M-particle case, scaled by kernel time)"}

@@ -129,7 +129,7 @@ int lfmm3d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, cons
  * hold more than max_leaf particles, at most tree_depth levels) with U, V, W, X
  * lists.  precision FP64 with max_leaf = 0 is the reference-parity path
  * (same as lfmm3d_solve); every other combination runs the scaled-expansion
- * solver (N <= 15). */
+ * solver (N <= 18). */
 typedef struct {
 	int N;            /* degrees (order p + 1), or LFMM_AUTO (from eps) */
 	int tree_depth;   /* uniform depth / maximum adaptive depth, or LFMM_AUTO */
@@ -163,7 +163,7 @@ int lfmm3d_solve_batch_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, 
 /* ---- solve plans: one geometry, many charge vectors (no counterpart in the
  * reference, which rebuilds the tree on every solve) ------------------------
  * lfmm3d_plan_create builds the tree of the positions once (device buffers;
- * opts as for lfmm3d_solve_ex, N given explicitly, N <= 15), warms every
+ * opts as for lfmm3d_solve_ex, N given explicitly, N <= 18), warms every
  * cache and captures the FMM passes in a CUDA graph on the context's stream.
  * lfmm3d_plan_execute (device buffers, input order, n_src each) enqueues: copy
  * the charges in, launch the graph, copy potential and field out; the results
@@ -235,20 +235,22 @@ int lfmm3d_direct_device_noalloc(lfmm_ctx* ctx, size_t n_src, const double* src_
 /* ---- learned order selection (no counterpart in the reference) -----------
  * The reference picks one order from eps by a fixed formula
  * (cpu/multipole3d.cpp:1328-1331).  Here a small MLP (16 per-leaf features ->
- * 64 -> 64 -> 6, FP32, ReLU) predicts log10 of each leaf box's error at the
- * orders p = 4, 6, ..., 14; a solve takes the lowest p whose predicted
- * particle-weighted error meets the tolerance.  All pointers to MLP data are
- * device pointers (FP32); parameters are W1[64][16] b1[64] W2[64][64] b2[64]
- * W3[6][64] b3[6]. */
+ * 64 -> 64 -> 14, FP32, ReLU) predicts, for each leaf box, log10 of the RMS
+ * absolute error of its outputs at the orders p = 4, 6, 8, 10, 12, 14, 16:
+ * outputs 0-6 the potential's, outputs 7-13 the field's (magnitude of the
+ * error vector); a solve takes the lowest p whose predicted
+ * particle-weighted errors of both meet the tolerance.  All pointers to MLP
+ * data are device pointers (FP32); parameters are W1[64][16] b1[64]
+ * W2[64][64] b2[64] W3[14][64] b3[14]. */
 #define LFMM_MLP_IN 16
 #define LFMM_MLP_HIDDEN 64
-#define LFMM_MLP_OUT 6
-#define LFMM_MLP_PARAMS (64 * 16 + 64 + 64 * 64 + 64 + 6 * 64 + 6)
+#define LFMM_MLP_OUT 14
+#define LFMM_MLP_PARAMS (64 * 16 + 64 + 64 * 64 + 64 + 14 * 64 + 14)
 
-/* Y[n][6] = MLP(X[n][16]) */
+/* Y[n][14] = MLP(X[n][16]) */
 int lfmm_mlp_forward(lfmm_ctx* ctx, const float* params, int n, const float* X, float* Y);
-/* Masked mean-squared-error loss sum M (Y - T)^2 / sum M over T, M [n][6];
- * grad[LFMM_MLP_PARAMS]; work >= n * (6 + 128) + 2 floats; *loss on the host.
+/* Masked mean-squared-error loss sum M (Y - T)^2 / sum M over T, M [n][14];
+ * grad[LFMM_MLP_PARAMS]; work >= n * (14 + 128) + 2 floats; *loss on the host.
  * Synchronises. */
 int lfmm_mlp_grad(lfmm_ctx* ctx, const float* params, int n, const float* X, const float* T, const float* M,
                   float* grad, float* work, float* loss);
@@ -278,7 +280,7 @@ int lfmm3d_features(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const do
  * potential (the reference computes none for vector charges).  Sources are
  * the particles with q != 0 (the reference's zero-charge rule); one tree,
  * three scalar passes combined by a cross product.  opts as lfmm3d_solve_ex
- * (max_leaf 0: the uniform tree; N <= 15); stats describe the tree and the
+ * (max_leaf 0: the uniform tree; N <= 18); stats describe the tree and the
  * last of the three passes.  Host and device-buffer variants; the host one
  * synchronises. */
 int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q3, size_t n_tgt,
@@ -290,26 +292,39 @@ int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t n_src, const double* src_xy
 typedef struct {
 	int order_N;                /* degrees of the final solve */
 	int predicted_N;            /* degrees the network chose */
-	int fallback;               /* 1: the sampled check missed tol and the solve was rerun at N = 15 */
+	int fallback;               /* 0: the prediction passed the judge; 1: it did not, and the solve was
+	                               rerun at the order picked again from predictions shifted by the
+	                               measured shortfall, which passed; 2: that missed too (or no such
+	                               order) and the solve was rerun at the fixed order N = 18 */
 	double predicted_error;     /* the network's rel-L2 estimate of the potential at predicted_N */
 	double checked_error;       /* sampled rel-L2 of the potential, self term removed (-1: no check) */
 	double checked_error_field; /* the same for the field */
-	int fp64_resolved;          /* problems rerun in the FP64 form at N = 15 because the mixed form
+	int fp64_resolved;          /* problems rerun in the FP64 form at N = 18 because the mixed form
 	                               missed tol even there (0 or 1 for a single solve) */
+	double predicted_error_field; /* the network's rel-L2 estimate of the field at predicted_N */
+	double judged_error;        /* what the judge compared with tol: the larger of the two upper
+	                               confidence bounds (mean + 2 standard errors) of the sampled
+	                               rel-L2 of potential and field (batches: the largest over problems) */
 } lfmm_learned_info;
 
-/* 3D solve at the order the network picks for tolerance tol (rel-L2 of the
- * potential without the self term).  The FP64 direct sum is first evaluated
- * at check_targets (>= 1) outputs spread through the output range; the
- * network predicts each leaf's absolute error at p = 4, 6, ..., 14, the
- * leaves' errors over the samples' RMS potential give the predicted rel-L2,
- * and the lowest p in 4..14 within tol is solved (else N = 15).  The same
- * samples then judge the result: a solve above tol is rerun at the fixed
- * order N = 15 (the fallback), and a mixed-precision solve still above tol
- * there is rerun in the FP64 form (fp64_resolved).  params: device pointer to the network
- * (LFMM_MLP_PARAMS floats, inputs unnormalised).  opts gives the tree
- * (tree_depth, max_leaf) and precision; opts->N and opts->eps are ignored.
- * Synchronises.  Host and device-buffer variants. */
+/* 3D solve at the order the network picks for tolerance tol, which bounds
+ * the rel-L2 of both outputs: the potential (self term removed) and the
+ * field.  The FP64 direct sum is first evaluated at check_targets (>= 1)
+ * outputs spread through the output range; the network predicts each leaf's
+ * absolute potential and field errors at p = 4, 6, ..., 14, 16, the leaves'
+ * errors over the samples' RMS potential and RMS field give the predicted
+ * rel-L2 of each, and the lowest p in 4..17 at which both are within
+ * 0.6 tol is solved (else N = 18).  The same samples then judge the result
+ * on an upper confidence bound of each sampled rel-L2 (the ratio estimate
+ * plus two standard errors, so a sample too small or too uneven to certify
+ * tol does not pass).  A solve whose bound exceeds tol is rerun once at the
+ * order picked again from the predictions shifted by the shortfall measured
+ * (bound over prediction), then, if that misses too, at the fixed order
+ * N = 18 (the fallback); a mixed-precision solve still above tol there is
+ * rerun in the FP64 form (fp64_resolved).  params: device pointer to the
+ * network (LFMM_MLP_PARAMS floats, inputs unnormalised).  opts gives the
+ * tree (tree_depth, max_leaf) and precision; opts->N and opts->eps are
+ * ignored.  Synchronises.  Host and device-buffer variants. */
 int lfmm3d_solve_learned(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                          const double* tgt_xyz, const lfmm_solve_opts* opts, const float* params, double tol,
                          int check_targets, double* pot, double* field, lfmm_learned_info* info, lfmm_stats* stats);
@@ -319,12 +334,13 @@ int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_x
                                 lfmm_learned_info* info, lfmm_stats* stats);
 /* The batch at the order the network picks for tolerance tol (as
  * lfmm3d_solve_learned; device buffers): up to check_targets sampled outputs
- * per problem normalise each problem's prediction and judge its result; the
- * batch runs at the highest order any problem needs, and reruns at N = 15
- * when a problem misses tol; a problem still above tol there (mixed form) is
- * rerun alone in the FP64 form into its slice of the outputs.  info: the
- * order used, the largest predicted and checked errors over the problems,
- * the number of FP64 reruns. */
+ * per problem normalise each problem's prediction and judge its result (the
+ * same upper confidence bounds, per problem); the batch runs at the highest
+ * order any problem needs, and reruns at N = 18 when a problem misses tol;
+ * a problem still above tol there (mixed form) is rerun alone in the FP64
+ * form into its slice of the outputs.  info: the order used, the largest
+ * predicted, checked and judged errors over the problems, the number of FP64
+ * reruns. */
 int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
                                       const double* src_q, const lfmm_solve_opts* opts, const float* params,
                                       double tol, int check_targets, double* pot, double* field,

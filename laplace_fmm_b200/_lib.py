@@ -62,7 +62,8 @@ class LfmmSolveOpts(ctypes.Structure):
 class LfmmLearnedInfo(ctypes.Structure):
     _fields_ = [("order_N", ctypes.c_int), ("predicted_N", ctypes.c_int), ("fallback", ctypes.c_int),
                 ("predicted_error", ctypes.c_double), ("checked_error", ctypes.c_double),
-                ("checked_error_field", ctypes.c_double), ("fp64_resolved", ctypes.c_int)]
+                ("checked_error_field", ctypes.c_double), ("fp64_resolved", ctypes.c_int),
+                ("predicted_error_field", ctypes.c_double), ("judged_error", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

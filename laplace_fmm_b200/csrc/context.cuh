@@ -102,17 +102,18 @@ struct Context {
 	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 	cudaEvent_t kev[32] = {};          // pairs around the tensor-core M2L launches (timing)
 	int kev_used = 0;
-	// M2L autotuner: slot split chosen per (operator rows, level-size bucket);
-	// 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0): the fixed rule.
-	int m2l_split[257][33] = {};
+	// M2L autotuner: slot split chosen per (operator rows / 16, level-size
+	// bucket); 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0): the fixed rule.
+	int m2l_split[18][33] = {};
 	int tune_m2l = 1;
 	int timing = 0;
 };
 
-// With 24 entries cached, evict the least recently used one no graph reads.
+// With 48 entries cached (four per order: FP64 and tensor-core M2L, M2M and
+// L2L operators), evict the least recently used one no graph reads.
 inline void opcache_make_room(Context& ctx)
 {
-	if (ctx.opcache.size() < 24) return;
+	if (ctx.opcache.size() < 48) return;
 	auto it = ctx.opcache.end();
 	for (auto j = ctx.opcache.begin(); j != ctx.opcache.end(); ++j)
 		if (!j->pinned && (it == ctx.opcache.end() || j->stamp < it->stamp)) it = j;

@@ -24,7 +24,7 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 // Scaled-expansion solver on the adaptive-form tree (max_leaf = 0: uniform
 // depth `depth`; > 0: adaptive, at most `depth` levels): precision 0 = FP64,
 // 1 = mixed (FP32 expansions / near field, FP64 M2L on levels 2-3, FP64 tile
-// sums and self term).  N <= 15.
+// sums and self term).  N <= 18.
 // Vector charges (in.srcq: 3 doubles per source): field = sum q x d / r^3.
 int fmm3d_solve_vector(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
                        double* field, SolveStats* stats);

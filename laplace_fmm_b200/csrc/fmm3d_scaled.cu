@@ -351,7 +351,7 @@ int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, 
                        double* pot, double* field, SolveStats* stats, DevTree* tree_out)
 {
 	if (N < 1 || N > MAXN3) { ctx.last_error = "order out of range (1 <= N <= 18)"; return ERR_ARG; }
-	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 15"; return ERR_UNSUPPORTED; }
+	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 18"; return ERR_UNSUPPORTED; }
 	if (max_leaf < 0) { ctx.last_error = "max_leaf must be >= 0"; return ERR_ARG; }
 	int st = upload_scaled_constants(ctx);
 	if (st) return st;
@@ -371,7 +371,7 @@ int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, d
                          SolveStats* stats)
 {
 	if (N < 1 || N > MAXN3 || !m2l_gemm_supported(N)) {
-		ctx.last_error = "scaled / mixed / adaptive forms support N <= 15";
+		ctx.last_error = "scaled / mixed / adaptive forms support N <= 18";
 		return ERR_UNSUPPORTED;
 	}
 	int st = upload_scaled_constants(ctx);

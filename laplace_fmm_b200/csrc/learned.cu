@@ -2,12 +2,14 @@
 // order from eps by a fixed formula, cpu/multipole3d.cpp:1328-1331).
 //
 //   tree (adaptive form) -> per-leaf features (16) -> MLP (mlp.cu) -> log10
-//   of each leaf's error at p = 4, 6, ..., 14 -> predicted rel-L2 of the
-//   potential per order = sqrt(sum_leaf w 10^(2 y) / sum_leaf w), w = the
-//   leaf's output particles -> the lowest order p (interpolated between the
-//   six) whose prediction is within the tolerance -> one solve at N = p + 1 on
-//   the same tree -> optional sampled check against the FP64 direct sum; a
-//   solve that misses the tolerance is rerun at the fixed fallback order.
+//   of each leaf's potential and field errors at p = 4, 6, ..., 14, 16 ->
+//   predicted rel-L2 of each output per order = sqrt(sum_leaf w 10^(2 y) /
+//   sum_leaf w) / (the sampled RMS of that output), w = the leaf's output
+//   particles -> the lowest order p (interpolated between the seven) at which
+//   both predictions are within the tolerance -> one solve at N = p + 1 on
+//   the same tree -> the sampled check against the FP64 direct sum judges it
+//   on an upper confidence bound of both errors; a solve that misses the
+//   tolerance is rerun at the fixed fallback order.
 #include "learned.cuh"
 #include "direct.cuh"
 #include <algorithm>
@@ -19,8 +21,16 @@ namespace lfmm {
 namespace {
 
 constexpr int NF = LFMM_MLP_IN, NO = LFMM_MLP_OUT;
-constexpr int FB_N = 15;            // fallback order (degrees): the highest the scaled solver runs
-constexpr double LEARNED_MARGIN = 1.0;   // the calibrated prediction must be within tol
+constexpr int NP = NO / 2;          // orders of the network's outputs (potential, then field)
+constexpr int ORDER_P[NP] = {4, 6, 8, 10, 12, 14, 16};
+constexpr int FB_N = 18;            // fallback order (degrees): the highest the scaled solver runs
+constexpr int NCHK = 10;            // sums per sampled check (see check_kernel)
+constexpr double JUDGE_Z = 2.0;     // standard errors added to the sampled rel-L2 by the judge
+// The calibrated prediction must be within LEARNED_MARGIN tol: the judge
+// passes a solve only when its sampled rel-L2 plus two standard errors is
+// within tol, so a pick aimed at tol itself is rejected (and solved again)
+// whenever the true error lands in the upper part of that band.
+constexpr double LEARNED_MARGIN = 0.6;
 
 __device__ __forceinline__ float lg(double x) { return (float)log10(x); }
 
@@ -172,37 +182,49 @@ __global__ void check_kernel(const double* __restrict__ pot, const double* __res
                              const double* __restrict__ q, const double* __restrict__ ep,
                              const double* __restrict__ ef, double* __restrict__ acc)
 {
-	double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+	// per sample: a = squared error, b = squared reference, for the potential
+	// (self term removed) and the field; sums of a, b, a^2, b^2, a b of each
+	double v[NCHK] = {};
 	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
 		const size_t j = i * stride;
 		const double self = q ? q[j] / FORCE_EPS : 0.0;
 		const double d = pot[j] - ep[i], r = ep[i] - self;
-		a0 += d * d; a1 += r * r;
+		double e2 = 0.0, f2 = 0.0;
 		for (int k = 0; k < 3; ++k) {
 			const double e = fld[3 * j + k] - ef[3 * i + k];
-			a2 += e * e; a3 += ef[3 * i + k] * ef[3 * i + k];
+			e2 += e * e; f2 += ef[3 * i + k] * ef[3 * i + k];
 		}
+		const double a0 = d * d, b0 = r * r;
+		v[0] += a0; v[1] += b0; v[2] += a0 * a0; v[3] += b0 * b0; v[4] += a0 * b0;
+		v[5] += e2; v[6] += f2; v[7] += e2 * e2; v[8] += f2 * f2; v[9] += e2 * f2;
 	}
-	for (int o = 16; o; o >>= 1) {
-		a0 += __shfl_xor_sync(0xffffffffu, a0, o); a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-		a2 += __shfl_xor_sync(0xffffffffu, a2, o); a3 += __shfl_xor_sync(0xffffffffu, a3, o);
-	}
-	if ((threadIdx.x & 31) == 0) {
-		atomicAdd(&acc[0], a0); atomicAdd(&acc[1], a1); atomicAdd(&acc[2], a2); atomicAdd(&acc[3], a3);
+#pragma unroll
+	for (int k = 0; k < NCHK; ++k) {
+		double x = v[k];
+		for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+		if ((threadIdx.x & 31) == 0) atomicAdd(&acc[k], x);
 	}
 }
 
-// acc[0] += sum over the samples of (direct potential - self term)^2
-__global__ void rms_kernel(const double* __restrict__ ep, size_t stride, size_t m, const double* __restrict__ q,
-                           double* __restrict__ acc)
+// acc[0] += sum over the samples of (direct potential - self term)^2,
+// acc[1] += sum of |direct field|^2
+__global__ void rms_kernel(const double* __restrict__ ep, const double* __restrict__ ef, size_t stride, size_t m,
+                           const double* __restrict__ q, double* __restrict__ acc)
 {
-	double a = 0;
+	double a = 0, b = 0;
 	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
 		const double r = ep[i] - (q ? q[i * stride] / FORCE_EPS : 0.0);
 		a += r * r;
+		b += ef[3 * i] * ef[3 * i] + ef[3 * i + 1] * ef[3 * i + 1] + ef[3 * i + 2] * ef[3 * i + 2];
 	}
-	for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-	if ((threadIdx.x & 31) == 0) atomicAdd(acc, a);
+	for (int o = 16; o; o >>= 1) {
+		a += __shfl_xor_sync(0xffffffffu, a, o);
+		b += __shfl_xor_sync(0xffffffffu, b, o);
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(&acc[0], a);
+		atomicAdd(&acc[1], b);
+	}
 }
 
 // Forest: acc[prob * (NO + 1) + k] += w 10^(2 y[k]) per leaf, by the leaf's problem
@@ -226,8 +248,8 @@ __global__ void gather_points_kernel(const double* __restrict__ pts, const uint3
 	for (int d = 0; d < 3; ++d) out[3 * i + d] = pts[3 * (size_t)idx[i] + d];
 }
 
-// Forest samples: acc[4 prob + 0..3] += (pot - direct)^2, (direct - self)^2,
-// |dfield|^2, |field|^2; pot == nullptr: only the reference sums (the RMS).
+// Forest samples: acc[NCHK prob + k] += the sums of check_kernel, by the
+// sample's problem; pot == nullptr: only the reference sums (the RMS values).
 __global__ void check_forest_kernel(const double* __restrict__ pot, const double* __restrict__ fld,
                                     const uint32_t* __restrict__ idx, const int32_t* __restrict__ prob, size_t m,
                                     const double* __restrict__ q, const double* __restrict__ ep,
@@ -236,18 +258,35 @@ __global__ void check_forest_kernel(const double* __restrict__ pot, const double
 	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= m) return;
 	const size_t j = idx[i];
-	double* a = acc + 4 * (size_t)prob[i];
+	double* a = acc + NCHK * (size_t)prob[i];
 	const double r = ep[i] - q[j] / FORCE_EPS;
-	atomicAdd(&a[1], r * r);
+	const double b0 = r * r;
 	double f2 = 0.0;
 	for (int k = 0; k < 3; ++k) f2 += ef[3 * i + k] * ef[3 * i + k];
-	atomicAdd(&a[3], f2);
+	atomicAdd(&a[1], b0); atomicAdd(&a[3], b0 * b0);
+	atomicAdd(&a[6], f2); atomicAdd(&a[8], f2 * f2);
 	if (!pot) return;
-	const double d = pot[j] - ep[i];
-	atomicAdd(&a[0], d * d);
+	const double d = pot[j] - ep[i], a0 = d * d;
 	double e2 = 0.0;
 	for (int k = 0; k < 3; ++k) { const double e = fld[3 * j + k] - ef[3 * i + k]; e2 += e * e; }
-	atomicAdd(&a[2], e2);
+	atomicAdd(&a[0], a0); atomicAdd(&a[2], a0 * a0); atomicAdd(&a[4], a0 * b0);
+	atomicAdd(&a[5], e2); atomicAdd(&a[7], e2 * e2); atomicAdd(&a[9], e2 * f2);
+}
+
+// Sampled rel-L2 of one output from the sums (a = squared error, b = squared
+// reference over m samples: sum a, sum b, sum a^2, sum b^2, sum a b):
+// est = sqrt(sum a / sum b), and the judge's upper confidence bound
+// sqrt(R + z se(R)) with R = mean a / mean b and se(R) its delta-method
+// standard error, sqrt((var a - 2 R cov(a, b) + R^2 var b) / m) / mean b.
+void rel_l2_bound(const double* h, double m, double* est, double* ucb)
+{
+	const double A = h[0] / m, B = h[1] / m;
+	if (!(B > 0.0)) { *est = *ucb = 0.0; return; }
+	const double R = A / B;
+	const double va = std::max(h[2] / m - A * A, 0.0), vb = std::max(h[3] / m - B * B, 0.0), cab = h[4] / m - A * B;
+	const double var = std::max(va - 2.0 * R * cab + R * R * vb, 0.0) / (m * B * B);
+	*est = std::sqrt(R);
+	*ucb = std::sqrt(R + JUDGE_Z * std::sqrt(var));
 }
 
 template <typename T>
@@ -272,14 +311,32 @@ int features_device(Context& ctx, const DevTree& t, float* feats, float* w)
 	return OK;
 }
 
-// log10 of the predicted rel-L2 at order p (4 <= p <= 14), interpolated
-// between the network's six orders.
+// log10 of the predicted rel-L2 at order p (4 <= p <= 17), interpolated
+// linearly between the network's seven orders (p = 17: extrapolated from the
+// last two).
 double predicted_log10(const double* e, int p)
 {
-	const double x = (p - 4) / 2.0;
-	const int k = std::min(4, (int)x);
-	const double f = x - k;
+	int k = 0;
+	while (k + 2 < NP && ORDER_P[k + 1] < p) ++k;
+	const double f = (double)(p - ORDER_P[k]) / (double)(ORDER_P[k + 1] - ORDER_P[k]);
 	return e[k] * (1.0 - f) + e[k + 1] * f;
+}
+
+// The lowest order p in 4..17 at which both predicted rel-L2 (log10: ep for
+// the potential, ef for the field, at the network's orders) are within
+// target; N = p + 1, or the fallback order when none is.
+void pick_order(const double* ep, const double* ef, double target, int& N, double& pp, double& pf)
+{
+	N = FB_N;
+	pp = std::pow(10.0, predicted_log10(ep, FB_N - 1));
+	pf = std::pow(10.0, predicted_log10(ef, FB_N - 1));
+	for (int p = 4; p < FB_N; ++p) {
+		const double lp = predicted_log10(ep, p), lf = predicted_log10(ef, p);
+		if (lp <= target && lf <= target) {
+			N = p + 1; pp = std::pow(10.0, lp); pf = std::pow(10.0, lf);
+			return;
+		}
+	}
 }
 
 // Features -> MLP -> the lowest order whose predicted rel-L2 (absolute
@@ -306,22 +363,19 @@ int learned_predict_launch(Context& ctx, const DevTree& t, const float* params, 
 	return OK;
 }
 
-// The order from the sums of learned_predict_launch and the RMS of the
-// sampled potential.  Synchronises.
-int learned_pick(Context& ctx, const double* acc, double tol, double rms, int& N, double& pred)
+// The predicted log10 rel-L2 of potential (ep) and field (ef) at the
+// network's orders, from the sums of learned_predict_launch and the RMS of
+// the sampled potential and field.  Synchronises.
+int learned_predictions(Context& ctx, const double* acc, const double rms[2], double* ep, double* ef)
 {
 	double h[NO + 1];
 	LFMM_CUDA(ctx, cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-	double e[NO];
-	const double lrms = std::log10(std::max(rms, 1e-300));
-	for (int k = 0; k < NO; ++k) e[k] = 0.5 * std::log10(std::max(h[k], 1e-300) / std::max(h[NO], 1.0)) - lrms;
-	const double target = std::log10(tol * LEARNED_MARGIN);
-	N = FB_N;
-	pred = std::pow(10.0, predicted_log10(e, 14));
-	for (int p = 4; p <= 14; ++p) {
-		const double lp = predicted_log10(e, p);
-		if (lp <= target) { N = p + 1; pred = std::pow(10.0, lp); break; }
+	const double W = std::max(h[NO], 1.0);
+	const double lp = std::log10(std::max(rms[0], 1e-300)), lf = std::log10(std::max(rms[1], 1e-300));
+	for (int k = 0; k < NP; ++k) {
+		ep[k] = 0.5 * std::log10(std::max(h[k], 1e-300) / W) - lp;
+		ef[k] = 0.5 * std::log10(std::max(h[NP + k], 1e-300) / W) - lf;
 	}
 	return OK;
 }
@@ -354,7 +408,7 @@ int direct_samples_launch(Context& ctx, const ParticleInput& in, size_t m, Sampl
 	S.sp = take<double>(ctx, 3 * S.m);
 	S.ep = take<double>(ctx, S.m);
 	S.ef = take<double>(ctx, 3 * S.m);
-	S.acc = take<double>(ctx, 4);
+	S.acc = take<double>(ctx, NCHK);
 	if (!S.sp || !S.ep || !S.ef || !S.acc) { ctx.last_error = "sampled check: allocation failed"; return ERR_OOM; }
 	LFMM_CUDA(ctx, cudaEventRecord(ctx.fork_ev, ctx.stream));
 	LFMM_CUDA(ctx, cudaStreamWaitEvent(ctx.side, ctx.fork_ev, 0));
@@ -366,10 +420,10 @@ int direct_samples_launch(Context& ctx, const ParticleInput& in, size_t m, Sampl
 		st = direct_device(ctx, 3, in.ns, in.src, in.srcq, S.m, S.sp, S.ep, S.ef, /*fast=*/true);
 		if (st == OK) {
 			// the RMS: the check against the direct sum itself (pot = direct, zero error)
-			cudaError_t e = cudaMemsetAsync(S.acc, 0, sizeof(double) * 4, s);
+			cudaError_t e = cudaMemsetAsync(S.acc, 0, sizeof(double) * NCHK, s);
 			if (e == cudaSuccess) {
 				rms_kernel<<<(unsigned)std::min<size_t>(div_up(S.m, 256), 64), 256, 0, s>>>(
-					S.ep, S.stride, S.m, in.nt ? nullptr : in.srcq, S.acc);
+					S.ep, S.ef, S.stride, S.m, in.nt ? nullptr : in.srcq, S.acc);
 				e = cudaGetLastError();
 			}
 			if (e == cudaSuccess) e = cudaEventRecord(ctx.join_ev, s);
@@ -380,29 +434,31 @@ int direct_samples_launch(Context& ctx, const ParticleInput& in, size_t m, Sampl
 	return st;
 }
 
-int samples_join(Context& ctx, const Samples& S, double* rms)
+int samples_join(Context& ctx, const Samples& S, double rms[2])
 {
 	LFMM_CUDA(ctx, cudaStreamWaitEvent(ctx.stream, ctx.join_ev, 0));
-	double h;
-	LFMM_CUDA(ctx, cudaMemcpyAsync(&h, S.acc, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+	double h[2];
+	LFMM_CUDA(ctx, cudaMemcpyAsync(h, S.acc, sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-	*rms = std::sqrt(h / (double)S.m);
+	rms[0] = std::sqrt(h[0] / (double)S.m);
+	rms[1] = std::sqrt(h[1] / (double)S.m);
 	return OK;
 }
 
-// rel-L2 of the potential (self term removed) and of the field at the samples.
+// Sampled rel-L2 of the potential (self term removed) and of the field:
+// out[0], out[1] the estimates, out[2], out[3] their upper confidence bounds.
 int sampled_error(Context& ctx, const ParticleInput& in, const Samples& S, const double* pot, const double* field,
-                  double out[2])
+                  double out[4])
 {
 	cudaStream_t s = ctx.stream;
-	LFMM_CUDA(ctx, cudaMemsetAsync(S.acc, 0, sizeof(double) * 4, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(S.acc, 0, sizeof(double) * NCHK, s));
 	check_kernel<<<(unsigned)std::min<size_t>(div_up(S.m, 256), 64), 256, 0, s>>>(
 		pot, field, S.stride, S.m, in.nt ? nullptr : in.srcq, S.ep, S.ef, S.acc);
-	double h[4];
+	double h[NCHK];
 	LFMM_CUDA(ctx, cudaMemcpyAsync(h, S.acc, sizeof(h), cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
-	out[0] = std::sqrt(h[0] / std::max(h[1], 1e-300));
-	out[1] = std::sqrt(h[2] / std::max(h[3], 1e-300));
+	rel_l2_bound(h, (double)S.m, &out[0], &out[2]);
+	rel_l2_bound(h + 5, (double)S.m, &out[1], &out[3]);
 	return OK;
 }
 
@@ -428,31 +484,48 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	if (st) return st;
 	DevTree t;
 	double* pacc = nullptr;
-	double rms = 0.0;
+	double rms[2] = {0.0, 0.0};
 	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t)) ||
 	    (timing && (st = cudaEventRecord(ctx.ev[1], s) == cudaSuccess ? OK : ERR_CUDA)) ||
-	    (st = learned_predict_launch(ctx, t, params, pacc)) || (st = samples_join(ctx, S, &rms))) {
+	    (st = learned_predict_launch(ctx, t, params, pacc)) || (st = samples_join(ctx, S, rms))) {
 		cudaStreamSynchronize(ctx.side);
 		return st;
 	}
 	int N = FB_N;
-	double pred = 0.0;
-	if ((st = learned_pick(ctx, pacc, tol, rms, N, pred))) return st;
 	lfmm_learned_info li{};
+	double ep[NP], ef[NP];
+	if ((st = learned_predictions(ctx, pacc, rms, ep, ef))) return st;
+	const double target = std::log10(tol * LEARNED_MARGIN);
+	pick_order(ep, ef, target, N, li.predicted_error, li.predicted_error_field);
 	li.predicted_N = N;
-	li.predicted_error = pred;
 	if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
-	double e[2];
+	double e[4];
 	if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
-	if (e[0] > tol && N < FB_N) {
-		// the fixed-order fallback judges and replaces a prediction that missed
-		N = FB_N;
+	auto judged = [&] { return std::max(e[2], e[3]); };
+	if (judged() > tol && N < FB_N - 1) {
+		// a prediction that missed: shift each output's predictions by the
+		// shortfall the judge measured at N (bound over prediction) and pick
+		// again, above N
+		const double sp = std::log10(std::max(e[2], 1e-300)) - std::log10(std::max(li.predicted_error, 1e-300));
+		const double sf = std::log10(std::max(e[3], 1e-300)) - std::log10(std::max(li.predicted_error_field, 1e-300));
+		double ep2[NP], ef2[NP], pp, pf;
+		for (int k = 0; k < NP; ++k) { ep2[k] = ep[k] + std::max(sp, 0.0); ef2[k] = ef[k] + std::max(sf, 0.0); }
+		int N2 = FB_N;
+		pick_order(ep2, ef2, target, N2, pp, pf);
+		N = std::max(N2, N + 1);
 		li.fallback = 1;
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
 		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
 	}
-	if (e[0] > tol && precision == LFMM_PRECISION_MIXED) {
-		// the mixed form cannot reach tol even at N = 15: the FP64 form
+	if (judged() > tol && N < FB_N) {
+		// the fixed-order fallback judges and replaces a prediction that missed
+		N = FB_N;
+		li.fallback = 2;
+		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+	}
+	if (judged() > tol && precision == LFMM_PRECISION_MIXED) {
+		// the mixed form cannot reach tol even at the fallback order: the FP64 form
 		if ((st = fmm3d_scaled_on_tree(ctx, t, FB_N, LFMM_PRECISION_FP64, pot, field, stats))) return st;
 		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
 		N = FB_N;
@@ -460,6 +533,7 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	}
 	li.checked_error = e[0];
 	li.checked_error_field = e[1];
+	li.judged_error = judged();
 	li.order_N = N;
 	if (info) *info = li;
 	return OK;
@@ -495,7 +569,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	double* sp = take<double>(ctx, 3 * m);
 	double* ep = take<double>(ctx, m);
 	double* ef = take<double>(ctx, 3 * m);
-	double* acc = take<double>(ctx, 4 * (size_t)P);
+	double* acc = take<double>(ctx, (size_t)NCHK * P);
 	double* accp = take<double>(ctx, (size_t)(NO + 1) * P);
 	if (!idx || !prob || !sp || !ep || !ef || !acc || !accp) { ctx.last_error = "learned batch: allocation failed"; return ERR_OOM; }
 	LFMM_CUDA(ctx, cudaMemcpyAsync(idx, hidx.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice, s));
@@ -508,7 +582,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 		                        sp + 3 * soff[k], ep + soff[k], ef + 3 * soff[k], /*fast=*/true)))
 			return st;
 	}
-	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * NCHK * P, s));
 	check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(nullptr, nullptr, idx, prob, m, in.srcq, ep, ef, acc);
 	// per-problem predictions
 	const size_t nl = t.nleaves;
@@ -520,56 +594,70 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	if ((st = mlp_forward_device(ctx, params, (int)nl, feats, Y))) return st;
 	LFMM_CUDA(ctx, cudaMemsetAsync(accp, 0, sizeof(double) * (NO + 1) * P, s));
 	predict_reduce_forest_kernel<<<div_up(std::max<size_t>(nl, 1), 256), 256, 0, s>>>(t, Y, w, accp);
-	std::vector<double> ha(4 * (size_t)P), hp((size_t)(NO + 1) * P);
+	std::vector<double> ha((size_t)NCHK * P), hp((size_t)(NO + 1) * P);
 	LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaMemcpyAsync(hp.data(), accp, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	int N = 5;
-	double pred = 0.0;
+	lfmm_learned_info li{};
 	for (int k = 0; k < P; ++k) {
 		const size_t mk = soff[k + 1] - soff[k];
-		if (!mk || hp[(size_t)k * (NO + 1) + NO] <= 0.0) continue;
-		const double rms = std::sqrt(ha[4 * (size_t)k + 1] / (double)mk);
-		if (!(rms > 0.0)) continue;    // nothing but self terms (one particle): no far-field error
-		double e[NO];
-		for (int j = 0; j < NO; ++j)
-			e[j] = 0.5 * std::log10(std::max(hp[(size_t)k * (NO + 1) + j], 1e-300) / hp[(size_t)k * (NO + 1) + NO]) -
-			       std::log10(std::max(rms, 1e-300));
-		int Nk = FB_N;
-		double pk = std::pow(10.0, predicted_log10(e, 14));
-		for (int p = 4; p <= 14; ++p) {
-			const double lp = predicted_log10(e, p);
-			if (lp <= std::log10(tol * LEARNED_MARGIN)) { Nk = p + 1; pk = std::pow(10.0, lp); break; }
+		const double* hk = hp.data() + (size_t)k * (NO + 1);
+		if (!mk || hk[NO] <= 0.0) continue;
+		const double rp = std::sqrt(ha[(size_t)NCHK * k + 1] / (double)mk);
+		const double rf = std::sqrt(ha[(size_t)NCHK * k + 6] / (double)mk);
+		if (!(rp > 0.0) || !(rf > 0.0)) continue;    // nothing but self terms (one particle): no far-field error
+		double e_p[NP], e_f[NP];
+		for (int j = 0; j < NP; ++j) {
+			e_p[j] = 0.5 * std::log10(std::max(hk[j], 1e-300) / hk[NO]) - std::log10(rp);
+			e_f[j] = 0.5 * std::log10(std::max(hk[NP + j], 1e-300) / hk[NO]) - std::log10(rf);
 		}
-		if (Nk > N || (Nk == N && pk > pred)) { N = Nk; pred = pk; }
+		int Nk;
+		double pk, fk;
+		pick_order(e_p, e_f, std::log10(tol * LEARNED_MARGIN), Nk, pk, fk);
+		if (Nk > N || (Nk == N && std::max(pk, fk) > std::max(li.predicted_error, li.predicted_error_field))) {
+			N = Nk;
+			li.predicted_error = pk;
+			li.predicted_error_field = fk;
+		}
 	}
-	lfmm_learned_info li{};
 	li.predicted_N = N;
-	li.predicted_error = pred;
+	// per problem: the estimates and the judge's bound of both outputs
+	std::vector<double> judged(P, 0.0);
+	auto check = [&](bool recheck) -> int {
+		if (recheck) {
+			LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * NCHK * P, s));
+			check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
+			LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
+			LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+		}
+		li.checked_error = li.checked_error_field = li.judged_error = 0.0;
+		for (int k = 0; k < P; ++k) {
+			const size_t mk = soff[k + 1] - soff[k];
+			judged[k] = 0.0;
+			if (!mk) continue;
+			double e[4];
+			rel_l2_bound(ha.data() + (size_t)NCHK * k, (double)mk, &e[0], &e[2]);
+			rel_l2_bound(ha.data() + (size_t)NCHK * k + 5, (double)mk, &e[1], &e[3]);
+			judged[k] = std::max(e[2], e[3]);
+			li.checked_error = std::max(li.checked_error, e[0]);
+			li.checked_error_field = std::max(li.checked_error_field, e[1]);
+			li.judged_error = std::max(li.judged_error, judged[k]);
+		}
+		return OK;
+	};
 	for (int pass = 0; pass < 2; ++pass) {
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
-		LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
-		check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
-		LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
-		LFMM_CUDA(ctx, cudaStreamSynchronize(s));
-		double ep_max = 0.0, ef_max = 0.0;
-		for (int k = 0; k < P; ++k) {
-			if (soff[k + 1] == soff[k]) continue;
-			ep_max = std::max(ep_max, std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)));
-			ef_max = std::max(ef_max, std::sqrt(ha[4 * (size_t)k + 2] / std::max(ha[4 * (size_t)k + 3], 1e-300)));
-		}
-		li.checked_error = ep_max;
-		li.checked_error_field = ef_max;
-		if (ep_max <= tol || N >= FB_N) break;
+		if ((st = check(true))) return st;
+		if (li.judged_error <= tol || N >= FB_N) break;
 		N = FB_N;                      // the fixed-order fallback for the whole batch
 		li.fallback = 1;
 	}
-	if (precision == LFMM_PRECISION_MIXED && li.checked_error > tol) {
-		// problems the mixed form cannot bring within tol even at N = 15:
-		// each rerun alone in the FP64 form, into its slice of the outputs
+	if (precision == LFMM_PRECISION_MIXED && li.judged_error > tol) {
+		// problems the mixed form cannot bring within tol even at the fallback
+		// order: each rerun alone in the FP64 form, into its slice of the outputs
 		for (int k = 0; k < P; ++k) {
-			if (soff[k + 1] == soff[k]) continue;
-			if (std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)) <= tol) continue;
+			if (soff[k + 1] == soff[k] || judged[k] <= tol) continue;
 			ParticleInput pk;
 			pk.dim = 3; pk.ns = hoff[k + 1] - hoff[k]; pk.nt = 0;
 			pk.src = in.src + 3 * hoff[k]; pk.srcq = in.srcq + hoff[k];
@@ -580,20 +668,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 			if (st) return st;
 			++li.fp64_resolved;
 		}
-		if (li.fp64_resolved) {
-			LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * 4 * P, s));
-			check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
-			LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
-			LFMM_CUDA(ctx, cudaStreamSynchronize(s));
-			double ep_max = 0.0, ef_max = 0.0;
-			for (int k = 0; k < P; ++k) {
-				if (soff[k + 1] == soff[k]) continue;
-				ep_max = std::max(ep_max, std::sqrt(ha[4 * (size_t)k] / std::max(ha[4 * (size_t)k + 1], 1e-300)));
-				ef_max = std::max(ef_max, std::sqrt(ha[4 * (size_t)k + 2] / std::max(ha[4 * (size_t)k + 3], 1e-300)));
-			}
-			li.checked_error = ep_max;
-			li.checked_error_field = ef_max;
-		}
+		if (li.fp64_resolved && (st = check(true))) return st;
 	}
 	li.order_N = N;
 	if (info) *info = li;

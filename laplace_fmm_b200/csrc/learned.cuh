@@ -6,7 +6,7 @@
 
 namespace lfmm {
 
-// Y[n][6] = MLP(X[n][16]) on ctx.stream (device pointers).
+// Y[n][14] = MLP(X[n][16]) on ctx.stream (device pointers).
 int mlp_forward_device(Context& ctx, const float* params, int n, const float* X, float* Y);
 
 // Tree (adaptive form: max_leaf > 0 splits, 0 = uniform depth), order from

@@ -891,6 +891,9 @@ int gemm_rt(Context& ctx, const M2LPlan& plan, const real* ops, const real* mult
 		case 6: e = go(m2l_gemm_dmma_kernel<6>); break;
 		case 7: e = go(m2l_gemm_dmma_kernel<7>); break;
 		case 8: e = go(m2l_gemm_dmma_kernel<8>); break;
+		case 9: e = go(m2l_gemm_dmma_kernel<9>); break;
+		case 10: e = go(m2l_gemm_dmma_kernel<10>); break;
+		case 11: e = go(m2l_gemm_dmma_kernel<11>); break;
 		default: ctx.last_error = "m2l gemm: order too large"; return ERR_UNSUPPORTED;
 		}
 		if (e != cudaSuccess) return cuda_fail(ctx, e, "m2l_gemm_dmma_kernel");
@@ -917,6 +920,7 @@ int gemm_rt(Context& ctx, const M2LPlan& plan, const real* ops, const real* mult
 	case 12: launch_gemm<real, 12, DIM>(grid, s, ops, mult, loc, plan, R, part); break;
 	case 14: launch_gemm<real, 14, DIM>(grid, s, ops, mult, loc, plan, R, part); break;
 	case 15: launch_gemm<real, 15, DIM>(grid, s, ops, mult, loc, plan, R, part); break;
+	case 17: launch_gemm<real, 17, DIM>(grid, s, ops, mult, loc, plan, R, part); break;
 	default: ctx.last_error = "m2l gemm: order too large"; return ERR_UNSUPPORTED;
 	}
 	if (S > 1) {

@@ -35,7 +35,7 @@ struct M2LPlan {
 
 // Padded operator size for N degrees: 2 N(N+1)/2 rounded up to 16.
 inline int m2l_padded(int N) { return ((N * (N + 1) + 15) / 16) * 16; }
-inline bool m2l_gemm_supported(int N) { return m2l_padded(N) <= 240; }
+inline bool m2l_gemm_supported(int N) { return m2l_padded(N) <= 352; }
 
 int m2l_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan);
 

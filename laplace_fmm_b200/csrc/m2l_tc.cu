@@ -181,26 +181,55 @@ __device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
 	}
 }
 
+// Column split of the NC output coefficients (triangular (n, m) order, so a
+// degree is a prefix): columns [0, NA) are the low degrees, whose MMA result
+// is drained to FP32 registers after every slot and which get the hi/lo
+// correction products; columns [NA, NC) are the high degrees, accumulated
+// across all slots in tensor memory from B_hi T_hi alone.  A coefficient of
+// degree >= 12 scales its term by at most (sqrt(3)/2)^12 ~ 0.18 at the target
+// and carries what is left of the far field beyond that degree (the
+// truncation error of a 12-degree expansion, ~1e-5 relative here), so the
+// TF32 rounding (2^-11) and the tensor-core accumulation (~1e-5 relative) of
+// those columns stay near 1e-9 of the result.  The corrections are applied to
+// the source degrees of the same range only (K blocks [0, KBC)), for the same
+// reason.  NA = NC keeps every column on the full path (low orders).
+//
+// TMEM columns: P = main of the drained columns [0, NA), fresh per slot;
+// Q = the high-degree columns [NA, NC), one accumulator over all slots;
+// C = corrections of the drained columns [NC, NC + NA), over all slots; the
+// stages' B_hi blocks (32 columns each) after C when two or more fit, else
+// B_hi goes to shared memory beside B_lo.  Shared memory per K block:
+// operator hi rows (NC x 128 bytes), then, for K blocks below KBC, the lo rows
+// of the drained columns (NA x 128 bytes) and the sources' lo block.
+//
 // TMEM_HI = false keeps the sources' hi parts in shared memory (the L2L
-// mode: one slot of 7 K blocks per tile leaves the TMEM stores' waits exposed)
-template <int NC, bool TMEM_HI = true>
+// mode: one slot of few K blocks per tile leaves the TMEM stores' waits exposed)
+template <int NC, int NA, bool TMEM_HI = true>
 struct TcCfg {
 	static constexpr int KB = (NC + 31) / 32;           // K blocks of 32 inputs
-	static constexpr int OP_BYTES = 2 * NC * 128;       // operator block: hi rows, then lo rows
+	static constexpr int KBC = (NA + 31) / 32;          // K blocks with corrections
+	static constexpr int HI_BYTES = NC * 128;           // operator hi rows of a K block
+	static constexpr int LO_BYTES = NA * 128;           // operator lo rows (drained columns) of a K block
 	static constexpr int A_BYTES = TC_M * 128;          // one 32-wide K block of the multipoles (hi or lo)
-	static constexpr uint32_t CORR_COL = 256;
-	static constexpr int GAP = (256 - NC) / 32;         // B_hi stages per TMEM gap
-	static constexpr bool HI_TMEM = TMEM_HI && GAP >= 1; // B_hi in TMEM (else in shared memory)
-	static constexpr int STAGE = OP_BYTES + (HI_TMEM ? 1 : 2) * A_BYTES;
-	static constexpr int NSTAGE = HI_TMEM ? (2 * GAP < NSTAGE_MAX ? 2 * GAP : NSTAGE_MAX) : 2;
-	static constexpr int HALF = NC / 2;                 // columns per epilogue warp
+	static constexpr size_t DIR_BYTES = (size_t)KB * HI_BYTES + (size_t)KBC * LO_BYTES;
+	static constexpr uint32_t Q_COL = NA, C_COL = NC;
+	static constexpr int FREE = (int)TMEM_COLS - NC - NA;
+	static constexpr bool HI_TMEM = TMEM_HI && FREE >= 64; // B_hi in TMEM (else in shared memory)
+	static constexpr int NSTAGE = HI_TMEM ? (FREE / 32 < NSTAGE_MAX ? FREE / 32 : NSTAGE_MAX) : 2;
+	static constexpr int STAGE = HI_BYTES + LO_BYTES + (HI_TMEM ? 1 : 2) * A_BYTES;
+	static constexpr int HALF = NA / 2;                 // drained columns per epilogue warp
+	static constexpr int HQ = (NC - NA) / 2;            // high-degree columns per epilogue warp
 	static constexpr int SMEM = NSTAGE * STAGE + 1024;
-	// TMEM column of stage s's B_hi: the gap after main, then the gap after corr
-	static __device__ __forceinline__ uint32_t hi_col(uint32_t s)
-	{ return s < (uint32_t)GAP ? NC + 32u * s : CORR_COL + NC + 32u * (s - GAP); }
-	static_assert(NC % 16 == 0 && NC >= 16 && NC <= 256, "MMA N");
-	static_assert(CORR_COL + NC <= TMEM_COLS, "TMEM columns");
-	static_assert(HALF % 8 == 0, "epilogue column split");
+	static __host__ __device__ __forceinline__ size_t op_off(int kb)
+	{ return (size_t)kb * HI_BYTES + (size_t)(kb < KBC ? kb : KBC) * LO_BYTES; }
+	static __host__ __device__ __forceinline__ uint32_t op_bytes(int kb)
+	{ return (uint32_t)(HI_BYTES + (kb < KBC ? LO_BYTES : 0)); }
+	static __device__ __forceinline__ uint32_t hi_col(uint32_t s) { return (uint32_t)(NC + NA) + 32u * s; }
+	static_assert(NC % 16 == 0 && NC >= 16 && NC <= 352, "operator rows");
+	static_assert(NA % 16 == 0 && NA >= 16 && NA <= NC && NA <= 256 && NC - NA <= 256, "MMA N");
+	static_assert(NC + NA <= (int)TMEM_COLS, "TMEM columns");
+	static_assert(HALF % 8 == 0 && HQ % 8 == 0, "epilogue column split");
+	static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 // grid (tiles, slot splits).  With S = gridDim.y > 1 split s handles slots
@@ -212,16 +241,20 @@ struct TcCfg {
 //             without its diagonal, loc += sum + diag[class] * parent (the
 //             diagonal, 2^-(n+1) on degree n, applied exactly in FP32: through
 //             the TF32 split the dominant coefficients would lose 2^-22 per level).
-template <int NC, int SLOTS, int MODE>
+// The K blocks of a slot are fed from the highest degrees down, so the
+// dominant low-degree products enter each FP32 accumulator last, when the
+// accumulator's own rounding has least left to act on.
+template <int NC, int NA, int SLOTS, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
               const float* __restrict__ diag, unsigned* flags)
 {
-	using C = TcCfg<NC, MODE != TC_L2L>;
+	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	extern __shared__ uint8_t dsm[];
 	constexpr int NSTAGE = C::NSTAGE;
+	constexpr int KB = C::KB, KBC = C::KBC;
 	__shared__ uint64_t full_bar[NSTAGE_MAX], empty_bar[NSTAGE_MAX];
 	__shared__ uint64_t tfull_bar, tempty_bar, drain_bar;
 	__shared__ uint32_t tmem_sh;
@@ -294,24 +327,39 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	const uint32_t tmem = tmem_sh;
 
 	if (warp < 4) {
-		// ---- producers: one target row each; thread 0 also copies the operator
+		// ---- producers: one target row each; thread 0 also copies the operator.
+		// The source block of the next iteration is loaded while the current
+		// one is split and stored (the gathers hit L2 and their latency is
+		// comparable with one K block of MMAs).
 		const int myt = tgt[tid];
 		uint32_t it = 0;
+		const int total = nact * KB;
+		// the gather of iteration i (slot active[i / KB], K block KB - 1 - i % KB) into w[16]
+		auto gather = [&](int i, float2 (&w)[16]) {
+			const int slot = active[i / KB];
+			const int kb = KB - 1 - i % KB;
+			const int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
+			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
+#pragma unroll
+			for (int q = 0; q < 16; ++q) {
+				const int k = kb * 32 + 2 * q;               // R is even: a pair is in or out
+				w[q] = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
+			}
+		};
+		float2 nxt[16];
+		if (total > 0) gather(0, nxt);
 		for (int j = 0; j < nact; ++j) {
 			const int slot = active[j];
 			const int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
-			const int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
-			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
 			bool ok = true;
-			for (int kb = 0; kb < C::KB; ++kb, ++it) {
+			for (int kq = 0; kq < KB; ++kq, ++it) {
+				const int kb = KB - 1 - kq;                  // highest degrees first
+				const bool corr = kb < KBC;
 				const uint32_t st = it % NSTAGE;
 				float v[32];
 #pragma unroll
-				for (int q = 0; q < 16; ++q) {
-					const int k = kb * 32 + 2 * q;           // R is even: a pair is in or out
-					const float2 w = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
-					v[2 * q] = w.x; v[2 * q + 1] = w.y;
-				}
+				for (int q = 0; q < 16; ++q) { v[2 * q] = nxt[q].x; v[2 * q + 1] = nxt[q].y; }
+				if ((int)it + 1 < total) gather((int)it + 1, nxt);
 				// the TMEM stores below are warp-collective: the warp gives up as one
 				const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
 				if (!__all_sync(0xffffffffu, got)) {
@@ -321,14 +369,15 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 				uint8_t* stage = base + st * C::STAGE;
 				if (tid == 0) {
-					mbar_expect_tx(smem_u32(&full_bar[st]), C::OP_BYTES);
-					bulk_g2s(smem_u32(stage), ops + ((size_t)dir * C::KB + kb) * C::OP_BYTES, C::OP_BYTES,
+					const uint32_t nb = C::op_bytes(kb);
+					mbar_expect_tx(smem_u32(&full_bar[st]), nb);
+					bulk_g2s(smem_u32(stage), ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb), nb,
 					         smem_u32(&full_bar[st]));
 				}
-				// lo to the stage's swizzled row tid; hi to TMEM columns
-				// [hi_col(st), +32) of lane tid (or to the row after lo's)
+				// lo (corrected K blocks only) to the stage's swizzled row tid;
+				// hi to TMEM columns [hi_col(st), +32) of lane tid (or to the row after lo's)
 				const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + C::hi_col(st);
-				uint8_t* rl = stage + C::OP_BYTES + tid * 128;
+				uint8_t* rl = stage + C::HI_BYTES + C::LO_BYTES + tid * 128;
 				uint8_t* rh = rl + C::A_BYTES;
 #pragma unroll
 				for (int hf = 0; hf < 2; ++hf) {
@@ -343,7 +392,9 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 #pragma unroll
 					for (int c = 0; c < 4; ++c) {
 						const int pc = (4 * hf + c) ^ (tid & 7);
-						*reinterpret_cast<uint4*>(rl + pc * 16) = make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
+						if (corr)
+							*reinterpret_cast<uint4*>(rl + pc * 16) =
+								make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
 						if constexpr (!C::HI_TMEM)
 							*reinterpret_cast<uint4*>(rh + pc * 16) =
 								make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
@@ -374,26 +425,37 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			for (int j = 0; j < nact && ok; ++j) {
 				if (j > 0 && !mbar_wait(smem_u32(&tempty_bar), (j - 1) & 1u, abort)) { ok = false; break; }
 				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-				for (int kb = 0; kb < C::KB; ++kb, ++it) {
+				for (int kq = 0; kq < KB; ++kq, ++it) {
+					const int kb = KB - 1 - kq;
 					const uint32_t st = it % NSTAGE;
 					if (!mbar_wait(smem_u32(&full_bar[st]), (it / NSTAGE) & 1u, abort)) { ok = false; break; }
 					asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 					const uint32_t sb = smem_u32(base + st * C::STAGE);
-					const uint32_t op_hi = sb, op_lo = sb + NC * 128, a_lo = sb + C::OP_BYTES;
+					const uint32_t op_hi = sb, op_lo = sb + C::HI_BYTES, a_lo = sb + C::HI_BYTES + C::LO_BYTES;
 					const uint32_t a_hi_t = tmem + C::hi_col(st), a_hi_s = a_lo + C::A_BYTES;
 #pragma unroll
-					for (int ks = 0; ks < 4; ++ks) {
-						const uint64_t bh = desc_sw128(op_hi + ks * 32), bl = desc_sw128(op_lo + ks * 32);
-						const uint64_t al = desc_sw128(a_lo + ks * 32);
+					for (int kk = 0; kk < 4; ++kk) {
+						const int ks = 3 - kk;
+						const uint32_t first = kq == 0 && kk == 0;          // first MMA of the slot
+						const uint64_t bh = desc_sw128(op_hi + ks * 32);
+						const uint64_t bq = desc_sw128(op_hi + NA * 128 + ks * 32);
 						if constexpr (C::HI_TMEM) {
-							mma_tf32_ta<NC>(tmem, a_hi_t + 8u * ks, bh, (kb | ks) != 0);
-							mma_tf32_ta<NC>(tmem + C::CORR_COL, a_hi_t + 8u * ks, bl, (j | kb | ks) != 0);
+							const uint32_t ah = a_hi_t + 8u * ks;
+							mma_tf32_ta<NA>(tmem, ah, bh, !first);
+							if constexpr (NC > NA) mma_tf32_ta<NC - NA>(tmem + C::Q_COL, ah, bq, !(first && j == 0));
 						} else {
 							const uint64_t ah = desc_sw128(a_hi_s + ks * 32);
-							mma_tf32<NC>(tmem, ah, bh, (kb | ks) != 0);
-							mma_tf32<NC>(tmem + C::CORR_COL, ah, bl, (j | kb | ks) != 0);
+							mma_tf32<NA>(tmem, ah, bh, !first);
+							if constexpr (NC > NA) mma_tf32<NC - NA>(tmem + C::Q_COL, ah, bq, !(first && j == 0));
 						}
-						mma_tf32<NC>(tmem + C::CORR_COL, al, bh, 1u);
+						if (kb < KBC) {
+							// the first correction of the tile: highest corrected block, ks = 3, slot 0
+							const uint32_t cfirst = j == 0 && kb == KBC - 1 && kk == 0;
+							const uint64_t bl = desc_sw128(op_lo + ks * 32), al = desc_sw128(a_lo + ks * 32);
+							if constexpr (C::HI_TMEM) mma_tf32_ta<NA>(tmem + C::C_COL, a_hi_t + 8u * ks, bl, !cfirst);
+							else mma_tf32<NA>(tmem + C::C_COL, desc_sw128(a_hi_s + ks * 32), bl, !cfirst);
+							mma_tf32<NA>(tmem + C::C_COL, al, bh, 1u);
+						}
 					}
 					mma_commit(smem_u32(&empty_bar[st]));
 				}
@@ -409,16 +471,20 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		}
 		__syncwarp();
 	} else {
-		// ---- epilogue: per slot, main -> FP32 registers
-		constexpr int W = C::HALF;
+		// ---- epilogue: per slot, the drained columns' main -> FP32 registers;
+		// at the end the corrections and the high-degree columns
+		constexpr int W = C::HALF, WQ = C::HQ;
 		const int quarter = warp & 3, half = (warp - EPI_WARP0) >> 2;
-		const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * W);
+		const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+		const uint32_t taddr = tmem + lanes + (uint32_t)(half * W);
 		float acc[W];
 #pragma unroll
 		for (int c = 0; c < W; ++c) acc[c] = 0.f;
 		bool ok = true;
 		for (int j = 0; j < nact; ++j) {
-			if (!mbar_wait(smem_u32(&tfull_bar), j & 1u, abort)) { ok = false; break; }
+			// the TMEM loads below are warp-collective: the warp gives up as one
+			const bool got = mbar_wait(smem_u32(&tfull_bar), j & 1u, abort);
+			if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
 			asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 			tmem_accumulate<W>(taddr, acc);
 			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -428,21 +494,48 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			*abort = 1;
 			atomicOr(flags, DEV_ERR_TIMEOUT);
 		} else {
-			if (nact > 0) tmem_accumulate<W>(taddr + C::CORR_COL, acc);
+			if (nact > 0) tmem_accumulate<W>(taddr + C::C_COL, acc);
 			const int tg = tgt[quarter * 32 + lane];
-			if (tg >= 0 && !*abort) {
-				float* o = out + (size_t)tg * R + half * W;
-				const int lim = R - half * W;
-				if (MODE == TC_L2L) {
-					const float* xs = mult + (size_t)vtab[tg] * R + half * W;
-					const float* dg = diag + oct * NC + half * W;
+			const bool store = tg >= 0 && !*abort;
+			const float* xs = nullptr;
+			const float* dg = nullptr;
+			if (MODE == TC_L2L && store) {
+				xs = mult + (size_t)vtab[tg] * R;
+				dg = diag + oct * NC;
+			}
+			if (store) {
+				const int c0 = half * W;
+				float* o = out + (size_t)tg * R + c0;
+				const int lim = R - c0;
 #pragma unroll
-					for (int c = 0; c < W; ++c)
-						if (c < lim) o[c] += acc[c] + dg[c] * xs[c];
-				} else {
+				for (int c = 0; c < W; ++c)
+					if (c < lim) {
+						if (MODE == TC_L2L) o[c] += acc[c] + dg[c0 + c] * xs[c0 + c];
+						else o[c] = acc[c];
+					}
+			}
+			if constexpr (WQ > 0) {
+				// high-degree columns [NA + half WQ, +WQ): read once (every lane of
+				// the warp takes part in the loads), stored where the target exists
+				const int c0 = NA + half * WQ;
+				const uint32_t qa = tmem + lanes + (uint32_t)c0;
 #pragma unroll
-					for (int c = 0; c < W; ++c)
-						if (c < lim) o[c] = acc[c];
+				for (int c = 0; c < WQ; c += 8) {
+					float v[8];
+					if (nact > 0) tmem_ld8(qa + c, v);
+					else {
+#pragma unroll
+						for (int e = 0; e < 8; ++e) v[e] = 0.f;
+					}
+					if (store) {
+						float* o = out + (size_t)tg * R + c0 + c;
+#pragma unroll
+						for (int e = 0; e < 8; ++e)
+							if (c0 + c + e < R) {
+								if (MODE == TC_L2L) o[e] += v[e] + dg[c0 + c + e] * xs[c0 + c + e];
+								else o[e] = v[e];
+							}
+					}
 				}
 			}
 		}
@@ -453,7 +546,6 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	if (warp == 4)
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS));
 }
-
 __global__ void tc_split_reduce_kernel(const float* __restrict__ part, float* __restrict__ loc, size_t n, int S)
 {
 	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,39 +555,43 @@ __global__ void tc_split_reduce_kernel(const float* __restrict__ part, float* __
 	loc[i] = s;
 }
 
-// FP64 scaled operators [ndir][NC][NC] -> per (direction, K block): hi rows
-// then lo rows, NC rows of 32 TF32 values, 16-byte chunk c of row r at c ^ (r & 7).
-__global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, int NC, int R, int KB,
+// FP64 scaled operators [ndir][NC][NC] -> per (direction, K block): the hi
+// rows of every output column, then (K blocks below KBC) the lo rows of the
+// drained columns [0, NA); rows of 32 TF32 values, 16-byte chunk c of row r
+// at c ^ (r & 7).  One thread per (direction, K block, row, value).
+__global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, int NC, int NA, int R, int KB,
                                     uint32_t* __restrict__ out)
 {
-	const size_t total = (size_t)ndir * KB * 2 * NC * 32;
+	const size_t total = (size_t)ndir * KB * NC * 32;
 	const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (e >= total) return;
 	const int j = (int)(e % 32);
 	size_t rest = e / 32;
 	const int row = (int)(rest % NC); rest /= NC;
-	const int x = (int)(rest % 2); rest /= 2;
 	const int kb = (int)(rest % KB);
 	const int dir = (int)(rest / KB);
+	const int KBC = (NA + 31) / 32;
 	const int k = kb * 32 + j;
 	const double v = (row < R && k < R) ? ops64[((size_t)dir * NC + row) * NC + k] : 0.0;
 	const uint32_t hi = tf32_rna((float)v);
 	const uint32_t lo = tf32_rna((float)(v - (double)__uint_as_float(hi)));
-	const size_t blk = ((size_t)dir * KB + kb) * 2 + x;
-	const size_t word = blk * NC * 32 + (size_t)row * 32 + (size_t)(((j >> 2) ^ (row & 7)) * 4) + (j & 3);
-	out[word] = x == 0 ? hi : lo;
+	const size_t dir_words = ((size_t)KB * NC + (size_t)KBC * NA) * 32;
+	const size_t blk = (size_t)dir * dir_words + ((size_t)kb * NC + (size_t)min(kb, KBC) * NA) * 32;
+	const size_t in_row = (size_t)(((j >> 2) ^ (row & 7)) * 4) + (j & 3);
+	out[blk + (size_t)row * 32 + in_row] = hi;
+	if (kb < KBC && row < NA) out[blk + (size_t)NC * 32 + (size_t)row * 32 + in_row] = lo;
 }
 
-template <int NC, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
+template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
            bool timed, const float* diag = nullptr)
 {
-	using C = TcCfg<NC, MODE != TC_L2L>;
+	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	dim3 grid(tiles, S);
 	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
-	m2l_tc_kernel<NC, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+	m2l_tc_kernel<NC, NA, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 		reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part, plan.cells,
 		diag, ctx.dev_flags);
 	if (timed) {
@@ -516,18 +612,18 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 // (operator rows, log2 tiles) pair times S = 1, 2, 4, 8 with CUDA events and
 // keeps the fastest for the context (the chosen S runs last, so the level's
 // result always comes from it).
-template <int NC>
+template <int NC, int NA>
 int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
 {
-	using C = TcCfg<NC>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, M2L_SLOTS, TC_M2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                                    C::SMEM));
+	using C = TcCfg<NC, NA>;
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L>,
+	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	int S = 1;
 	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
 	int bucket = 0;
 	while ((1u << bucket) < tiles && bucket < 32) ++bucket;
-	int& tuned = ctx.m2l_split[NC][bucket];
+	int& tuned = ctx.m2l_split[NC / 16][bucket];
 	const bool tune = ctx.tune_m2l && tuned == 0;
 	if (ctx.tune_m2l && !tune) S = tuned;
 	float* part = nullptr;
@@ -546,7 +642,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		int bestS = S;
 		for (int cand = 1; cand <= 8; cand *= 2) {
 			LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-			int st = run_tc<NC>(ctx, plan, ops, mult, loc, R, cand, part, false);
+			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false);
 			if (st) return st;
 			LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
 			LFMM_CUDA(ctx, cudaEventSynchronize(e1));
@@ -559,25 +655,25 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		tuned = bestS;
 		S = bestS;
 	}
-	return run_tc<NC>(ctx, plan, ops, mult, loc, R, S, part, true);
+	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
-template <int NC>
+template <int NC, int NA>
 int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int R)
 {
-	using C = TcCfg<NC>;
-	using CL = TcCfg<NC, false>;
+	using C = TcCfg<NC, NA>;
+	using CL = TcCfg<NC, NA, false>;
 	if (mode == TC_M2M) {
-		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 8, TC_M2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                    C::SMEM));
-		return run_tc<NC, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false);
+		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M>,
+		                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false);
 	}
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, 1, TC_L2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                                    CL::SMEM));
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L>,
+	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
-	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + (size_t)8 * C::KB * C::OP_BYTES);
-	return run_tc<NC, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, diag);
+	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + 8 * C::DIR_BYTES);
+	return run_tc<NC, NA, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, diag);
 }
 
 std::mutex g_upload_mu;
@@ -603,16 +699,17 @@ const uint4* m2l_ops_tc(Context& ctx, int N)
 		if (e.N == N && e.prec == 3) { e.stamp = ++ctx.opcache_clock; return static_cast<const uint4*>(e.ptr); }
 	const double* d = m2l_ops_fp64(ctx, N, 1.0);
 	if (!d) return nullptr;
-	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N);
-	const size_t words = (size_t)343 * KB * 2 * NC * 32;
+	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N), NA = m2l_tc_drained(N);
+	const size_t bytes = tc_ops_bytes(343, N);
 	OpCacheEntry e;
-	e.N = N; e.prec = 3; e.h = 1.0; e.bytes = words * 4; e.stamp = ++ctx.opcache_clock;
+	e.N = N; e.prec = 3; e.h = 1.0; e.bytes = bytes; e.stamp = ++ctx.opcache_clock;
 	if (cudaMalloc(&e.ptr, e.bytes) != cudaSuccess) {
 		cudaGetLastError();
 		ctx.last_error = "tensor-core operators: out of memory";
 		return nullptr;
 	}
-	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(d, 343, NC, R, KB, static_cast<uint32_t*>(e.ptr));
+	const size_t threads = (size_t)343 * KB * NC * 32;
+	build_tc_ops_kernel<<<div_up(threads, 256), 256, 0, ctx.stream>>>(d, 343, NC, NA, R, KB, static_cast<uint32_t*>(e.ptr));
 	if (cudaGetLastError() != cudaSuccess) {
 		cudaFree(e.ptr);
 		ctx.last_error = "tensor-core operators: launch failed";
@@ -622,55 +719,47 @@ const uint4* m2l_ops_tc(Context& ctx, int N)
 	return static_cast<const uint4*>(e.ptr);
 }
 
-size_t tc_ops_bytes(int ndir, int N) { return (size_t)ndir * m2l_tc_kblocks(N) * 2 * m2l_padded(N) * 128; }
+size_t tc_ops_bytes(int ndir, int N)
+{
+	const int NC = m2l_padded(N), NA = m2l_tc_drained(N);
+	const size_t KB = (size_t)m2l_tc_kblocks(N), KBC = (size_t)(NA + 31) / 32;
+	return (size_t)ndir * (KB * NC + KBC * NA) * 128;
+}
 
 int tc_ops_convert(Context& ctx, const double* ops64, int ndir, int N, void* out)
 {
-	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N);
-	const size_t words = tc_ops_bytes(ndir, N) / 4;
-	build_tc_ops_kernel<<<div_up(words, 256), 256, 0, ctx.stream>>>(ops64, ndir, NC, R, KB, static_cast<uint32_t*>(out));
+	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N), NA = m2l_tc_drained(N);
+	const size_t threads = (size_t)ndir * KB * NC * 32;
+	build_tc_ops_kernel<<<div_up(threads, 256), 256, 0, ctx.stream>>>(ops64, ndir, NC, NA, R, KB,
+	                                                                 static_cast<uint32_t*>(out));
 	LFMM_CUDA(ctx, cudaGetLastError());
 	return OK;
 }
 
+// The (operator rows, drained columns) pairs built: every order 7 <= N <= 18.
+#define LFMM_TC_ORDERS(X) X(64, 64) X(80, 80) X(96, 96) X(112, 112) X(144, 144) X(160, 160) \
+	X(192, 160) X(224, 160) X(240, 160) X(272, 160) X(320, 160) X(352, 160)
+
 int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N)
 {
 	if (mode != TC_M2M && mode != TC_L2L) { ctx.last_error = "tensor-core shift: bad mode"; return ERR_ARG; }
-	const int R = N * (N + 1);
-	switch (m2l_padded(N)) {
-	case 64: return launch_shift_tc<64>(ctx, mode, plan, ops, src, dst, R);
-	case 80: return launch_shift_tc<80>(ctx, mode, plan, ops, src, dst, R);
-	case 96: return launch_shift_tc<96>(ctx, mode, plan, ops, src, dst, R);
-	case 112: return launch_shift_tc<112>(ctx, mode, plan, ops, src, dst, R);
-	case 144: return launch_shift_tc<144>(ctx, mode, plan, ops, src, dst, R);
-	case 160: return launch_shift_tc<160>(ctx, mode, plan, ops, src, dst, R);
-	case 192: return launch_shift_tc<192>(ctx, mode, plan, ops, src, dst, R);
-	case 224: return launch_shift_tc<224>(ctx, mode, plan, ops, src, dst, R);
-	case 240: return launch_shift_tc<240>(ctx, mode, plan, ops, src, dst, R);
-	default:
-		ctx.last_error = "tensor-core shift: unsupported order";
-		return ERR_UNSUPPORTED;
-	}
+	const int R = N * (N + 1), NC = m2l_padded(N), NA = m2l_tc_drained(N);
+#define LFMM_TC_SHIFT(nc, na) if (NC == nc && NA == na) return launch_shift_tc<nc, na>(ctx, mode, plan, ops, src, dst, R);
+	LFMM_TC_ORDERS(LFMM_TC_SHIFT)
+#undef LFMM_TC_SHIFT
+	ctx.last_error = "tensor-core shift: unsupported order";
+	return ERR_UNSUPPORTED;
 }
 
 int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N)
 {
 	if (int st = upload_slot_dirs(ctx)) return st;
-	const int R = N * (N + 1);
-	switch (m2l_padded(N)) {
-	case 64: return launch_tc<64>(ctx, plan, ops, mult, loc, R);
-	case 80: return launch_tc<80>(ctx, plan, ops, mult, loc, R);
-	case 96: return launch_tc<96>(ctx, plan, ops, mult, loc, R);
-	case 112: return launch_tc<112>(ctx, plan, ops, mult, loc, R);
-	case 144: return launch_tc<144>(ctx, plan, ops, mult, loc, R);
-	case 160: return launch_tc<160>(ctx, plan, ops, mult, loc, R);
-	case 192: return launch_tc<192>(ctx, plan, ops, mult, loc, R);
-	case 224: return launch_tc<224>(ctx, plan, ops, mult, loc, R);
-	case 240: return launch_tc<240>(ctx, plan, ops, mult, loc, R);
-	default:
-		ctx.last_error = "tensor-core M2L: unsupported order";
-		return ERR_UNSUPPORTED;
-	}
+	const int R = N * (N + 1), NC = m2l_padded(N), NA = m2l_tc_drained(N);
+#define LFMM_TC_M2L(nc, na) if (NC == nc && NA == na) return launch_tc<nc, na>(ctx, plan, ops, mult, loc, R);
+	LFMM_TC_ORDERS(LFMM_TC_M2L)
+#undef LFMM_TC_M2L
+	ctx.last_error = "tensor-core M2L: unsupported order";
+	return ERR_UNSUPPORTED;
 }
 
 } // namespace lfmm

@@ -17,12 +17,20 @@ constexpr unsigned DEV_ERR_TIMEOUT = 8u;
 
 // Operator rows (MMA N) = m2l_padded(N); K blocks of 32 inputs (128 bytes of TF32).
 inline int m2l_tc_kblocks(int N) { return (m2l_padded(N) + 31) / 32; }
-inline bool m2l_tc_supported(int N) { return N >= 7 && N <= 15; }
+inline bool m2l_tc_supported(int N) { return N >= 7 && N <= 18; }
+// Output columns on the full-accuracy path (drained to FP32 after every slot,
+// hi/lo corrections): all of them up to N = 12, the coefficients of degree
+// < 12 (156 reals, padded to 160) above; the higher degrees accumulate in
+// tensor memory from the hi products alone (their terms are at the
+// truncation-error level).
+inline int m2l_tc_drained(int N) { return m2l_padded(N) <= 160 ? m2l_padded(N) : 160; }
 
-// Operators in the tensor-core layout: per (direction, K block): hi rows then
-// lo rows, m2l_padded(N) rows of 128 bytes each, 128-byte swizzled (16-byte
-// chunk c of row r stored at chunk c ^ (r & 7)); built from the FP64 scaled
-// operators, cached per context.
+// Operators in the tensor-core layout: per (direction, K block): the hi rows
+// of all m2l_padded(N) output columns, then, for the K blocks of the drained
+// columns' source degrees, the lo rows of the m2l_tc_drained(N) drained
+// columns; rows of 128 bytes, 128-byte swizzled (16-byte chunk c of row r
+// stored at chunk c ^ (r & 7)); built from the FP64 scaled operators, cached
+// per context.
 const uint4* m2l_ops_tc(Context& ctx, int N);
 
 // loc = sum over slots of T_dir mult[src] for every cell of the level (FP32).

@@ -1,8 +1,9 @@
-// Order-selection MLP: 16 features -> 64 -> 64 -> 6 outputs (FP32, ReLU),
+// Order-selection MLP: 16 features -> 64 -> 64 -> 14 outputs (FP32, ReLU),
 // trained on the GPU by these kernels (forward, masked-MSE backward, Adam).
-// Output k predicts log10 of a leaf box's error at order p = 4 + 2k.
+// Outputs 0-6 predict log10 of a leaf box's potential error at the orders
+// p = 4, 6, 8, 10, 12, 14, 16; outputs 7-13 its field error at the same orders.
 //
-// Parameter layout (floats): W1[64][16] b1[64] W2[64][64] b2[64] W3[6][64] b3[6].
+// Parameter layout (floats): W1[64][16] b1[64] W2[64][64] b2[64] W3[14][64] b3[14].
 #include "learned.cuh"
 
 namespace lfmm {
@@ -204,7 +205,7 @@ int lfmm_mlp_grad(lfmm_ctx* h, const float* params, int n, const float* X, const
 	if (!h || !params || !X || !T || !M || !grad || !work || n <= 0) return LFMM_ERR_ARG;
 	Context& c = ctx_of(h);
 	cudaStream_t s = c.stream;
-	// work: Y[n*6] A1[n*64] A2[n*64] acc[2]
+	// work: Y[n*14] A1[n*64] A2[n*64] acc[2]
 	float* Y = work;
 	float* A1 = Y + (size_t)n * O;
 	float* A2 = A1 + (size_t)n * H;

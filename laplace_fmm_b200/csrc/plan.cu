@@ -125,7 +125,7 @@ int lfmm3d_plan_create(lfmm_ctx* h, size_t n_src, const double* src_xyz, const d
 		return LFMM_ERR_ARG;
 	}
 	if (o->N == LFMM_AUTO || o->N < 1 || !m2l_gemm_supported(o->N)) {
-		c.last_error = "plan: N must be given, 1 <= N <= 15";
+		c.last_error = "plan: N must be given, 1 <= N <= 18";
 		return LFMM_ERR_ARG;
 	}
 	const int depth = o->tree_depth != LFMM_AUTO

@@ -53,7 +53,7 @@ int fmm3d_solve_vector(Context& ctx, const ParticleInput& in, int N, int depth, 
                        double* field, SolveStats* stats)
 {
 	if (N < 1 || N > MAXN3) { ctx.last_error = "order out of range (1 <= N <= 18)"; return ERR_ARG; }
-	if (!m2l_gemm_supported(N)) { ctx.last_error = "vector charges use the scaled form: N <= 15"; return ERR_UNSUPPORTED; }
+	if (!m2l_gemm_supported(N)) { ctx.last_error = "vector charges use the scaled form: N <= 18"; return ERR_UNSUPPORTED; }
 	if (max_leaf < 0) { ctx.last_error = "max_leaf must be >= 0"; return ERR_ARG; }
 	cudaStream_t s = ctx.stream;
 	const size_t n_out = in.nt ? in.nt : in.ns;

@@ -1,7 +1,8 @@
 """Learned order selection: host side of the MLP kernels in ``csrc/mlp.cu``.
 
-The network maps 16 features of a leaf box to log10 of that box's relative
-error at the orders p = 4, 6, ..., 14 (``ORDERS``).  Training, inference and
+The network maps 16 features of a leaf box to log10 of that box's RMS
+absolute potential error (outputs 0-6) and field error (outputs 7-13) at the
+orders p = 4, 6, 8, 10, 12, 14, 16 (``ORDERS``).  Training, inference and
 the optimiser all run in the library's CUDA kernels (``lfmm_mlp_forward``,
 ``lfmm_mlp_grad``, ``lfmm_mlp_adam``); torch only holds the device buffers.
 The reference has no counterpart: it derives one order from eps by a fixed
@@ -16,9 +17,10 @@ import numpy as np
 
 from ._lib import PRECISION, Context, LfmmError, LfmmLearnedInfo, LfmmSolveOpts, LfmmStats, default_context
 
-N_IN, N_HIDDEN, N_OUT = 16, 64, 6
+N_IN, N_HIDDEN, N_OUT = 16, 64, 14
 N_PARAMS = N_HIDDEN * N_IN + N_HIDDEN + N_HIDDEN * N_HIDDEN + N_HIDDEN + N_OUT * N_HIDDEN + N_OUT
-ORDERS = tuple(range(4, 15, 2))          # expansion order p of each output (N = p + 1 degrees)
+ORDERS = (4, 6, 8, 10, 12, 14, 16)       # expansion order p of each output pair (N = p + 1 degrees)
+N_ORD = len(ORDERS)
 WEIGHTS = Path(__file__).resolve().parent / "order_mlp.npz"
 
 
@@ -76,7 +78,7 @@ class OrderMLP:
 
     # -- network ops -------------------------------------------------------
     def forward(self, X: np.ndarray, normalised: bool = False) -> np.ndarray:
-        """log10 error predictions [n][6] for feature rows X [n][16]."""
+        """log10 error predictions [n][14] for feature rows X [n][16]."""
         torch = _torch()
         Xn = np.asarray(X, np.float32) if normalised else self.normalise(X)
         n = len(Xn)
@@ -122,14 +124,18 @@ class OrderMLP:
     def params_host(self) -> np.ndarray:
         return self.params.cpu().numpy()
 
-    def shift_outputs(self, delta: float):
-        """Add delta to every output (log10 error): the calibration offset."""
-        self.params[N_PARAMS - N_OUT:] += float(delta)
+    def shift_outputs(self, delta: float, delta_field: float | None = None):
+        """Add the calibration offsets to the outputs (log10 errors): delta to
+        the potential's, delta_field (default: delta) to the field's."""
+        b = N_PARAMS - N_OUT
+        self.params[b:b + N_ORD] += float(delta)
+        self.params[b + N_ORD:] += float(delta if delta_field is None else delta_field)
 
     def predicted_log10(self, feats: np.ndarray) -> np.ndarray:
-        """log10 of the predicted rel-L2 of a problem at each of the six orders,
-        from its leaves' features (leaves weighted by their particles), as the
-        solver aggregates them."""
+        """log10 of the problem-level RMS absolute error at each output (the
+        potential's at the seven orders, then the field's), from its leaves'
+        features (leaves weighted by their particles), as the solver aggregates
+        them; minus log10 of the RMS potential / field it is the rel-L2."""
         Y = self.forward(feats).astype(np.float64)
         w = 10.0 ** feats[:, 0].astype(np.float64) - 1.0
         return 0.5 * np.log10((w[:, None] * 10.0 ** (2.0 * Y)).sum(0) / max(w.sum(), 1.0))

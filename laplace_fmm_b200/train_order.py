@@ -8,19 +8,20 @@ centres uniform in the unit cube), N log-uniform in [1e4, 1e6], charges
 uniform in [-1, 1]; plus larger ones (1e6-8e6 particles, Gaussian clusters or
 a Plummer sphere in a uniform background) so that the network covers
 millions of particles; adaptive octree (<= 10 levels, <= 64 per leaf).  Each
-problem is labelled by solving it (mixed form) at p = 4, 6, ..., 14 and
-comparing with the FP64 direct sum at 1024 sampled targets: the label of a
-leaf at order p is log10 of the RMS absolute potential error of its sampled
-targets, so that the leaves' labels, weighted by their particle counts and
-divided by the RMS potential (self term removed), give the problem's rel-L2.
-The solver gets that RMS potential from the same sampled direct sum that
+problem is labelled by solving it (mixed form) at p = 4, 6, ..., 14, 16 and
+comparing with the FP64 direct sum at 1024 sampled targets: the labels of a
+leaf at order p are log10 of the RMS absolute potential error and of the RMS
+field error magnitude of its sampled targets, so that the leaves' labels,
+weighted by their particle counts and divided by the RMS potential (self
+term removed) or the RMS field, give the problem's rel-L2 of each output.
+The solver gets those RMS values from the same sampled direct sum that
 judges its result.  Leaves without a sampled target are masked out.
 
 Training: Adam (lr 1e-3), batches of 4096 leaves, masked mean-squared error,
 all in the library's CUDA kernels.  The held-out problems measure what the
-network gains over the fixed order: the order it picks for tolerance 1e-6,
-the error reached there, and the fastest fixed order that meets the
-tolerance on every training problem.  Writes ``order_mlp.npz`` beside this
+network gains over the fixed order: the order it picks for tolerance 1e-6
+(on both outputs), the error reached there, and the fastest fixed order
+that meets the tolerance on every training problem.  Writes ``order_mlp.npz`` beside this
 file (parameters with the input normalisation folded in, plus the
 normalisation, the loss curve and the held-out summary).
 """
@@ -34,7 +35,7 @@ from pathlib import Path
 import numpy as np
 
 from ._lib import LfmmSolveOpts, default_context
-from .order import N_OUT, ORDERS, WEIGHTS, LearnedSolver, OrderMLP, features
+from .order import N_ORD, N_OUT, ORDERS, WEIGHTS, LearnedSolver, OrderMLP, features
 from .workloads import gaussian_mix3d, plummer_mix3d
 
 DEPTH, MAX_LEAF, SAMPLES = 10, 64, 1024
@@ -66,7 +67,7 @@ def solve(ctx, pos, q, N):
     ctx.check(ctx.lib.lfmm3d_solve_ex(ctx.handle, len(pos), pos.ctypes.data_as(vp), q.ctypes.data_as(vp), 0, None,
                                       ctypes.byref(opts), pot.ctypes.data_as(vp), fld.ctypes.data_as(vp), None),
               "solve")
-    return pot
+    return pot, fld
 
 
 def direct(ctx, pos, q, idx):
@@ -78,32 +79,40 @@ def direct(ctx, pos, q, idx):
     ctx.check(ctx.lib.lfmm3d_direct(ctx.handle, len(pos), pos.ctypes.data_as(vp), q.ctypes.data_as(vp), len(idx),
                                     tgt.ctypes.data_as(vp), pot.ctypes.data_as(vp), fld.ctypes.data_as(vp)),
               "direct")
-    return pot
+    return pot, fld
 
 
 def label(ctx, pos, q, seed):
-    """Features, per-leaf labels [leaves][6], mask, and the sampled rel-L2 of
-    the whole problem at each order."""
+    """Features, per-leaf labels [leaves][14] (potential, then field), mask,
+    and the sampled rel-L2 of the whole problem at each order: err[7] of the
+    potential, errf[7] of the field; the RMS potential and RMS field."""
     feats, leaf_of = features(pos, q, tree_depth=DEPTH, max_leaf=MAX_LEAF, ctx=ctx)
     g = np.random.default_rng(seed)
     idx = np.sort(g.choice(len(pos), min(SAMPLES, len(pos)), replace=False))
     self_term = q[idx] * 1e4
-    exact = direct(ctx, pos, q, idx) - self_term
+    exact, exact_f = direct(ctx, pos, q, idx)
+    exact = exact - self_term
     scale = np.sqrt(np.mean(exact ** 2))           # RMS potential: rel-L2 = RMS error / scale
+    fscale = np.sqrt(np.mean(np.sum(exact_f ** 2, 1)))
     nl = len(feats)
     T = np.zeros((nl, N_OUT), np.float32)
     M = np.zeros((nl, N_OUT), np.float32)
     leaves = leaf_of[idx]
     counts = np.bincount(leaves, minlength=nl)
     has = counts > 0
-    err = np.zeros(N_OUT)
+    err, errf = np.zeros(N_ORD), np.zeros(N_ORD)
     for k, p in enumerate(ORDERS):
-        e = solve(ctx, pos, q, p + 1)[idx] - self_term - exact      # absolute error
+        pot, fld = solve(ctx, pos, q, p + 1)
+        e = pot[idx] - self_term - exact                             # absolute errors
+        ef2 = np.sum((fld[idx] - exact_f) ** 2, 1)
         err[k] = np.sqrt(np.mean(e ** 2)) / scale
+        errf[k] = np.sqrt(np.mean(ef2)) / fscale
         ms = np.bincount(leaves, weights=e ** 2, minlength=nl)
+        mf = np.bincount(leaves, weights=ef2, minlength=nl)
         T[has, k] = 0.5 * np.log10(ms[has] / counts[has] + 1e-30)
-        M[has, k] = 1.0
-    return feats, T, M, err, scale
+        T[has, N_ORD + k] = 0.5 * np.log10(mf[has] / counts[has] + 1e-30)
+        M[has, k] = M[has, N_ORD + k] = 1.0
+    return feats, T, M, err, errf, scale, fscale
 
 
 def main(argv=None):
@@ -131,9 +140,10 @@ def main(argv=None):
     if a.data:
         blob = {}
         for kind in ("train", "heldout"):
-            for i, (n, feats, T_, M_, err, scale) in enumerate(data[kind]):
+            for i, (n, feats, T_, M_, err, errf, scale, fscale) in enumerate(data[kind]):
                 blob.update({f"{kind}{i}_feats": feats, f"{kind}{i}_T": T_, f"{kind}{i}_M": M_,
-                             f"{kind}{i}_err": err, f"{kind}{i}_scale": np.float64(scale), f"{kind}{i}_n": np.int64(n)})
+                             f"{kind}{i}_err": err, f"{kind}{i}_errf": errf, f"{kind}{i}_scale": np.float64(scale),
+                             f"{kind}{i}_fscale": np.float64(fscale), f"{kind}{i}_n": np.int64(n)})
         np.savez_compressed(a.data, **blob)
     X = np.concatenate([d[1] for d in data["train"]])
     T = np.concatenate([d[2] for d in data["train"]])
@@ -154,22 +164,27 @@ def main(argv=None):
         losses.append(tot / len(perm))
     t_train = time.time() - t0 - t_label
     # calibration: the network's problem-level prediction against the measured
-    # rel-L2 of every training problem near the tolerance; the 90th percentile
-    # of the shortfall is added to the outputs (folded into their biases)
-    res = []
-    for n, feats, T_t, M_t, err, scale in data["train"]:
-        pred = net.predicted_log10(feats) - np.log10(scale)
-        for k in range(N_OUT):
+    # rel-L2 of every training problem near the tolerance, for the potential
+    # and the field apart; a quantile of each output's shortfall is added to
+    # its outputs (folded into their biases)
+    res, resf = [], []
+    for n, feats, T_t, M_t, err, errf, scale, fscale in data["train"]:
+        pred = net.predicted_log10(feats)
+        for k in range(N_ORD):
             if 1e-3 * a.tol <= err[k] <= 1e3 * a.tol:
-                res.append(np.log10(err[k]) - pred[k])
+                res.append(np.log10(err[k]) - (pred[k] - np.log10(scale)))
+            if 1e-3 * a.tol <= errf[k] <= 1e3 * a.tol:
+                resf.append(np.log10(errf[k]) - (pred[N_ORD + k] - np.log10(fscale)))
     delta = float(np.quantile(res, a.quantile)) if res else 0.0
-    net.shift_outputs(delta)
+    delta_f = float(np.quantile(resf, a.quantile)) if resf else 0.0
+    net.shift_outputs(delta, delta_f)
     # held-out: the learned solve (with its sampled check and fallback) against
-    # the fixed order that meets the tolerance on every training problem
-    fixed = next((p for k, p in enumerate(ORDERS) if all(d[4][k] <= a.tol for d in data["train"])), ORDERS[-1])
+    # the fixed order that meets the tolerance (both outputs) on every training problem
+    ok = lambda d, k: d[4][k] <= a.tol and d[5][k] <= a.tol
+    fixed = next((p for k, p in enumerate(ORDERS) if all(ok(d, k) for d in data["train"])), ORDERS[-1])
     solver = LearnedSolver(net.folded_params(), ctx=ctx)
     picked, first_ok, final_ok, best, t_learned, t_fixed = [], 0, 0, [], 0.0, 0.0
-    for i, (n, feats, T_h, M_h, err, scale) in enumerate(data["heldout"]):
+    for i, (n, feats, T_h, M_h, err, errf, scale, fscale) in enumerate(data["heldout"]):
         pos, q = problem(i, "heldout")
         solve(ctx, pos, q, fixed + 1)                        # warm the operator caches
         s0 = time.perf_counter()
@@ -182,12 +197,13 @@ def main(argv=None):
         info = r["info"]
         picked.append(info["predicted_N"] - 1)
         first_ok += int(not info["fallback"])
-        final_ok += int(info["checked_error"] <= a.tol)
-        best.append(next((pp for k, pp in enumerate(ORDERS) if err[k] <= a.tol), ORDERS[-1]))
+        final_ok += int(max(info["checked_error"], info["checked_error_field"]) <= a.tol)
+        best.append(next((pp for k, pp in enumerate(ORDERS) if err[k] <= a.tol and errf[k] <= a.tol), ORDERS[-1]))
     summary = {"train_problems": a.train, "large_problems": a.large, "heldout_problems": a.heldout,
                "leaves": int(len(X)),
                "loss_first": losses[0], "loss_last": losses[-1], "label_s": t_label, "train_s": t_train,
-               "calibration_log10": delta, "calibration_residuals": len(res),
+               "calibration_log10": delta, "calibration_log10_field": delta_f,
+               "calibration_residuals": len(res) + len(resf),
                "fixed_p_all_train": fixed, "heldout_mean_p_picked": float(np.mean(picked)),
                "heldout_mean_p_best_even": float(np.mean(best)), "heldout_no_fallback": first_ok,
                "heldout_within_tol": final_ok, "heldout_s_learned": t_learned, "heldout_s_fixed": t_fixed}

@@ -6,13 +6,13 @@ checker for the CUDA forward / backward / Adam kernels in
 ``laplace_fmm_b200/csrc/mlp.cu``: same parameter layout, same masked
 mean-squared-error loss, same Adam update with bias correction.
 
-Layout (floats): W1[64][16] b1[64] W2[64][64] b2[64] W3[6][64] b3[6].
+Layout (floats): W1[64][16] b1[64] W2[64][64] b2[64] W3[14][64] b3[14].
 """
 from __future__ import annotations
 
 import numpy as np
 
-F, H, O = 16, 64, 6
+F, H, O = 16, 64, 14
 SHAPES = [("W1", (H, F)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (O, H)), ("b3", (O,))]
 NPARAM = sum(int(np.prod(s)) for _, s in SHAPES)
 

@@ -66,10 +66,11 @@ def test_learned_batch_within_tolerance(ctx, problems):
         pytest.skip("trained network not present")
     solver = LearnedSolver(ctx=ctx)
     out, info = solver.solve_batch(problems, tol=1e-6, tree_depth=8, check_targets=64)
-    assert 5 <= info["order_N"] <= 15 and info["checked_error"] <= 1e-6
+    assert 5 <= info["order_N"] <= 18
+    assert info["checked_error"] <= 1e-6 and info["checked_error_field"] <= 1e-6
     ref = solve_batch(problems, N=info["order_N"], tree_depth=8, max_leaf=64, ctx=ctx)
-    for (pos, q), (pot, fld), (rp, rf) in zip(problems, out, ref):
-        if len(pos) < 2:
+    for k, ((pos, q), (pot, fld), (rp, rf)) in enumerate(zip(problems, out, ref)):
+        if len(pos) < 2 or info["fp64_resolved"]:
             continue
         assert rel_l2(noself(pot, q), noself(rp, q)) < 1e-12
         assert rel_l2(fld, rf) < 1e-12

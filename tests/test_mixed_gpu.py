@@ -49,8 +49,9 @@ def test_mixed_source_target(ctx):
     assert rel_l2(b.forces, a.forces) < MIXED_TOL
 
 
-def test_mixed_rejects_high_order(ctx):
-    from laplace_fmm_b200 import LfmmError
-    src, q = uniform3d(1000, seed=1)
-    with pytest.raises(LfmmError):
-        FastMultipole3d((src, q), N=16, tree_depth=3, precision="mixed")
+def test_mixed_clamps_the_order_like_the_reference(ctx):
+    """N above 18 runs at 18, as the reference clamps it (common/defs.h:31)."""
+    src, q = uniform3d(3000, seed=1)
+    a = FastMultipole3d((src, q), N=25, tree_depth=3, precision="mixed")
+    b = FastMultipole3d((src, q), N=18, tree_depth=3, precision="mixed")
+    assert np.array_equal(a.potentials, b.potentials) and np.array_equal(a.forces, b.forces)

@@ -18,7 +18,7 @@ def _batch(n, seed):
 def test_oracle_gradient_matches_finite_differences():
     X, T, M = _batch(37, 1)
     p = om.init(3).astype(np.float64)
-    p[om.NPARAM - 6:] = 0.1
+    p[om.NPARAM - om.O:] = 0.1
     _, g = om.loss_and_grad(p, X, T, M)
     rng = np.random.default_rng(2)
     for i in rng.choice(om.NPARAM, 40, replace=False):
@@ -45,7 +45,7 @@ def test_forward_matches_oracle(ctx, n):
     from laplace_fmm_b200.order import OrderMLP
     X, _, _ = _batch(n, n)
     p = om.init(n)
-    p[-6:] = 0.3
+    p[-om.O:] = 0.3
     net = OrderMLP(p, ctx=ctx)
     Y = net.forward(X, normalised=True)
     ref = om.forward(p, X)

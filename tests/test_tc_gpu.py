@@ -40,7 +40,7 @@ def noself(p, q):
     return p - q * 1e4
 
 
-@pytest.mark.parametrize("N", [13, 9, 7, 11, 14, 15])
+@pytest.mark.parametrize("N", [13, 9, 7, 11, 14, 15, 16])
 def test_tc_engine_uniform(tc, simt, ctx, N):
     src, q = uniform3d(262144, seed=40 + N)
     a = FastMultipole3d((src, q), N=N, tree_depth=6, precision="mixed", ctx=tc)
@@ -62,10 +62,11 @@ def test_tc_shifts_keep_fp32_accuracy(tc, ctx):
     assert rel_l2(noself(a.potentials, q), noself(c.potentials, q)) < 5e-7
 
 
-def test_tc_engine_adaptive(tc, ctx):
+@pytest.mark.parametrize("N", [13, 16])
+def test_tc_engine_adaptive(tc, ctx, N):
     src, q = plummer_mix3d(400000, seed=41)
-    a = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, precision="mixed", ctx=tc)
-    c = FastMultipole3d((src, q), N=13, tree_depth=10, max_leaf=64, ctx=ctx)
+    a = FastMultipole3d((src, q), N=N, tree_depth=10, max_leaf=64, precision="mixed", ctx=tc)
+    c = FastMultipole3d((src, q), N=N, tree_depth=10, max_leaf=64, ctx=ctx)
     assert rel_l2(noself(a.potentials, q), noself(c.potentials, q)) < TOL
     assert rel_l2(a.forces, c.forces) < TOL
 
