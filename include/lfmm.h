@@ -213,6 +213,34 @@ int lfmm_tree_list_sizes(lfmm_ctx* ctx, int level, long long* n_close, long long
 int lfmm_tree_lists(lfmm_ctx* ctx, int level, long long* close, long long* far);
 int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
 
+/* ---- adaptive tree inspection (no counterpart in the reference, which
+ * builds only the uniform tree) -------------------------------------------
+ * lfmm_tree_build_adaptive builds the adaptive octree the solver uses
+ * (host input buffers as lfmm_tree_build, 3D; tree_depth levels at most,
+ * cells split while they hold more than max_leaf particles) with its U, W,
+ * X lists and the V lists the M2L slot tables give, and keeps it in the
+ * context until the next tree or solve call.  *n_cells, *n_leaves, and
+ * list_sizes[4] = the entries of U, W, X, V.  Cells are numbered globally,
+ * level by level.  lfmm_tree_adaptive_cells reads (any may be NULL) per
+ * cell: level, Morton code at its level, parent (-1 for the root),
+ * particle range [pbeg, pend) in tree order and its sources [pbeg, send)
+ * (leaves; sources first), leaf flag; the leaves' cell indices
+ * (n_leaves); positions[i] = tree position of input particle i (targets
+ * first, then sources).  lfmm_tree_adaptive_lists reads one list kind in
+ * CSR form: kind 0 U (rows = leaves in the order of the leaves array:
+ * adjacent leaves of any level, the leaf itself excluded; P2P), 1 W (rows =
+ * leaves: cells whose multipole is evaluated at the leaf's targets; M2P),
+ * 2 X (rows = cells: leaves whose sources form the cell's local expansion;
+ * P2L), 3 V (rows = cells: M2L sources); off has rows + 1 entries, idx
+ * holds global cell indices. */
+int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                             const double* tgt_xyz, int tree_depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
+                             size_t* list_sizes);
+int lfmm_tree_adaptive_cells(lfmm_ctx* ctx, int* level, unsigned long long* code, long long* parent,
+                             long long* pbeg, long long* pend, long long* send, unsigned char* is_leaf,
+                             long long* leaves, long long* positions);
+int lfmm_tree_adaptive_lists(lfmm_ctx* ctx, int kind, long long* off, long long* idx);
+
 /* ---- direct sum without allocation (no counterpart in the reference) -----
  * Same result as lfmm3d_direct_device, but the call allocates no device
  * memory: its source-chunk scratch is a static device array of

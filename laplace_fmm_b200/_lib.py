@@ -26,6 +26,7 @@ EXPORTS = [
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
     "lfmm3d_direct_device_noalloc",
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
+    "lfmm_tree_build_adaptive", "lfmm_tree_adaptive_cells", "lfmm_tree_adaptive_lists",
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
     "lfmm3d_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
@@ -113,6 +114,9 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_tree_list_sizes.argtypes = [P, I, P, P]
         L.lfmm_tree_lists.argtypes = [P, I, P, P]
         L.lfmm_tree_positions.argtypes = [P, P]
+        L.lfmm_tree_build_adaptive.argtypes = [P, SZ, P, P, SZ, P, I, I, P, P, P]
+        L.lfmm_tree_adaptive_cells.argtypes = [P, P, P, P, P, P, P, P, P, P]
+        L.lfmm_tree_adaptive_lists.argtypes = [P, I, P, P]
         L.lfmm_wignerd_slot.argtypes = [P, I, ctypes.POINTER(D), P]
         L.lfmm_mlp_forward.argtypes = [P, P, I, P, P]
         L.lfmm_mlp_grad.argtypes = [P, P, I, P, P, P, P, P, ctypes.POINTER(ctypes.c_float)]

@@ -5,6 +5,7 @@
 #include "fmm2d.cuh"
 #include "direct.cuh"
 #include "learned.cuh"
+#include "m2l_gemm.cuh"
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -15,6 +16,9 @@ struct lfmm_ctx {
 	lfmm::Context c;
 	lfmm::DevTree tree;
 	bool has_tree = false;
+	// adaptive tree inspection: the V lists of every cell (global indices,
+	// CSR), read from the M2L slot tables when the tree is built
+	std::vector<long long> v_off, v_idx;
 };
 
 namespace lfmm {
@@ -861,6 +865,120 @@ int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions)
 	std::vector<uint32_t> orig(t.n);
 	if ((st = fetch(c, orig.data(), t.orig, t.n))) return st;
 	for (size_t s = 0; s < t.n; ++s) positions[orig[s]] = (long long)s;
+	return LFMM_OK;
+}
+
+int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+                             const double* tgt, int depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
+                             size_t* list_sizes)
+{
+	if (!ctx || max_leaf < 0) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return LFMM_ERR_ARG; }
+	if ((ns && !src) || (nt && !tgt)) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
+	c.arena.reset();
+	ctx->has_tree = false;
+	ctx->v_off.clear();
+	ctx->v_idx.clear();
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	if (!dsrc || !dq || !dtgt) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+		if (q) LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+		else LFMM_CUDA(c, cudaMemsetAsync(dq, 0, sizeof(double) * ns, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+	ParticleInput in;
+	in.dim = 3; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
+	DevTree& t = ctx->tree;
+	int st = tree_build_adaptive(c, in, resolve_depth(3, depth, ns + nt), max_leaf, t);
+	if (st || (st = check_flags(c))) return st;
+	// V lists: the M2L slot table of every level (what the solver's M2L reads)
+	ctx->v_off.assign(t.ncells + 1, 0);
+	std::vector<std::vector<long long>> per(t.ncells);
+	for (int L = 2; L < t.depth; ++L) {
+		if (!t.lsize[L]) continue;
+		const size_t mark = c.arena.mark();
+		M2LPlan plan;
+		if ((st = m2l_plan_build(c, t, L, plan)) || (st = check_flags(c))) return st;
+		std::vector<int32_t> vt(t.lsize[L] * (size_t)M2L_SLOTS);
+		if ((st = fetch(c, vt.data(), plan.vtab, vt.size()))) return st;
+		c.arena.rewind(mark);
+		for (size_t k = 0; k < t.lsize[L]; ++k)
+			for (int sl = 0; sl < M2L_SLOTS; ++sl) {
+				const int32_t v = vt[k * M2L_SLOTS + sl];
+				if (v >= 0) per[t.loff[L] + k].push_back((long long)(t.loff[L] + (size_t)v));
+			}
+	}
+	for (size_t g = 0; g < t.ncells; ++g) {
+		ctx->v_off[g + 1] = ctx->v_off[g] + (long long)per[g].size();
+		ctx->v_idx.insert(ctx->v_idx.end(), per[g].begin(), per[g].end());
+	}
+	ctx->has_tree = true;
+	if (n_cells) *n_cells = t.ncells;
+	if (n_leaves) *n_leaves = t.nleaves;
+	if (list_sizes) {
+		list_sizes[0] = t.n_u; list_sizes[1] = t.n_w; list_sizes[2] = t.n_x; list_sizes[3] = ctx->v_idx.size();
+	}
+	return LFMM_OK;
+}
+
+int lfmm_tree_adaptive_cells(lfmm_ctx* ctx, int* level, unsigned long long* code, long long* parent,
+                             long long* pbeg, long long* pend, long long* send, unsigned char* is_leaf,
+                             long long* leaves, long long* positions)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	if (!ctx->has_tree || !t.adaptive) { c.last_error = "no adaptive tree: call lfmm_tree_build_adaptive first"; return LFMM_ERR_ARG; }
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	const size_t C = t.ncells;
+	int st;
+	std::vector<uint8_t> lv(C);
+	if ((st = fetch(c, lv.data(), t.lev, C))) return st;
+	if (level) for (size_t g = 0; g < C; ++g) level[g] = lv[g];
+	if (code && (st = fetch(c, code, t.code, C))) return st;
+	if (parent) {
+		std::vector<int32_t> p(C);
+		if ((st = fetch(c, p.data(), t.parent, C))) return st;
+		for (size_t g = 0; g < C; ++g) parent[g] = lv[g] ? (long long)(t.loff[lv[g] - 1] + (size_t)p[g]) : -1;
+	}
+	if (pbeg && (st = fetch(c, pbeg, t.pbeg, C))) return st;
+	if (pend && (st = fetch(c, pend, t.pend, C))) return st;
+	if (send && (st = fetch(c, send, t.send, C))) return st;
+	if (is_leaf && (st = fetch(c, is_leaf, t.is_leaf, C))) return st;
+	if (leaves && (st = fetch(c, leaves, t.leaves, t.nleaves))) return st;
+	if (positions) {
+		std::vector<uint32_t> orig(t.n);
+		if ((st = fetch(c, orig.data(), t.orig, t.n))) return st;
+		for (size_t p = 0; p < t.n; ++p) positions[orig[p]] = (long long)p;
+	}
+	return LFMM_OK;
+}
+
+int lfmm_tree_adaptive_lists(lfmm_ctx* ctx, int kind, long long* off, long long* idx)
+{
+	if (!ctx || kind < 0 || kind > 3) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	DevTree& t = ctx->tree;
+	if (!ctx->has_tree || !t.adaptive) { c.last_error = "no adaptive tree: call lfmm_tree_build_adaptive first"; return LFMM_ERR_ARG; }
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (kind == 3) {
+		if (off) std::copy(ctx->v_off.begin(), ctx->v_off.end(), off);
+		if (idx) std::copy(ctx->v_idx.begin(), ctx->v_idx.end(), idx);
+		return LFMM_OK;
+	}
+	const uint32_t* o = kind == 0 ? t.u_off : kind == 1 ? t.w_off : t.x_off;
+	const int32_t* ix = kind == 0 ? t.u_idx : kind == 1 ? t.w_idx : t.x_idx;
+	const size_t rows = kind == 2 ? t.ncells : t.nleaves;
+	const size_t total = kind == 0 ? t.n_u : kind == 1 ? t.n_w : t.n_x;
+	int st;
+	if (off && (st = fetch(c, off, o, rows + 1))) return st;
+	if (idx && (st = fetch(c, idx, ix, total))) return st;
 	return LFMM_OK;
 }
 

@@ -82,3 +82,36 @@ def assert_trees_equal(a, b, n, exact_positions=True, check_far=True):
         for (sa, ta), (sb_, tb_) in zip(ma, mb):
             np.testing.assert_array_equal(sa, sb_)
             np.testing.assert_array_equal(ta, tb_)
+
+
+def gpu_adaptive_tree(ctx, pts, q, depth, max_leaf, targets=None):
+    """Build the adaptive tree on the GPU and read its cells and U / W / X / V
+    lists back (CSR, global cell indices), in the layout of oracle/adaptive.py."""
+    L = ctx.lib
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    nt = 0 if targets is None else len(targets)
+    tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.float64)
+    nc, nl = ctypes.c_size_t(), ctypes.c_size_t()
+    sizes = np.zeros(4, np.uint64)
+    ctx.check(L.lfmm_tree_build_adaptive(ctx.handle, len(pts), ptr(pts), ptr(q), nt, ptr(tg), depth, max_leaf,
+                                         ctypes.byref(nc), ctypes.byref(nl), ptr(sizes)), "tree_build_adaptive")
+    C, NL = nc.value, nl.value
+    level = np.zeros(C, np.int32)
+    code = np.zeros(C, np.uint64)
+    parent, pbeg, pend, send = (np.zeros(C, np.int64) for _ in range(4))
+    leaf = np.zeros(C, np.uint8)
+    leaves = np.zeros(NL, np.int64)
+    pos = np.zeros(len(pts) + nt, np.int64)
+    ctx.check(L.lfmm_tree_adaptive_cells(ctx.handle, ptr(level), ptr(code), ptr(parent), ptr(pbeg), ptr(pend),
+                                         ptr(send), ptr(leaf), ptr(leaves), ptr(pos)), "adaptive_cells")
+    lists = {}
+    for kind, name in enumerate("UWXV"):
+        rows = NL if kind < 2 else C
+        off = np.zeros(rows + 1, np.int64)
+        idx = np.zeros(int(sizes[kind]), np.int64)
+        ctx.check(L.lfmm_tree_adaptive_lists(ctx.handle, kind, ptr(off), ptr(idx)), "adaptive_lists")
+        lists[name] = [np.sort(idx[off[r]:off[r + 1]]) for r in range(rows)]
+    cells = dict(level=level.astype(np.int64), code=code, parent=parent, pbeg=pbeg, pend=pend,
+                 is_leaf=leaf.astype(bool), leaves=leaves)
+    return cells, lists, send, pos

@@ -73,3 +73,40 @@ def test_adaptive_single_leaf_is_direct(ctx):
     f = FastMultipole3d((src, q), N=5, tree_depth=6, max_leaf=5000)
     pe, fe = direct(src, q, np.arange(3000))
     assert rel_l2(f.potentials, pe) < 1e-6 and rel_l2(f.forces, fe) < 1e-6
+
+
+@pytest.mark.parametrize("kind,n,depth,max_leaf", [("plummer", 20000, 10, 64), ("plummer", 4000, 8, 16),
+                                                   ("gaussian", 12000, 9, 64), ("uniform", 3000, 5, 16)])
+def test_adaptive_lists_match_the_restatement(ctx, oracle, kind, n, depth, max_leaf):
+    """The GPU's adaptive cells equal the CPU restatement's (built from the
+    oracle's uniform tree): levels, codes, parents, particle ranges, leaf
+    flags; its U, W, X lists and the V lists of its M2L slot tables equal the
+    restatement's as sets, row by row; and on the GPU's own lists every
+    (target leaf, source particle) pair is covered exactly once."""
+    from helpers import gpu_adaptive_tree
+    from laplace_fmm_b200.workloads import gaussian_mix3d
+    from oracle import adaptive as A
+    gen = {"plummer": plummer_mix3d, "gaussian": gaussian_mix3d, "uniform": uniform3d}[kind]
+    pos, q = gen(n, seed=170 + depth)
+    cells, lists, send, _ = gpu_adaptive_tree(ctx, pos, q, depth, max_leaf)
+    ref = A.adaptive_from_uniform(oracle.tree(3, pos, q, depth, halved=False), max_leaf)
+    for key in ("level", "code", "parent", "pbeg", "pend", "is_leaf", "leaves"):
+        np.testing.assert_array_equal(cells[key], ref[key], err_msg=key)
+    R = A.lists(ref)
+    for name in "UWXV":
+        assert len(lists[name]) == len(R[name])
+        for r, (a, b) in enumerate(zip(lists[name], R[name])):
+            np.testing.assert_array_equal(a, b, err_msg=f"{name} row {r}")
+    cells["coords"] = ref["coords"]
+    A.assert_covered_once(cells, lists, n, send)
+
+
+def test_adaptive_lists_with_targets_cover_every_source(ctx):
+    """Separate targets (zero charges) share the leaves with sources; the
+    lists still account once for every (target leaf, source) pair."""
+    from helpers import gpu_adaptive_tree
+    from oracle import adaptive as A
+    src, q = plummer_mix3d(6000, seed=181)
+    tgt = np.random.default_rng(182).random((2000, 3))
+    cells, lists, send, _ = gpu_adaptive_tree(ctx, src, q, 9, 32, targets=tgt)
+    A.assert_covered_once(cells, lists, 8000, send)
