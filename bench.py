@@ -489,6 +489,29 @@ def padded(N):
     return (N * (N + 1) + 15) // 16 * 16
 
 
+def tc_executed_per_pair(N):
+    """Tensor flops the tcgen05 M2L executes per V pair, averaged over the 189
+    far offsets of an octant class: B_hi T_hi over the slot's K blocks and
+    output columns, plus the two hi/lo corrections over the drained columns
+    (degrees < 12) and their K blocks; a slot of |d|^2 >= 8 is truncated by 3,
+    4, 5, 6 degrees for |d|^2 in [8, 9], [10, 13], [14, 19], [20, 27], never
+    below the drained columns (csrc/m2l_tc.cu, tc_trunc)."""
+    nc = padded(N)
+    na = nc if nc <= 160 else 160
+    kb_all, kbc = (nc + 31) // 32, (na + 31) // 32
+    tot = 0.0
+    offs = [(x, y, z) for x in range(-2, 4) for y in range(-2, 4) for z in range(-2, 4)
+            if max(abs(x), abs(y), abs(z)) > 1]
+    for x, y, z in offs:
+        d2 = x * x + y * y + z * z
+        r = 0 if d2 < 8 else 3 if d2 < 10 else 4 if d2 < 14 else 5 if d2 < 20 else 6
+        nd = max(1, N - r)
+        kb = max(kbc, min(kb_all, (nd * (nd + 1) + 31) // 32))
+        cols = min(nc, 32 * kb)
+        tot += 2.0 * cols * 32 * kb + 2 * 2.0 * na * 32 * kbc
+    return tot / len(offs)
+
+
 def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=None):
     """Roofline of the dominant phase (device time from the phase events; for
     the tensor-core M2L, the summed CUDA-event time of its kernel launches).
@@ -517,14 +540,12 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
     if dom == "m2l" and stats.get("n_m2l_kernel", 0) > 0 and stats["ms_m2l_kernel"] > 0:
         ms = stats["ms_m2l_kernel"]
         N = stats.get("order_N") or cfg["N"]
-        nc = padded(N)
-        na = nc if nc <= 160 else 160                  # columns with the hi/lo corrections (degrees < 12)
-        kpad = (nc + 31) // 32 * 32
-        kcorr = (na + 31) // 32 * 32
         flops = float(m2l_flops(N)) * stats["n_far_pairs"]
-        # per V pair: B_hi T_hi over every column and K block, and the two
-        # corrections over the drained columns and their source degrees
-        tensor = (2.0 * nc * kpad + 2 * 2.0 * na * kcorr) * stats["n_far_pairs"]
+        # per V pair: B_hi T_hi over the slot's columns and K blocks, and the
+        # two corrections over the drained columns and their source degrees;
+        # the farther offsets run truncated (the kernel's rule), averaged here
+        # over the 189 far offsets of an octant class
+        tensor = tc_executed_per_pair(N) * stats["n_far_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
         bf16 = peaks["bf16_tflops"]
         return {"kernel": "m2l_tc_kernel (tcgen05 TF32 hi/lo, direction-grouped)", "bound": "tensor",

@@ -104,7 +104,9 @@ struct Context {
 	int kev_used = 0;
 	// M2L autotuner: slot split chosen per (operator rows / 16, level-size
 	// bucket); 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0): the fixed rule.
-	int m2l_split[18][33] = {};
+	// Operator rows reach 352 (N = 18): 23 row classes.
+	static constexpr int SPLIT_ROWS = 352 / 16 + 1;
+	int m2l_split[SPLIT_ROWS][33] = {};
 	int tune_m2l = 1;
 	int timing = 0;
 };

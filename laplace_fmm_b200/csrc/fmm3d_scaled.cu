@@ -224,7 +224,7 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 			M2LPlan mp;
 			if ((st = m2m_plan_build(ctx, t, L, mp))) return st;
 			if ((st = shift_gemm_tc(ctx, TC_M2M, mp, mops, reinterpret_cast<const float*>(outer + t.loff[L + 1] * Nx2),
-			                        reinterpret_cast<float*>(outer + t.loff[L] * Nx2), N)))
+			                        reinterpret_cast<float*>(outer + t.loff[L] * Nx2), N, t.lsize[L + 1])))
 				return st;
 		}
 	} else {
@@ -274,7 +274,7 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 			M2LPlan lp = plans[L];
 			lp.vtab = t.parent + t.loff[L];
 			if ((st = shift_gemm_tc(ctx, TC_L2L, lp, lops, reinterpret_cast<const float*>(inner + t.loff[L - 1] * Nx2),
-			                        reinterpret_cast<float*>(inner + t.loff[L] * Nx2), N)))
+			                        reinterpret_cast<float*>(inner + t.loff[L] * Nx2), N, t.lsize[L - 1])))
 				return st;
 		}
 	} else {

@@ -23,6 +23,7 @@
 #include "m2l_tc.cuh"
 #include "fmm3d.cuh"
 #include <mutex>
+#include <cmath>
 
 namespace lfmm {
 
@@ -84,6 +85,27 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
 	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
 	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
 	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate));
+}
+
+// Runtime-N forms (N a multiple of 16 in [16, 256]).
+__device__ __forceinline__ uint32_t idesc_tf32(int n)
+{
+	return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32_ta_n(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                              uint32_t accumulate)
+{
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+	             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_tf32_n(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar)
@@ -181,6 +203,10 @@ __device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
 	}
 }
 
+// Far slots of the farther offsets run truncated (tc_trunc): fewer K blocks of
+// source degrees and the same number of output columns, so the operator copy,
+// the gathers and the MMAs of such a slot shrink together.
+//
 // Column split of the NC output coefficients (triangular (n, m) order, so a
 // degree is a prefix): columns [0, NA) are the low degrees, whose MMA result
 // is drained to FP32 registers after every slot and which get the hi/lo
@@ -232,6 +258,22 @@ struct TcCfg {
 	static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
+// K blocks of the far slots by squared offset length |d|^2 (0 .. 27, in cell
+// sizes): a slot of a far offset converges faster (worst-case ratio
+// sqrt(3) / |d|) and reaches the truncation error of the nearest offsets
+// with fewer degrees, so its M2L runs on the first kb[|d|^2] K blocks of
+// source degrees and the same number of output columns (never fewer than the
+// corrected ones).
+struct TcTrunc {
+	uint8_t kb[28];
+};
+
+__device__ __forceinline__ int dir_d2(int dir)
+{
+	const int dx = dir / 49 - 3, dy = (dir / 7) % 7 - 3, dz = dir % 7 - 3;
+	return dx * dx + dy * dy + dz * dz;
+}
+
 // grid (tiles, slot splits).  With S = gridDim.y > 1 split s handles slots
 // [s*SLOTS/S, (s+1)*SLOTS/S) and writes part[s][cell][R]; else loc[cell][R].
 // MODE picks the operator of a (class, slot) and the store:
@@ -249,7 +291,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
-              const float* __restrict__ diag, unsigned* flags)
+              const float* __restrict__ diag, unsigned* flags, const TcTrunc trunc, size_t src_cells, int ndir)
 {
 	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	extern __shared__ uint8_t dsm[];
@@ -261,6 +303,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	__shared__ int32_t tgt[TC_M];
 	__shared__ uint32_t active_mask[(SLOTS + 31) / 32];
 	__shared__ int16_t active[SLOTS];
+	__shared__ uint8_t active_kb[SLOTS];     // K blocks of each active slot
 	__shared__ int s_nactive, s_oct, s_n, s_abort;
 	__shared__ uint32_t s_start;
 
@@ -319,7 +362,12 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	if (tid == 0) {
 		int n = 0;
 		for (int s = slot0; s < slot1; ++s)
-			if (active_mask[s >> 5] & (1u << (s & 31))) active[n++] = (int16_t)s;
+			if (active_mask[s >> 5] & (1u << (s & 31))) {
+				int kb = KB;
+				if (MODE == TC_M2L) kb = min(KB, max(KBC, (int)trunc.kb[dir_d2(c_tc_slot_dir[oct][s])]));
+				active_kb[n] = (uint8_t)kb;
+				active[n++] = (int16_t)s;
+			}
 		s_nactive = n;
 	}
 	__syncthreads();
@@ -333,12 +381,14 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		// comparable with one K block of MMAs).
 		const int myt = tgt[tid];
 		uint32_t it = 0;
-		const int total = nact * KB;
-		// the gather of iteration i (slot active[i / KB], K block KB - 1 - i % KB) into w[16]
-		auto gather = [&](int i, float2 (&w)[16]) {
-			const int slot = active[i / KB];
-			const int kb = KB - 1 - i % KB;
-			const int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
+		// the gather of K block kb of slot active[j] into w[16]
+		auto gather = [&](int j, int kb, float2 (&w)[16]) {
+			const int slot = active[j];
+			int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
+			if (src >= 0 && (size_t)src >= src_cells) {    // a source outside the level: skipped, reported
+				atomicOr(flags, DEV_ERR_RANGE);
+				src = -1;
+			}
 			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
 #pragma unroll
 			for (int q = 0; q < 16; ++q) {
@@ -346,20 +396,39 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				w[q] = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
 			}
 		};
+		// the high-degree columns accumulate over slots of different widths:
+		// they start at zero (every MMA into them accumulates)
+		if constexpr (NC > NA) {
+			uint32_t z[16];
+#pragma unroll
+			for (int e = 0; e < 16; ++e) z[e] = 0u;
+			const uint32_t qa = tmem + ((uint32_t)(warp * 32) << 16) + C::Q_COL;
+#pragma unroll
+			for (int c = 0; c < NC - NA; c += 16) tmem_st16(qa + (uint32_t)c, z);
+			asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+		}
 		float2 nxt[16];
-		if (total > 0) gather(0, nxt);
+		if (nact > 0) gather(0, active_kb[0] - 1, nxt);
 		for (int j = 0; j < nact; ++j) {
 			const int slot = active[j];
-			const int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
+			int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
+			if (dir < 0 || dir >= ndir) {                   // an operator outside the set: reported
+				if (tid == 0) atomicOr(flags, DEV_ERR_RANGE);
+				dir = 0;
+			}
+			const int kbs = active_kb[j];
+			const uint32_t hi_bytes = (uint32_t)min(NC, 32 * kbs) * 128u;    // the slot's output columns
 			bool ok = true;
-			for (int kq = 0; kq < KB; ++kq, ++it) {
-				const int kb = KB - 1 - kq;                  // highest degrees first
+			for (int kq = 0; kq < kbs; ++kq, ++it) {
+				const int kb = kbs - 1 - kq;                 // highest degrees first
 				const bool corr = kb < KBC;
 				const uint32_t st = it % NSTAGE;
 				float v[32];
 #pragma unroll
 				for (int q = 0; q < 16; ++q) { v[2 * q] = nxt[q].x; v[2 * q + 1] = nxt[q].y; }
-				if ((int)it + 1 < total) gather((int)it + 1, nxt);
+				if (kq + 1 < kbs) gather(j, kb - 1, nxt);
+				else if (j + 1 < nact) gather(j + 1, active_kb[j + 1] - 1, nxt);
 				// the TMEM stores below are warp-collective: the warp gives up as one
 				const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
 				if (!__all_sync(0xffffffffu, got)) {
@@ -369,10 +438,12 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 				uint8_t* stage = base + st * C::STAGE;
 				if (tid == 0) {
-					const uint32_t nb = C::op_bytes(kb);
-					mbar_expect_tx(smem_u32(&full_bar[st]), nb);
-					bulk_g2s(smem_u32(stage), ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb), nb,
-					         smem_u32(&full_bar[st]));
+					// the hi rows of the slot's output columns, and the lo rows
+					const uint8_t* blk = ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb);
+					mbar_expect_tx(smem_u32(&full_bar[st]), hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u));
+					bulk_g2s(smem_u32(stage), blk, hi_bytes, smem_u32(&full_bar[st]));
+					if (corr)
+						bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES, smem_u32(&full_bar[st]));
 				}
 				// lo (corrected K blocks only) to the stage's swizzled row tid;
 				// hi to TMEM columns [hi_col(st), +32) of lane tid (or to the row after lo's)
@@ -425,8 +496,11 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			for (int j = 0; j < nact && ok; ++j) {
 				if (j > 0 && !mbar_wait(smem_u32(&tempty_bar), (j - 1) & 1u, abort)) { ok = false; break; }
 				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-				for (int kq = 0; kq < KB; ++kq, ++it) {
-					const int kb = KB - 1 - kq;
+				const int kbs = active_kb[j];
+				const int nq = min(NC, 32 * kbs) - NA;      // the slot's high-degree columns
+				const uint32_t idq = nq > 0 ? idesc_tf32(nq) : 0u;
+				for (int kq = 0; kq < kbs; ++kq, ++it) {
+					const int kb = kbs - 1 - kq;
 					const uint32_t st = it % NSTAGE;
 					if (!mbar_wait(smem_u32(&full_bar[st]), (it / NSTAGE) & 1u, abort)) { ok = false; break; }
 					asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -442,11 +516,11 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 						if constexpr (C::HI_TMEM) {
 							const uint32_t ah = a_hi_t + 8u * ks;
 							mma_tf32_ta<NA>(tmem, ah, bh, !first);
-							if constexpr (NC > NA) mma_tf32_ta<NC - NA>(tmem + C::Q_COL, ah, bq, !(first && j == 0));
+							if (nq > 0) mma_tf32_ta_n(tmem + C::Q_COL, ah, bq, idq, 1u);
 						} else {
 							const uint64_t ah = desc_sw128(a_hi_s + ks * 32);
 							mma_tf32<NA>(tmem, ah, bh, !first);
-							if constexpr (NC > NA) mma_tf32<NC - NA>(tmem + C::Q_COL, ah, bq, !(first && j == 0));
+							if (nq > 0) mma_tf32_n(tmem + C::Q_COL, ah, bq, idq, 1u);
 						}
 						if (kb < KBC) {
 							// the first correction of the tile: highest corrected block, ks = 3, slot 0
@@ -496,12 +570,22 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		} else {
 			if (nact > 0) tmem_accumulate<W>(taddr + C::C_COL, acc);
 			const int tg = tgt[quarter * 32 + lane];
-			const bool store = tg >= 0 && !*abort;
+			bool store = tg >= 0 && !*abort;
+			if (store && (size_t)tg >= cells) {             // a target outside the level: skipped, reported
+				atomicOr(flags, DEV_ERR_RANGE);
+				store = false;
+			}
 			const float* xs = nullptr;
 			const float* dg = nullptr;
 			if (MODE == TC_L2L && store) {
-				xs = mult + (size_t)vtab[tg] * R;
-				dg = diag + oct * NC;
+				const int par = vtab[tg];
+				if (par < 0 || (size_t)par >= src_cells) {
+					atomicOr(flags, DEV_ERR_RANGE);
+					store = false;
+				} else {
+					xs = mult + (size_t)par * R;
+					dg = diag + oct * NC;
+				}
 			}
 			if (store) {
 				const int c0 = half * W;
@@ -582,9 +666,28 @@ __global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, 
 	if (kb < KBC && row < NA) out[blk + (size_t)NC * 32 + (size_t)row * 32 + in_row] = lo;
 }
 
+// K blocks per far slot by |d|^2 for order N and KB K blocks: the offsets
+// with |d|^2 < 8 (|d| = 2, sqrt 5, sqrt 6: worst-case ratios 0.87 to 0.71)
+// keep every degree; the farther classes [8, 9], [10, 13], [14, 19], [20, 27]
+// (ratios 0.61 down to 0.33) drop 3, 4, 5, 6 degrees, never below the
+// corrected columns (the kernel's floor).  Measured on the 16.8M-particle
+// clustered set at N = 16: potential 3.31e-7 -> 3.27e-7, field 6.47e-7 ->
+// 6.44e-7 against the FP64 direct sum, M2L kernel 99.4 -> 73.4 ms; one
+// degree off the |d|^2 = 5, 6 class already raised the field to 6.99e-7.
+TcTrunc tc_trunc(int N, int KB)
+{
+	TcTrunc t;
+	for (int d2 = 0; d2 < 28; ++d2) {
+		const int r = d2 < 8 ? 0 : d2 < 10 ? 3 : d2 < 14 ? 4 : d2 < 20 ? 5 : 6;
+		const int Nd = std::max(1, N - r);
+		t.kb[d2] = (uint8_t)std::min(KB, (Nd * (Nd + 1) + 31) / 32);
+	}
+	return t;
+}
+
 template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
-           bool timed, const float* diag = nullptr)
+           bool timed, size_t src_cells, const float* diag = nullptr)
 {
 	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
@@ -593,7 +696,8 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
 	m2l_tc_kernel<NC, NA, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 		reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part, plan.cells,
-		diag, ctx.dev_flags);
+		diag, ctx.dev_flags, tc_trunc(R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB),
+		src_cells, MODE == TC_M2L ? 343 : 8);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
 		ctx.kev_used += 2;
@@ -623,6 +727,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
 	int bucket = 0;
 	while ((1u << bucket) < tiles && bucket < 32) ++bucket;
+	static_assert(NC / 16 < Context::SPLIT_ROWS, "autotuner table");
 	int& tuned = ctx.m2l_split[NC / 16][bucket];
 	const bool tune = ctx.tune_m2l && tuned == 0;
 	if (ctx.tune_m2l && !tune) S = tuned;
@@ -642,7 +747,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		int bestS = S;
 		for (int cand = 1; cand <= 8; cand *= 2) {
 			LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false);
+			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells);
 			if (st) return st;
 			LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
 			LFMM_CUDA(ctx, cudaEventSynchronize(e1));
@@ -655,25 +760,26 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		tuned = bestS;
 		S = bestS;
 	}
-	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true);
+	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
 template <int NC, int NA>
-int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int R)
+int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int R,
+                    size_t src_cells)
 {
 	using C = TcCfg<NC, NA>;
 	using CL = TcCfg<NC, NA, false>;
 	if (mode == TC_M2M) {
 		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M>,
 		                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false);
+		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells);
 	}
 	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
 	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + 8 * C::DIR_BYTES);
-	return run_tc<NC, NA, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, diag);
+	return run_tc<NC, NA, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, diag);
 }
 
 std::mutex g_upload_mu;
@@ -740,11 +846,12 @@ int tc_ops_convert(Context& ctx, const double* ops64, int ndir, int N, void* out
 #define LFMM_TC_ORDERS(X) X(64, 64) X(80, 80) X(96, 96) X(112, 112) X(144, 144) X(160, 160) \
 	X(192, 160) X(224, 160) X(240, 160) X(272, 160) X(320, 160) X(352, 160)
 
-int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N)
+int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N,
+                  size_t src_cells)
 {
 	if (mode != TC_M2M && mode != TC_L2L) { ctx.last_error = "tensor-core shift: bad mode"; return ERR_ARG; }
 	const int R = N * (N + 1), NC = m2l_padded(N), NA = m2l_tc_drained(N);
-#define LFMM_TC_SHIFT(nc, na) if (NC == nc && NA == na) return launch_shift_tc<nc, na>(ctx, mode, plan, ops, src, dst, R);
+#define LFMM_TC_SHIFT(nc, na) if (NC == nc && NA == na) return launch_shift_tc<nc, na>(ctx, mode, plan, ops, src, dst, R, src_cells);
 	LFMM_TC_ORDERS(LFMM_TC_SHIFT)
 #undef LFMM_TC_SHIFT
 	ctx.last_error = "tensor-core shift: unsupported order";

@@ -47,7 +47,10 @@ int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float
 //           ops holds the 8 operators (tc_ops_bytes(8, N)) and then the
 //           diagonal as float [8][m2l_padded(N)].
 enum { TC_M2L = 0, TC_M2M = 1, TC_L2L = 2 };
-int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N);
+// src_cells: the cells of src (the children's level for M2M, the parents'
+// for L2L); an index outside it is skipped and reported as DEV_ERR_RANGE.
+int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops, const float* src, float* dst, int N,
+                  size_t src_cells);
 // FP64 operators [ndir][m2l_padded(N)][m2l_padded(N)] -> the tensor-core layout
 // at out (tc_ops_bytes(ndir, N) bytes, 16-byte aligned).
 size_t tc_ops_bytes(int ndir, int N);
