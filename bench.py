@@ -1,6 +1,7 @@
 """Benchmark: Mparticles/s of one FMM solve on one B200, with its accuracy.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c1|c2|c3] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c1|c2|c3|c5|c6]
+                    [--impl ours|reference|reference-gpu]
 
 A step is one full solve (tree build through outputs in input order) of the
 configuration's seeded synthetic particle set.  ``value`` times solves on
@@ -18,7 +19,11 @@ configuration (weak scaling, replicas), rank 0 prints the line.
 
 ``--impl reference`` times the reference's own CPU FMM (compiled from its
 sources into oracle/_ref) on the host cores, on a bounded sample of the same
-configuration; only rank 0 runs it.
+configuration; only rank 0 runs it.  ``--impl reference-gpu`` times the
+reference's own CUDA FMM (its unmodified sources built for sm_100a into
+oracle/_ref/libfmmref_gpu.so) on the same particles, with its uniform tree
+(the configuration's depth; ``--depth`` for the adaptive configurations), and
+states its accuracy against the FP64 direct sum.
 """
 from __future__ import annotations
 
@@ -86,7 +91,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the mixed one")
@@ -853,9 +858,74 @@ def run_vector(args, cfg):
     return 0
 
 
+def run_reference_gpu(args, cfg):
+    """The reference's CUDA FMM, timed per constructor call (its whole solve:
+    particles copied in, a device synchronisation after every kernel, results
+    copied out, so the wall time is its end-to-end time), and its accuracy at
+    the 4096 sampled targets against our GPU FP64 direct sum.  The reference
+    has only the uniform tree: the configuration's depth, or ``--depth`` for the
+    adaptive configurations (default 8)."""
+    from oracle.oracle import REF_GPU_SO, ReferenceGPU
+    from laplace_fmm_b200 import Context
+    from laplace_fmm_b200.workloads import rel_l2, sample_targets
+    if not REF_GPU_SO.exists():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference CUDA build (oracle/_ref/libfmmref_gpu.so) "
+                                                                  "is absent: make -C oracle ref-gpu"}))
+        return 0
+    if cfg.get("batch") or cfg.get("vector"):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference GPU path solves one scalar-charge "
+                                                                  "problem per call (fmm::gpu::FastMultipole3d<double>)"}))
+        return 0
+    dim = cfg["dim"]
+    adaptive = cfg.get("max_leaf", 0) > 0
+    depth = args.depth or (8 if adaptive else cfg["depth"])
+    pos, q = make_particles(cfg)
+    n = len(pos)
+    ref = ReferenceGPU()
+    fn = ref.fmm3d if dim == 3 else ref.fmm2d
+    secs = []
+    for k in range(args.warmup + args.steps):
+        pot, fld, sec = fn(pos, q, N=cfg["N"], depth=depth)
+        if k >= args.warmup:
+            secs.append(sec)
+    s = float(np.median(secs))
+    ctx = Context(0)
+    idx = sample_targets(n)
+    tgt = np.ascontiguousarray(pos[idx])
+    ep = np.zeros(len(idx)); ef = np.zeros((len(idx), dim))
+    direct = ctx.lib.lfmm3d_direct if dim == 3 else ctx.lib.lfmm2d_direct
+    vp = ctypes.c_void_p
+    ctx.check(direct(ctx.handle, n, pos.ctypes.data_as(vp), q.ctypes.data_as(vp), len(idx), tgt.ctypes.data_as(vp),
+                     ep.ctypes.data_as(vp), ef.ctypes.data_as(vp)), "direct")
+    ctx.close()
+    self_term = q[idx] * (1e4 if dim == 3 else np.log(1e-4))
+    acc = {"rel_l2_pot_noself": rel_l2(pot[idx] - self_term, ep - self_term), "rel_l2_pot": rel_l2(pot[idx], ep),
+           "rel_l2_field": rel_l2(fld[idx], ef), "targets": int(len(idx)),
+           "finite": bool(np.isfinite(pot).all() and np.isfinite(fld).all())}
+    v = n / s / 1e6
+    conf = base_config(cfg, 1)
+    conf.update(tree_depth=depth, tree="uniform", precision="fp64")
+    if adaptive:
+        conf["workload"] += f" [reference GPU: uniform octree depth {depth}, FP64, N = {cfg['N']}]"
+    print(json.dumps({"impl": "reference-gpu", "metric": cfg.get("metric", METRIC), "value": v,
+                      "unit": "Mparticles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic (seeded PCG64)", "config": conf, "accuracy": acc,
+                      "seconds_per_solve": secs,
+                      "what": "fmm::gpu::FastMultipole3d<double> / fmm::gpu::FastMultipole (unmodified reference "
+                              "CUDA sources, sm_100a, allocations zero-filled); wall time of the constructor",
+                      "e2e": {"value": v, "unit": "Mparticles/s", "h2d_bytes_per_step": int(n * (dim + 2) * 8),
+                              "d2h_bytes_per_step": int(n * (dim + 1) * 8)}}))
+    return 0
+
+
 def main():
     args = parse()
     cfg = args.cfg
+    if args.impl == "reference-gpu":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        return run_reference_gpu(args, cfg)
     if cfg.get("batch"):
         return run_batch(args, cfg)
     if cfg.get("vector") and args.impl == "ours":

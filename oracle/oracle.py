@@ -21,6 +21,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libfmm_oracle.so"
 REF_SO = HERE / "_ref" / "libfmmref.so"
+REF_GPU_SO = HERE / "_ref" / "libfmmref_gpu.so"
 AUTO = 2**31 - 1  # the reference's FMM_AUTO (std::numeric_limits<int>::max())
 
 _P = ctypes.c_void_p
@@ -324,6 +325,38 @@ class Reference:
             return _export_tree(self.lib, f"ref_tree{d}_", h, dim, depth, len(pts), None)
         finally:
             getattr(self.lib, f"ref_tree{d}_free")(h)
+
+
+class ReferenceGPU:
+    """The reference's own CUDA FMM (unmodified sources, built for sm_100a by
+    ``make -C oracle ref-gpu``; allocations zero-filled by the link, see
+    ref_gpu_wrapper.cu).  Timed as a comparison point; its outputs are not a
+    parity oracle (its M2L sums uninitialised work arrays)."""
+
+    def __init__(self, path: Path = REF_GPU_SO):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (needs the reference sources; make -C oracle ref-gpu)")
+        L = ctypes.CDLL(str(path))
+        self.lib = L
+        for f in ("ref_gpu_fmm3d", "ref_gpu_fmm2d"):
+            getattr(L, f).argtypes = [_SZ, _P, _P, _I, _I, _D, _P, _P, _P]
+            getattr(L, f).restype = _I
+        L.ref_gpu_set_verbose.argtypes = [_I]
+
+    def _solve(self, fn, dim, src, q, N, depth, eps):
+        src = _f64(src).reshape(-1, dim); q = _f64(q)
+        pot = np.zeros(len(src)); fld = np.zeros((len(src), dim)); sec = np.zeros(1)
+        rc = fn(len(src), _ptr(src), _ptr(q), int(N), int(depth), float(eps), _ptr(pot), _ptr(fld), _ptr(sec))
+        if rc != 0:
+            raise RuntimeError(f"reference GPU solve failed (status {rc})")
+        return pot, fld, float(sec[0])
+
+    def fmm3d(self, src, q, N=AUTO, depth=AUTO, eps=1e-8):
+        """(potential, field, seconds of the reference's constructor)"""
+        return self._solve(self.lib.ref_gpu_fmm3d, 3, src, q, N, depth, eps)
+
+    def fmm2d(self, src, q, N=AUTO, depth=AUTO, eps=1e-8):
+        return self._solve(self.lib.ref_gpu_fmm2d, 2, src, q, N, depth, eps)
 
 
 def rel_l2(x, ref):
