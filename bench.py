@@ -47,11 +47,13 @@ CONFIGS = {
     "c1": dict(dim=3, n=131072, gen="uniform3d", seed=12345, N=9, depth=5, precision="fp64",
                metric="3D FMM Mparticles/s, plain FP64 form at p=8",
                workload="3D uniform 131,072 particles, FP64, p=8 (N=9), uniform octree depth 5"),
-    # 2D clustered, 4,194,304 particles, p = 20 (N = 21), FP64
-    "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=11, precision="fp64",
-               metric="2D FMM Mparticles/s, FP64 at p=20",
+    # 2D clustered, 4,194,304 particles, p = 20 (N = 21), FP64, adaptive
+    # quadtree (<= 12 levels, <= 32 per leaf); the reference's uniform
+    # quadtree (depth 11) timed beside it
+    "c2": dict(dim=2, n=4194304, gen="clustered2d", seed=4242, N=21, depth=12, max_leaf=32, uniform_depth=11,
+               precision="fp64", metric="2D FMM Mparticles/s, FP64 at p=20",
                workload="2D half uniform / half 64 Gaussian clusters (sigma 0.005) 4,194,304 particles, FP64, "
-                        "p=20 (N=21), uniform quadtree depth 11"),
+                        "p=20 (N=21), adaptive quadtree (<=12 levels, <=32 per leaf)"),
     # 3D clustered, 16,777,216 particles (Plummer a = 0.05 + uniform), adaptive octree
     # mixed form at the order the network picks for rel-L2 <= 1e-6 on potential
     # and field (sampled check of 256 outputs judged on its upper confidence
@@ -73,6 +75,16 @@ CONFIGS = {
                         "cluster (sigma 0.05) each, mixed precision at the learned order for rel-L2 <= 1e-6 "
                         "(32 checked outputs per problem), adaptive octrees (<=10 levels, <=64 per leaf); "
                         "plain FP64 p=10 one problem at a time beside it"),
+    # learned order on the 64 held-out problems of the order network (1-8
+    # Gaussian clusters, N log-uniform in [1e4, 1e6]) at tol 1e-6 on potential
+    # and field, against the lowest single fixed order that meets tol on all 64
+    "c4": dict(dim=3, heldout=True, count=64, n=0, N=17, depth=10, max_leaf=64, precision="mixed", learned=True,
+               tol=1e-6, check_targets=256,
+               metric="3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: learned order vs best fixed order",
+               workload="learned order, 3D: the 64 held-out problems (1-8 Gaussian clusters, sigma log-uniform in "
+                        "[0.005, 0.2], N log-uniform in [1e4, 1e6]), mixed precision, adaptive octrees (<=10 levels, "
+                        "<=64 per leaf), tol 1e-6 on potential and field; the lowest fixed order meeting tol on all 64 "
+                        "beside it"),
     # vector charges (the reference's FastMultipole3d<Vector3d>): 4,194,304 particles of the
     # clustered mixture, charges U(-1, 1)^3, mixed precision, N = 12, adaptive octree;
     # the FP64 form beside it
@@ -289,6 +301,15 @@ def launches_per_solve(depth, dim, radix_passes, adaptive, precision, learned=Fa
         leaves = 2 if precision == "mixed" else 1               # FP32: near field, then the expansions
         fmm = 1 + 1 + m2m + m2l + 1 + max(0, depth - 3) + leaves
         return (tree, fmm) if parts else tree + fmm + extra
+    if adaptive and dim == 2:
+        tree += depth + depth * (1 + scan) + depth + 1 + scan + 1 + 1 + lists + 2 + 2 + 3 * scan
+        # P2M, M2M per level, per M2L level: class count, scatter, slot table,
+        # Hankel M2L (+ a split reduction on the small levels); P2L, L2L adds,
+        # leaf work units (count + scan) and the leaves
+        levels = max(0, depth - 2)
+        split = sum(1 for L in range(2, depth) if 4 ** L < 37000)
+        fmm = 1 + (depth - 1) + 4 * levels + split + 1 + max(0, depth - 3) + 1 + scan + 1
+        return (tree, fmm) if parts else tree + fmm
     tree += lists
     if dim == 3:
         fmm = 1 + (depth - 1) + max(0, depth - 2) * 5 + max(0, depth - 3) + 1
@@ -335,9 +356,11 @@ def run_ours(args, cfg, rank, world, local_rank):
         from laplace_fmm_b200.order import load_params
         d_params = torch.from_numpy(load_params()).cuda()
 
-    def call(c, device, precision, stats=None, host=None):
+    def call(c, device, precision, stats=None, host=None, tree=None):
         """One solve through the C ABI (device buffers, or pinned host buffers);
-        the configuration's precision runs the learned solve when it has one."""
+        the configuration's precision runs the learned solve when it has one.
+        tree = (depth, max_leaf) overrides the configuration's tree."""
+        depth_, max_leaf_ = tree if tree else (depth, max_leaf)
         src, qq, pot, fld = host if host else (d_src, d_q, d_pot, d_fld)
         sp = ctypes.byref(stats) if stats is not None else None
         if dim == 3 and learned and precision == prec:
@@ -348,14 +371,17 @@ def run_ours(args, cfg, rank, world, local_rank):
                     vp(d_params.data_ptr()), cfg["tol"], cfg["check_targets"], vp(pot.data_ptr()),
                     vp(fld.data_ptr()), ctypes.byref(info), sp)
             info_box.update(info.as_dict())
-        elif dim == 3:
-            opts = LfmmSolveOpts(N, depth, max_leaf, precision, 1e-8)
-            fn = L.lfmm3d_solve_ex_device if device else L.lfmm3d_solve_ex
+        elif dim == 3 or max_leaf_ > 0:
+            opts = LfmmSolveOpts(N, depth_, max_leaf_, precision, 1e-8)
+            if dim == 3:
+                fn = L.lfmm3d_solve_ex_device if device else L.lfmm3d_solve_ex
+            else:
+                fn = L.lfmm2d_solve_ex_device if device else L.lfmm2d_solve_ex
             st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, ctypes.byref(opts),
                     vp(pot.data_ptr()), vp(fld.data_ptr()), sp)
         else:
             fn = L.lfmm2d_solve_device if device else L.lfmm2d_solve
-            st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, N, depth, 1e-8, precision,
+            st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, N, depth_, 1e-8, precision,
                     vp(pot.data_ptr()), vp(fld.data_ptr()), sp)
         c.check(st, "solve")
 
@@ -407,6 +433,24 @@ def run_ours(args, cfg, rank, world, local_rank):
         t1.synchronize()
         pms = t0.elapsed_time(t1) / reps
         plain = {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms, "precision": "fp64"}
+    # 2D: the reference's uniform quadtree on the same particles beside the adaptive one
+    if dim == 2 and max_leaf > 0 and cfg.get("uniform_depth") and not args.no_plain:
+        ut = (cfg["uniform_depth"], 0)
+        for _ in range(2):
+            call(ctx_t, True, prec, tree=ut)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t0.record()
+        for _ in range(reps):
+            call(ctx_t, True, prec, tree=ut)
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t1.record()
+        t1.synchronize()
+        pms = t0.elapsed_time(t1) / reps
+        plain = {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms, "precision": "fp64",
+                 "tree": f"uniform quadtree depth {cfg['uniform_depth']} (the reference's tree)"}
     ctx_t.close()
     # a solve plan at the same order: the tree and a CUDA graph built once,
     # charges changed per execution (device buffers)
@@ -598,7 +642,7 @@ def cpu_sample(cfg):
     tree).  Returns (stride, depth, description)."""
     if cfg["n"] <= 200000:
         return 1, cfg["depth"], "full problem"
-    d = max(3, cfg["depth"] - 3)
+    d = max(3, cfg.get("uniform_depth", cfg["depth"]) - 3)
     return 64, d, f"every 64th particle of the seeded set ({cfg['n'] // 64}), uniform depth {d}"
 
 
@@ -858,6 +902,153 @@ def run_vector(args, cfg):
     return 0
 
 
+def run_heldout(args, cfg):
+    """The learned order on the network's held-out problems: per problem the
+    learned solve (features, network, order, solve, sampled check and
+    fallback) and the solve at the lowest single fixed order that meets tol
+    on every one of them, both on device buffers and timed with CUDA events
+    on the solver's stream (the learned solve's host synchronisations count);
+    accuracy of both at up to 4096 sampled targets against the FP64 direct
+    sum.  value = all particles / the summed learned solve time."""
+    import torch
+    from laplace_fmm_b200 import Context
+    from laplace_fmm_b200._lib import PRECISION, LfmmLearnedInfo, LfmmSolveOpts
+    from laplace_fmm_b200.order import load_params
+    from laplace_fmm_b200.train_order import problem
+    from laplace_fmm_b200.workloads import rel_l2, sample_targets
+    probs = [problem(i, "heldout") for i in range(cfg["count"])]
+    ctx = Context(0)
+    L = ctx.lib
+    vp = ctypes.c_void_p
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    d_params = torch.from_numpy(load_params()).cuda()
+    prec, tol, depth, ml = PRECISION[cfg["precision"]], cfg["tol"], cfg["depth"], cfg["max_leaf"]
+    dev = []
+    for pos, q in probs:
+        n = len(pos)
+        idx = sample_targets(n)
+        ds, dq = torch.from_numpy(pos).cuda(), torch.from_numpy(q).cuda()
+        tgt = torch.from_numpy(np.ascontiguousarray(pos[idx])).cuda()
+        ep = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+        ef = torch.empty(len(idx), 3, dtype=torch.float64, device="cuda")
+        ctx.check(L.lfmm3d_direct_device(ctx.handle, n, vp(ds.data_ptr()), vp(dq.data_ptr()), len(idx),
+                                         vp(tgt.data_ptr()), vp(ep.data_ptr()), vp(ef.data_ptr())), "direct")
+        stream.synchronize()
+        self_t = q[idx] * 1e4
+        dev.append(dict(n=n, ds=ds, dq=dq, idx=idx, ep=ep.cpu().numpy() - self_t, ef=ef.cpu().numpy(), self_t=self_t,
+                        pot=torch.empty(n, dtype=torch.float64, device="cuda"),
+                        fld=torch.empty(n, 3, dtype=torch.float64, device="cuda")))
+    info = LfmmLearnedInfo()
+
+    def learned(d):
+        opts = LfmmSolveOpts(cfg["N"], depth, ml, prec, tol)
+        ctx.check(L.lfmm3d_solve_learned_device(ctx.handle, d["n"], vp(d["ds"].data_ptr()), vp(d["dq"].data_ptr()),
+                                                0, None, ctypes.byref(opts), vp(d_params.data_ptr()), tol,
+                                                cfg["check_targets"], vp(d["pot"].data_ptr()),
+                                                vp(d["fld"].data_ptr()), ctypes.byref(info), None), "learned")
+
+    def fixed(d, N):
+        opts = LfmmSolveOpts(N, depth, ml, prec, 1e-8)
+        ctx.check(L.lfmm3d_solve_ex_device(ctx.handle, d["n"], vp(d["ds"].data_ptr()), vp(d["dq"].data_ptr()), 0,
+                                           None, ctypes.byref(opts), vp(d["pot"].data_ptr()), vp(d["fld"].data_ptr()),
+                                           None), "fixed")
+
+    def errors(d):
+        stream.synchronize()
+        pot, fld = d["pot"].cpu().numpy()[d["idx"]], d["fld"].cpu().numpy()[d["idx"]]
+        return rel_l2(pot - d["self_t"], d["ep"]), rel_l2(fld, d["ef"])
+
+    # the lowest fixed order meeting tol (both outputs) on every problem
+    fixed_N = 18
+    for Nf in range(10, 19):
+        ok = True
+        for d in dev:
+            fixed(d, Nf)
+            ep_, ef_ = errors(d)
+            if max(ep_, ef_) > tol:
+                ok = False
+                break
+        if ok:
+            fixed_N = Nf
+            break
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            t0.record()
+        for _ in range(args.steps):
+            fn()
+        with torch.cuda.stream(stream):
+            t1.record()
+        t1.synchronize()
+        return t0.elapsed_time(t1) / args.steps
+
+    rows = []
+    with ClockSampler(0) as clk:
+        for d in dev:
+            tf = timed(lambda: fixed(d, fixed_N))
+            ef_fixed = errors(d)
+            tl = timed(lambda: learned(d))
+            el = errors(d)
+            rows.append(dict(n=d["n"], N=info.order_N, predicted_N=info.predicted_N, fallback=info.fallback,
+                             fp64=info.fp64_resolved, ms_learned=tl, ms_fixed=tf, err_pot=el[0], err_field=el[1],
+                             err_pot_fixed=ef_fixed[0], err_field_fixed=ef_fixed[1]))
+    ctx.close()
+    ntot = sum(r["n"] for r in rows)
+    tl, tf = sum(r["ms_learned"] for r in rows), sum(r["ms_fixed"] for r in rows)
+    big = [r for r in rows if r["n"] >= 100000]
+    line = {"metric": cfg["metric"], "value": ntot / (tl * 1e-3) / 1e6, "unit": "Mparticles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tl, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32", "data": "synthetic (seeded PCG64)",
+            "config": {"workload": cfg["workload"], "problems": len(rows), "particles": ntot,
+                       "tree_depth": depth, "max_leaf": ml, "precision": cfg["precision"], "tol": tol,
+                       "parallelism": "single GPU", "l2": "each problem's working set is below L2; no flush"},
+            "fixed_order": {"N_degrees": fixed_N, "value": ntot / (tf * 1e-3) / 1e6, "unit": "Mparticles/s",
+                            "ms_total": tf, "what": "lowest single fixed order meeting tol on all problems"},
+            "gain_vs_fixed": tf / tl,
+            "gain_vs_fixed_problems_over_1e5": (sum(r["ms_fixed"] for r in big) / sum(r["ms_learned"] for r in big)
+                                                if big else None),
+            "within_tol": sum(1 for r in rows if max(r["err_pot"], r["err_field"]) <= tol),
+            "max_err_pot": max(r["err_pot"] for r in rows), "max_err_field": max(r["err_field"] for r in rows),
+            "mean_N_learned": float(np.mean([r["N"] for r in rows])),
+            "fallbacks": sum(1 for r in rows if r["fallback"]), "fp64_reruns": sum(r["fp64"] for r in rows),
+            "per_problem": rows, "clocks": clk.summary(),
+            "e2e": None, "gpu_launches": None}
+    print(json.dumps(line))
+    return 0
+
+
+def run_heldout_reference(args, cfg):
+    """The reference's CPU FMM on the first held-out problems (a bounded
+    sample) at the fixed order N = 17 and its own automatic depth."""
+    from laplace_fmm_b200.train_order import problem
+    solver, kind = cpu_solver()
+    cores = os.cpu_count() or 1
+    solver.set_threads(cores)
+    probs = [problem(i, "heldout") for i in range(4)]
+    ntot, secs = 0, 0.0
+    for k in range(args.warmup + args.steps):
+        for pos, q in probs:
+            t0 = time.perf_counter()
+            solver.fmm3d(pos, q, N=cfg["N"])
+            if k >= args.warmup:
+                secs += time.perf_counter() - t0
+                ntot += len(pos)
+    v = ntot / secs / 1e6
+    sample = f"held-out problems 0-3 ({sum(len(p) for p, _ in probs)} particles), N = {cfg['N']}, the reference's depth"
+    print(json.dumps({"impl": "reference", "metric": cfg["metric"], "value": v, "unit": "Mparticles/s",
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": secs * 1e3 / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+                      "config": {"workload": cfg["workload"]},
+                      "cpu_baseline": {"value": v, "unit": "Mparticles/s", "cores": cores, "kind": kind, "sample": sample},
+                      "e2e": {"value": v, "unit": "Mparticles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def run_reference_gpu(args, cfg):
     """The reference's CUDA FMM, timed per constructor call (its whole solve:
     particles copied in, a device synchronisation after every kernel, results
@@ -928,6 +1119,8 @@ def main():
         return run_reference_gpu(args, cfg)
     if cfg.get("batch"):
         return run_batch(args, cfg)
+    if cfg.get("heldout") and args.impl == "ours":
+        return run_heldout(args, cfg)
     if cfg.get("vector") and args.impl == "ours":
         return run_vector(args, cfg)
     rank = int(os.environ.get("RANK", "0"))
@@ -938,6 +1131,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
+        if cfg.get("heldout"):
+            return run_heldout_reference(args, cfg)
         pos, q = make_particles(cfg)
         if cfg.get("vector"):
             # the reference's vector FMM on the same particles and charges (sample as run_vector's)
@@ -1017,8 +1212,12 @@ def main():
         if r["plan"]:
             line["plan_execute"] = r["plan"]
         if r["plain"]:
-            line["plain_fp64"] = r["plain"]
-            line["speedup_vs_plain_fp64"] = r["plain"]["ms_per_step"] / r["ms"]
+            if cfg["dim"] == 2:
+                line["uniform_tree"] = r["plain"]
+                line["speedup_vs_uniform_tree"] = r["plain"]["ms_per_step"] / r["ms"]
+            else:
+                line["plain_fp64"] = r["plain"]
+                line["speedup_vs_plain_fp64"] = r["plain"]["ms_per_step"] / r["ms"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -144,6 +144,21 @@ int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, c
                            const double* tgt_xyz, const lfmm_solve_opts* opts, double* pot, double* field,
                            lfmm_stats* stats);
 
+/* Per-level M2L orders (no counterpart in the reference, whose order is one
+ * number for the whole solve, cpu/multipole3d.cpp:1328-1331): opts as for
+ * lfmm3d_solve_ex; level_N[L] (L < n_levels <= 22; 0 or >= opts->N: opts->N)
+ * is the order of level L's M2L, the degrees of the source multipoles it uses,
+ * on the mixed form's tensor-core levels (level 4 and finer); the expansions,
+ * the shifts and the coarse FP64 levels keep opts->N degrees.  The fine levels
+ * hold most of the M2L work and, for charges of either sign, the smallest
+ * share of the far field's error, so they can run lower orders. */
+int lfmm3d_solve_levels(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                        const double* tgt_xyz, const lfmm_solve_opts* opts, const int* level_N, int n_levels,
+                        double* pot, double* field, lfmm_stats* stats);
+int lfmm3d_solve_levels_device(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q,
+                               size_t n_tgt, const double* tgt_xyz, const lfmm_solve_opts* opts, const int* level_N,
+                               int n_levels, double* pot, double* field, lfmm_stats* stats);
+
 /* ---- batched 3D solves (no counterpart in the reference, which solves one
  * problem per constructor call) ---------------------------------------------
  * n_prob independent problems in one solve: problem k is the sources
@@ -184,6 +199,17 @@ int lfmm2d_solve(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double
 int lfmm2d_solve_device(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
                         const double* tgt_xy, int N, int tree_depth, double eps, int precision, double* pot,
                         double* field, lfmm_stats* stats);
+/* Extended 2D solve (the reference's uniform quadtree only,
+ * cpu/multipole.cpp:473-522, is what max_leaf = 0 keeps): max_leaf > 0 builds
+ * an adaptive quadtree (cells split while they hold more than max_leaf
+ * particles, at most tree_depth levels) with U, V, W, X lists, so clustered
+ * sets do not crowd a few leaves.  FP64 (the precision field is accepted and
+ * runs the FP64 form); N <= 30; field as (re, im) pairs. */
+int lfmm2d_solve_ex(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                    const double* tgt_xy, const lfmm_solve_opts* opts, double* pot, double* field, lfmm_stats* stats);
+int lfmm2d_solve_ex_device(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                           const double* tgt_xy, const lfmm_solve_opts* opts, double* pot, double* field,
+                           lfmm_stats* stats);
 
 /* ---- FP64 direct sums (the accuracy oracle on the GPU) -------------------
  * Every target against every source, same clamp and self term as the FMM.
@@ -236,6 +262,11 @@ int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions);
 int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                              const double* tgt_xyz, int tree_depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
                              size_t* list_sizes);
+/* The same for the adaptive quadtree of lfmm2d_solve_ex (2D points; the
+ * cells and lists are read with the two calls below). */
+int lfmm2d_tree_build_adaptive(lfmm_ctx* ctx, size_t n_src, const double* src_xy, const double* src_q, size_t n_tgt,
+                               const double* tgt_xy, int tree_depth, int max_leaf, size_t* n_cells,
+                               size_t* n_leaves, size_t* list_sizes);
 int lfmm_tree_adaptive_cells(lfmm_ctx* ctx, int* level, unsigned long long* code, long long* parent,
                              long long* pbeg, long long* pend, long long* send, unsigned char* is_leaf,
                              long long* leaves, long long* positions);

@@ -21,12 +21,14 @@ EXPORTS = [
     "lfmm_create", "lfmm_destroy", "lfmm_last_error", "lfmm_version", "lfmm_stream", "lfmm_check",
     "lfmm_debug_raise_flags",
     "lfmm3d_solve", "lfmm3d_solve_device", "lfmm3d_solve_ex", "lfmm3d_solve_ex_device",
+    "lfmm3d_solve_levels", "lfmm3d_solve_levels_device",
     "lfmm3d_solve_vector", "lfmm3d_solve_vector_device",
-    "lfmm2d_solve", "lfmm2d_solve_device",
+    "lfmm2d_solve", "lfmm2d_solve_device", "lfmm2d_solve_ex", "lfmm2d_solve_ex_device",
     "lfmm3d_direct", "lfmm3d_direct_device", "lfmm2d_direct", "lfmm2d_direct_device",
     "lfmm3d_direct_device_noalloc",
     "lfmm_tree_build", "lfmm_tree_level", "lfmm_tree_list_sizes", "lfmm_tree_lists", "lfmm_tree_positions",
-    "lfmm_tree_build_adaptive", "lfmm_tree_adaptive_cells", "lfmm_tree_adaptive_lists",
+    "lfmm_tree_build_adaptive", "lfmm2d_tree_build_adaptive", "lfmm_tree_adaptive_cells",
+    "lfmm_tree_adaptive_lists",
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
     "lfmm3d_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
@@ -100,8 +102,11 @@ def load(path: Path | str = LIB_PATH):
         solve = [P, SZ, P, P, SZ, P, I, I, D, I, P, P, ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_solve", "lfmm3d_solve_device", "lfmm2d_solve", "lfmm2d_solve_device"):
             getattr(L, f).argtypes = solve
-        for f in ("lfmm3d_solve_ex", "lfmm3d_solve_ex_device"):
+        for f in ("lfmm3d_solve_ex", "lfmm3d_solve_ex_device", "lfmm2d_solve_ex", "lfmm2d_solve_ex_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, P,
+                                      ctypes.POINTER(LfmmStats)]
+        for f in ("lfmm3d_solve_levels", "lfmm3d_solve_levels_device"):
+            getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P, I, P, P,
                                       ctypes.POINTER(LfmmStats)]
         for f in ("lfmm3d_solve_vector", "lfmm3d_solve_vector_device"):
             getattr(L, f).argtypes = [P, SZ, P, P, SZ, P, ctypes.POINTER(LfmmSolveOpts), P,
@@ -115,6 +120,7 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_tree_lists.argtypes = [P, I, P, P]
         L.lfmm_tree_positions.argtypes = [P, P]
         L.lfmm_tree_build_adaptive.argtypes = [P, SZ, P, P, SZ, P, I, I, P, P, P]
+        L.lfmm2d_tree_build_adaptive.argtypes = [P, SZ, P, P, SZ, P, I, I, P, P, P]
         L.lfmm_tree_adaptive_cells.argtypes = [P, P, P, P, P, P, P, P, P, P]
         L.lfmm_tree_adaptive_lists.argtypes = [P, I, P, P]
         L.lfmm_wignerd_slot.argtypes = [P, I, ctypes.POINTER(D), P]

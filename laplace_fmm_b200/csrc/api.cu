@@ -153,7 +153,7 @@ int select_device(lfmm_ctx* ctx)
 // Device solve shared by the host and device entry points.
 int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                  int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats,
-                 bool arena_reset, int max_leaf = 0)
+                 bool arena_reset, int max_leaf = 0, const int* level_N = nullptr)
 {
 	Context& c = ctx->c;
 	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return ERR_ARG; }
@@ -169,9 +169,11 @@ int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const dou
 	in.dim = dim; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q; in.tgt = tgt;
 	SolveStats ss;
 	int st;
-	if (dim == 2 && max_leaf > 0) { c.last_error = "adaptive trees are 3D only"; return ERR_UNSUPPORTED; }
-	if (dim == 3 && (precision == LFMM_PRECISION_MIXED || max_leaf > 0))
-		st = fmm3d_solve_scaled(c, in, Nr, Dr, max_leaf, precision, pot, field, stats ? &ss : nullptr);
+	if (dim == 2 && max_leaf > 0)   // 2D: one FP64 form (the mixed request runs it too)
+		st = fmm2d_solve_adaptive(c, in, Nr, Dr, max_leaf, pot, field, stats ? &ss : nullptr);
+	else if (dim == 3 && (precision == LFMM_PRECISION_MIXED || max_leaf > 0))
+		st = fmm3d_solve_scaled(c, in, Nr, Dr, max_leaf, precision, pot, field, stats ? &ss : nullptr, nullptr,
+		                        level_N);
 	else if (dim == 3)
 		st = fmm3d_solve_device(c, in, Nr, Dr, pot, field, stats ? &ss : nullptr);
 	else   // 2D: one FP64 form (the mixed request runs it too)
@@ -183,7 +185,7 @@ int solve_device(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const dou
 
 int solve_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                int N, int depth, double eps, int precision, double* pot, double* field, lfmm_stats* stats,
-               int max_leaf = 0)
+               int max_leaf = 0, const int* level_N = nullptr)
 {
 	Context& c = ctx->c;
 	if (select_device(ctx)) return ERR_CUDA;
@@ -204,7 +206,7 @@ int solve_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const doubl
 	}
 	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
 	int st = solve_device(ctx, dim, ns, dsrc, dq, nt, dtgt, N, depth, eps, precision, dpot, dfld, stats, false,
-	                      max_leaf);
+	                      max_leaf, level_N);
 	if (st == OK) {
 		LFMM_CUDA(c, cudaMemcpyAsync(pot, dpot, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
 		LFMM_CUDA(c, cudaMemcpyAsync(field, dfld, sizeof(double) * dim * nout, cudaMemcpyDeviceToHost, s));
@@ -494,6 +496,52 @@ int lfmm3d_solve_ex_device(lfmm_ctx* ctx, size_t ns, const double* src, const do
 	return st;
 }
 
+namespace {
+
+// The per-level M2L orders of lfmm3d_solve_levels[_device], checked and
+// padded to MAX_LEVELS entries (0: the solve's N).
+int level_orders(lfmm_ctx* ctx, const lfmm_solve_opts* o, const int* level_N, int n_levels, int out[MAX_LEVELS])
+{
+	if (!o || n_levels < 0 || n_levels > MAX_LEVELS || (n_levels && !level_N)) {
+		ctx->c.last_error = "per-level orders: 0 <= n_levels <= 22 entries required";
+		return LFMM_ERR_ARG;
+	}
+	for (int L = 0; L < MAX_LEVELS; ++L) out[L] = 0;
+	for (int L = 0; L < n_levels; ++L) {
+		if (level_N[L] < 0) { ctx->c.last_error = "per-level orders must be >= 0"; return LFMM_ERR_ARG; }
+		out[L] = level_N[L];
+	}
+	return LFMM_OK;
+}
+
+} // namespace
+
+int lfmm3d_solve_levels(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                        const lfmm_solve_opts* o, const int* level_N, int n_levels, double* pot, double* field,
+                        lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	int lv[MAX_LEVELS];
+	if (int st = level_orders(ctx, o, level_N, n_levels, lv)) return st;
+	return solve_host(ctx, 3, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                  o->max_leaf, lv);
+}
+
+int lfmm3d_solve_levels_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+                               const double* tgt, const lfmm_solve_opts* o, const int* level_N, int n_levels,
+                               double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx) return LFMM_ERR_ARG;
+	int lv[MAX_LEVELS];
+	if (int st = level_orders(ctx, o, level_N, n_levels, lv)) return st;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = solve_device(ctx, 3, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                      true, o->max_leaf, lv);
+	if (st == OK) st = stats ? check_flags(ctx->c) : latch_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
+}
+
 int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt,
                                const double* tgt, const lfmm_solve_opts* o, double* field, lfmm_stats* stats)
 {
@@ -565,6 +613,28 @@ int lfmm2d_solve(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, s
 {
 	if (!ctx) return LFMM_ERR_ARG;
 	return solve_host(ctx, 2, ns, src, q, nt, tgt, N, depth, eps, precision, pot, field, stats);
+}
+
+int lfmm2d_solve_ex(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                    const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	if (o->max_leaf < 0) { ctx->c.last_error = "max_leaf must be >= 0"; return LFMM_ERR_ARG; }
+	return solve_host(ctx, 2, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                  o->max_leaf);
+}
+
+int lfmm2d_solve_ex_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                           const lfmm_solve_opts* o, double* pot, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	if (o->max_leaf < 0) { ctx->c.last_error = "max_leaf must be >= 0"; return LFMM_ERR_ARG; }
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	int st = solve_device(ctx, 2, ns, src, q, nt, tgt, o->N, o->tree_depth, o->eps, o->precision, pot, field, stats,
+	                      true, o->max_leaf);
+	if (st == OK) st = stats ? check_flags(ctx->c) : latch_flags(ctx->c);
+	ctx->c.arena.settle();
+	return st;
 }
 
 int lfmm2d_solve_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
@@ -868,7 +938,9 @@ int lfmm_tree_positions(lfmm_ctx* ctx, long long* positions)
 	return LFMM_OK;
 }
 
-int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+namespace {
+
+int tree_build_adaptive_host(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,
                              const double* tgt, int depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
                              size_t* list_sizes)
 {
@@ -881,21 +953,21 @@ int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const 
 	ctx->has_tree = false;
 	ctx->v_off.clear();
 	ctx->v_idx.clear();
-	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(ns, 1)));
 	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
-	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * dim * std::max<size_t>(nt, 1)));
 	if (!dsrc || !dq || !dtgt) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
 	cudaStream_t s = c.stream;
 	if (ns) {
-		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * dim * ns, cudaMemcpyHostToDevice, s));
 		if (q) LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
 		else LFMM_CUDA(c, cudaMemsetAsync(dq, 0, sizeof(double) * ns, s));
 	}
-	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * dim * nt, cudaMemcpyHostToDevice, s));
 	ParticleInput in;
-	in.dim = 3; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
+	in.dim = dim; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
 	DevTree& t = ctx->tree;
-	int st = tree_build_adaptive(c, in, resolve_depth(3, depth, ns + nt), max_leaf, t);
+	int st = tree_build_adaptive(c, in, resolve_depth(dim, depth, ns + nt), max_leaf, t);
 	if (st || (st = check_flags(c))) return st;
 	// V lists: the M2L slot table of every level (what the solver's M2L reads)
 	ctx->v_off.assign(t.ncells + 1, 0);
@@ -904,13 +976,16 @@ int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const 
 		if (!t.lsize[L]) continue;
 		const size_t mark = c.arena.mark();
 		M2LPlan plan;
-		if ((st = m2l_plan_build(c, t, L, plan)) || (st = check_flags(c))) return st;
-		std::vector<int32_t> vt(t.lsize[L] * (size_t)M2L_SLOTS);
+		if ((st = dim == 3 ? m2l_plan_build(c, t, L, plan) : m2l_plan_build2d(c, t, L, plan)) ||
+		    (st = check_flags(c)))
+			return st;
+		const int slots = dim == 3 ? M2L_SLOTS : M2L_SLOTS2;
+		std::vector<int32_t> vt(t.lsize[L] * (size_t)slots);
 		if ((st = fetch(c, vt.data(), plan.vtab, vt.size()))) return st;
 		c.arena.rewind(mark);
 		for (size_t k = 0; k < t.lsize[L]; ++k)
-			for (int sl = 0; sl < M2L_SLOTS; ++sl) {
-				const int32_t v = vt[k * M2L_SLOTS + sl];
+			for (int sl = 0; sl < slots; ++sl) {
+				const int32_t v = vt[k * slots + sl];
 				if (v >= 0) per[t.loff[L] + k].push_back((long long)(t.loff[L] + (size_t)v));
 			}
 	}
@@ -925,6 +1000,22 @@ int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const 
 		list_sizes[0] = t.n_u; list_sizes[1] = t.n_w; list_sizes[2] = t.n_x; list_sizes[3] = ctx->v_idx.size();
 	}
 	return LFMM_OK;
+}
+
+} // namespace
+
+int lfmm_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+                             const double* tgt, int depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
+                             size_t* list_sizes)
+{
+	return tree_build_adaptive_host(ctx, 3, ns, src, q, nt, tgt, depth, max_leaf, n_cells, n_leaves, list_sizes);
+}
+
+int lfmm2d_tree_build_adaptive(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt,
+                               const double* tgt, int depth, int max_leaf, size_t* n_cells, size_t* n_leaves,
+                               size_t* list_sizes)
+{
+	return tree_build_adaptive_host(ctx, 2, ns, src, q, nt, tgt, depth, max_leaf, n_cells, n_leaves, list_sizes);
 }
 
 int lfmm_tree_adaptive_cells(lfmm_ctx* ctx, int* level, unsigned long long* code, long long* parent,

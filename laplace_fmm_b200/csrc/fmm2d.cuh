@@ -8,4 +8,9 @@ namespace lfmm {
 int fmm2d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, double* pot, double* field,
                        SolveStats* stats);
 
+// Adaptive quadtree (cells split while they hold more than max_leaf
+// particles, at most depth levels) with U / V / W / X lists; FP64.
+int fmm2d_solve_adaptive(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, double* pot,
+                         double* field, SolveStats* stats);
+
 } // namespace lfmm

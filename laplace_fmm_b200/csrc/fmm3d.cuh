@@ -28,12 +28,16 @@ int fmm3d_solve_device(Context& ctx, const ParticleInput& in, int N, int depth, 
 // Vector charges (in.srcq: 3 doubles per source): field = sum q x d / r^3.
 int fmm3d_solve_vector(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
                        double* field, SolveStats* stats);
+// level_N (optional, depth entries): the M2L order of each level, the
+// degrees of the source multipoles its M2L uses (0 or >= N: N); honoured on
+// the tensor-core (mixed-form FP32) levels, whose expansions keep N degrees.
 int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
-                       double* pot, double* field, SolveStats* stats, DevTree* tree_out = nullptr);
+                       double* pot, double* field, SolveStats* stats, DevTree* tree_out = nullptr,
+                       const int* level_N = nullptr);
 // The same on a tree built by tree_build_adaptive (phase events 0 and 1, the
 // tree build, are the caller's when timing).
 int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, double* pot, double* field,
-                         SolveStats* stats);
+                         SolveStats* stats, const int* level_N = nullptr);
 
 // Dense FP64 M2L operators [343][MT][MT] for cell size h (h = 1: the
 // level-independent scaled operators), cached in the context.

@@ -180,7 +180,8 @@ int m2m_plan_build(Context& ctx, const DevTree& t, int L, M2LPlan& plan)
 }
 
 template <typename real>
-int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, SolveStats* stats)
+int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, SolveStats* stats,
+            const int* level_N)
 {
 	using v2 = typename V2<real>::t;
 	cudaStream_t s = ctx.stream;
@@ -255,7 +256,8 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 				// tcgen05 TF32 hi/lo GEMM on the FP32 levels
 				const uint4* tc = m2l_ops_tc(ctx, N);
 				if (!tc) return ERR_OOM;
-				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N)))
+				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N,
+				                      level_N ? level_N[L] : 0)))
 					return st;
 			} else {
 				if ((st = m2l_gemm<real>(ctx, plan, ops, mL, lL, N))) return st;
@@ -307,28 +309,6 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 	return OK;
 }
 
-__global__ void adaptive_counts_kernel(DevTree t, unsigned long long* out)
-{
-	size_t li = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-	unsigned long long p2p = 0, m2p = 0, u = 0;
-	if (li < t.nleaves) {
-		size_t g = t.leaves[li];
-		unsigned long long nt = t.tend[g] - t.tbeg[g];
-		unsigned long long ns = t.send[g] - t.pbeg[g];
-		for (uint32_t e = t.u_off[li]; e < t.u_off[li + 1]; ++e) { size_t k = t.u_idx[e]; ns += t.send[k] - t.pbeg[k]; }
-		p2p = nt * ns;
-		m2p = nt * (t.w_off[li + 1] - t.w_off[li]);
-		u = t.u_off[li + 1] - t.u_off[li];
-	}
-	unsigned long long far = 0;
-	for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < t.ncells; c += (size_t)gridDim.x * blockDim.x)
-		far += (unsigned long long)t.far_cnt[c];
-	p2p = warp_sum(p2p); m2p = warp_sum(m2p); u = warp_sum(u); far = warp_sum(far);
-	if ((threadIdx.x & 31) == 0) {
-		atomicAdd(out, far); atomicAdd(out + 1, u); atomicAdd(out + 2, p2p); atomicAdd(out + 3, m2p);
-	}
-}
-
 } // namespace
 
 float* m2l_ops_fp32(Context& ctx, int N)
@@ -348,7 +328,7 @@ float* m2l_ops_fp32(Context& ctx, int N)
 }
 
 int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, int max_leaf, int precision,
-                       double* pot, double* field, SolveStats* stats, DevTree* tree_out)
+                       double* pot, double* field, SolveStats* stats, DevTree* tree_out, const int* level_N)
 {
 	if (N < 1 || N > MAXN3) { ctx.last_error = "order out of range (1 <= N <= 18)"; return ERR_ARG; }
 	if (!m2l_gemm_supported(N)) { ctx.last_error = "scaled / mixed / adaptive forms support N <= 18"; return ERR_UNSUPPORTED; }
@@ -362,13 +342,13 @@ int fmm3d_solve_scaled(Context& ctx, const ParticleInput& in, int N, int depth, 
 	DevTree t;
 	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t))) return st;
 	if (timing) LFMM_CUDA(ctx, cudaEventRecord(ctx.ev[1], s));
-	if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+	if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats, level_N))) return st;
 	if (tree_out) *tree_out = t;
 	return OK;
 }
 
 int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, double* pot, double* field,
-                         SolveStats* stats)
+                         SolveStats* stats, const int* level_N)
 {
 	if (N < 1 || N > MAXN3 || !m2l_gemm_supported(N)) {
 		ctx.last_error = "scaled / mixed / adaptive forms support N <= 18";
@@ -378,16 +358,12 @@ int fmm3d_scaled_on_tree(Context& ctx, const DevTree& t, int N, int precision, d
 	if (st) return st;
 	cudaStream_t s = ctx.stream;
 	const bool timing = ctx.timing != 0;
-	st = precision == 1 ? solve_t<float>(ctx, t, N, pot, field, stats) : solve_t<double>(ctx, t, N, pot, field, stats);
+	st = precision == 1 ? solve_t<float>(ctx, t, N, pot, field, stats, level_N)
+	                    : solve_t<double>(ctx, t, N, pot, field, stats, level_N);
 	if (st) return st;
 	if (stats) {
-		unsigned long long* dc = static_cast<unsigned long long*>(ctx.arena.take(64));
-		if (!dc) return ERR_OOM;
-		LFMM_CUDA(ctx, cudaMemsetAsync(dc, 0, 64, s));
-		adaptive_counts_kernel<<<div_up(std::max<size_t>(t.nleaves, 1), 256), 256, 0, s>>>(t, dc);
 		unsigned long long h[4];
-		LFMM_CUDA(ctx, cudaMemcpyAsync(h, dc, 32, cudaMemcpyDeviceToHost, s));
-		LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+		if ((st = tree_adaptive_counts(ctx, t, h))) return st;
 		stats->N = N; stats->depth = t.depth;
 		stats->n_particles = t.n; stats->n_cells = t.ncells; stats->n_leaves = t.nleaves;
 		stats->targets_num = t.targets_num;

@@ -687,7 +687,7 @@ TcTrunc tc_trunc(int N, int KB)
 
 template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
-           bool timed, size_t src_cells, const float* diag = nullptr)
+           bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0)
 {
 	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
@@ -696,7 +696,8 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
 	m2l_tc_kernel<NC, NA, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 		reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part, plan.cells,
-		diag, ctx.dev_flags, tc_trunc(R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB),
+		diag, ctx.dev_flags,
+		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB),
 		src_cells, MODE == TC_M2L ? 343 : 8);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
@@ -717,7 +718,7 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 // keeps the fastest for the context (the chosen S runs last, so the level's
 // result always comes from it).
 template <int NC, int NA>
-int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R)
+int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int n_src)
 {
 	using C = TcCfg<NC, NA>;
 	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L>,
@@ -747,7 +748,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		int bestS = S;
 		for (int cand = 1; cand <= 8; cand *= 2) {
 			LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells);
+			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells, nullptr, n_src);
 			if (st) return st;
 			LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
 			LFMM_CUDA(ctx, cudaEventSynchronize(e1));
@@ -760,7 +761,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		tuned = bestS;
 		S = bestS;
 	}
-	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells);
+	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr, n_src);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
@@ -858,11 +859,12 @@ int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops,
 	return ERR_UNSUPPORTED;
 }
 
-int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N)
+int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N, int n_src)
 {
 	if (int st = upload_slot_dirs(ctx)) return st;
 	const int R = N * (N + 1), NC = m2l_padded(N), NA = m2l_tc_drained(N);
-#define LFMM_TC_M2L(nc, na) if (NC == nc && NA == na) return launch_tc<nc, na>(ctx, plan, ops, mult, loc, R);
+	const int ns = n_src > 0 && n_src < N ? n_src : 0;
+#define LFMM_TC_M2L(nc, na) if (NC == nc && NA == na) return launch_tc<nc, na>(ctx, plan, ops, mult, loc, R, ns);
 	LFMM_TC_ORDERS(LFMM_TC_M2L)
 #undef LFMM_TC_M2L
 	ctx.last_error = "tensor-core M2L: unsupported order";

@@ -34,7 +34,11 @@ inline int m2l_tc_drained(int N) { return m2l_padded(N) <= 160 ? m2l_padded(N) :
 const uint4* m2l_ops_tc(Context& ctx, int N);
 
 // loc = sum over slots of T_dir mult[src] for every cell of the level (FP32).
-int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N);
+// n_src in (0, N): the level's M2L order, the degrees of the sources it uses
+// (the nearest offsets use n_src degrees, the farther ones the truncation
+// rule's fewer, never below the corrected K blocks); 0: N.
+int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N,
+                int n_src = 0);
 
 // The same engine for the level-to-level shifts, whose scaled operators are
 // one per child octant:

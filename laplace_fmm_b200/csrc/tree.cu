@@ -16,7 +16,42 @@ __device__ __forceinline__ void load_point(const ParticleInput in, size_t i, dou
 	for (int d = 0; d < DIM; ++d) p[d] = b[d];
 }
 
-constexpr int BBOX_BLOCKS = 296;
+// Element e of the input coordinates read as one array: the targets' nt x DIM
+// doubles followed by the sources' (both interleaved, one particle per DIM
+// consecutive doubles).  Walking e with consecutive lanes makes every warp
+// load 32 consecutive doubles (256 bytes).
+template <int DIM>
+__device__ __forceinline__ double point_elem(const ParticleInput& in, size_t e)
+{
+	const size_t te = in.nt * DIM;
+	return e < te ? __ldg(in.tgt + e) : __ldg(in.src + (e - te));
+}
+
+// Min / max of coordinate d over the elements [e, e_end) taken with stride S by
+// this thread; the coordinate of element e is e mod DIM, kept incrementally.
+// Four independent loads per iteration keep enough requests in flight.
+template <int DIM>
+__device__ __forceinline__ void minmax_elems(const ParticleInput& in, size_t e, size_t e_end, size_t S,
+                                             double* mn, double* mx)
+{
+	int d = (int)(e % DIM);
+	const int dS = (int)(S % DIM);
+	auto take = [&](double v) {
+#pragma unroll
+		for (int k = 0; k < DIM; ++k)
+			if (d == k) { mn[k] = fmin(mn[k], v); mx[k] = fmax(mx[k], v); }
+		d += dS;
+		if (d >= DIM) d -= DIM;
+	};
+	for (; e + 3 * S < e_end; e += 4 * S) {
+		const double v0 = point_elem<DIM>(in, e), v1 = point_elem<DIM>(in, e + S);
+		const double v2 = point_elem<DIM>(in, e + 2 * S), v3 = point_elem<DIM>(in, e + 3 * S);
+		take(v0); take(v1); take(v2); take(v3);
+	}
+	for (; e < e_end; e += S) take(point_elem<DIM>(in, e));
+}
+
+constexpr int BBOX_BLOCKS = 1184;               // 8 per SM
 constexpr int BBOX_THREADS = 256;
 
 template <int DIM>
@@ -29,12 +64,8 @@ __global__ void __launch_bounds__(BBOX_THREADS) bbox_partial_kernel(const Partic
 #pragma unroll
 		for (int d = 0; d < DIM; ++d) mn[d] = mx[d] = p[d];
 	}
-	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-		double p[DIM];
-		load_point<DIM>(in, i, p);
-#pragma unroll
-		for (int d = 0; d < DIM; ++d) { mn[d] = fmin(mn[d], p[d]); mx[d] = fmax(mx[d], p[d]); }
-	}
+	minmax_elems<DIM>(in, (size_t)blockIdx.x * blockDim.x + threadIdx.x, n * DIM, (size_t)gridDim.x * blockDim.x,
+	                  mn, mx);
 #pragma unroll
 	for (int d = 0; d < DIM; ++d)
 		for (int o = 16; o > 0; o >>= 1) {
@@ -54,14 +85,22 @@ __global__ void __launch_bounds__(BBOX_THREADS) bbox_partial_kernel(const Partic
 }
 
 // shift = min - 1e-7, scale = largest extent + 1e-6 (reference cpu/morton_tree.cpp:293-301)
+// One warp: lane l folds the partials l, l + 32, ..., then shuffles.
 template <int DIM>
 __global__ void bbox_final_kernel(const double* partial, int nb, double* geo)
 {
-	if (threadIdx.x != 0) return;
+	const int lane = threadIdx.x;
+	if (lane >= 32) return;
 	double mn[DIM], mx[DIM];
 	for (int d = 0; d < DIM; ++d) { mn[d] = partial[d]; mx[d] = partial[DIM + d]; }
-	for (int b = 1; b < nb; ++b)
+	for (int b = lane; b < nb; b += 32)
 		for (int d = 0; d < DIM; ++d) { mn[d] = fmin(mn[d], partial[b * 2 * DIM + d]); mx[d] = fmax(mx[d], partial[b * 2 * DIM + DIM + d]); }
+	for (int d = 0; d < DIM; ++d)
+		for (int o = 16; o > 0; o >>= 1) {
+			mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+			mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+		}
+	if (lane != 0) return;
 	double dw = mx[0] - mn[0];
 	for (int d = 1; d < DIM; ++d) dw = fmax(dw, mx[d] - mn[d]);
 	for (int d = 0; d < 3; ++d) geo[d] = d < DIM ? mn[d] - 1.e-7 : 0.0;
@@ -77,12 +116,7 @@ __global__ void __launch_bounds__(BBOX_THREADS) bbox_segment_kernel(const Partic
 	double mn[DIM], mx[DIM];
 #pragma unroll
 	for (int d = 0; d < DIM; ++d) { mn[d] = 1e300; mx[d] = -1e300; }
-	for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-		double p[DIM];
-		load_point<DIM>(in, i, p);
-#pragma unroll
-		for (int d = 0; d < DIM; ++d) { mn[d] = fmin(mn[d], p[d]); mx[d] = fmax(mx[d], p[d]); }
-	}
+	minmax_elems<DIM>(in, (size_t)b * DIM + threadIdx.x, (size_t)e * DIM, blockDim.x, mn, mx);
 #pragma unroll
 	for (int d = 0; d < DIM; ++d)
 		for (int o = 16; o > 0; o >>= 1) {
@@ -108,14 +142,26 @@ __global__ void __launch_bounds__(BBOX_THREADS) bbox_segment_kernel(const Partic
 // code = interleave(trunc(2^(depth-1) * (x - shift) / scale)), x highest
 // (reference cpu/morton_tree.cpp:48-99); IEEE-rounded ops, no contraction.
 // Forest: the particle's problem index above the Morton bits, the problem's box.
+// The block's positions are staged through shared memory with coalesced loads.
+constexpr int CODES_THREADS = 256;
+
 template <int DIM>
-__global__ void codes_kernel(const ParticleInput in, size_t n, const double* __restrict__ geo_all, int depth,
-                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
+__global__ void __launch_bounds__(CODES_THREADS) codes_kernel(const ParticleInput in, size_t n,
+                                                              const double* __restrict__ geo_all, int depth,
+                                                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
 {
-	size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	__shared__ double sp[CODES_THREADS * DIM];
+	const size_t first = (size_t)blockIdx.x * CODES_THREADS;
+	for (int j = threadIdx.x; j < CODES_THREADS * DIM; j += CODES_THREADS) {
+		const size_t e = first * DIM + j;
+		if (e < n * DIM) sp[j] = point_elem<DIM>(in, e);
+	}
+	__syncthreads();
+	size_t i = first + threadIdx.x;
 	if (i >= n) return;
 	double p[DIM];
-	load_point<DIM>(in, i, p);
+#pragma unroll
+	for (int d = 0; d < DIM; ++d) p[d] = sp[threadIdx.x * DIM + d];
 	uint64_t prob = 0;
 	if (in.nprob > 1) {
 		int lo = 0, hi = in.nprob;          // last k with poff[k] <= i
@@ -417,15 +463,15 @@ int tree_build(Context& ctx, const ParticleInput& in, int depth, DevTree& t, boo
 	const unsigned TB = 256;
 	if (dim == 3 && nprob > 1) {
 		bbox_segment_kernel<3><<<nprob, BBOX_THREADS, 0, s>>>(in, t.geo);
-		codes_kernel<3><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
+		codes_kernel<3><<<div_up(n, CODES_THREADS), CODES_THREADS, 0, s>>>(in, n, t.geo, depth, keys, vals);
 	} else if (dim == 3) {
 		bbox_partial_kernel<3><<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(in, n, partial);
 		bbox_final_kernel<3><<<1, 32, 0, s>>>(partial, BBOX_BLOCKS, t.geo);
-		codes_kernel<3><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
+		codes_kernel<3><<<div_up(n, CODES_THREADS), CODES_THREADS, 0, s>>>(in, n, t.geo, depth, keys, vals);
 	} else {
 		bbox_partial_kernel<2><<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(in, n, partial);
 		bbox_final_kernel<2><<<1, 32, 0, s>>>(partial, BBOX_BLOCKS, t.geo);
-		codes_kernel<2><<<div_up(n, TB), TB, 0, s>>>(in, n, t.geo, depth, keys, vals);
+		codes_kernel<2><<<div_up(n, CODES_THREADS), CODES_THREADS, 0, s>>>(in, n, t.geo, depth, keys, vals);
 	}
 	int which = radix_sort_pairs(keys, vals, keys2, vals2, n, 0, dim * (depth - 1) + pbits, scratch, s);
 	uint64_t* sk = which ? keys2 : keys;

@@ -86,8 +86,12 @@ int tree_lists(Context& ctx, DevTree& t);
 // than max_leaf particles and is above level depth-1 (max_leaf = 0 splits
 // every cell: the uniform tree in adaptive form).  Leaves may sit on any
 // level; beg/end hold child ranges (empty for leaves), pbeg/pend particle
-// ranges; U/W/X lists are built (3D only).
+// ranges; U/W/X lists are built (quadtree or octree).
 int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& t);
+
+// Interaction counts of an adaptive tree (synchronises): out[0] V pairs,
+// out[1] U entries, out[2] P2P particle pairs, out[3] M2P (target, cell) pairs.
+int tree_adaptive_counts(Context& ctx, const DevTree& t, unsigned long long* out);
 
 // Fill a CSR far list of level L (level-local source indices) in the
 // reference's order; far_off must hold lsize[L] + 1 entries.

@@ -1,4 +1,4 @@
-// Adaptive octree and its U / V / W / X interaction lists (3D).
+// Adaptive octree / quadtree and its U / V / W / X interaction lists.
 //
 // The reference builds only uniform-depth trees (cpu/morton_tree.cpp:286-493);
 // this builder starts from the same bit-exact uniform tree (all levels down to
@@ -11,8 +11,8 @@
 //               to B and parent(D) adjacent to B                          (M2P)
 //   X(B)        leaves C coarser than B, adjacent to parent(B), not
 //               adjacent to B (the transpose of W)                         (P2L)
-// Adjacency of cubes on different levels is exact integer arithmetic on the
-// Morton coordinates (touching faces, edges or corners count).
+// Adjacency of cubes (squares) on different levels is exact integer arithmetic
+// on the Morton coordinates (touching faces, edges or corners count).
 #include "tree.cuh"
 #include "primitives.cuh"
 
@@ -22,15 +22,20 @@ namespace {
 
 constexpr int STACK = 160;
 
-__device__ __forceinline__ void coords3(uint64_t code, int* c)
-{ c[0] = (int)compact3(code >> 2); c[1] = (int)compact3(code >> 1); c[2] = (int)compact3(code); }
+template <int DIM>
+__device__ __forceinline__ void coords(uint64_t code, int* c)
+{
+	if (DIM == 3) { c[0] = (int)compact3(code >> 2); c[1] = (int)compact3(code >> 1); c[2] = (int)compact3(code); }
+	else { c[0] = (int)compact2(code >> 1); c[1] = (int)compact2(code); }
+}
 
 // Cube C (level lc, coords c) and cube B (level lb >= lc, coords b) touch or overlap.
+template <int DIM>
 __device__ __forceinline__ bool touch(int lc, const int* c, int lb, const int* b)
 {
 	int s = lb - lc;
 #pragma unroll
-	for (int d = 0; d < 3; ++d) {
+	for (int d = 0; d < DIM; ++d) {
 		int lo = c[d] << s, hi = (c[d] + 1) << s;
 		if (b[d] < lo - 1 || b[d] > hi) return false;
 	}
@@ -77,7 +82,8 @@ __global__ void emit_kernel(DevTree u, int L, const uint8_t* __restrict__ keep, 
 	if (!keep[g]) return;
 	size_t ag = a.loff[L] + map[g];
 	a.code[ag] = u.code[g];
-	a.cx[ag] = u.cx[g]; a.cy[ag] = u.cy[g]; a.cz[ag] = u.cz[g];
+	a.cx[ag] = u.cx[g]; a.cy[ag] = u.cy[g];
+	if (a.cz) a.cz[ag] = u.cz[g];
 	a.pbeg[ag] = pb[g]; a.pend[ag] = pe[g];
 	a.lev[ag] = (uint8_t)L;
 	a.is_leaf[ag] = split[g] ? 0 : 1;
@@ -127,7 +133,8 @@ __global__ void partition_leaves_kernel(DevTree a, double* x2, double* y2, doubl
 		unsigned bt = __ballot_sync(0xffffffffu, valid && !src);
 		if (valid) {
 			uint32_t dst = src ? ws + __popc(bs & lt) : wt + __popc(bt & lt);
-			x2[dst] = a.x[i]; y2[dst] = a.y[i]; z2[dst] = a.z[i];
+			x2[dst] = a.x[i]; y2[dst] = a.y[i];
+			if (z2) z2[dst] = a.z[i];
 			q2[dst] = a.q[i]; o2[dst] = a.orig[i]; c2[dst] = a.pcode[i];
 		}
 		ws += __popc(bs); wt += __popc(bt);
@@ -145,6 +152,7 @@ __global__ void source_ranges_kernel(DevTree a)
 }
 
 // U and W lists of one leaf (pass 0: count, pass 1: fill at the offsets).
+template <int DIM>
 __global__ void uw_kernel(DevTree a, int pass, uint32_t* __restrict__ ucnt, uint32_t* __restrict__ wcnt, unsigned* flags)
 {
 	size_t li = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -152,7 +160,7 @@ __global__ void uw_kernel(DevTree a, int pass, uint32_t* __restrict__ ucnt, uint
 	const int32_t g = a.leaves[li];
 	const int L = a.lev[g];
 	int me[3];
-	coords3(a.code[g], me);
+	coords<DIM>(a.code[g], me);
 	uint32_t nu = 0, nw = 0;
 	const uint32_t ub = pass ? a.u_off[li] : 0, wb = pass ? a.w_off[li] : 0;
 	int32_t stack[STACK];
@@ -175,8 +183,8 @@ __global__ void uw_kernel(DevTree a, int pass, uint32_t* __restrict__ ucnt, uint
 			int32_t D = stack[--sp];
 			int ld = a.lev[D];
 			int d[3];
-			coords3(a.code[D], d);
-			if (touch(L, me, ld, d)) {
+			coords<DIM>(a.code[D], d);
+			if (touch<DIM>(L, me, ld, d)) {
 				if (a.is_leaf[D]) {
 					if (pass) a.u_idx[ub + nu] = D;
 					nu++;
@@ -203,8 +211,8 @@ __global__ void uw_kernel(DevTree a, int pass, uint32_t* __restrict__ ucnt, uint
 			int32_t C = (int32_t)(a.loff[l] + al[e]);
 			if (!a.is_leaf[C]) continue;
 			int c[3];
-			coords3(a.code[C], c);
-			if (touch(l, c, L, me)) {
+			coords<DIM>(a.code[C], c);
+			if (touch<DIM>(l, c, L, me)) {
 				if (pass) a.u_idx[ub + nu] = C;
 				nu++;
 			}
@@ -215,6 +223,7 @@ __global__ void uw_kernel(DevTree a, int pass, uint32_t* __restrict__ ucnt, uint
 
 // X list of one cell: leaf colleagues C of an ancestor, touching parent(B)
 // but not B.
+template <int DIM>
 __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 {
 	size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -224,9 +233,9 @@ __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 	const uint32_t xb = pass ? a.x_off[g] : 0;
 	if (L >= 2) {
 		int me[3], pc[3];
-		coords3(a.code[g], me);
+		coords<DIM>(a.code[g], me);
 		int32_t A = (int32_t)(a.loff[L - 1] + a.parent[g]);
-		coords3(a.code[A], pc);
+		coords<DIM>(a.code[A], pc);
 		for (int l = L - 1; l >= 1; --l) {
 			if (l < L - 1) A = (int32_t)(a.loff[l] + a.parent[A]);
 			const int na = a.close_cnt[A];
@@ -235,8 +244,8 @@ __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 				int32_t C = (int32_t)(a.loff[l] + al[e]);
 				if (!a.is_leaf[C]) continue;
 				int c[3];
-				coords3(a.code[C], c);
-				if (touch(l, c, L - 1, pc) && !touch(l, c, L, me)) {
+				coords<DIM>(a.code[C], c);
+				if (touch<DIM>(l, c, L - 1, pc) && !touch<DIM>(l, c, L, me)) {
 					if (pass) a.x_idx[xb + nx] = C;
 					nx++;
 				}
@@ -246,6 +255,31 @@ __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 	if (!pass) xcnt[g] = nx;
 }
 
+// Interaction counts of an adaptive tree: far (V) pairs, U entries, P2P
+// particle pairs (targets x sources of the leaf and its U list), M2P
+// (target, W cell) pairs.
+__global__ void adaptive_counts_kernel(DevTree t, unsigned long long* out)
+{
+	size_t li = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long p2p = 0, m2p = 0, u = 0;
+	if (li < t.nleaves) {
+		size_t g = t.leaves[li];
+		unsigned long long nt = t.tend[g] - t.tbeg[g];
+		unsigned long long ns = t.send[g] - t.pbeg[g];
+		for (uint32_t e = t.u_off[li]; e < t.u_off[li + 1]; ++e) { size_t k = t.u_idx[e]; ns += t.send[k] - t.pbeg[k]; }
+		p2p = nt * ns;
+		m2p = nt * (t.w_off[li + 1] - t.w_off[li]);
+		u = t.u_off[li + 1] - t.u_off[li];
+	}
+	unsigned long long far = 0;
+	for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < t.ncells; c += (size_t)gridDim.x * blockDim.x)
+		far += (unsigned long long)t.far_cnt[c];
+	p2p = warp_sum(p2p); m2p = warp_sum(m2p); u = warp_sum(u); far = warp_sum(far);
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(out, far); atomicAdd(out + 1, u); atomicAdd(out + 2, p2p); atomicAdd(out + 3, m2p);
+	}
+}
+
 template <typename T>
 T* take(Context& ctx, size_t count) { return static_cast<T*>(ctx.arena.take(sizeof(T) * (count ? count : 1))); }
 
@@ -253,7 +287,6 @@ T* take(Context& ctx, size_t count) { return static_cast<T*>(ctx.arena.take(size
 
 int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& a)
 {
-	if (in.dim != 3) { ctx.last_error = "adaptive tree: 3D only"; return ERR_UNSUPPORTED; }
 	if (depth < 1 || depth > 16) { ctx.last_error = "adaptive tree: depth must be in [1, 16]"; return ERR_ARG; }
 	DevTree u;
 	int st = tree_build(ctx, in, depth, u, /*partition=*/false, /*lists=*/false);
@@ -282,12 +315,13 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	LFMM_CUDA(ctx, cudaMemcpyAsync(ht, tot, sizeof(uint32_t) * depth, cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	a = DevTree();
-	a.dim = 3; a.depth = depth; a.n = u.n; a.nt = u.nt; a.targets_num = u.targets_num;
+	const int dim = in.dim;
+	a.dim = dim; a.depth = depth; a.n = u.n; a.nt = u.nt; a.targets_num = u.targets_num;
 	a.geo = u.geo;
 	a.nprob = u.nprob;
 	for (int d = 0; d < 4; ++d) a.geo_host[d] = u.geo_host[d];
 	a.x = u.x; a.y = u.y; a.z = u.z; a.q = u.q; a.orig = u.orig; a.pcode = u.pcode;
-	a.close_stride = 26;
+	a.close_stride = dim == 3 ? 26 : 8;
 	a.adaptive = true; a.max_leaf = max_leaf;
 	a.ncells = 0;
 	int used_depth = 0;
@@ -303,7 +337,7 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	a.tbeg = take<uint32_t>(ctx, C); a.tend = take<uint32_t>(ctx, C);
 	a.pbeg = take<uint32_t>(ctx, C); a.pend = take<uint32_t>(ctx, C); a.send = take<uint32_t>(ctx, C);
 	a.parent = take<int32_t>(ctx, C);
-	a.cx = take<double>(ctx, C); a.cy = take<double>(ctx, C); a.cz = take<double>(ctx, C);
+	a.cx = take<double>(ctx, C); a.cy = take<double>(ctx, C); a.cz = dim == 3 ? take<double>(ctx, C) : nullptr;
 	a.is_leaf = take<uint8_t>(ctx, C); a.lev = take<uint8_t>(ctx, C);
 	a.close_cnt = take<int32_t>(ctx, C);
 	a.close_idx = take<int32_t>(ctx, C * a.close_stride);
@@ -328,9 +362,10 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	// sources / targets inside the leaves
 	if (a.targets_num > 0) {
 		const size_t n = a.n;
-		double* x2 = take<double>(ctx, n); double* y2 = take<double>(ctx, n); double* z2 = take<double>(ctx, n);
+		double* x2 = take<double>(ctx, n); double* y2 = take<double>(ctx, n);
+		double* z2 = dim == 3 ? take<double>(ctx, n) : nullptr;
 		double* q2 = take<double>(ctx, n); uint32_t* o2 = take<uint32_t>(ctx, n); uint64_t* c2 = take<uint64_t>(ctx, n);
-		if (!x2 || !y2 || !z2 || !q2 || !o2 || !c2) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
+		if (!x2 || !y2 || (dim == 3 && !z2) || !q2 || !o2 || !c2) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
 		source_ranges_kernel<<<div_up(C, TB), TB, 0, s>>>(a);
 		partition_leaves_kernel<<<div_up(nl * 32, TB), TB, 0, s>>>(a, x2, y2, z2, q2, o2, c2);
 		a.x = x2; a.y = y2; a.z = z2; a.q = q2; a.orig = o2; a.pcode = c2;
@@ -345,8 +380,13 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	uint32_t* xcnt = take<uint32_t>(ctx, C + 1);
 	uint32_t* tots = take<uint32_t>(ctx, 4);
 	if (!ucnt || !wcnt || !xcnt || !tots) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
-	uw_kernel<<<div_up(nl, 128), 128, 0, s>>>(a, 0, ucnt, wcnt, ctx.dev_flags);
-	x_kernel<<<div_up(C, 128), 128, 0, s>>>(a, 0, xcnt);
+	if (dim == 3) {
+		uw_kernel<3><<<div_up(nl, 128), 128, 0, s>>>(a, 0, ucnt, wcnt, ctx.dev_flags);
+		x_kernel<3><<<div_up(C, 128), 128, 0, s>>>(a, 0, xcnt);
+	} else {
+		uw_kernel<2><<<div_up(nl, 128), 128, 0, s>>>(a, 0, ucnt, wcnt, ctx.dev_flags);
+		x_kernel<2><<<div_up(C, 128), 128, 0, s>>>(a, 0, xcnt);
+	}
 	scan_exclusive_u32(ucnt, a.u_off, nl, a.u_off + nl, scr, s);
 	scan_exclusive_u32(wcnt, a.w_off, nl, a.w_off + nl, scr, s);
 	scan_exclusive_u32(xcnt, a.x_off, C, a.x_off + C, scr, s);
@@ -361,9 +401,26 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	a.w_idx = take<int32_t>(ctx, a.n_w);
 	a.x_idx = take<int32_t>(ctx, a.n_x);
 	if (!a.u_idx || !a.w_idx || !a.x_idx) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
-	uw_kernel<<<div_up(nl, 128), 128, 0, s>>>(a, 1, ucnt, wcnt, ctx.dev_flags);
-	x_kernel<<<div_up(C, 128), 128, 0, s>>>(a, 1, xcnt);
+	if (dim == 3) {
+		uw_kernel<3><<<div_up(nl, 128), 128, 0, s>>>(a, 1, ucnt, wcnt, ctx.dev_flags);
+		x_kernel<3><<<div_up(C, 128), 128, 0, s>>>(a, 1, xcnt);
+	} else {
+		uw_kernel<2><<<div_up(nl, 128), 128, 0, s>>>(a, 1, ucnt, wcnt, ctx.dev_flags);
+		x_kernel<2><<<div_up(C, 128), 128, 0, s>>>(a, 1, xcnt);
+	}
 	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+int tree_adaptive_counts(Context& ctx, const DevTree& t, unsigned long long* out)
+{
+	cudaStream_t s = ctx.stream;
+	unsigned long long* dc = take<unsigned long long>(ctx, 8);
+	if (!dc) { ctx.last_error = "adaptive counts: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemsetAsync(dc, 0, 32, s));
+	adaptive_counts_kernel<<<div_up(std::max<size_t>(t.nleaves, 1), 256), 256, 0, s>>>(t, dc);
+	LFMM_CUDA(ctx, cudaMemcpyAsync(out, dc, 32, cudaMemcpyDeviceToHost, s));
+	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	return OK;
 }
 

@@ -81,7 +81,7 @@ class _Solver:
     dim = 3
 
     def __init__(self, *args, eps: float = 1.0e-8, N: int = FMM_AUTO, tree_depth: int = FMM_AUTO,
-                 precision: str = "fp64", max_leaf: int = 0, ctx: Context | None = None):
+                 precision: str = "fp64", max_leaf: int = 0, level_orders=None, ctx: Context | None = None):
         # reference overloads: (particles, eps, N, depth) and (sources, targets, eps, N, depth)
         args = list(args)
         if not args:
@@ -120,10 +120,18 @@ class _Solver:
             self.N = stats.order_N
             self.tree_depth = stats.depth
             return
-        if dim == 3 and max_leaf:
+        if level_orders is not None and dim == 3:
+            # per-level M2L orders (degrees of the sources each level's M2L uses)
             opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
-            st = ctx.lib.lfmm3d_solve_ex(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos),
-                                         ctypes.byref(opts), _ptr(pot), _ptr(fld), ctypes.byref(stats))
+            lv = (ctypes.c_int * max(1, len(level_orders)))(*[int(v) for v in level_orders])
+            st = ctx.lib.lfmm3d_solve_levels(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos),
+                                             ctypes.byref(opts), lv, len(level_orders), _ptr(pot), _ptr(fld),
+                                             ctypes.byref(stats))
+        elif max_leaf:
+            opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], float(eps))
+            fn = ctx.lib.lfmm3d_solve_ex if dim == 3 else ctx.lib.lfmm2d_solve_ex
+            st = fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos), ctypes.byref(opts), _ptr(pot),
+                    _ptr(fld), ctypes.byref(stats))
         else:
             fn = ctx.lib.lfmm3d_solve if dim == 3 else ctx.lib.lfmm2d_solve
             st = fn(ctx.handle, len(spos), _ptr(spos), _ptr(sq), nt, _ptr(tpos), int(N), int(tree_depth),

@@ -1,5 +1,6 @@
-"""CPU restatement of the adaptive octree and its U / V / W / X interaction
-lists, and the coverage property they must satisfy.  TEST INFRASTRUCTURE.
+"""CPU restatement of the adaptive octree / quadtree and its U / V / W / X
+interaction lists, and the coverage property they must satisfy.  TEST
+INFRASTRUCTURE.
 
 The reference builds only uniform trees (cpu/morton_tree.cpp:286-493); the
 adaptive tree has no reference counterpart, so this module restates its
@@ -35,21 +36,22 @@ from __future__ import annotations
 import numpy as np
 
 
-def _coords(code: np.ndarray) -> np.ndarray:
-    """Integer cube coordinates (x, y, z) of level-local Morton codes
-    (bits x<<2 | y<<1 | z per level, the reference's interleave)."""
+def _coords(code: np.ndarray, dim: int = 3) -> np.ndarray:
+    """Integer cube (square) coordinates of level-local Morton codes (bits
+    x<<2 | y<<1 | z per level in 3D, x<<1 | y in 2D: the reference's
+    interleave, cpu/morton_tree.cpp:48-99)."""
     code = np.asarray(code, dtype=np.uint64)
-    out = np.zeros((len(code), 3), np.int64)
-    for d, shift in enumerate((2, 1, 0)):
-        v = code >> np.uint64(shift)
+    out = np.zeros((len(code), dim), np.int64)
+    for d in range(dim):
+        v = code >> np.uint64(dim - 1 - d)
         r = np.zeros(len(code), np.int64)
-        for b in range(21):
-            r |= (((v >> np.uint64(3 * b)) & np.uint64(1)).astype(np.int64)) << b
+        for b in range(64 // dim):
+            r |= (((v >> np.uint64(dim * b)) & np.uint64(1)).astype(np.int64)) << b
         out[:, d] = r
     return out
 
 
-def adaptive_from_uniform(tree: dict, max_leaf: int) -> dict:
+def adaptive_from_uniform(tree: dict, max_leaf: int, dim: int = 3) -> dict:
     """The adaptive tree kept from a uniform tree (the oracle's export: per
     level code, child / particle ranges sb, se, parent) in the solver's
     numbering: kept cells level by level, in the uniform tree's order.
@@ -89,7 +91,7 @@ def adaptive_from_uniform(tree: dict, max_leaf: int) -> dict:
         cells["pend"].append(pe[L][idx].astype(np.int64))
         cells["is_leaf"].append(~sp[idx])
     out = {k_: np.concatenate(v) for k_, v in cells.items()}
-    out["coords"] = _coords(out["code"])
+    out["coords"] = _coords(out["code"], dim)
     out["leaves"] = np.nonzero(out["is_leaf"])[0]
     out["depth"] = D
     return out
@@ -101,7 +103,7 @@ def _touch_matrix(lc, cc, lb, cb):
     lc = np.asarray(lc)[:, None]; lb = np.asarray(lb)[None, :]
     fine = np.maximum(lc, lb)
     ok = np.ones((len(cc), len(cb)), bool)
-    for d in range(3):
+    for d in range(cc.shape[1]):
         a0 = cc[:, d][:, None] << (fine - lc)
         a1 = (cc[:, d][:, None] + 1) << (fine - lc)
         b0 = cb[:, d][None, :] << (fine - lb)

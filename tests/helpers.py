@@ -84,9 +84,10 @@ def assert_trees_equal(a, b, n, exact_positions=True, check_far=True):
             np.testing.assert_array_equal(ta, tb_)
 
 
-def gpu_adaptive_tree(ctx, pts, q, depth, max_leaf, targets=None):
-    """Build the adaptive tree on the GPU and read its cells and U / W / X / V
-    lists back (CSR, global cell indices), in the layout of oracle/adaptive.py."""
+def gpu_adaptive_tree(ctx, pts, q, depth, max_leaf, targets=None, dim=3):
+    """Build the adaptive tree (octree, or quadtree with dim = 2) on the GPU
+    and read its cells and U / W / X / V lists back (CSR, global cell
+    indices), in the layout of oracle/adaptive.py."""
     L = ctx.lib
     pts = np.ascontiguousarray(pts, dtype=np.float64)
     q = np.ascontiguousarray(q, dtype=np.float64)
@@ -94,8 +95,9 @@ def gpu_adaptive_tree(ctx, pts, q, depth, max_leaf, targets=None):
     tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.float64)
     nc, nl = ctypes.c_size_t(), ctypes.c_size_t()
     sizes = np.zeros(4, np.uint64)
-    ctx.check(L.lfmm_tree_build_adaptive(ctx.handle, len(pts), ptr(pts), ptr(q), nt, ptr(tg), depth, max_leaf,
-                                         ctypes.byref(nc), ctypes.byref(nl), ptr(sizes)), "tree_build_adaptive")
+    build = L.lfmm_tree_build_adaptive if dim == 3 else L.lfmm2d_tree_build_adaptive
+    ctx.check(build(ctx.handle, len(pts), ptr(pts), ptr(q), nt, ptr(tg), depth, max_leaf,
+                    ctypes.byref(nc), ctypes.byref(nl), ptr(sizes)), "tree_build_adaptive")
     C, NL = nc.value, nl.value
     level = np.zeros(C, np.int32)
     code = np.zeros(C, np.uint64)

@@ -7,7 +7,7 @@ catches a missing or doubled interaction planted in those lists."""
 import numpy as np
 import pytest
 
-from laplace_fmm_b200.workloads import gaussian_mix3d, plummer_mix3d, uniform3d
+from laplace_fmm_b200.workloads import clustered2d, gaussian_mix3d, plummer_mix3d, uniform3d
 from oracle import adaptive as A
 
 CASES = [("plummer", 4000, 8, 16), ("plummer", 20000, 10, 64), ("gaussian", 6000, 8, 16),
@@ -58,6 +58,52 @@ def _planted(L, kind, row, how):
                                       ("U", "drop"), ("U", "double")])
 def test_planted_mistake_is_caught(built, kind, how):
     cells, L, n = built[1]
+    rows = [i for i, r in enumerate(L[kind]) if len(r)]
+    M = _planted(L, kind, rows[len(rows) // 2], how)
+    with pytest.raises(AssertionError, match="covered"):
+        A.assert_covered_once(cells, M, n)
+
+
+# quadtrees: the 2D half-uniform / half-clustered mixture (64 Gaussians of
+# sigma 0.005 and wider ones) and a uniform set
+CASES2 = [("clustered", 6000, 10, 16, 0.005), ("clustered", 12000, 12, 32, 0.005),
+          ("clustered", 8000, 9, 16, 0.05), ("uniform", 3000, 6, 16, None)]
+
+
+def _set2(kind, n, seed, sigma):
+    if kind == "clustered":
+        return clustered2d(n, seed=seed, clusters=8, sigma=sigma)
+    g = np.random.Generator(np.random.PCG64(seed))
+    return g.random((n, 2)), g.uniform(-1, 1, n)
+
+
+@pytest.fixture(scope="module")
+def built2(oracle):
+    out = {}
+    for i, (kind, n, depth, ml, sig) in enumerate(CASES2):
+        pos, q = _set2(kind, n, 90 + i, sig)
+        cells = A.adaptive_from_uniform(oracle.tree(2, pos, q, depth, halved=False), ml, dim=2)
+        out[i] = (cells, A.lists(cells), n)
+    return out
+
+
+@pytest.mark.parametrize("case", range(len(CASES2)))
+def test_quadtree_every_pair_covered_once(built2, case):
+    cells, L, n = built2[case]
+    assert len(cells["leaves"]) > 1
+    A.assert_covered_once(cells, L, n)
+
+
+def test_quadtree_lists_are_adaptive(built2):
+    cells, L, _ = built2[1]
+    assert len(np.unique(cells["level"][cells["leaves"]])) >= 3
+    assert sum(len(w) for w in L["W"]) > 0
+    assert sum(len(w) for w in L["W"]) == sum(len(x) for x in L["X"])
+
+
+@pytest.mark.parametrize("kind,how", [("V", "drop"), ("W", "drop"), ("X", "double"), ("U", "drop")])
+def test_quadtree_planted_mistake_is_caught(built2, kind, how):
+    cells, L, n = built2[1]
     rows = [i for i, r in enumerate(L[kind]) if len(r)]
     M = _planted(L, kind, rows[len(rows) // 2], how)
     with pytest.raises(AssertionError, match="covered"):

@@ -40,7 +40,7 @@ def test_golden(ctx, name):
     assert rel_l2(fld, g["field"]) < TOL
 
 
-@pytest.mark.parametrize("n,N,depth", [(100000, 21, 7), (20000, 10, 5), (5000, 30, 4), (3000, 1, 4)])
+@pytest.mark.parametrize("n,N,depth", [(100000, 21, 7), (20000, 10, 5), (5000, 30, 4), (3000, 1, 4), (300000, 21, 9)])
 def test_parity_with_oracle(ctx, oracle, n, N, depth):
     g = rng(n + N)
     src = g.random((n, 2)); q = g.uniform(-1, 1, n)
@@ -108,3 +108,14 @@ def test_m2l_engines_agree(ctx, n, N, depth):
     for other in (b, c):
         assert rel_l2(a.potentials, other.potentials) < 1e-13
         assert rel_l2(a.forces, other.forces) < 1e-13
+
+
+@pytest.mark.parametrize("n,depth", [(200000, 10), (200000, 11)])
+def test_parity_with_oracle_deep_clustered(ctx, oracle, n, depth):
+    """The configuration's clustered mixture on the reference's uniform
+    quadtree at the depths its full size uses (10-11 levels)."""
+    src, q = clustered2d(n, seed=depth)
+    f = FastMultipole((src, q), N=21, tree_depth=depth)
+    pot, fld = oracle.fmm2d(src, q, N=21, depth=depth)
+    assert rel_l2(f.potentials, pot) < TOL
+    assert rel_l2(np.stack([f.forces.real, f.forces.imag], 1), fld) < TOL
