@@ -61,10 +61,10 @@ CONFIGS = {
     # (N = 16), the lowest fixed order at which both outputs reach 1e-6 here
     # (N = 15: field 1.007e-6)
     "c3": dict(dim=3, n=16777216, gen="plummer_mix3d", seed=2024, N=16, depth=10, max_leaf=64, precision="mixed",
-               learned=True, tol=1e-6, check_targets=256,
-               workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels, "
-                        "<=64 per leaf), mixed precision at the learned order for rel-L2 <= 1e-6 on potential and "
-                        "field (plain FP64 form at p=15, N=16)"),
+               learned=True, learned_leaf=True, tol=1e-6, check_targets=256,
+               workload="3D Plummer (a=0.05) + uniform 16,777,216 particles, adaptive octree (<=10 levels), mixed "
+                        "precision at the learned order and learned leaf size for rel-L2 <= 1e-6 on potential and "
+                        "field; beside it the plain FP64 form and the mixed form at p=15 (N=16), <=64 per leaf"),
     # 1024 independent problems, N log-uniform in [2048, 262144] (about 60M particles),
     # each uniform in its own unit cube or one Gaussian cluster (sigma 0.05), solved
     # as one batch (mixed, N = 14); the plain FP64 form (p = 10, N = 11) one problem
@@ -352,9 +352,10 @@ def run_ours(args, cfg, rank, world, local_rank):
     learned = bool(cfg.get("learned")) and not args.no_learned
     d_params = None
     info_box = {}
+    learned_leaf = learned and bool(cfg.get("learned_leaf")) and args.max_leaf is None
     if learned:
         from laplace_fmm_b200.order import load_params
-        d_params = torch.from_numpy(load_params()).cuda()
+        d_params = torch.from_numpy(load_params(leaf=learned_leaf)).cuda()
 
     def call(c, device, precision, stats=None, host=None, tree=None):
         """One solve through the C ABI (device buffers, or pinned host buffers);
@@ -363,8 +364,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         depth_, max_leaf_ = tree if tree else (depth, max_leaf)
         src, qq, pot, fld = host if host else (d_src, d_q, d_pot, d_fld)
         sp = ctypes.byref(stats) if stats is not None else None
-        if dim == 3 and learned and precision == prec:
-            opts = LfmmSolveOpts(N, depth, max_leaf, precision, cfg["tol"])
+        if dim == 3 and learned and precision == prec and tree is None:
+            opts = LfmmSolveOpts(N, depth, 2147483647 if learned_leaf else max_leaf, precision, cfg["tol"])
             info = LfmmLearnedInfo()
             fn = L.lfmm3d_solve_learned_device if device else L.lfmm3d_solve_learned
             st = fn(c.handle, n, vp(src.data_ptr()), vp(qq.data_ptr()), 0, None, ctypes.byref(opts),
@@ -433,6 +434,27 @@ def run_ours(args, cfg, rank, world, local_rank):
         t1.synchronize()
         pms = t0.elapsed_time(t1) / reps
         plain = {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pms, "precision": "fp64"}
+    # the mixed form at the configuration's fixed order and leaf size (what the
+    # learned order and leaf size are measured against)
+    mixed_fixed = None
+    if dim == 3 and learned and not args.no_plain:
+        ft = (depth, max_leaf)
+        for _ in range(2):
+            call(ctx_t, True, prec, tree=ft)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t0.record()
+        for _ in range(reps):
+            call(ctx_t, True, prec, tree=ft)
+        with torch.cuda.stream(torch.cuda.ExternalStream(ctx_t.stream)):
+            t1.record()
+        t1.synchronize()
+        fms = t0.elapsed_time(t1) / reps
+        mixed_fixed = {"value": n / (fms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": fms,
+                       "precision": cfg["precision"], "N_degrees": N, "max_leaf": max_leaf,
+                       "what": "the mixed form at the fixed order and leaf size, no prediction or check"}
     # 2D: the reference's uniform quadtree on the same particles beside the adaptive one
     if dim == 2 and max_leaf > 0 and cfg.get("uniform_depth") and not args.no_plain:
         ut = (cfg["uniform_depth"], 0)
@@ -458,7 +480,8 @@ def run_ours(args, cfg, rank, world, local_rank):
     if dim == 3 and max_leaf > 0 and not args.no_plan:
         Nplan = stats.get("order_N") or N
         hp = ctypes.c_void_p()
-        popts = LfmmSolveOpts(Nplan, depth, max_leaf, prec, 1e-8)
+        ml_plan = info_box.get("max_leaf") or max_leaf if learned_leaf else max_leaf
+        popts = LfmmSolveOpts(Nplan, depth, ml_plan, prec, 1e-8)
         ctx.check(L.lfmm3d_plan_create(ctx.handle, n, vp(d_src.data_ptr()), vp(d_q.data_ptr()), ctypes.byref(popts),
                                        ctypes.byref(hp)), "plan")
         for _ in range(max(1, args.warmup)):
@@ -473,7 +496,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         pl_ms = p0.elapsed_time(p1) / args.steps
         L.lfmm3d_plan_destroy(hp)
         plan_line = {"value": world * n / (pl_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pl_ms,
-                     "N_degrees": Nplan, "what": "repeated solves on one geometry: tree and CUDA graph built once"}
+                     "N_degrees": Nplan, "max_leaf": ml_plan,
+                     "what": "repeated solves on one geometry: tree and CUDA graph built once"}
     # accuracy on 4096 seeded targets against the FP64 direct sum (on the GPU)
     idx = sample_targets(n)
     tgt = torch.from_numpy(np.ascontiguousarray(pos[idx])).cuda()
@@ -516,7 +540,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                "h2d_bytes_per_step": int(h_src.numel() * 8 + h_q.numel() * 8),
                "d2h_bytes_per_step": int(h_pot.numel() * 8 + h_fld.numel() * 8)}
     return dict(ms=ms, stats=stats, acc=acc, e2e=e2e, clocks=clk.summary(), torch=torch, dist=dist, ctx=ctx,
-                plain=plain, learned=dict(info_box) if learned else None, plan=plan_line)
+                plain=plain, learned=dict(info_box) if learned else None, plan=plan_line, mixed_fixed=mixed_fixed)
 
 
 def m2l_flops(N):
@@ -1211,6 +1235,9 @@ def main():
             line["config"]["plain_fp64_N_degrees"] = cfg["N"]
         if r["plan"]:
             line["plan_execute"] = r["plan"]
+        if r.get("mixed_fixed"):
+            line["mixed_fixed"] = r["mixed_fixed"]
+            line["speedup_vs_mixed_fixed"] = r["mixed_fixed"]["ms_per_step"] / r["ms"]
         if r["plain"]:
             if cfg["dim"] == 2:
                 line["uniform_tree"] = r["plain"]

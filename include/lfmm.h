@@ -364,6 +364,8 @@ typedef struct {
 	double judged_error;        /* what the judge compared with tol: the larger of the two upper
 	                               confidence bounds (mean + 2 standard errors) of the sampled
 	                               rel-L2 of potential and field (batches: the largest over problems) */
+	int max_leaf;               /* the leaf-size threshold of the tree (picked by the threshold
+	                               network when opts->max_leaf is LFMM_AUTO) */
 } lfmm_learned_info;
 
 /* 3D solve at the order the network picks for tolerance tol, which bounds
@@ -383,7 +385,14 @@ typedef struct {
  * rerun in the FP64 form (fp64_resolved).  params: device pointer to the
  * network (LFMM_MLP_PARAMS floats, inputs unnormalised).  opts gives the
  * tree (tree_depth, max_leaf) and precision; opts->N and opts->eps are
- * ignored.  Synchronises.  Host and device-buffer variants. */
+ * ignored.  opts->max_leaf = LFMM_AUTO: the leaf-size threshold is learned
+ * too -- params then holds the order network followed by the threshold
+ * network (2 LFMM_MLP_PARAMS floats), which predicts the solve's time for
+ * each threshold in {16, 24, 32, 48, 64, 96, 128, 192} from the counts of the
+ * adaptive tree it would give (lfmm3d_leaf_features) at the reference's
+ * automatic order for tol, and the fastest is built (info->max_leaf).  The
+ * reference has a uniform tree and no leaf size (cpu/multipole3d.cpp:1334-1337).
+ * Synchronises.  Host and device-buffer variants. */
 int lfmm3d_solve_learned(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
                          const double* tgt_xyz, const lfmm_solve_opts* opts, const float* params, double tol,
                          int check_targets, double* pot, double* field, lfmm_learned_info* info, lfmm_stats* stats);
@@ -404,6 +413,13 @@ int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int n_prob, const size_t* o
                                       const double* src_q, const lfmm_solve_opts* opts, const float* params,
                                       double tol, int check_targets, double* pot, double* field,
                                       lfmm_learned_info* info, lfmm_stats* stats);
+
+/* The threshold network's inputs: for each candidate leaf-size threshold
+ * cand[k] (K <= 8), 16 features of the adaptive tree it would give (counts of
+ * cells, leaves, sums of squared leaf sizes ...) for a solve at order N;
+ * feats [K][16] (host buffers).  No counterpart in the reference. */
+int lfmm3d_leaf_features(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q, size_t n_tgt,
+                         const double* tgt_xyz, int tree_depth, int N, const int* cand, int K, float* feats);
 
 /* ---- rotation tables (tests) --------------------------------------------
  * Wigner small-d matrix for table slot `slot` (layout n(n+1)(4n-1)/6 +

@@ -31,7 +31,7 @@ EXPORTS = [
     "lfmm_tree_adaptive_lists",
     "lfmm_wignerd_slot",
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
-    "lfmm3d_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
+    "lfmm3d_features", "lfmm3d_leaf_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
     "lfmm3d_solve_batch", "lfmm3d_solve_batch_device", "lfmm3d_solve_batch_learned_device",
     "lfmm3d_plan_create", "lfmm3d_plan_execute", "lfmm3d_plan_destroy",
 ]
@@ -66,7 +66,8 @@ class LfmmLearnedInfo(ctypes.Structure):
     _fields_ = [("order_N", ctypes.c_int), ("predicted_N", ctypes.c_int), ("fallback", ctypes.c_int),
                 ("predicted_error", ctypes.c_double), ("checked_error", ctypes.c_double),
                 ("checked_error_field", ctypes.c_double), ("fp64_resolved", ctypes.c_int),
-                ("predicted_error_field", ctypes.c_double), ("judged_error", ctypes.c_double)]
+                ("predicted_error_field", ctypes.c_double), ("judged_error", ctypes.c_double),
+                ("max_leaf", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -119,6 +120,7 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm_tree_list_sizes.argtypes = [P, I, P, P]
         L.lfmm_tree_lists.argtypes = [P, I, P, P]
         L.lfmm_tree_positions.argtypes = [P, P]
+        L.lfmm3d_leaf_features.argtypes = [P, SZ, P, P, SZ, P, I, I, P, I, P]
         L.lfmm_tree_build_adaptive.argtypes = [P, SZ, P, P, SZ, P, I, I, P, P, P]
         L.lfmm2d_tree_build_adaptive.argtypes = [P, SZ, P, P, SZ, P, I, I, P, P, P]
         L.lfmm_tree_adaptive_cells.argtypes = [P, P, P, P, P, P, P, P, P, P]

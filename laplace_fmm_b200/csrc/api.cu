@@ -823,6 +823,34 @@ int lfmm3d_features(lfmm_ctx* ctx, size_t ns, const double* src, const double* q
 	return st;
 }
 
+int lfmm3d_leaf_features(lfmm_ctx* ctx, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                         int depth, int N, const int* cand, int K, float* feats)
+{
+	if (!ctx || !cand || !feats || K < 1 || K > LEAF_CAND_MAX) return LFMM_ERR_ARG;
+	Context& c = ctx->c;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return LFMM_ERR_ARG; }
+	if ((ns && (!src || !q)) || (nt && !tgt)) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
+	c.arena.reset();
+	ctx->has_tree = false;
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	if (!dsrc || !dq || !dtgt) { c.last_error = "device allocation failed"; return LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
+	if (ns) {
+		LFMM_CUDA(c, cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+	}
+	if (nt) LFMM_CUDA(c, cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+	ParticleInput in;
+	in.dim = 3; in.ns = ns; in.nt = nt; in.src = dsrc; in.srcq = dq; in.tgt = dtgt;
+	int st = leaf_features_host(c, in, resolve_depth(3, depth, ns + nt), N, cand, K, feats);
+	if (st == OK) st = check_flags(c);
+	c.arena.settle();
+	return st;
+}
+
 // ---- tree inspection -------------------------------------------------------
 
 int lfmm_tree_build(lfmm_ctx* ctx, int dim, size_t ns, const double* src, const double* q, size_t nt,

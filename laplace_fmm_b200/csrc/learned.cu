@@ -462,7 +462,74 @@ int sampled_error(Context& ctx, const ParticleInput& in, const Samples& S, const
 	return OK;
 }
 
+// ---- learned leaf-size threshold -------------------------------------------
+// The candidates and the threshold network's 16 inputs for candidate m of a
+// tree of n particles solved at order N, from the counts of the adaptive tree
+// m would give (LeafChooser): the network (same architecture as the order
+// network, output 0 used) predicts log10 of the solve's time, and the
+// fastest candidate is built.
+constexpr int LEAF_CAND[LEAF_CAND_MAX] = {16, 24, 32, 48, 64, 96, 128, 192};
+
+void leaf_features(const unsigned long long* c, int m, int N, size_t n, int depth, float* f)
+{
+	auto lg1 = [](double x) { return (float)std::log10(1.0 + x); };
+	const double cells = (double)c[0], leaves = (double)c[1], c2 = (double)c[2], c4 = (double)c[3];
+	const double s2 = (double)c[4], snp = (double)c[5], last = (double)c[6], deepest = (double)c[7];
+	const double maxleaf = (double)c[8], nn = std::max<double>((double)n, 1.0);
+	f[0] = lg1(nn); f[1] = (float)std::log10((double)m); f[2] = (float)N / 18.f; f[3] = lg1(leaves);
+	f[4] = lg1(cells); f[5] = lg1(c2); f[6] = lg1(c4); f[7] = lg1(s2); f[8] = lg1(snp); f[9] = lg1(s2 / nn);
+	f[10] = (float)(deepest / std::max(depth, 1)); f[11] = lg1(maxleaf); f[12] = (float)(last / nn);
+	f[13] = lg1(nn / std::max(leaves, 1.0)); f[14] = lg1((double)N * N * c2); f[15] = lg1((double)N * N * leaves);
+}
+
+// The reference's automatic order for a tolerance (cpu/multipole3d.cpp:1328-1331),
+// clamped to the network's range: the order the threshold is chosen for
+// before the tree (and so the order prediction) exists.
+int guess_order(double tol)
+{
+	const double e = std::max(tol, 1e-11);
+	const int N = (int)(54.2 - 10.73 * std::sqrt(std::log(2.4 * e) + 25.5));
+	return std::min(std::max(N, 5), FB_N);
+}
+
+// The chooser for tree_build_adaptive: features on the host (8 rows), the
+// network's forward pass on the device, the candidate of least predicted
+// time.  st: the status of the network's launch.
+LeafChooser leaf_chooser(Context& ctx, const float* lparams, int N, size_t n, int depth, int& st)
+{
+	LeafChooser ch;
+	ch.K = LEAF_CAND_MAX;
+	for (int k = 0; k < LEAF_CAND_MAX; ++k) ch.cand[k] = LEAF_CAND[k];
+	ch.pick = [&ctx, lparams, N, n, depth, &st](const unsigned long long* cs) -> int {
+		float F[LEAF_CAND_MAX * NF], Y[LEAF_CAND_MAX * NO];
+		for (int k = 0; k < LEAF_CAND_MAX; ++k) leaf_features(cs + k * LEAF_STATS, LEAF_CAND[k], N, n, depth, F + k * NF);
+		float* dX = take<float>(ctx, LEAF_CAND_MAX * NF);
+		float* dY = take<float>(ctx, LEAF_CAND_MAX * NO);
+		if (!dX || !dY) { ctx.last_error = "leaf threshold: allocation failed"; st = ERR_OOM; return -1; }
+		cudaError_t e = cudaMemcpyAsync(dX, F, sizeof(F), cudaMemcpyHostToDevice, ctx.stream);
+		if (e != cudaSuccess) { st = cuda_fail(ctx, e, "leaf threshold"); return -1; }
+		if ((st = mlp_forward_device(ctx, lparams, LEAF_CAND_MAX, dX, dY))) return -1;
+		e = cudaMemcpyAsync(Y, dY, sizeof(Y), cudaMemcpyDeviceToHost, ctx.stream);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+		if (e != cudaSuccess) { st = cuda_fail(ctx, e, "leaf threshold"); return -1; }
+		int best = 0;
+		for (int k = 1; k < LEAF_CAND_MAX; ++k)
+			if (Y[k * NO] < Y[best * NO]) best = k;
+		return best;
+	};
+	return ch;
+}
+
 } // namespace
+
+int leaf_features_host(Context& ctx, const ParticleInput& in, int depth, int N, const int* cand, int K, float* feats)
+{
+	unsigned long long cs[LEAF_CAND_MAX * LEAF_STATS];
+	int st = leaf_candidate_stats(ctx, in, depth, cand, K, cs);
+	if (st) return st;
+	for (int k = 0; k < K; ++k) leaf_features(cs + k * LEAF_STATS, cand[k], N, in.ns + in.nt, depth, feats + k * NF);
+	return OK;
+}
 
 int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int max_leaf, int precision,
                          const float* params, double tol, int check_targets, double* pot, double* field,
@@ -485,14 +552,20 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	DevTree t;
 	double* pacc = nullptr;
 	double rms[2] = {0.0, 0.0};
-	if ((st = tree_build_adaptive(ctx, in, depth, max_leaf, t)) ||
+	// max_leaf LFMM_AUTO: the threshold network (following the order network in params) picks it
+	const bool auto_leaf = max_leaf == LFMM_AUTO;
+	int cst = OK;
+	LeafChooser chooser;
+	if (auto_leaf) chooser = leaf_chooser(ctx, params + LFMM_MLP_PARAMS, guess_order(tol), in.ns + in.nt, depth, cst);
+	if ((st = tree_build_adaptive(ctx, in, depth, auto_leaf ? 0 : max_leaf, t, auto_leaf ? &chooser : nullptr)) ||
 	    (timing && (st = cudaEventRecord(ctx.ev[1], s) == cudaSuccess ? OK : ERR_CUDA)) ||
 	    (st = learned_predict_launch(ctx, t, params, pacc)) || (st = samples_join(ctx, S, rms))) {
 		cudaStreamSynchronize(ctx.side);
-		return st;
+		return cst ? cst : st;
 	}
 	int N = FB_N;
 	lfmm_learned_info li{};
+	li.max_leaf = auto_leaf ? chooser.cand[chooser.chosen] : max_leaf;
 	double ep[NP], ef[NP];
 	if ((st = learned_predictions(ctx, pacc, rms, ep, ef))) return st;
 	const double target = std::log10(tol * LEARNED_MARGIN);
@@ -551,8 +624,12 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	const int P = in.nprob;
 	cudaStream_t s = ctx.stream;
 	DevTree t;
-	int st = tree_build_adaptive(ctx, in, depth, max_leaf, t);
-	if (st) return st;
+	const bool auto_leaf = max_leaf == LFMM_AUTO;
+	int cst = OK;
+	LeafChooser chooser;
+	if (auto_leaf) chooser = leaf_chooser(ctx, params + LFMM_MLP_PARAMS, guess_order(tol), in.ns, depth, cst);
+	int st = tree_build_adaptive(ctx, in, depth, auto_leaf ? 0 : max_leaf, t, auto_leaf ? &chooser : nullptr);
+	if (st) return cst ? cst : st;
 	// samples: up to check_targets outputs of every problem, evenly spaced
 	std::vector<uint32_t> hidx;
 	std::vector<int32_t> hprob;
@@ -600,6 +677,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	int N = 5;
 	lfmm_learned_info li{};
+	li.max_leaf = auto_leaf ? chooser.cand[chooser.chosen] : max_leaf;
 	for (int k = 0; k < P; ++k) {
 		const size_t mk = soff[k + 1] - soff[k];
 		const double* hk = hp.data() + (size_t)k * (NO + 1);
@@ -662,8 +740,8 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 			pk.dim = 3; pk.ns = hoff[k + 1] - hoff[k]; pk.nt = 0;
 			pk.src = in.src + 3 * hoff[k]; pk.srcq = in.srcq + hoff[k];
 			const size_t mark = ctx.arena.mark();
-			st = fmm3d_solve_scaled(ctx, pk, FB_N, depth, max_leaf, LFMM_PRECISION_FP64, pot + hoff[k], field + 3 * hoff[k],
-			                        nullptr, nullptr);
+			st = fmm3d_solve_scaled(ctx, pk, FB_N, depth, li.max_leaf, LFMM_PRECISION_FP64, pot + hoff[k],
+			                        field + 3 * hoff[k], nullptr, nullptr);
 			ctx.arena.rewind(mark);
 			if (st) return st;
 			++li.fp64_resolved;

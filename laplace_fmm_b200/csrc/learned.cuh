@@ -24,6 +24,10 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
                                int precision, const float* params, double tol, int check_targets, double* pot,
                                double* field, lfmm_learned_info* info, SolveStats* stats);
 
+// The threshold network's inputs [K][16] for candidate leaf-size thresholds
+// cand[K] (K <= 8) at order N (host buffer).
+int leaf_features_host(Context& ctx, const ParticleInput& in, int depth, int N, const int* cand, int K, float* feats);
+
 // Per-leaf features [n_leaves][16] and the leaf of every input particle
 // (host buffers; either may be null).
 int features_tree(Context& ctx, const ParticleInput& in, int depth, int max_leaf, float* feats_host, size_t cap,

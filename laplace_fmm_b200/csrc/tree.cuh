@@ -2,6 +2,7 @@
 // reference's MortonTree (reference cpu/morton_tree.cpp:286-493).
 #pragma once
 #include "context.cuh"
+#include <functional>
 
 namespace lfmm {
 
@@ -87,7 +88,27 @@ int tree_lists(Context& ctx, DevTree& t);
 // every cell: the uniform tree in adaptive form).  Leaves may sit on any
 // level; beg/end hold child ranges (empty for leaves), pbeg/pend particle
 // ranges; U/W/X lists are built (quadtree or octree).
-int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& t);
+// Leaf-size candidates: the counts of the adaptive tree each candidate
+// threshold would give, taken from the uniform tree in one pass per level
+// (a cell is kept when its parent holds more than m particles -- counts only
+// shrink down the tree -- and a kept cell is a leaf when it holds at most m
+// or sits on the last level).  Per candidate, LEAF_STATS words: cells,
+// leaves, cells on levels >= 2, cells on levels >= 4, sum over leaves of n^2,
+// sum over leaves of n * n(parent), particles in last-level leaves, deepest
+// kept level, largest leaf.
+constexpr int LEAF_STATS = 9, LEAF_CAND_MAX = 8;
+struct LeafChooser {
+	int K = 0;
+	int cand[LEAF_CAND_MAX] = {};
+	// called with [K][LEAF_STATS] counts; returns the index of the candidate to build
+	std::function<int(const unsigned long long* stats)> pick;
+	int chosen = -1;     // set by tree_build_adaptive
+};
+int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& t,
+                        LeafChooser* choose = nullptr);
+// The candidates' counts alone (no adaptive tree is built): stats [K][LEAF_STATS] on the host.
+int leaf_candidate_stats(Context& ctx, const ParticleInput& in, int depth, const int* cand, int K,
+                         unsigned long long* stats);
 
 // Interaction counts of an adaptive tree (synchronises): out[0] V pairs,
 // out[1] U entries, out[2] P2P particle pairs, out[3] M2P (target, cell) pairs.

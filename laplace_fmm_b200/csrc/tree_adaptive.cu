@@ -255,6 +255,46 @@ __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 	if (!pass) xcnt[g] = nx;
 }
 
+// Candidate thresholds' counts for the uniform cells of level L (see
+// LeafChooser); acc [K][LEAF_STATS].
+__global__ void leaf_candidates_kernel(DevTree u, int L, const uint32_t* __restrict__ pb,
+                                       const uint32_t* __restrict__ pe, const int* __restrict__ cand, int K,
+                                       unsigned long long* __restrict__ acc)
+{
+	const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const bool valid = c < u.lsize[L];
+	unsigned long long n = 0, np = 0;
+	if (valid) {
+		const size_t g = u.loff[L] + c;
+		n = pe[g] - pb[g];
+		if (L > 0) {
+			const size_t gp = u.loff[L - 1] + (size_t)u.parent[g];
+			np = pe[gp] - pb[gp];
+		}
+	}
+	const bool last = L == u.depth - 1;
+	for (int k = 0; k < K; ++k) {
+		const unsigned long long m = (unsigned long long)cand[k];
+		const bool kept = valid && (L == 0 || np > m);
+		const bool leaf = kept && (n <= m || last);
+		unsigned long long v[LEAF_STATS] = {kept, leaf, kept && L >= 2, kept && L >= 4, leaf ? n * n : 0,
+		                                    leaf ? n * np : 0, leaf && last ? n : 0, kept ? (unsigned long long)L : 0,
+		                                    leaf ? n : 0};
+#pragma unroll
+		for (int j = 0; j < LEAF_STATS; ++j) {
+			unsigned long long x = v[j];
+			for (int o = 16; o; o >>= 1) {
+				const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+				x = j >= 7 ? (x > y ? x : y) : x + y;
+			}
+			if ((threadIdx.x & 31) == 0 && x) {
+				if (j >= 7) atomicMax(&acc[k * LEAF_STATS + j], x);
+				else atomicAdd(&acc[k * LEAF_STATS + j], x);
+			}
+		}
+	}
+}
+
 // Interaction counts of an adaptive tree: far (V) pairs, U entries, P2P
 // particle pairs (targets x sources of the leaf and its U list), M2P
 // (target, W cell) pairs.
@@ -285,17 +325,72 @@ T* take(Context& ctx, size_t count) { return static_cast<T*>(ctx.arena.take(size
 
 } // namespace
 
-int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& a)
+namespace {
+
+// The uniform tree and the particle range of each of its cells (pb, pe).
+int uniform_with_ranges(Context& ctx, const ParticleInput& in, int depth, DevTree& u, uint32_t*& pb, uint32_t*& pe)
 {
 	if (depth < 1 || depth > 16) { ctx.last_error = "adaptive tree: depth must be in [1, 16]"; return ERR_ARG; }
-	DevTree u;
 	int st = tree_build(ctx, in, depth, u, /*partition=*/false, /*lists=*/false);
 	if (st) return st;
+	pb = take<uint32_t>(ctx, u.ncells);
+	pe = take<uint32_t>(ctx, u.ncells);
+	if (!pb || !pe) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
+	for (int L = depth - 1; L >= 0; --L)
+		uprange_kernel<<<div_up(u.lsize[L], 256), 256, 0, ctx.stream>>>(u, L, pb, pe);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
+
+int candidate_counts(Context& ctx, const DevTree& u, const uint32_t* pb, const uint32_t* pe, const int* cand, int K,
+                     unsigned long long* stats)
+{
+	if (K < 1 || K > LEAF_CAND_MAX) { ctx.last_error = "leaf candidates: 1 to 8 thresholds"; return ERR_ARG; }
+	for (int k = 0; k < K; ++k)
+		if (cand[k] < 1) { ctx.last_error = "leaf candidates: thresholds must be >= 1"; return ERR_ARG; }
+	cudaStream_t s = ctx.stream;
+	int* dc = take<int>(ctx, LEAF_CAND_MAX);
+	unsigned long long* acc = take<unsigned long long>(ctx, LEAF_CAND_MAX * LEAF_STATS);
+	if (!dc || !acc) { ctx.last_error = "leaf candidates: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemcpyAsync(dc, cand, sizeof(int) * K, cudaMemcpyHostToDevice, s));
+	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * K * LEAF_STATS, s));
+	for (int L = 0; L < u.depth; ++L)
+		if (u.lsize[L]) leaf_candidates_kernel<<<div_up(u.lsize[L], 256), 256, 0, s>>>(u, L, pb, pe, dc, K, acc);
+	LFMM_CUDA(ctx, cudaMemcpyAsync(stats, acc, sizeof(unsigned long long) * K * LEAF_STATS, cudaMemcpyDeviceToHost, s));
+	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
+	return OK;
+}
+
+} // namespace
+
+int leaf_candidate_stats(Context& ctx, const ParticleInput& in, int depth, const int* cand, int K,
+                         unsigned long long* stats)
+{
+	DevTree u;
+	uint32_t *pb = nullptr, *pe = nullptr;
+	int st = uniform_with_ranges(ctx, in, depth, u, pb, pe);
+	if (st) return st;
+	return candidate_counts(ctx, u, pb, pe, cand, K, stats);
+}
+
+int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int max_leaf, DevTree& a,
+                        LeafChooser* choose)
+{
+	DevTree u;
+	uint32_t *pb = nullptr, *pe = nullptr;
+	int st = uniform_with_ranges(ctx, in, depth, u, pb, pe);
+	if (st) return st;
+	if (choose) {
+		unsigned long long cs[LEAF_CAND_MAX * LEAF_STATS];
+		if ((st = candidate_counts(ctx, u, pb, pe, choose->cand, choose->K, cs))) return st;
+		const int k = choose->pick(cs);
+		if (k < 0 || k >= choose->K) { ctx.last_error = "leaf candidates: no threshold picked"; return ERR_CUDA; }
+		choose->chosen = k;
+		max_leaf = choose->cand[k];
+	}
 	cudaStream_t s = ctx.stream;
 	const unsigned TB = 256;
 	const size_t UC = u.ncells;
-	uint32_t* pb = take<uint32_t>(ctx, UC);
-	uint32_t* pe = take<uint32_t>(ctx, UC);
 	uint8_t* keep = take<uint8_t>(ctx, UC);
 	uint8_t* split = take<uint8_t>(ctx, UC);
 	uint32_t* keep32 = take<uint32_t>(ctx, UC);
@@ -304,9 +399,7 @@ int tree_build_adaptive(Context& ctx, const ParticleInput& in, int depth, int ma
 	size_t maxl = 0;
 	for (int L = 0; L < depth; ++L) maxl = std::max(maxl, u.lsize[L]);
 	uint32_t* scr = take<uint32_t>(ctx, scan_scratch_words(std::max(UC, maxl)) + 64);
-	if (!pb || !pe || !keep || !split || !keep32 || !map || !tot || !scr) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
-	for (int L = depth - 1; L >= 0; --L)
-		uprange_kernel<<<div_up(u.lsize[L], TB), TB, 0, s>>>(u, L, pb, pe);
+	if (!keep || !split || !keep32 || !map || !tot || !scr) { ctx.last_error = "adaptive tree: allocation failed"; return ERR_OOM; }
 	for (int L = 0; L < depth; ++L) {
 		keep_kernel<<<div_up(u.lsize[L], TB), TB, 0, s>>>(u, L, pb, pe, keep, split, keep32 + u.loff[L], max_leaf);
 		scan_exclusive_u32(keep32 + u.loff[L], map + u.loff[L], u.lsize[L], tot + L, scr, s);

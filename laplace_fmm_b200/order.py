@@ -199,20 +199,54 @@ def features(src, q, targets=None, tree_depth: int = 10, max_leaf: int = 64, ctx
     return feats[:nl.value].copy(), leaf_of
 
 
-def load_params(path: Path | str = WEIGHTS) -> np.ndarray:
-    """The trained network (input normalisation folded in) shipped with the package."""
-    return np.load(path)["folded"].astype(np.float32)
+def load_params(path: Path | str = WEIGHTS, leaf: bool = False) -> np.ndarray:
+    """The trained order network (input normalisation folded in) shipped with
+    the package; leaf=True appends the leaf-size threshold network, the
+    buffer the solver takes when the threshold is learned too (max_leaf
+    LFMM_AUTO)."""
+    z = np.load(path)
+    p = z["folded"].astype(np.float32)
+    if leaf:
+        if "leaf_folded" not in z:
+            raise LfmmError(f"{path} holds no threshold network (train it: python -m laplace_fmm_b200.train_order --leaf)")
+        p = np.concatenate([p, z["leaf_folded"].astype(np.float32)])
+    return p
+
+
+# the leaf-size thresholds the threshold network chooses among (the solver's list)
+LEAF_CANDIDATES = (16, 24, 32, 48, 64, 96, 128, 192)
+
+
+def leaf_features(src, q, N: int, tree_depth: int = 10, candidates=LEAF_CANDIDATES, ctx: Context | None = None):
+    """The threshold network's inputs [K][16]: per candidate threshold, the
+    counts of the adaptive tree it would give, at order N."""
+    ctx = ctx or default_context(0)
+    src, q = _f64(src, 3), _f64(q, 0)
+    cand = (ctypes.c_int * len(candidates))(*candidates)
+    feats = np.zeros((len(candidates), N_IN), np.float32)
+    ctx.check(ctx.lib.lfmm3d_leaf_features(ctx.handle, len(src), _p(src), _p(q), 0, None, int(tree_depth), int(N),
+                                           cand, len(candidates), _p(feats)), "lfmm3d_leaf_features")
+    return feats
 
 
 class LearnedSolver:
     """3D solve at the order the network picks for a tolerance, with the
     fixed-order fallback judged by a sampled FP64 direct-sum check."""
 
-    def __init__(self, params: np.ndarray | None = None, ctx: Context | None = None):
+    def __init__(self, params: np.ndarray | None = None, ctx: Context | None = None, leaf: bool = False):
+        """leaf=True: the threshold network too (solve with max_leaf="auto")."""
         torch = _torch()
         self.ctx = ctx or default_context(0)
-        p = load_params() if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        p = load_params(leaf=leaf) if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        self.leaf = len(p) == 2 * N_PARAMS
         self.d_params = torch.from_numpy(p).to(torch.device("cuda", self.ctx.device))
+
+    def _leaf(self, max_leaf):
+        if max_leaf == "auto":
+            if not self.leaf:
+                raise LfmmError("max_leaf='auto' needs the threshold network (LearnedSolver(leaf=True))")
+            return 2147483647
+        return int(max_leaf)
 
     def solve(self, src, q, targets=None, tol: float = 1e-6, tree_depth: int = 10, max_leaf: int = 64,
               precision: str = "mixed", check_targets: int = 256, stats: bool = False):
@@ -222,7 +256,7 @@ class LearnedSolver:
         nout = nt if nt else len(src)
         pot = np.zeros(nout)
         fld = np.zeros((nout, 3))
-        opts = LfmmSolveOpts(0, tree_depth, max_leaf, PRECISION[precision], tol)
+        opts = LfmmSolveOpts(0, tree_depth, self._leaf(max_leaf), PRECISION[precision], tol)
         info = LfmmLearnedInfo()
         st = LfmmStats()
         _torch().cuda.synchronize(self.d_params.device)
@@ -250,7 +284,7 @@ class LearnedSolver:
         n = int(offs[-1])
         d_pot = torch.empty(n, dtype=torch.float64, device=dev)
         d_fld = torch.empty(n, 3, dtype=torch.float64, device=dev)
-        opts = LfmmSolveOpts(0, tree_depth, max_leaf, PRECISION[precision], tol)
+        opts = LfmmSolveOpts(0, tree_depth, self._leaf(max_leaf), PRECISION[precision], tol)
         info = LfmmLearnedInfo()
         vp = ctypes.c_void_p
         torch.cuda.synchronize(dev)

@@ -17,6 +17,13 @@ term removed) or the RMS field, give the problem's rel-L2 of each output.
 The solver gets those RMS values from the same sampled direct sum that
 judges its result.  Leaves without a sampled target are masked out.
 
+Threshold network (``--leaf``): the same architecture, output 0 = log10 of
+the solve's device time; rows = (problem, order N in {12, 16}, leaf-size
+threshold in {16, ..., 192}), inputs = the counts of the adaptive tree that
+threshold gives (``lfmm3d_leaf_features``), labels = the timed mixed solve
+(least of three after a warm-up); the solver builds the threshold of least
+predicted time.
+
 Training: Adam (lr 1e-3), batches of 4096 leaves, masked mean-squared error,
 all in the library's CUDA kernels.  The held-out problems measure what the
 network gains over the fixed order: the order it picks for tolerance 1e-6
@@ -35,7 +42,8 @@ from pathlib import Path
 import numpy as np
 
 from ._lib import LfmmSolveOpts, default_context
-from .order import N_ORD, N_OUT, ORDERS, WEIGHTS, LearnedSolver, OrderMLP, features
+from .order import (LEAF_CANDIDATES, N_ORD, N_OUT, N_PARAMS, ORDERS, WEIGHTS, LearnedSolver, OrderMLP, features,
+                    leaf_features)
 from .workloads import gaussian_mix3d, plummer_mix3d
 
 DEPTH, MAX_LEAF, SAMPLES = 10, 64, 1024
@@ -46,8 +54,13 @@ def problem(i: int, kind: str):
     N log-uniform in [1e4, 1e6]) or 'large' (N log-uniform in [1e6, 8e6]:
     Gaussian clusters, or a Plummer sphere of scale radius log-uniform in
     [0.02, 0.1] mixed 50/50 with a uniform background)."""
-    base = {"train": 10_000, "heldout": 90_000, "large": 50_000}[kind]
+    base = {"train": 10_000, "heldout": 90_000, "large": 50_000, "xl": 70_000}[kind]
     g = np.random.default_rng(base + i)
+    if kind == "xl":
+        # 8e6-16.8e6 particles: a Plummer sphere in a uniform background
+        n = int(round(10 ** g.uniform(np.log10(8e6), np.log10(16.8e6))))
+        a = float(10 ** g.uniform(np.log10(0.03), np.log10(0.08)))
+        return plummer_mix3d(n, seed=base + i, a=a)
     if kind != "large":
         n = int(round(10 ** g.uniform(4.0, 6.0)))
         return gaussian_mix3d(n, seed=base + i)
@@ -115,6 +128,106 @@ def label(ctx, pos, q, seed):
     return feats, T, M, err, errf, scale, fscale
 
 
+LEAF_ORDERS = (12, 16)       # orders (degrees) the threshold labels are timed at
+
+
+def time_solves(ctx, pos, q, N, thresholds, reps=3):
+    """Device time (ms, CUDA events on the solver's stream, the least of reps
+    after one warm-up) of the mixed solve at order N for each leaf-size
+    threshold."""
+    import ctypes
+    import torch
+    vp = ctypes.c_void_p
+    n = len(pos)
+    ds, dq = torch.from_numpy(pos).cuda(), torch.from_numpy(q).cuda()
+    pot = torch.empty(n, dtype=torch.float64, device="cuda")
+    fld = torch.empty(n, 3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = []
+    for m in thresholds:
+        opts = LfmmSolveOpts(N, DEPTH, int(m), 1, 1e-8)
+        best = 1e30
+        for r in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(ctx.lib.lfmm3d_solve_ex_device(ctx.handle, n, vp(ds.data_ptr()), vp(dq.data_ptr()), 0, None,
+                                                     ctypes.byref(opts), vp(pot.data_ptr()), vp(fld.data_ptr()),
+                                                     None), "solve")
+            e1.record(stream)
+            e1.synchronize()
+            if r:
+                best = min(best, e0.elapsed_time(e1))
+        out.append(best)
+    return np.array(out)
+
+
+def label_leaf(ctx, pos, q):
+    """Threshold-network rows of one problem: features [len(LEAF_ORDERS) * K][16]
+    and the log10 solve time of each (order, threshold)."""
+    X, T = [], []
+    for N in LEAF_ORDERS:
+        X.append(leaf_features(pos, q, N, tree_depth=DEPTH, ctx=ctx))
+        T.append(np.log10(time_solves(ctx, pos, q, N, LEAF_CANDIDATES)))
+    return np.concatenate(X), np.concatenate(T)
+
+
+def train_leaf(a, ctx):
+    """Label, train and evaluate the threshold network; stores it beside the
+    order network in the weights file.  Returns the summary."""
+    t0 = time.time()
+    rows = {"train": [], "heldout": []}
+    sets = (("train", a.leaf_train), ("large", a.large), ("xl", a.xl), ("heldout", a.leaf_heldout))
+    for kind, count in sets:
+        for i in range(count):
+            pos, q = problem(i, kind)
+            X, T = label_leaf(ctx, pos, q)
+            rows["heldout" if kind == "heldout" else "train"].append((kind, i, len(pos), X, T))
+    t_label = time.time() - t0
+    X = np.concatenate([r[3] for r in rows["train"]])
+    Tl = np.concatenate([r[4] for r in rows["train"]])
+    T = np.zeros((len(X), N_OUT), np.float32)
+    M = np.zeros((len(X), N_OUT), np.float32)
+    T[:, 0] = Tl
+    M[:, 0] = 1.0
+    net = OrderMLP(seed=5, ctx=ctx, x_mean=X.mean(0), x_std=X.std(0) + 1e-6)
+    Xn = net.normalise(X)
+    g = np.random.default_rng(4)
+    losses = []
+    for ep in range(a.leaf_epochs):
+        perm = g.permutation(len(Xn))
+        tot = 0.0
+        for b in range(0, len(perm), a.leaf_batch):
+            j = perm[b:b + a.leaf_batch]
+            tot += net.train_step(Xn[j], T[j], M[j], lr=a.lr) * len(j)
+        losses.append(tot / len(perm))
+    K = len(LEAF_CANDIDATES)
+
+    def evaluate(rs):
+        picked_ratio, at64_ratio, hits = [], [], 0
+        for kind, i, n, Xr, Tr in rs:
+            for j in range(len(LEAF_ORDERS)):
+                y = net.forward(Xr[j * K:(j + 1) * K])[:, 0]
+                t = 10.0 ** Tr[j * K:(j + 1) * K]
+                k = int(np.argmin(y))
+                picked_ratio.append(t[k] / t.min())
+                at64_ratio.append(t[LEAF_CANDIDATES.index(64)] / t[k])
+                hits += int(k == int(np.argmin(t)))
+        return {"mean_time_over_best": float(np.mean(picked_ratio)),
+                "worst_time_over_best": float(np.max(picked_ratio)),
+                "mean_speedup_over_64": float(np.mean(at64_ratio)),
+                "best_picked": hits, "cases": len(picked_ratio)}
+
+    summary = {"leaf_train_problems": len(rows["train"]), "leaf_heldout_problems": len(rows["heldout"]),
+               "rows": int(len(X)), "candidates": list(LEAF_CANDIDATES), "orders": list(LEAF_ORDERS),
+               "loss_first": losses[0], "loss_last": losses[-1], "label_s": t_label,
+               "train": evaluate(rows["train"]), "heldout": evaluate(rows["heldout"])}
+    z = dict(np.load(a.out))
+    z.update(leaf_params=net.params_host(), leaf_folded=net.folded_params(), leaf_x_mean=net.x_mean,
+             leaf_x_std=net.x_std, leaf_losses=np.array(losses), leaf_summary=np.asarray(json.dumps(summary)))
+    np.savez(a.out, **z)
+    return summary
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=512)
@@ -128,8 +241,19 @@ def main(argv=None):
                     help="calibration: the quantile of the training problems' shortfall added to the outputs")
     ap.add_argument("--data", default=None, help="save the labelled problems here (npz)")
     ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--leaf", action="store_true",
+                    help="train only the leaf-size threshold network (the order network in --out is kept)")
+    ap.add_argument("--leaf-train", type=int, default=256, help="training problems timed for the threshold labels")
+    ap.add_argument("--leaf-heldout", type=int, default=32)
+    ap.add_argument("--xl", type=int, default=4, help="problems of 8e6-16.8e6 particles in the threshold labels")
+    ap.add_argument("--leaf-epochs", type=int, default=400)
+    ap.add_argument("--leaf-batch", type=int, default=256)
     a = ap.parse_args(argv)
     ctx = default_context(0)
+    if a.leaf:
+        summary = train_leaf(a, ctx)
+        print(json.dumps(summary))
+        return 0
     t0 = time.time()
     data = {"train": [], "heldout": []}
     for kind, count in (("train", a.train), ("large", a.large), ("heldout", a.heldout)):

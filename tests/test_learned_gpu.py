@@ -144,3 +144,29 @@ def test_shipped_weights_have_the_kernel_layout():
         pytest.skip("trained network not present")
     p = load_params()
     assert p.shape == (N_PARAMS,) and np.all(np.isfinite(p))
+
+
+def test_shipped_threshold_network():
+    if not WEIGHTS.exists():
+        pytest.skip("trained network not present")
+    p = load_params(leaf=True)
+    assert p.shape == (2 * N_PARAMS,) and np.all(np.isfinite(p))
+
+
+def test_learned_leaf_size(ctx):
+    """max_leaf 'auto': the threshold network picks one of the candidates from
+    the counts of the trees they give; the solve is within tolerance and equals
+    the plain solve at that order and leaf size."""
+    from laplace_fmm_b200.order import LEAF_CANDIDATES, leaf_features
+    src, q = gaussian_mix3d(200000, seed=90041)
+    X = leaf_features(src, q, 16, ctx=ctx)
+    assert X.shape == (len(LEAF_CANDIDATES), 16) and np.all(np.isfinite(X))
+    assert np.all(np.diff(X[:, 3]) <= 0)      # fewer leaves as the threshold grows
+    s = LearnedSolver(ctx=ctx, leaf=True)
+    r = s.solve(src, q, tol=TOL, max_leaf="auto", check_targets=1024)
+    info = r["info"]
+    assert info["max_leaf"] in LEAF_CANDIDATES
+    assert max(info["checked_error"], info["checked_error_field"]) <= TOL
+    f = FastMultipole3d((src, q), N=info["order_N"], tree_depth=10, max_leaf=info["max_leaf"], precision="mixed",
+                        ctx=ctx)
+    assert rel_l2(noself(r["potentials"], q), noself(f.potentials, q)) < 1e-12
