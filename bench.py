@@ -70,21 +70,21 @@ CONFIGS = {
     # as one batch (mixed, N = 14); the plain FP64 form (p = 10, N = 11) one problem
     # at a time beside it
     "c5": dict(dim=3, batch=True, count=1024, seed=5150, N=14, plain_N=11, depth=10, max_leaf=64,
-               precision="mixed", n=0, learned=True, tol=1e-6, check_targets=32,
+               precision="mixed", n=0, learned=True, learned_leaf=True, tol=1e-6, check_targets=128,
                workload="batched 3D: 1024 problems, N log-uniform in [2048, 262144], uniform or one Gaussian "
-                        "cluster (sigma 0.05) each, mixed precision at the learned order for rel-L2 <= 1e-6 "
-                        "(32 checked outputs per problem), adaptive octrees (<=10 levels, <=64 per leaf); "
+                        "cluster (sigma 0.05) each, mixed precision at the learned order and leaf size for rel-L2 "
+                        "<= 1e-6 (128 checked outputs per problem), adaptive octrees (<=10 levels); "
                         "plain FP64 p=10 one problem at a time beside it"),
     # learned order on the 64 held-out problems of the order network (1-8
     # Gaussian clusters, N log-uniform in [1e4, 1e6]) at tol 1e-6 on potential
     # and field, against the lowest single fixed order that meets tol on all 64
     "c4": dict(dim=3, heldout=True, count=64, n=0, N=17, depth=10, max_leaf=64, precision="mixed", learned=True,
-               tol=1e-6, check_targets=256,
+               learned_leaf=True, tol=1e-6, check_targets=1024,
                metric="3D FMM Mparticles/s at rel-L2<=1e-6 vs FP64 direct: learned order vs best fixed order",
                workload="learned order, 3D: the 64 held-out problems (1-8 Gaussian clusters, sigma log-uniform in "
-                        "[0.005, 0.2], N log-uniform in [1e4, 1e6]), mixed precision, adaptive octrees (<=10 levels, "
-                        "<=64 per leaf), tol 1e-6 on potential and field; the lowest fixed order meeting tol on all 64 "
-                        "beside it"),
+                        "[0.005, 0.2], N log-uniform in [1e4, 1e6]), mixed precision, adaptive octrees (<=10 levels), "
+                        "learned order and leaf size, tol 1e-6 on potential and field (1024 checked outputs); the "
+                        "lowest fixed order meeting tol on all 64 at <=64 per leaf beside it"),
     # vector charges (the reference's FastMultipole3d<Vector3d>): 4,194,304 particles of the
     # clustered mixture, charges U(-1, 1)^3, mixed precision, N = 12, adaptive octree;
     # the FP64 form beside it
@@ -105,6 +105,9 @@ def parse():
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-series", action="store_true",
+                    help="with --impl reference: the reference CPU FMM on 1/64, 1/16 and 1/4 of the set (one solve "
+                         "each, uniform depth three levels below its own automatic depth)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the mixed one")
     ap.add_argument("--no-learned", action="store_true", help="mixed form at the fixed order N instead of the learned one")
@@ -725,12 +728,14 @@ def run_batch(args, cfg):
     d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
     d_fld = torch.empty(n, 3, dtype=torch.float64, device="cuda")
     stream = torch.cuda.ExternalStream(ctx.stream)
-    opts = LfmmSolveOpts(cfg["N"], cfg["depth"], cfg["max_leaf"], PRECISION[cfg["precision"]], 1e-8)
     learned = bool(cfg.get("learned")) and not args.no_learned
+    learned_leaf = learned and bool(cfg.get("learned_leaf"))
+    opts = LfmmSolveOpts(cfg["N"], cfg["depth"], 2147483647 if learned_leaf else cfg["max_leaf"],
+                         PRECISION[cfg["precision"]], 1e-8)
     info = LfmmLearnedInfo()
     if learned:
         from laplace_fmm_b200.order import load_params
-        d_params = torch.from_numpy(load_params()).cuda()
+        d_params = torch.from_numpy(load_params(leaf=learned_leaf)).cuda()
 
     def step():
         if learned:
@@ -755,12 +760,13 @@ def run_batch(args, cfg):
             ends[k].record(stream)
         torch.cuda.synchronize()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
-    # per-problem accuracy: 64 evenly spread targets of every problem against its own FP64 direct sum
+    # per-problem accuracy against its own FP64 direct sum: every output of a problem of up to 8192
+    # particles, 64 evenly spread outputs of a larger one
     pot, fld = d_pot.cpu().numpy(), d_fld.cpu().numpy()
     errs_p, errs_f = [], []
     for k, (p, c) in enumerate(probs):
         b = int(offs[k])
-        idx = np.arange(0, len(p), max(1, len(p) // 64))
+        idx = np.arange(len(p)) if len(p) <= 8192 else np.arange(0, len(p), len(p) // 64)
         tgt = torch.from_numpy(np.ascontiguousarray(p[idx])).cuda()
         ep = torch.empty(len(idx), dtype=torch.float64, device="cuda")
         ef = torch.empty(len(idx), 3, dtype=torch.float64, device="cuda")
@@ -771,16 +777,17 @@ def run_batch(args, cfg):
         self_t = c[idx] * 1e4
         errs_p.append(rel_l2(pot[b + idx] - self_t, ep.cpu().numpy() - self_t))
         errs_f.append(rel_l2(fld[b + idx], ef.cpu().numpy()))
-    # the plain FP64 form, one problem at a time (uniform octree, automatic depth)
-    def plain_all():
-        for k, (p, c) in enumerate(probs):
+    # the plain FP64 form, one problem at a time (uniform octree, automatic
+    # depth); warmed on the first problems, timed once over all of them
+    def plain_all(count=None):
+        for k, (p, c) in enumerate(probs[:count]):
             b = int(offs[k])
             ctx.check(L.lfmm3d_solve_device(ctx.handle, len(p), vp(d_src.data_ptr() + 24 * b),
                                             vp(d_q.data_ptr() + 8 * b), 0, None, cfg["plain_N"], 2147483647, 1e-8,
                                             0, vp(d_pot.data_ptr() + 8 * b), vp(d_fld.data_ptr() + 24 * b), None),
                       "plain")
 
-    plain_all()
+    plain_all(8)
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
@@ -789,6 +796,8 @@ def run_batch(args, cfg):
     t1.synchronize()
     pms = t0.elapsed_time(t1)
     ep_ = np.array(errs_p); ef_ = np.array(errs_f)
+    worst = [{"problem": int(k), "particles": int(len(probs[k][0])), "rel_l2_pot_noself": float(ep_[k]),
+              "rel_l2_field": float(ef_[k])} for k in np.argsort(-np.maximum(ep_, ef_))[:5]]
     line = {"metric": "batched 3D FMM aggregate Mparticles/s", "value": n / (ms * 1e-3) / 1e6,
             "unit": "Mparticles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32",
@@ -799,13 +808,37 @@ def run_batch(args, cfg):
             "accuracy": {"rel_l2_pot_noself_median": float(np.median(ep_)), "rel_l2_pot_noself_p95":
                          float(np.quantile(ep_, 0.95)), "rel_l2_pot_noself_max": float(ep_.max()),
                          "rel_l2_field_median": float(np.median(ef_)), "rel_l2_field_max": float(ef_.max()),
-                         "targets_per_problem": 64},
+                         "targets_per_problem": "every output up to 8192 particles, else 64", "within_tol": int(np.sum(np.maximum(ep_, ef_) <= cfg["tol"])),
+                         "worst_problems": worst},
             "plain_fp64_one_at_a_time": {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s",
                                          "ms": pms, "N_degrees": cfg["plain_N"]},
             "speedup_vs_plain_fp64": pms / ms, "clocks": clk.summary()}
     if learned:
         line["learned_order"] = dict(info.as_dict(), tol=cfg["tol"], check_targets_per_problem=cfg["check_targets"])
         line["config"]["N_degrees"] = info.order_N
+    # the same batch as a batch plan (forest and one CUDA graph built once, new
+    # charges per execution) at the order and leaf size the learned solve used
+    if not args.no_plan:
+        Np = info.order_N if learned else cfg["N"]
+        mlp = (info.max_leaf or cfg["max_leaf"]) if learned else cfg["max_leaf"]
+        popts = LfmmSolveOpts(Np, cfg["depth"], mlp, PRECISION[cfg["precision"]], 1e-8)
+        hp = ctypes.c_void_p()
+        ctx.check(L.lfmm3d_plan_create_batch(ctx.handle, len(probs), offs.ctypes.data_as(vp), vp(d_src.data_ptr()),
+                                             vp(d_q.data_ptr()), ctypes.byref(popts), ctypes.byref(hp)), "batch plan")
+        for _ in range(max(1, args.warmup)):
+            ctx.check(L.lfmm3d_plan_execute(hp, vp(d_q.data_ptr()), vp(d_pot.data_ptr()), vp(d_fld.data_ptr())), "plan")
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            ctx.check(L.lfmm3d_plan_execute(hp, vp(d_q.data_ptr()), vp(d_pot.data_ptr()), vp(d_fld.data_ptr())), "plan")
+        p1.record(stream)
+        p1.synchronize()
+        pl_ms = p0.elapsed_time(p1) / args.steps
+        L.lfmm3d_plan_destroy(hp)
+        line["batch_plan_execute"] = {"value": n / (pl_ms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": pl_ms,
+                                      "N_degrees": Np, "max_leaf": mlp,
+                                      "what": "repeated batch solves: forest and one CUDA graph built once"}
     ctx.close()
     print(json.dumps(line))
     return 0
@@ -945,7 +978,8 @@ def run_heldout(args, cfg):
     L = ctx.lib
     vp = ctypes.c_void_p
     stream = torch.cuda.ExternalStream(ctx.stream)
-    d_params = torch.from_numpy(load_params()).cuda()
+    learned_leaf = bool(cfg.get("learned_leaf"))
+    d_params = torch.from_numpy(load_params(leaf=learned_leaf)).cuda()
     prec, tol, depth, ml = PRECISION[cfg["precision"]], cfg["tol"], cfg["depth"], cfg["max_leaf"]
     dev = []
     for pos, q in probs:
@@ -965,7 +999,7 @@ def run_heldout(args, cfg):
     info = LfmmLearnedInfo()
 
     def learned(d):
-        opts = LfmmSolveOpts(cfg["N"], depth, ml, prec, tol)
+        opts = LfmmSolveOpts(cfg["N"], depth, 2147483647 if learned_leaf else ml, prec, tol)
         ctx.check(L.lfmm3d_solve_learned_device(ctx.handle, d["n"], vp(d["ds"].data_ptr()), vp(d["dq"].data_ptr()),
                                                 0, None, ctypes.byref(opts), vp(d_params.data_ptr()), tol,
                                                 cfg["check_targets"], vp(d["pot"].data_ptr()),
@@ -1017,7 +1051,8 @@ def run_heldout(args, cfg):
             ef_fixed = errors(d)
             tl = timed(lambda: learned(d))
             el = errors(d)
-            rows.append(dict(n=d["n"], N=info.order_N, predicted_N=info.predicted_N, fallback=info.fallback,
+            rows.append(dict(n=d["n"], N=info.order_N, predicted_N=info.predicted_N, max_leaf=info.max_leaf,
+                             fallback=info.fallback,
                              fp64=info.fp64_resolved, ms_learned=tl, ms_fixed=tf, err_pot=el[0], err_field=el[1],
                              err_pot_fixed=ef_fixed[0], err_field_fixed=ef_fixed[1]))
     ctx.close()
@@ -1042,6 +1077,31 @@ def run_heldout(args, cfg):
             "per_problem": rows, "clocks": clk.summary(),
             "e2e": None, "gpu_launches": None}
     print(json.dumps(line))
+    return 0
+
+
+def run_cpu_series(args, cfg, pos, q):
+    """The reference's CPU FMM on growing strided samples of the configuration
+    (1/64, 1/16, 1/4), one solve each: how its throughput falls with the
+    sample's size on a uniform tree (its automatic depth plus 3, the depth
+    the default sample uses)."""
+    import math
+    solver, kind = cpu_solver()
+    cores = os.cpu_count() or 1
+    solver.set_threads(cores)
+    series = []
+    for stride in (64, 16, 4):
+        p, qq = np.ascontiguousarray(pos[::stride]), np.ascontiguousarray(q[::stride])
+        auto = int(max(2.0, 1 + math.log(len(p) / 100.0) / math.log(8.0)))
+        depth = auto + 3
+        t0 = time.perf_counter()
+        solver.fmm3d(p, qq, N=cfg["N"], depth=depth)
+        sec = time.perf_counter() - t0
+        series.append({"stride": stride, "particles": len(p), "tree_depth": depth, "seconds": sec,
+                       "Mparticles_per_s": len(p) / sec / 1e6})
+        print(json.dumps(series[-1]), file=sys.stderr, flush=True)
+    print(json.dumps({"impl": "reference", "metric": cfg.get("metric", METRIC), "cpu_series": series,
+                      "cores": cores, "kind": kind, "N_degrees": cfg["N"], "workload": cfg["workload"]}))
     return 0
 
 
@@ -1158,6 +1218,8 @@ def main():
         if cfg.get("heldout"):
             return run_heldout_reference(args, cfg)
         pos, q = make_particles(cfg)
+        if args.cpu_series:
+            return run_cpu_series(args, cfg, pos, q)
         if cfg.get("vector"):
             # the reference's vector FMM on the same particles and charges (sample as run_vector's)
             q = np.random.Generator(np.random.PCG64(cfg["seed"] + 1)).uniform(-1, 1, (cfg["n"], 3))

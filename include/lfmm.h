@@ -189,6 +189,14 @@ int lfmm3d_solve_batch_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, 
 typedef struct lfmm_plan lfmm_plan;
 int lfmm3d_plan_create(lfmm_ctx* ctx, size_t n_src, const double* src_xyz, const double* src_q,
                        const lfmm_solve_opts* opts, lfmm_plan** plan);
+/* A plan for a batch: the forest of n_prob independent problems (offsets as
+ * for lfmm3d_solve_batch, host array) built once and its FMM passes captured
+ * in one CUDA graph, so that repeated batch solves with new charges skip the
+ * forest's build and every host synchronisation.  opts->N and opts->max_leaf
+ * must be given.  Executed and destroyed like any plan (charges, potential
+ * and field in the concatenated input order). */
+int lfmm3d_plan_create_batch(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
+                             const double* src_q, const lfmm_solve_opts* opts, lfmm_plan** plan);
 int lfmm3d_plan_execute(lfmm_plan* plan, const double* src_q, double* pot, double* field);
 void lfmm3d_plan_destroy(lfmm_plan* plan);
 
@@ -366,6 +374,8 @@ typedef struct {
 	                               rel-L2 of potential and field (batches: the largest over problems) */
 	int max_leaf;               /* the leaf-size threshold of the tree (picked by the threshold
 	                               network when opts->max_leaf is LFMM_AUTO) */
+	int order_groups;           /* batches: the distinct orders the problems were solved at (each
+	                               order's problems as one forest); 1 for a single solve */
 } lfmm_learned_info;
 
 /* 3D solve at the order the network picks for tolerance tol, which bounds
@@ -400,15 +410,20 @@ int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_x
                                 size_t n_tgt, const double* tgt_xyz, const lfmm_solve_opts* opts,
                                 const float* params, double tol, int check_targets, double* pot, double* field,
                                 lfmm_learned_info* info, lfmm_stats* stats);
-/* The batch at the order the network picks for tolerance tol (as
+/* The batch at the orders the network picks for tolerance tol (as
  * lfmm3d_solve_learned; device buffers): up to check_targets sampled outputs
- * per problem normalise each problem's prediction and judge its result (the
- * same upper confidence bounds, per problem); the batch runs at the highest
- * order any problem needs, and reruns at N = 18 when a problem misses tol;
- * a problem still above tol there (mixed form) is rerun alone in the FP64
- * form into its slice of the outputs.  info: the order used, the largest
- * predicted, checked and judged errors over the problems, the number of FP64
- * reruns. */
+ * per problem, every output of a problem of at most 8192 particles (their
+ * FP64 direct sums in one launch), normalise each
+ * problem's prediction and judge its result (the same upper confidence
+ * bounds, per problem).  Every problem runs at its own predicted order: when
+ * the problems need several, the problems of each order are solved together
+ * as their own forest (order_groups in info), and the problems an order
+ * left above tol are solved again together at N = 18; a problem still above
+ * tol there (mixed form) is rerun alone in the FP64 form into its slice of
+ * the outputs.  opts->max_leaf LFMM_AUTO: the threshold network picks the
+ * leaf size for the whole batch (params as for lfmm3d_solve_learned).  info:
+ * the highest order used, the largest predicted, checked and judged errors
+ * over the problems, the number of FP64 reruns. */
 int lfmm3d_solve_batch_learned_device(lfmm_ctx* ctx, int n_prob, const size_t* offsets, const double* src_xyz,
                                       const double* src_q, const lfmm_solve_opts* opts, const float* params,
                                       double tol, int check_targets, double* pot, double* field,

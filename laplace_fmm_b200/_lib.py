@@ -33,7 +33,7 @@ EXPORTS = [
     "lfmm_mlp_forward", "lfmm_mlp_grad", "lfmm_mlp_adam",
     "lfmm3d_features", "lfmm3d_leaf_features", "lfmm3d_solve_learned", "lfmm3d_solve_learned_device",
     "lfmm3d_solve_batch", "lfmm3d_solve_batch_device", "lfmm3d_solve_batch_learned_device",
-    "lfmm3d_plan_create", "lfmm3d_plan_execute", "lfmm3d_plan_destroy",
+    "lfmm3d_plan_create", "lfmm3d_plan_create_batch", "lfmm3d_plan_execute", "lfmm3d_plan_destroy",
 ]
 
 
@@ -67,7 +67,7 @@ class LfmmLearnedInfo(ctypes.Structure):
                 ("predicted_error", ctypes.c_double), ("checked_error", ctypes.c_double),
                 ("checked_error_field", ctypes.c_double), ("fp64_resolved", ctypes.c_int),
                 ("predicted_error_field", ctypes.c_double), ("judged_error", ctypes.c_double),
-                ("max_leaf", ctypes.c_int)]
+                ("max_leaf", ctypes.c_int), ("order_groups", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -138,6 +138,7 @@ def load(path: Path | str = LIB_PATH):
         L.lfmm3d_solve_batch_learned_device.argtypes = [P, I, P, P, P, ctypes.POINTER(LfmmSolveOpts), P, D, I, P, P,
                                                          ctypes.POINTER(LfmmLearnedInfo), ctypes.POINTER(LfmmStats)]
         L.lfmm3d_plan_create.argtypes = [P, SZ, P, P, ctypes.POINTER(LfmmSolveOpts), ctypes.POINTER(P)]
+        L.lfmm3d_plan_create_batch.argtypes = [P, I, P, P, P, ctypes.POINTER(LfmmSolveOpts), ctypes.POINTER(P)]
         L.lfmm3d_plan_execute.argtypes = [P, P, P, P]
         L.lfmm3d_plan_destroy.argtypes = [P]
         L.lfmm3d_plan_destroy.restype = None

@@ -127,7 +127,57 @@ __global__ void direct_reduce_kernel(size_t nt, int S, const double* __restrict_
 	for (int k = 0; k < DIM; ++k) fld[DIM * i + k] = a[1 + k];
 }
 
+// Target i against the sources of its own segment [poff[seg[i]], poff[seg[i] + 1])
+// (the sampled checks of a batch of problems in one launch): one block per
+// target, the threads splitting the segment's sources, then a block
+// reduction in fixed order.  3D, 1/r as in the FAST sums.
+__global__ void __launch_bounds__(DT) direct_segments_kernel(const double* __restrict__ src,
+                                                             const double* __restrict__ q,
+                                                             const uint32_t* __restrict__ poff,
+                                                             const int32_t* __restrict__ seg, size_t m,
+                                                             const double* __restrict__ tgt,
+                                                             double* __restrict__ pot, double* __restrict__ fld)
+{
+	const size_t i = blockIdx.x;
+	if (i >= m) return;
+	const int k = seg[i];
+	const size_t lo = poff[k], hi = poff[k + 1];
+	const double xi = tgt[3 * i], yi = tgt[3 * i + 1], zi = tgt[3 * i + 2];
+	double v[4] = {0, 0, 0, 0};
+	for (size_t j = lo + threadIdx.x; j < hi; j += DT) {
+		const double dx = xi - src[3 * j], dy = yi - src[3 * j + 1], dz = zi - src[3 * j + 2];
+		const double inv = rsqrt_refined(fmax(dx * dx + dy * dy + dz * dz, FORCE_EPS2));
+		const double qr = q[j] * inv;
+		const double qr3 = qr * inv * inv;
+		v[0] += qr;
+		v[1] = fma(dx, qr3, v[1]); v[2] = fma(dy, qr3, v[2]); v[3] = fma(dz, qr3, v[3]);
+	}
+	__shared__ double red[DT / 32][4];
+#pragma unroll
+	for (int c = 0; c < 4; ++c) {
+		double x = v[c];
+		for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+		if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][c] = x;
+	}
+	__syncthreads();
+	if (threadIdx.x < 4) {
+		double x = 0.0;
+		for (int w = 0; w < DT / 32; ++w) x += red[w][threadIdx.x];
+		if (threadIdx.x == 0) pot[i] = x;
+		else fld[3 * i + threadIdx.x - 1] = x;
+	}
+}
+
 } // namespace
+
+int direct_segments_device(Context& ctx, const double* src, const double* q, const uint32_t* poff,
+                           const int32_t* seg, size_t m, const double* tgt, double* pot, double* fld)
+{
+	if (m == 0) return OK;
+	direct_segments_kernel<<<(unsigned)m, DT, 0, ctx.stream>>>(src, q, poff, seg, m, tgt, pot, fld);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return OK;
+}
 
 int direct_chunks(size_t ns, size_t nt, int num_sms, size_t max_chunks)
 {

@@ -21,4 +21,9 @@ int direct_preload3(Context& ctx);
 int direct_device(Context& ctx, int dim, size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                   double* pot, double* fld, bool fast = false);
 
+// Target i (3D) against the sources of its segment [poff[seg[i]], poff[seg[i] + 1])
+// only: the sampled checks of a batch of problems in one launch (FAST 1/r).
+int direct_segments_device(Context& ctx, const double* src, const double* q, const uint32_t* poff,
+                           const int32_t* seg, size_t m, const double* tgt, double* pot, double* fld);
+
 } // namespace lfmm

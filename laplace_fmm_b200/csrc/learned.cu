@@ -31,6 +31,17 @@ constexpr double JUDGE_Z = 2.0;     // standard errors added to the sampled rel-
 // within tol, so a pick aimed at tol itself is rejected (and solved again)
 // whenever the true error lands in the upper part of that band.
 constexpr double LEARNED_MARGIN = 0.6;
+// After a miss the predictions are shifted by the shortfall the judge
+// measured on this problem (its upper bound over the prediction), which is
+// already an upper estimate: the retry aims at RETRY_MARGIN tol.  With 0.6
+// here too the retries of the 64 held-out problems went to N = 18 where
+// one order above the miss passed.
+constexpr double RETRY_MARGIN = 0.85;
+// A learned batch solves its problems in at most this many orders.
+constexpr int MAX_ORDER_GROUPS = 3;
+// Problems of a learned batch with at most this many particles are checked at
+// every output.
+constexpr size_t EXACT_CHECK = 8192;
 
 __device__ __forceinline__ float lg(double x) { return (float)log10(x); }
 
@@ -462,6 +473,67 @@ int sampled_error(Context& ctx, const ParticleInput& in, const Samples& S, const
 	return OK;
 }
 
+// ---- per-problem orders in a batch ----------------------------------------
+// Problem j of a group: its sources at [src_off, src_off + cnt) of the batch
+// and at [dst_off, ...) of the group's contiguous copy.
+struct GroupPart { uint32_t src_off, dst_off, cnt; };
+
+__global__ void gather_group_kernel(const GroupPart* __restrict__ parts, const double* __restrict__ src,
+                                    const double* __restrict__ q, double* __restrict__ gsrc, double* __restrict__ gq)
+{
+	const GroupPart g = parts[blockIdx.x];
+	for (uint32_t i = threadIdx.x; i < 3 * g.cnt; i += blockDim.x) gsrc[3 * (size_t)g.dst_off + i] = src[3 * (size_t)g.src_off + i];
+	for (uint32_t i = threadIdx.x; i < g.cnt; i += blockDim.x) gq[g.dst_off + i] = q[g.src_off + i];
+}
+
+__global__ void scatter_group_kernel(const GroupPart* __restrict__ parts, const double* __restrict__ gpot,
+                                     const double* __restrict__ gfld, double* __restrict__ pot,
+                                     double* __restrict__ fld)
+{
+	const GroupPart g = parts[blockIdx.x];
+	for (uint32_t i = threadIdx.x; i < g.cnt; i += blockDim.x) pot[g.src_off + i] = gpot[g.dst_off + i];
+	for (uint32_t i = threadIdx.x; i < 3 * g.cnt; i += blockDim.x) fld[3 * (size_t)g.src_off + i] = gfld[3 * (size_t)g.dst_off + i];
+}
+
+// The problems `members` of a batch solved together at order N as their own
+// forest; their results written into their slices of pot / field.
+int solve_group(Context& ctx, const ParticleInput& in, const size_t* hoff, const std::vector<int>& members, int N,
+                int depth, int max_leaf, int precision, double* pot, double* field)
+{
+	if (members.empty()) return OK;
+	cudaStream_t s = ctx.stream;
+	std::vector<GroupPart> hp;
+	std::vector<uint32_t> goff(1, 0);
+	for (int k : members) {
+		const uint32_t cnt = (uint32_t)(hoff[k + 1] - hoff[k]);
+		hp.push_back(GroupPart{(uint32_t)hoff[k], goff.back(), cnt});
+		goff.push_back(goff.back() + cnt);
+	}
+	const size_t ng = goff.back(), G = members.size();
+	const size_t mark = ctx.arena.mark();
+	GroupPart* dparts = take<GroupPart>(ctx, G);
+	uint32_t* dgoff = take<uint32_t>(ctx, G + 1);
+	double* gsrc = take<double>(ctx, 3 * ng);
+	double* gq = take<double>(ctx, ng);
+	double* gpot = take<double>(ctx, ng);
+	double* gfld = take<double>(ctx, 3 * ng);
+	if (!dparts || !dgoff || !gsrc || !gq || !gpot || !gfld) { ctx.last_error = "learned batch: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemcpyAsync(dparts, hp.data(), sizeof(GroupPart) * G, cudaMemcpyHostToDevice, s));
+	LFMM_CUDA(ctx, cudaMemcpyAsync(dgoff, goff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
+	gather_group_kernel<<<(unsigned)G, 256, 0, s>>>(dparts, in.src, in.srcq, gsrc, gq);
+	ParticleInput gi;
+	gi.dim = 3; gi.ns = ng; gi.nt = 0; gi.src = gsrc; gi.srcq = gq; gi.poff = dgoff; gi.nprob = (int)G;
+	int st = fmm3d_solve_scaled(ctx, gi, N, depth, max_leaf, precision, gpot, gfld, nullptr, nullptr);
+	if (st == OK) {
+		scatter_group_kernel<<<(unsigned)G, 256, 0, s>>>(dparts, gpot, gfld, pot, field);
+		cudaError_t e = cudaGetLastError();
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // the host vectors above outlive the copies
+		if (e != cudaSuccess) st = cuda_fail(ctx, e, "learned batch groups");
+	}
+	ctx.arena.rewind(mark);
+	return st;
+}
+
 // ---- learned leaf-size threshold -------------------------------------------
 // The candidates and the threshold network's 16 inputs for candidate m of a
 // tree of n particles solved at order N, from the counts of the adaptive tree
@@ -565,6 +637,7 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	}
 	int N = FB_N;
 	lfmm_learned_info li{};
+	li.order_groups = 1;
 	li.max_leaf = auto_leaf ? chooser.cand[chooser.chosen] : max_leaf;
 	double ep[NP], ef[NP];
 	if ((st = learned_predictions(ctx, pacc, rms, ep, ef))) return st;
@@ -584,7 +657,7 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 		double ep2[NP], ef2[NP], pp, pf;
 		for (int k = 0; k < NP; ++k) { ep2[k] = ep[k] + std::max(sp, 0.0); ef2[k] = ef[k] + std::max(sf, 0.0); }
 		int N2 = FB_N;
-		pick_order(ep2, ef2, target, N2, pp, pf);
+		pick_order(ep2, ef2, std::log10(tol * RETRY_MARGIN), N2, pp, pf);
 		N = std::max(N2, N + 1);
 		li.fallback = 1;
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
@@ -630,13 +703,16 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	if (auto_leaf) chooser = leaf_chooser(ctx, params + LFMM_MLP_PARAMS, guess_order(tol), in.ns, depth, cst);
 	int st = tree_build_adaptive(ctx, in, depth, auto_leaf ? 0 : max_leaf, t, auto_leaf ? &chooser : nullptr);
 	if (st) return cst ? cst : st;
-	// samples: up to check_targets outputs of every problem, evenly spaced
+	// samples: every output of a problem of at most EXACT_CHECK particles (its
+	// check is then its exact rel-L2: a small problem's few badly converged
+	// targets weigh too much for a sample to be trusted), else check_targets
+	// outputs evenly spaced
 	std::vector<uint32_t> hidx;
 	std::vector<int32_t> hprob;
 	std::vector<size_t> soff(P + 1, 0);
 	for (int k = 0; k < P; ++k) {
 		const size_t nk = hoff[k + 1] - hoff[k];
-		const size_t mk = std::min<size_t>((size_t)check_targets, nk);
+		const size_t mk = nk <= EXACT_CHECK ? nk : std::min<size_t>((size_t)check_targets, nk);
 		for (size_t j = 0; j < mk; ++j) { hidx.push_back((uint32_t)(hoff[k] + j * (nk / mk))); hprob.push_back(k); }
 		soff[k + 1] = hidx.size();
 	}
@@ -652,13 +728,8 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	LFMM_CUDA(ctx, cudaMemcpyAsync(idx, hidx.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice, s));
 	LFMM_CUDA(ctx, cudaMemcpyAsync(prob, hprob.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice, s));
 	gather_points_kernel<<<div_up(m, 256), 256, 0, s>>>(in.src, idx, m, sp);
-	for (int k = 0; k < P; ++k) {
-		const size_t mk = soff[k + 1] - soff[k];
-		if (!mk) continue;
-		if ((st = direct_device(ctx, 3, hoff[k + 1] - hoff[k], in.src + 3 * hoff[k], in.srcq + hoff[k], mk,
-		                        sp + 3 * soff[k], ep + soff[k], ef + 3 * soff[k], /*fast=*/true)))
-			return st;
-	}
+	// every problem's samples against its own sources, one launch
+	if ((st = direct_segments_device(ctx, in.src, in.srcq, in.poff, prob, m, sp, ep, ef))) return st;
 	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * NCHK * P, s));
 	check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(nullptr, nullptr, idx, prob, m, in.srcq, ep, ef, acc);
 	// per-problem predictions
@@ -678,6 +749,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	int N = 5;
 	lfmm_learned_info li{};
 	li.max_leaf = auto_leaf ? chooser.cand[chooser.chosen] : max_leaf;
+	std::vector<int> Nk_of(P, 5);      // each problem's own order (5: no far-field error to bound)
 	for (int k = 0; k < P; ++k) {
 		const size_t mk = soff[k + 1] - soff[k];
 		const double* hk = hp.data() + (size_t)k * (NO + 1);
@@ -693,6 +765,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 		int Nk;
 		double pk, fk;
 		pick_order(e_p, e_f, std::log10(tol * LEARNED_MARGIN), Nk, pk, fk);
+		Nk_of[k] = Nk;
 		if (Nk > N || (Nk == N && std::max(pk, fk) > std::max(li.predicted_error, li.predicted_error_field))) {
 			N = Nk;
 			li.predicted_error = pk;
@@ -724,12 +797,59 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 		}
 		return OK;
 	};
-	for (int pass = 0; pass < 2; ++pass) {
-		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+	// problems grouped by their own order: one group solves on the forest
+	// already built; several solve as separate forests of their problems
+	// (gathered, solved, scattered back), so that no problem runs at the
+	// order another one needs
+	std::vector<int> orders(Nk_of.begin(), Nk_of.end());
+	std::sort(orders.begin(), orders.end());
+	orders.erase(std::unique(orders.begin(), orders.end()), orders.end());
+	// at most MAX_ORDER_GROUPS forests (each costs a tree build and a pass's
+	// launches): the order holding the fewest particles joins the next
+	// higher one (its problems run at that order) until few enough remain
+	if (orders.size() > (size_t)MAX_ORDER_GROUPS) {
+		std::vector<size_t> part(orders.size(), 0);
+		for (int k = 0; k < P; ++k)
+			part[std::lower_bound(orders.begin(), orders.end(), Nk_of[k]) - orders.begin()] += hoff[k + 1] - hoff[k];
+		while (orders.size() > (size_t)MAX_ORDER_GROUPS) {
+			size_t j = 0;
+			for (size_t i = 1; i + 1 < orders.size(); ++i)
+				if (part[i] < part[j]) j = i;
+			for (int k = 0; k < P; ++k)
+				if (Nk_of[k] == orders[j]) Nk_of[k] = orders[j + 1];
+			part[j + 1] += part[j];
+			orders.erase(orders.begin() + j);
+			part.erase(part.begin() + j);
+		}
+	}
+	li.order_groups = (int)orders.size();
+	if (orders.size() <= 1) {
+		for (int pass = 0; pass < 2; ++pass) {
+			if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
+			if ((st = check(true))) return st;
+			if (li.judged_error <= tol || N >= FB_N) break;
+			N = FB_N;                      // the fixed-order fallback for the whole batch
+			li.fallback = 1;
+		}
+	} else {
+		for (int Ng : orders) {
+			std::vector<int> members;
+			for (int k = 0; k < P; ++k)
+				if (Nk_of[k] == Ng) members.push_back(k);
+			if ((st = solve_group(ctx, in, hoff, members, Ng, depth, li.max_leaf, precision, pot, field))) return st;
+		}
 		if ((st = check(true))) return st;
-		if (li.judged_error <= tol || N >= FB_N) break;
-		N = FB_N;                      // the fixed-order fallback for the whole batch
-		li.fallback = 1;
+		// the problems a group's order left above tol: again at the fallback order, as one group
+		std::vector<int> miss;
+		for (int k = 0; k < P; ++k)
+			if (judged[k] > tol && Nk_of[k] < FB_N) miss.push_back(k);
+		if (!miss.empty()) {
+			li.fallback = 1;
+			if ((st = solve_group(ctx, in, hoff, miss, FB_N, depth, li.max_leaf, precision, pot, field))) return st;
+			for (int k : miss) Nk_of[k] = FB_N;
+			if ((st = check(true))) return st;
+		}
+		N = *std::max_element(Nk_of.begin(), Nk_of.end());
 	}
 	if (precision == LFMM_PRECISION_MIXED && li.judged_error > tol) {
 		// problems the mixed form cannot bring within tol even at the fallback

@@ -274,8 +274,12 @@ __device__ __forceinline__ int dir_d2(int dir)
 	return dx * dx + dy * dy + dz * dz;
 }
 
-// grid (tiles, slot splits).  With S = gridDim.y > 1 split s handles slots
-// [s*SLOTS/S, (s+1)*SLOTS/S) and writes part[s][cell][R]; else loc[cell][R].
+// A persistent grid (about one block per SM) taking work items from a
+// counter: item w is tile w / S and slot split w % S.  With S > 1 split s
+// handles slots [s*SLOTS/S, (s+1)*SLOTS/S) and writes part[s][cell][R]; else
+// loc[cell][R].  Tensor memory is allocated once per block; the barriers are
+// initialised afresh for every item (every copy, MMA and arrival of the
+// previous item has completed by then).
 // MODE picks the operator of a (class, slot) and the store:
 //   TC_M2L    189 far slots, operator c_tc_slot_dir[class][slot], loc = sum;
 //   TC_M2M    8 slots (child octants), operator = slot, loc = sum;
@@ -286,12 +290,13 @@ __device__ __forceinline__ int dir_d2(int dir)
 // The K blocks of a slot are fed from the highest degrees down, so the
 // dominant low-degree products enter each FP32 accumulator last, when the
 // accumulator's own rounding has least left to act on.
-template <int NC, int NA, int SLOTS, int MODE>
+template <int NC, int NA, int SLOTS, int MODE, bool PERSIST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
-              const float* __restrict__ diag, unsigned* flags, const TcTrunc trunc, size_t src_cells, int ndir)
+              const float* __restrict__ diag, unsigned* flags, const TcTrunc trunc, size_t src_cells, int ndir,
+              unsigned* __restrict__ work, int S, unsigned total)
 {
 	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	extern __shared__ uint8_t dsm[];
@@ -305,18 +310,40 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	__shared__ int16_t active[SLOTS];
 	__shared__ uint8_t active_kb[SLOTS];     // K blocks of each active slot
 	__shared__ int s_nactive, s_oct, s_n, s_abort;
-	__shared__ uint32_t s_start;
+	__shared__ uint32_t s_start, s_work;
 
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-	const int S = gridDim.y, sidx = blockIdx.y;
-	const int slot0 = sidx * SLOTS / S, slot1 = (sidx + 1) * SLOTS / S;
-	float* out = S > 1 ? part + (size_t)sidx * cells * R : loc;
 	uint8_t* base = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
 	volatile int* abort = &s_abort;
+	if (tid == 0) s_abort = 0;
+	if (warp == 4) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		             :: "r"(smem_u32(&tmem_sh)), "r"(TMEM_COLS));
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	const uint32_t tmem = tmem_sh;
+
+	for (int round = 0;; ++round) {
+	uint32_t witem;
+	if constexpr (PERSIST) {
+		if (tid == 0) s_work = *abort ? total : atomicAdd(work, 1u);
+		__syncthreads();
+		witem = s_work;
+	} else {
+		if (round > 0) break;         // one item per block: item = block
+		witem = blockIdx.x;
+	}
+	if (witem >= total) break;
+	const int sidx = (int)(witem % (uint32_t)S);
+	const int slot0 = sidx * SLOTS / S, slot1 = (sidx + 1) * SLOTS / S;
+	float* out = S > 1 ? part + (size_t)sidx * cells * R : loc;
 
 	if (tid == 0) {
-		// this block's (octant, tile): tiles of each octant class in turn
-		uint32_t b = blockIdx.x, start = 0;
+		// this item's (octant, tile): tiles of each octant class in turn
+		uint32_t b = witem / (uint32_t)S, start = 0;
 		int oct = -1, nn = 0;
 		for (int o = 0; o < 8; ++o) {
 			const uint32_t cnt = oct_count[o];
@@ -324,18 +351,16 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			if (b < tiles) { oct = o; start += b * TC_M; nn = (int)min((uint32_t)TC_M, cnt - b * TC_M); break; }
 			b -= tiles; start += cnt;
 		}
-		s_oct = oct; s_n = nn; s_start = start; s_abort = 0; s_nactive = 0;
+		s_oct = oct; s_n = nn; s_start = start; s_nactive = 0;
 	}
 	if (tid < (SLOTS + 31) / 32) active_mask[tid] = 0u;
 	__syncthreads();
-	if (s_oct < 0) return;
+	if (s_oct < 0) {
+		__syncthreads();    // every thread has read s_oct before the next item rewrites it
+		continue;
+	}
 	const int oct = s_oct;
 	if (tid < TC_M) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
-	if (warp == 4) {
-		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-		             :: "r"(smem_u32(&tmem_sh)), "r"(TMEM_COLS));
-		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-	}
 	if (tid == 0) {
 		for (int s = 0; s < NSTAGE; ++s) {
 			mbar_init(smem_u32(&full_bar[s]), TC_M);
@@ -372,7 +397,6 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	}
 	__syncthreads();
 	const int nact = s_nactive;
-	const uint32_t tmem = tmem_sh;
 
 	if (warp < 4) {
 		// ---- producers: one target row each; thread 0 also copies the operator.
@@ -624,6 +648,12 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			}
 		}
 	}
+	// the item's TMEM reads, copies and MMAs are complete: the next item may
+	// re-initialise the barriers and overwrite the accumulators
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	}
 	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -685,20 +715,31 @@ TcTrunc tc_trunc(int N, int KB)
 	return t;
 }
 
+// persistent: about one block per SM taking items from the counter; else one
+// block per item (the hardware's block scheduler hands them out).
 template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
-           bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0)
+           bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0, bool persistent = true)
 {
 	using C = TcCfg<NC, NA, MODE != TC_L2L>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
-	dim3 grid(tiles, S);
+	const unsigned total = tiles * (unsigned)S;
+	unsigned* work = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
+	if (!work) { ctx.last_error = "tensor-core M2L: allocation failed"; return ERR_OOM; }
+	LFMM_CUDA(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned), ctx.stream));
+	const unsigned grid = persistent ? std::min(total, (unsigned)ctx.num_sms) : total;
 	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
-	m2l_tc_kernel<NC, NA, SLOTS, MODE><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
-		reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part, plan.cells,
-		diag, ctx.dev_flags,
-		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB),
-		src_cells, MODE == TC_M2L ? 343 : 8);
+	const TcTrunc tr =
+		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB);
+	if (persistent)
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, true><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
+			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total);
+	else
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, false><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
+			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
 		ctx.kev_used += 2;
@@ -711,17 +752,22 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 	return OK;
 }
 
-// The slot split S (blocks per tile, each taking 189 / S of the far slots,
-// partials added in fixed order): without tuning, the smallest power of two
-// that gives about two waves of blocks; with tuning, the first level of each
-// (operator rows, log2 tiles) pair times S = 1, 2, 4, 8 with CUDA events and
-// keeps the fastest for the context (the chosen S runs last, so the level's
-// result always comes from it).
+// The work-item shape and the grid: the slot split S (items per tile, each
+// taking 189 / S of the far slots, partials added in fixed order) and the
+// launch (persistent blocks taking items from a counter, or one block per
+// item).  Without tuning: the smallest power of two S that gives about two
+// waves of items, one block per item.  With tuning, the first level of each
+// (operator rows, log2 tiles) pair times the 8 pairs S = 1, 2, 4, 8 x
+// {persistent, one block per item} with CUDA events and keeps the fastest
+// for the context (stored as S | 16 for persistent; the chosen pair runs
+// last, so the level's result always comes from it).
 template <int NC, int NA>
 int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int n_src)
 {
 	using C = TcCfg<NC, NA>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, true>,
+	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, false>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	int S = 1;
@@ -731,10 +777,14 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 	static_assert(NC / 16 < Context::SPLIT_ROWS, "autotuner table");
 	int& tuned = ctx.m2l_split[NC / 16][bucket];
 	const bool tune = ctx.tune_m2l && tuned == 0;
-	if (ctx.tune_m2l && !tune) S = tuned;
+	bool pers = false;
+	if (ctx.tune_m2l && !tune) { S = tuned & 15; pers = (tuned & 16) != 0; }
+	// the tuner tries splits up to 8 where their partials fit in 1 GiB (a level
+	// that large has tiles enough for S = 1; only the launch is tuned there)
+	const int maxS = sizeof(float) * 8 * plan.cells * (size_t)R <= ((size_t)1 << 30) ? 8 : 1;
 	float* part = nullptr;
-	if (tune || S > 1) {
-		part = static_cast<float*>(ctx.arena.take(sizeof(float) * (tune ? 8 : S) * plan.cells * (size_t)R));
+	if ((tune && maxS > 1) || S > 1) {
+		part = static_cast<float*>(ctx.arena.take(sizeof(float) * (tune ? maxS : S) * plan.cells * (size_t)R));
 		if (!part) {
 			ctx.last_error = "tensor-core M2L: allocation failed";
 			return ERR_OOM;
@@ -746,22 +796,26 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		LFMM_CUDA(ctx, cudaEventCreate(&e1));
 		float best = 1e30f;
 		int bestS = S;
-		for (int cand = 1; cand <= 8; cand *= 2) {
-			LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-			int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells, nullptr, n_src);
-			if (st) return st;
-			LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
-			LFMM_CUDA(ctx, cudaEventSynchronize(e1));
-			float ms = 0.f;
-			LFMM_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
-			if (ms < best) { best = ms; bestS = cand; }
-		}
+		bool bestP = true;
+		for (int mode = 0; mode < 2; ++mode)
+			for (int cand = 1; cand <= maxS; cand *= 2) {
+				LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
+				int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells, nullptr, n_src,
+				                        mode == 0);
+				if (st) return st;
+				LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
+				LFMM_CUDA(ctx, cudaEventSynchronize(e1));
+				float ms = 0.f;
+				LFMM_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+				if (ms < best) { best = ms; bestS = cand; bestP = mode == 0; }
+			}
 		cudaEventDestroy(e0);
 		cudaEventDestroy(e1);
-		tuned = bestS;
+		tuned = bestS | (bestP ? 16 : 0);
 		S = bestS;
+		pers = bestP;
 	}
-	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr, n_src);
+	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr, n_src, pers);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
@@ -772,15 +826,16 @@ int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* op
 	using C = TcCfg<NC, NA>;
 	using CL = TcCfg<NC, NA, false>;
 	if (mode == TC_M2M) {
-		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M>,
+		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M, false>,
 		                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells);
+		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, nullptr, 0,
+		                                 false);
 	}
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L, false>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
 	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + 8 * C::DIR_BYTES);
-	return run_tc<NC, NA, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, diag);
+	return run_tc<NC, NA, 1, TC_L2L>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, diag, 0, false);
 }
 
 std::mutex g_upload_mu;

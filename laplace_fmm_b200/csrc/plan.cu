@@ -1,5 +1,5 @@
 // Solve plans: one geometry, many charge vectors.  The adaptive tree of the
-// positions is built once, every cache the solve uses is warmed (operators,
+// positions (or the forest of a batch of independent problems) is built once, every cache the solve uses is warmed (operators,
 // constants, the M2L autotuner), and the FMM passes are captured in a CUDA
 // graph on the context's stream; each execution copies the new charges in,
 // scatters them into tree order and launches the graph.  No counterpart in
@@ -21,6 +21,7 @@ struct lfmm_plan {
 	lfmm::DevTree tree;
 	int N = 0, precision = 0;
 	size_t n = 0;
+	int nprob = 1;                     // > 1: a batch plan (forest of independent problems)
 	double* q_in = nullptr;            // charges in input order (graph input)
 	double* pot = nullptr;             // outputs in input order (graph output)
 	double* fld = nullptr;
@@ -49,20 +50,38 @@ int take_io(Context& c, lfmm_plan* p)
 	return OK;
 }
 
-// Build the plan in the context with the plan's arena swapped in.
-int build(Context& c, lfmm_plan* p, const double* src, const double* q, int depth, int max_leaf)
+// Build the plan in the context with the plan's arena swapped in.  hoff
+// (host, nprob + 1 entries) for a batch plan, else null.
+int build(Context& c, lfmm_plan* p, const double* src, const double* q, int depth, int max_leaf, const size_t* hoff)
 {
 	ParticleInput in;
 	in.dim = 3; in.ns = p->n; in.nt = 0; in.src = src; in.srcq = q;
+	std::vector<uint32_t> h;
+	if (hoff) {
+		h.resize(p->nprob + 1);
+		for (int k = 0; k <= p->nprob; ++k) h[k] = (uint32_t)hoff[k];
+	}
+	// the forest's device offsets, taken (and re-taken in pass 2) before the
+	// tree so that both passes lay the arena out alike
+	auto take_offsets = [&]() -> int {
+		if (!hoff) return OK;
+		uint32_t* poff = static_cast<uint32_t*>(c.arena.take(sizeof(uint32_t) * (p->nprob + 1)));
+		if (!poff) { c.last_error = "plan: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(c, cudaMemcpyAsync(poff, h.data(), sizeof(uint32_t) * (p->nprob + 1), cudaMemcpyHostToDevice,
+		                             c.stream));
+		in.poff = poff;
+		in.nprob = p->nprob;
+		return OK;
+	};
 	// pass 1: sizes the arena and warms every cache (operators, autotuner)
 	int st = take_io(c, p);
-	if (st) return st;
+	if (st || (st = take_offsets())) return st;
 	if ((st = tree_build_adaptive(c, in, depth, max_leaf, p->tree))) return st;
 	if ((st = fmm3d_scaled_on_tree(c, p->tree, p->N, p->precision, p->pot, p->fld, nullptr))) return st;
 	c.arena.settle();                  // one block of the high-water size
 	// pass 2: the final layout, one more warm solve, then the capture replays it
 	c.arena.reset();
-	if ((st = take_io(c, p))) return st;
+	if ((st = take_io(c, p)) || (st = take_offsets())) return st;
 	LFMM_CUDA(c, cudaMemcpyAsync(p->q_in, q, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, c.stream));
 	if ((st = tree_build_adaptive(c, in, depth, max_leaf, p->tree))) return st;
 	const size_t mark = c.arena.mark();
@@ -137,7 +156,49 @@ int lfmm3d_plan_create(lfmm_ctx* h, size_t n_src, const double* src_xyz, const d
 	if (!p) return LFMM_ERR_OOM;
 	p->ctx = h; p->n = n_src; p->N = o->N; p->precision = o->precision;
 	c.arena.swap(p->arena);
-	int st = build(c, p, src_xyz, src_q, depth, o->max_leaf);
+	int st = build(c, p, src_xyz, src_q, depth, o->max_leaf, nullptr);
+	c.arena.swap(p->arena);
+	if (st) {
+		unpin_and_delete(p);
+		return st;
+	}
+	*out = p;
+	return LFMM_OK;
+}
+
+int lfmm3d_plan_create_batch(lfmm_ctx* h, int n_prob, const size_t* offsets, const double* src_xyz,
+                             const double* src_q, const lfmm_solve_opts* o, lfmm_plan** out)
+{
+	if (!h || !o || !out || !offsets || !src_xyz || !src_q || n_prob < 1) return LFMM_ERR_ARG;
+	*out = nullptr;
+	Context& c = ctx_of(h);
+	if (offsets[0] != 0) { c.last_error = "batch plan: offsets[0] must be 0"; return LFMM_ERR_ARG; }
+	size_t big = 0;
+	for (int k = 0; k < n_prob; ++k) {
+		if (offsets[k + 1] < offsets[k]) { c.last_error = "batch plan: offsets must not decrease"; return LFMM_ERR_ARG; }
+		big = std::max(big, offsets[k + 1] - offsets[k]);
+	}
+	const size_t n = offsets[n_prob];
+	if (n == 0 || n >= 0xffffffffull) { c.last_error = "batch plan: total particle count out of range"; return LFMM_ERR_ARG; }
+	if (o->max_leaf < 0 || o->max_leaf == LFMM_AUTO ||
+	    (o->precision != LFMM_PRECISION_FP64 && o->precision != LFMM_PRECISION_MIXED)) {
+		c.last_error = "batch plan: bad options (max_leaf must be given)";
+		return LFMM_ERR_ARG;
+	}
+	if (o->N == LFMM_AUTO || o->N < 1 || !m2l_gemm_supported(o->N)) {
+		c.last_error = "batch plan: N must be given, 1 <= N <= 18";
+		return LFMM_ERR_ARG;
+	}
+	const int depth = o->tree_depth != LFMM_AUTO
+	                      ? o->tree_depth
+	                      : (int)std::max(2.0, 1 + std::log((double)big / 100.0) / std::log(8.0));
+	cudaError_t e = cudaSetDevice(c.device);
+	if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+	lfmm_plan* p = new (std::nothrow) lfmm_plan();
+	if (!p) return LFMM_ERR_OOM;
+	p->ctx = h; p->n = n; p->N = o->N; p->precision = o->precision; p->nprob = n_prob;
+	c.arena.swap(p->arena);
+	int st = build(c, p, src_xyz, src_q, depth, o->max_leaf, offsets);
 	c.arena.swap(p->arena);
 	if (st) {
 		unpin_and_delete(p);

@@ -264,3 +264,36 @@ class Plan3d:
             self.close()
         except Exception:
             pass
+
+
+class BatchPlan3d(Plan3d):
+    """A batch of independent problems solved repeatedly with new charges: the
+    forest of their trees and a CUDA graph of the FMM passes over all of them
+    are built once (lfmm3d_plan_create_batch); ``execute(charges)`` takes and
+    returns the problems' values concatenated in input order."""
+
+    def __init__(self, problems, N: int, tree_depth: int = FMM_AUTO, max_leaf: int = 64, precision: str = "mixed",
+                 ctx: Context | None = None):
+        import torch
+        self.ctx = ctx or default_context()
+        parts = [_split((p, c), 3) for p, c in problems]
+        self.offsets = np.zeros(len(parts) + 1, dtype=np.uint64)
+        self.offsets[1:] = np.cumsum([len(p) for p, _ in parts])
+        pos = np.ascontiguousarray(np.concatenate([p for p, _ in parts]))
+        q = np.ascontiguousarray(np.concatenate([c for _, c in parts]))
+        self.n = len(pos)
+        dev = torch.device("cuda", self.ctx.device)
+        self._torch, self._dev = torch, dev
+        d_pos = torch.from_numpy(pos).to(dev)
+        self._q = torch.from_numpy(q).to(dev)
+        self._pot = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self._fld = torch.empty(self.n, 3, dtype=torch.float64, device=dev)
+        opts = LfmmSolveOpts(int(N), int(tree_depth), int(max_leaf), PRECISION[precision], 1e-8)
+        self.handle = ctypes.c_void_p()
+        torch.cuda.synchronize(dev)
+        vp = ctypes.c_void_p
+        self.ctx.check(self.ctx.lib.lfmm3d_plan_create_batch(self.ctx.handle, len(parts),
+                                                             self.offsets.ctypes.data_as(vp), vp(d_pos.data_ptr()),
+                                                             vp(self._q.data_ptr()), ctypes.byref(opts),
+                                                             ctypes.byref(self.handle)), "lfmm3d_plan_create_batch")
+

@@ -68,9 +68,36 @@ def test_learned_batch_within_tolerance(ctx, problems):
     out, info = solver.solve_batch(problems, tol=1e-6, tree_depth=8, check_targets=64)
     assert 5 <= info["order_N"] <= 18
     assert info["checked_error"] <= 1e-6 and info["checked_error_field"] <= 1e-6
+    if info["order_groups"] != 1:
+        pytest.skip("the problems ran at several orders (the per-order groups are tested below)")
     ref = solve_batch(problems, N=info["order_N"], tree_depth=8, max_leaf=64, ctx=ctx)
     for k, ((pos, q), (pot, fld), (rp, rf)) in enumerate(zip(problems, out, ref)):
         if len(pos) < 2 or info["fp64_resolved"]:
             continue
         assert rel_l2(noself(pot, q), noself(rp, q)) < 1e-12
         assert rel_l2(fld, rf) < 1e-12
+
+
+def test_learned_batch_orders_per_problem(ctx):
+    """Problems that need different orders (uniform sets and tight clusters):
+    each runs at its own order, the problems of each order solved together;
+    every problem within the tolerance at its samples against the FP64 direct
+    sum, and the threshold network picks the batch's leaf size."""
+    from laplace_fmm_b200.order import WEIGHTS, LEAF_CANDIDATES, LearnedSolver
+    from laplace_fmm_b200.workloads import gaussian_mix3d, uniform3d
+    if not WEIGHTS.exists():
+        pytest.skip("trained network not present")
+    probs = [uniform3d(20000, seed=s) for s in range(3)]
+    probs += [gaussian_mix3d(40000, seed=300 + s, kmin=1, kmax=1, smin=0.005, smax=0.006) for s in range(3)]
+    probs += [gaussian_mix3d(30000, seed=310 + s) for s in range(4)]
+    solver = LearnedSolver(ctx=ctx, leaf=True)
+    out, info = solver.solve_batch(probs, tol=1e-6, tree_depth=10, max_leaf="auto", check_targets=64)
+    assert info["max_leaf"] in LEAF_CANDIDATES
+    assert info["order_groups"] >= 1
+    for (pos, q), (pot, fld) in zip(probs, out):
+        n = len(pos)
+        idx = np.arange(64) * (n // 64)
+        pe = compute_exact(InteractionType.Potential3d, (pos, q), pos[idx], ctx=ctx) - q[idx] * 1e4
+        fe = compute_exact(InteractionType.Force3d, (pos, q), pos[idx], ctx=ctx)
+        assert rel_l2(noself(pot[idx], q[idx]), pe) <= 1e-6
+        assert rel_l2(fld[idx], fe) <= 1e-6
