@@ -760,13 +760,14 @@ def run_batch(args, cfg):
             ends[k].record(stream)
         torch.cuda.synchronize()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
-    # per-problem accuracy against its own FP64 direct sum: every output of a problem of up to 8192
-    # particles, 64 evenly spread outputs of a larger one
+    # per-problem accuracy against its own FP64 direct sum: every output of a problem of up to 65536
+    # particles, 8192 evenly spread outputs of a larger one (a sample of a few dozen outputs can miss the
+    # high-field targets that dominate the norm and overstate a problem's rel-L2 several times)
     pot, fld = d_pot.cpu().numpy(), d_fld.cpu().numpy()
     errs_p, errs_f = [], []
     for k, (p, c) in enumerate(probs):
         b = int(offs[k])
-        idx = np.arange(len(p)) if len(p) <= 8192 else np.arange(0, len(p), len(p) // 64)
+        idx = np.arange(len(p)) if len(p) <= 65536 else np.arange(0, len(p), len(p) // 8192)
         tgt = torch.from_numpy(np.ascontiguousarray(p[idx])).cuda()
         ep = torch.empty(len(idx), dtype=torch.float64, device="cuda")
         ef = torch.empty(len(idx), 3, dtype=torch.float64, device="cuda")
@@ -808,7 +809,7 @@ def run_batch(args, cfg):
             "accuracy": {"rel_l2_pot_noself_median": float(np.median(ep_)), "rel_l2_pot_noself_p95":
                          float(np.quantile(ep_, 0.95)), "rel_l2_pot_noself_max": float(ep_.max()),
                          "rel_l2_field_median": float(np.median(ef_)), "rel_l2_field_max": float(ef_.max()),
-                         "targets_per_problem": "every output up to 8192 particles, else 64", "within_tol": int(np.sum(np.maximum(ep_, ef_) <= cfg["tol"])),
+                         "targets_per_problem": "every output up to 65536 particles, else 8192 evenly spread", "within_tol": int(np.sum(np.maximum(ep_, ef_) <= cfg["tol"])),
                          "worst_problems": worst},
             "plain_fp64_one_at_a_time": {"value": n / (pms * 1e-3) / 1e6, "unit": "Mparticles/s",
                                          "ms": pms, "N_degrees": cfg["plain_N"]},

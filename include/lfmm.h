@@ -376,6 +376,8 @@ typedef struct {
 	                               network when opts->max_leaf is LFMM_AUTO) */
 	int order_groups;           /* batches: the distinct orders the problems were solved at (each
 	                               order's problems as one forest); 1 for a single solve */
+	int checked_targets;        /* the sampled outputs the final judgement used (batches: over all
+	                               problems) */
 } lfmm_learned_info;
 
 /* 3D solve at the order the network picks for tolerance tol, which bounds
@@ -388,7 +390,10 @@ typedef struct {
  * 0.6 tol is solved (else N = 18).  The same samples then judge the result
  * on an upper confidence bound of each sampled rel-L2 (the ratio estimate
  * plus two standard errors, so a sample too small or too uneven to certify
- * tol does not pass).  A solve whose bound exceeds tol is rerun once at the
+ * tol does not pass).  When the bound exceeds tol while the estimate is
+ * within 0.75 tol, three times more outputs (between the first ones) are
+ * summed directly and the result judged again on all of them.  A solve
+ * whose bound still exceeds tol is rerun once at the
  * order picked again from the predictions shifted by the shortfall measured
  * (bound over prediction), then, if that misses too, at the fixed order
  * N = 18 (the fallback); a mixed-precision solve still above tol there is
@@ -415,7 +420,8 @@ int lfmm3d_solve_learned_device(lfmm_ctx* ctx, size_t n_src, const double* src_x
  * per problem, every output of a problem of at most 8192 particles (their
  * FP64 direct sums in one launch), normalise each
  * problem's prediction and judge its result (the same upper confidence
- * bounds, per problem).  Every problem runs at its own predicted order: when
+ * bounds, per problem, and the same threefold extension of the samples of a
+ * problem whose estimate is within 0.75 tol but whose bound is not).  Every problem runs at its own predicted order: when
  * the problems need several, the problems of each order are solved together
  * as their own forest (order_groups in info), and the problems an order
  * left above tol are solved again together at N = 18; a problem still above

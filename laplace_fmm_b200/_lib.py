@@ -67,7 +67,8 @@ class LfmmLearnedInfo(ctypes.Structure):
                 ("predicted_error", ctypes.c_double), ("checked_error", ctypes.c_double),
                 ("checked_error_field", ctypes.c_double), ("fp64_resolved", ctypes.c_int),
                 ("predicted_error_field", ctypes.c_double), ("judged_error", ctypes.c_double),
-                ("max_leaf", ctypes.c_int), ("order_groups", ctypes.c_int)]
+                ("max_leaf", ctypes.c_int), ("order_groups", ctypes.c_int),
+                ("checked_targets", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

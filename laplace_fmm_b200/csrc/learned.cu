@@ -37,6 +37,11 @@ constexpr double LEARNED_MARGIN = 0.6;
 // here too the retries of the 64 held-out problems went to N = 18 where
 // one order above the miss passed.
 constexpr double RETRY_MARGIN = 0.85;
+// A solve whose sampled estimate is within EXTEND_ESTIMATE tol but whose
+// upper bound is not gets three times more samples before any rerun: the
+// bound is then loose because a few outputs with large errors dominate the
+// sample's variance, which more samples narrow at a fraction of a solve's cost.
+constexpr double EXTEND_ESTIMATE = 0.75;
 // A learned batch solves its problems in at most this many orders.
 constexpr int MAX_ORDER_GROUPS = 3;
 // Problems of a learned batch with at most this many particles are checked at
@@ -179,25 +184,36 @@ __global__ void predict_reduce_kernel(const float* __restrict__ Y, const float* 
 }
 
 // Sampled check: positions of the sampled outputs (every stride-th output).
-__global__ void sample_points_kernel(const double* __restrict__ pts, size_t stride, size_t m, double* __restrict__ out)
+// The output index of sample i: sub = 1, every stride-th output from 0; sub =
+// 3, the three outputs at the quarters of the stride between consecutive
+// samples of the sub = 1 set (stride >= 4), so that both sets together are
+// evenly spaced at a quarter of the stride.
+__device__ __forceinline__ size_t sample_index(size_t i, size_t stride, int sub)
+{
+	return sub == 1 ? i * stride : (i / 3) * stride + (i % 3 + 1) * (stride / 4);
+}
+
+__global__ void sample_points_kernel(const double* __restrict__ pts, size_t stride, int sub, size_t m,
+                                     double* __restrict__ out)
 {
 	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= m) return;
-	for (int d = 0; d < 3; ++d) out[3 * i + d] = pts[3 * (i * stride) + d];
+	const size_t j = sample_index(i, stride, sub);
+	for (int d = 0; d < 3; ++d) out[3 * i + d] = pts[3 * j + d];
 }
 
 // acc: [0] sum (pot - direct)^2, [1] sum (direct - self)^2, [2] sum |dfield|^2,
 // [3] sum |field|^2 over the sampled outputs.  q: the outputs' charges (null
 // in target mode: no self term).
-__global__ void check_kernel(const double* __restrict__ pot, const double* __restrict__ fld, size_t stride, size_t m,
-                             const double* __restrict__ q, const double* __restrict__ ep,
+__global__ void check_kernel(const double* __restrict__ pot, const double* __restrict__ fld, size_t stride, int sub,
+                             size_t m, const double* __restrict__ q, const double* __restrict__ ep,
                              const double* __restrict__ ef, double* __restrict__ acc)
 {
 	// per sample: a = squared error, b = squared reference, for the potential
 	// (self term removed) and the field; sums of a, b, a^2, b^2, a b of each
 	double v[NCHK] = {};
 	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
-		const size_t j = i * stride;
+		const size_t j = sample_index(i, stride, sub);
 		const double self = q ? q[j] / FORCE_EPS : 0.0;
 		const double d = pot[j] - ep[i], r = ep[i] - self;
 		double e2 = 0.0, f2 = 0.0;
@@ -399,6 +415,7 @@ int learned_predictions(Context& ctx, const double* acc, const double rms[2], do
 // main stream wait for it and returns the RMS.
 struct Samples {
 	size_t m = 0, stride = 1;
+	int sub = 1;                // sample_index's form
 	double *sp = nullptr, *ep = nullptr, *ef = nullptr, *acc = nullptr;
 };
 
@@ -427,7 +444,7 @@ int direct_samples_launch(Context& ctx, const ParticleInput& in, size_t m, Sampl
 	{
 		OnSideStream on_side(ctx);
 		cudaStream_t s = ctx.stream;
-		sample_points_kernel<<<div_up(S.m, 256), 256, 0, s>>>(pts, S.stride, S.m, S.sp);
+		sample_points_kernel<<<div_up(S.m, 256), 256, 0, s>>>(pts, S.stride, 1, S.m, S.sp);
 		st = direct_device(ctx, 3, in.ns, in.src, in.srcq, S.m, S.sp, S.ep, S.ef, /*fast=*/true);
 		if (st == OK) {
 			// the RMS: the check against the direct sum itself (pot = direct, zero error)
@@ -456,20 +473,50 @@ int samples_join(Context& ctx, const Samples& S, double rms[2])
 	return OK;
 }
 
-// Sampled rel-L2 of the potential (self term removed) and of the field:
-// out[0], out[1] the estimates, out[2], out[3] their upper confidence bounds.
-int sampled_error(Context& ctx, const ParticleInput& in, const Samples& S, const double* pot, const double* field,
-                  double out[4])
+// Three more samples per sample of S, between S's (sample_index, sub = 3),
+// their FP64 direct sums on the stream.  ERR_UNSUPPORTED when S's stride is
+// below 4 (S already covers at least a quarter of the outputs).
+int direct_samples_extend(Context& ctx, const ParticleInput& in, const Samples& S, Samples& X)
+{
+	if (S.stride < 4) return ERR_UNSUPPORTED;
+	X.m = 3 * S.m;
+	X.stride = S.stride;
+	X.sub = 3;
+	X.sp = take<double>(ctx, 3 * X.m);
+	X.ep = take<double>(ctx, X.m);
+	X.ef = take<double>(ctx, 3 * X.m);
+	X.acc = take<double>(ctx, NCHK);
+	if (!X.sp || !X.ep || !X.ef || !X.acc) { ctx.last_error = "sampled check: allocation failed"; return ERR_OOM; }
+	sample_points_kernel<<<div_up(X.m, 256), 256, 0, ctx.stream>>>(in.nt ? in.tgt : in.src, X.stride, 3, X.m, X.sp);
+	LFMM_CUDA(ctx, cudaGetLastError());
+	return direct_device(ctx, 3, in.ns, in.src, in.srcq, X.m, X.sp, X.ep, X.ef, /*fast=*/true);
+}
+
+// Sampled rel-L2 of the potential (self term removed) and of the field over
+// the samples of S and, when X is given, X too: out[0], out[1] the
+// estimates, out[2], out[3] their upper confidence bounds.
+int sampled_error(Context& ctx, const ParticleInput& in, const Samples& S, const Samples* X, const double* pot,
+                  const double* field, double out[4])
 {
 	cudaStream_t s = ctx.stream;
-	LFMM_CUDA(ctx, cudaMemsetAsync(S.acc, 0, sizeof(double) * NCHK, s));
-	check_kernel<<<(unsigned)std::min<size_t>(div_up(S.m, 256), 64), 256, 0, s>>>(
-		pot, field, S.stride, S.m, in.nt ? nullptr : in.srcq, S.ep, S.ef, S.acc);
-	double h[NCHK];
+	double h[NCHK], hx[NCHK];
+	size_t m = S.m;
+	for (const Samples* P : {&S, X}) {
+		if (!P) continue;
+		LFMM_CUDA(ctx, cudaMemsetAsync(P->acc, 0, sizeof(double) * NCHK, s));
+		check_kernel<<<(unsigned)std::min<size_t>(div_up(P->m, 256), 64), 256, 0, s>>>(
+			pot, field, P->stride, P->sub, P->m, in.nt ? nullptr : in.srcq, P->ep, P->ef, P->acc);
+		LFMM_CUDA(ctx, cudaGetLastError());
+	}
 	LFMM_CUDA(ctx, cudaMemcpyAsync(h, S.acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+	if (X) LFMM_CUDA(ctx, cudaMemcpyAsync(hx, X->acc, sizeof(hx), cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
-	rel_l2_bound(h, (double)S.m, &out[0], &out[2]);
-	rel_l2_bound(h + 5, (double)S.m, &out[1], &out[3]);
+	if (X) {
+		for (int k = 0; k < NCHK; ++k) h[k] += hx[k];
+		m += X->m;
+	}
+	rel_l2_bound(h, (double)m, &out[0], &out[2]);
+	rel_l2_bound(h + 5, (double)m, &out[1], &out[3]);
 	return OK;
 }
 
@@ -646,8 +693,20 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 	li.predicted_N = N;
 	if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
 	double e[4];
-	if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+	Samples X;
+	const Samples* XP = nullptr;
+	if ((st = sampled_error(ctx, in, S, XP, pot, field, e))) return st;
 	auto judged = [&] { return std::max(e[2], e[3]); };
+	li.checked_targets = (int)S.m;
+	if (judged() > tol && std::max(e[0], e[1]) <= EXTEND_ESTIMATE * tol && S.stride >= 4) {
+		// the estimate is well within tol but its bound is not (a few outputs
+		// with large errors dominate the sample's variance): three times more
+		// samples, between the first ones, before any rerun
+		if ((st = direct_samples_extend(ctx, in, S, X))) return st;
+		XP = &X;
+		li.checked_targets = (int)(S.m + X.m);
+		if ((st = sampled_error(ctx, in, S, XP, pot, field, e))) return st;
+	}
 	if (judged() > tol && N < FB_N - 1) {
 		// a prediction that missed: shift each output's predictions by the
 		// shortfall the judge measured at N (bound over prediction) and pick
@@ -661,19 +720,19 @@ int solve_learned_device(Context& ctx, const ParticleInput& in, int depth, int m
 		N = std::max(N2, N + 1);
 		li.fallback = 1;
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
-		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+		if ((st = sampled_error(ctx, in, S, XP, pot, field, e))) return st;
 	}
 	if (judged() > tol && N < FB_N) {
 		// the fixed-order fallback judges and replaces a prediction that missed
 		N = FB_N;
 		li.fallback = 2;
 		if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
-		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+		if ((st = sampled_error(ctx, in, S, XP, pot, field, e))) return st;
 	}
 	if (judged() > tol && precision == LFMM_PRECISION_MIXED) {
 		// the mixed form cannot reach tol even at the fallback order: the FP64 form
 		if ((st = fmm3d_scaled_on_tree(ctx, t, FB_N, LFMM_PRECISION_FP64, pot, field, stats))) return st;
-		if ((st = sampled_error(ctx, in, S, pot, field, e))) return st;
+		if ((st = sampled_error(ctx, in, S, XP, pot, field, e))) return st;
 		N = FB_N;
 		li.fp64_resolved = 1;
 	}
@@ -773,29 +832,75 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 		}
 	}
 	li.predicted_N = N;
-	// per problem: the estimates and the judge's bound of both outputs
-	std::vector<double> judged(P, 0.0);
+	li.checked_targets = (int)m;
+	// per problem: the estimates and the judge's bound of both outputs, over
+	// the samples and the extension samples (xm: the extension's count)
+	std::vector<double> judged(P, 0.0), estimate(P, 0.0);
+	std::vector<size_t> xcount(P, 0);
+	size_t xm = 0;
+	uint32_t* xidx = nullptr;
+	int32_t* xprob = nullptr;
+	double *xep = nullptr, *xef = nullptr;
 	auto check = [&](bool recheck) -> int {
 		if (recheck) {
 			LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(double) * NCHK * P, s));
 			check_forest_kernel<<<div_up(m, 256), 256, 0, s>>>(pot, field, idx, prob, m, in.srcq, ep, ef, acc);
+			if (xm)
+				check_forest_kernel<<<div_up(xm, 256), 256, 0, s>>>(pot, field, xidx, xprob, xm, in.srcq, xep, xef, acc);
 			LFMM_CUDA(ctx, cudaMemcpyAsync(ha.data(), acc, sizeof(double) * ha.size(), cudaMemcpyDeviceToHost, s));
 			LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 		}
 		li.checked_error = li.checked_error_field = li.judged_error = 0.0;
 		for (int k = 0; k < P; ++k) {
-			const size_t mk = soff[k + 1] - soff[k];
-			judged[k] = 0.0;
+			const size_t mk = soff[k + 1] - soff[k] + xcount[k];
+			judged[k] = estimate[k] = 0.0;
 			if (!mk) continue;
 			double e[4];
 			rel_l2_bound(ha.data() + (size_t)NCHK * k, (double)mk, &e[0], &e[2]);
 			rel_l2_bound(ha.data() + (size_t)NCHK * k + 5, (double)mk, &e[1], &e[3]);
 			judged[k] = std::max(e[2], e[3]);
+			estimate[k] = std::max(e[0], e[1]);
 			li.checked_error = std::max(li.checked_error, e[0]);
 			li.checked_error_field = std::max(li.checked_error_field, e[1]);
 			li.judged_error = std::max(li.judged_error, judged[k]);
 		}
 		return OK;
+	};
+	// the problems whose estimate is within EXTEND_ESTIMATE tol but whose
+	// bound is not: three times more samples each, between their first ones
+	// (sample_index's sub = 3 form over the problem's own stride), their
+	// direct sums in one launch, and the judgement again over all samples
+	auto extend = [&]() -> int {
+		if (xm || li.judged_error <= tol) return OK;
+		std::vector<uint32_t> hx;
+		std::vector<int32_t> hxp;
+		for (int k = 0; k < P; ++k) {
+			const size_t mk = soff[k + 1] - soff[k], nk = hoff[k + 1] - hoff[k];
+			if (!mk || judged[k] <= tol || estimate[k] > EXTEND_ESTIMATE * tol) continue;
+			const size_t stride = nk / mk;
+			if (stride < 4) continue;
+			for (size_t j = 0; j < 3 * mk; ++j) {
+				hx.push_back((uint32_t)(hoff[k] + (j / 3) * stride + (j % 3 + 1) * (stride / 4)));
+				hxp.push_back(k);
+			}
+			xcount[k] = 3 * mk;
+		}
+		if (hx.empty()) return OK;
+		const size_t n_x = hx.size();
+		xidx = take<uint32_t>(ctx, n_x);
+		xprob = take<int32_t>(ctx, n_x);
+		double* xsp = take<double>(ctx, 3 * n_x);
+		xep = take<double>(ctx, n_x);
+		xef = take<double>(ctx, 3 * n_x);
+		if (!xidx || !xprob || !xsp || !xep || !xef) { ctx.last_error = "learned batch: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(ctx, cudaMemcpyAsync(xidx, hx.data(), sizeof(uint32_t) * n_x, cudaMemcpyHostToDevice, s));
+		LFMM_CUDA(ctx, cudaMemcpyAsync(xprob, hxp.data(), sizeof(int32_t) * n_x, cudaMemcpyHostToDevice, s));
+		gather_points_kernel<<<div_up(n_x, 256), 256, 0, s>>>(in.src, xidx, n_x, xsp);
+		int st2 = direct_segments_device(ctx, in.src, in.srcq, in.poff, xprob, n_x, xsp, xep, xef);
+		if (st2) return st2;
+		xm = n_x;
+		li.checked_targets = (int)(m + xm);
+		return check(true);
 	};
 	// problems grouped by their own order: one group solves on the forest
 	// already built; several solve as separate forests of their problems
@@ -826,7 +931,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 	if (orders.size() <= 1) {
 		for (int pass = 0; pass < 2; ++pass) {
 			if ((st = fmm3d_scaled_on_tree(ctx, t, N, precision, pot, field, stats))) return st;
-			if ((st = check(true))) return st;
+			if ((st = check(true)) || (st = extend())) return st;
 			if (li.judged_error <= tol || N >= FB_N) break;
 			N = FB_N;                      // the fixed-order fallback for the whole batch
 			li.fallback = 1;
@@ -838,7 +943,7 @@ int solve_learned_batch_device(Context& ctx, const ParticleInput& in, const size
 				if (Nk_of[k] == Ng) members.push_back(k);
 			if ((st = solve_group(ctx, in, hoff, members, Ng, depth, li.max_leaf, precision, pot, field))) return st;
 		}
-		if ((st = check(true))) return st;
+		if ((st = check(true)) || (st = extend())) return st;
 		// the problems a group's order left above tol: again at the fallback order, as one group
 		std::vector<int> miss;
 		for (int k = 0; k < P; ++k)

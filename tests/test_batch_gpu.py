@@ -68,6 +68,8 @@ def test_learned_batch_within_tolerance(ctx, problems):
     out, info = solver.solve_batch(problems, tol=1e-6, tree_depth=8, check_targets=64)
     assert 5 <= info["order_N"] <= 18
     assert info["checked_error"] <= 1e-6 and info["checked_error_field"] <= 1e-6
+    # every output of a problem of up to 8192 particles, else 64 (more where the judge extended them)
+    assert info["checked_targets"] >= sum(len(p) if len(p) <= 8192 else 64 for p, _ in problems)
     if info["order_groups"] != 1:
         pytest.skip("the problems ran at several orders (the per-order groups are tested below)")
     ref = solve_batch(problems, N=info["order_N"], tree_depth=8, max_leaf=64, ctx=ctx)

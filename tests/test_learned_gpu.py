@@ -92,19 +92,45 @@ def test_judge_catches_an_error_just_under_tol_on_too_few_samples(ctx):
     the blind network's solve (N = 5) with a loose tol gives the estimates and
     the bound on 32 samples of a clustered set; then tol is set between the
     larger estimate and the bound, where a judge of the estimate alone would
-    pass the N = 5 solve."""
+    pass the N = 5 solve.  tol stays below est / 0.75, so the samples are not
+    extended (the next test covers that)."""
     s = LearnedSolver(_blind_network(), ctx=ctx)
     src, q = gaussian_mix3d(60000, seed=90031)
     r = s.solve(src, q, tol=1.0, tree_depth=10, max_leaf=64, check_targets=32)
     info = r["info"]
-    assert info["order_N"] == 5 and info["fallback"] == 0
+    assert info["order_N"] == 5 and info["fallback"] == 0 and info["checked_targets"] == 32
     est = max(info["checked_error"], info["checked_error_field"])
     assert info["judged_error"] > 1.2 * est
-    tol = np.sqrt(est * info["judged_error"])
+    tol = min(np.sqrt(est * info["judged_error"]), est / 0.8)
     r2 = s.solve(src, q, tol=tol, tree_depth=10, max_leaf=64, check_targets=32)
     i2 = r2["info"]
     assert i2["predicted_N"] == 5 and i2["fallback"] >= 1 and i2["order_N"] > 5
-    assert i2["judged_error"] <= tol
+    assert i2["judged_error"] <= tol and i2["checked_targets"] == 32
+
+
+def test_judge_extends_the_samples_of_a_loose_bound(ctx):
+    """An estimate within 0.75 tol whose bound exceeds tol: before any rerun
+    the judge sums three times more outputs directly (the three quarter
+    points between consecutive samples) and judges again on all of them; the
+    reported check is the rel-L2 over those 4 m outputs."""
+    from laplace_fmm_b200 import InteractionType, compute_exact
+    s = LearnedSolver(_blind_network(), ctx=ctx)
+    src, q = gaussian_mix3d(60000, seed=90031)
+    m = 16
+    r = s.solve(src, q, tol=1.0, tree_depth=10, max_leaf=64, check_targets=m)
+    info = r["info"]
+    est = max(info["checked_error"], info["checked_error_field"])
+    tol = est / 0.7
+    assert info["judged_error"] > tol          # a bound too loose for tol on 16 samples
+    r2 = s.solve(src, q, tol=tol, tree_depth=10, max_leaf=64, check_targets=m)
+    i2 = r2["info"]
+    assert i2["checked_targets"] == 4 * m and i2["judged_error"] <= tol
+    st = len(src) // m
+    idx = np.sort(np.concatenate([np.arange(m) * st] + [np.arange(m) * st + k * (st // 4) for k in (1, 2, 3)]))
+    pe = compute_exact(InteractionType.Potential3d, (src, q), src[idx], ctx=ctx) - q[idx] * 1e4
+    fe = compute_exact(InteractionType.Force3d, (src, q), src[idx], ctx=ctx)
+    assert i2["checked_error"] == pytest.approx(rel_l2(r2["potentials"][idx] - q[idx] * 1e4, pe), rel=1e-6)
+    assert i2["checked_error_field"] == pytest.approx(rel_l2(r2["forces"][idx], fe), rel=1e-6)
 
 
 def test_fp64_rerun_below_the_mixed_floor(solver, ctx):
