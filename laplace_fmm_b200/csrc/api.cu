@@ -359,11 +359,13 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	if (!ctx) return LFMM_ERR_OOM;
 	Context& c = ctx->c;
 	if (opt) { c.device = opt->device; c.verbose = opt->verbose; c.timing = opt->timing; }
-	// M2L engine (LFMM_M2L): tc (default) = tcgen05 TF32 hi/lo GEMMs on the FP32
+	// M2L engine (LFMM_M2L): tc (default) = tcgen05 hi/lo GEMMs on the FP32
 	// levels and SIMT GEMMs elsewhere; simt = SIMT GEMMs only; rotation =
-	// per-pair rotations on the plain path
+	// per-pair rotations on the plain path.  LFMM_M2L_TYPE: f16 (default) or
+	// tf32, the tcgen05 M2L's operand type.
 	c.m2l_engine = 3;
 	if (const char* e = std::getenv("LFMM_M2L_TUNE")) c.tune_m2l = std::strcmp(e, "0") != 0;
+	if (const char* e = std::getenv("LFMM_M2L_TYPE")) c.m2l_f16 = std::strcmp(e, "tf32") != 0;
 	if (const char* e = std::getenv("LFMM_M2L"))
 		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 0 : 3);
 	int ndev = 0;

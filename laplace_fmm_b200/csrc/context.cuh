@@ -78,6 +78,7 @@ struct OpCacheEntry {
 	size_t bytes = 0;
 	unsigned long long stamp = 0;
 	int pinned = 0;                   // > 0: a captured graph reads it (never evicted)
+	float aux = 1.f;                  // FP16 tensor-core operators: the inverse of their scale
 };
 
 struct Context {
@@ -102,11 +103,14 @@ struct Context {
 	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 	cudaEvent_t kev[32] = {};          // pairs around the tensor-core M2L launches (timing)
 	int kev_used = 0;
-	// M2L autotuner: slot split chosen per (operator rows / 16, level-size
-	// bucket); 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0): the fixed rule.
-	// Operator rows reach 352 (N = 18): 23 row classes.
+	// tcgen05 M2L operands: FP16 hi / lo pairs (1, the default) or TF32 hi / lo
+	// pairs (0; LFMM_M2L_TYPE=tf32)
+	int m2l_f16 = 1;
+	// M2L autotuner: slot split chosen per (operand type, operator rows / 16,
+	// level-size bucket); 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0):
+	// the fixed rule.  Operator rows reach 352 (N = 18): 23 row classes.
 	static constexpr int SPLIT_ROWS = 352 / 16 + 1;
-	int m2l_split[SPLIT_ROWS][33] = {};
+	int m2l_split[2][SPLIT_ROWS][33] = {};
 	int tune_m2l = 1;
 	int timing = 0;
 };

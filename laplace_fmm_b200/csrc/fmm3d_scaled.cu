@@ -253,11 +253,12 @@ int solve_t(Context& ctx, const DevTree& t, int N, double* pot, double* field, S
 				if ((st = m2l_gemm<double>(ctx, plan, opd, cv_in, cv_out, N))) return st;
 				convert_back_kernel<real><<<div_up(m, 256), 256, 0, s>>>(cv_out, lL, m);
 			} else if (sizeof(real) == sizeof(float) && ctx.m2l_engine == 3 && m2l_tc_supported(N)) {
-				// tcgen05 TF32 hi/lo GEMM on the FP32 levels
-				const uint4* tc = m2l_ops_tc(ctx, N);
+				// tcgen05 hi/lo GEMM on the FP32 levels (FP16 or TF32 operands)
+				float t_inv = 1.f;
+				const uint4* tc = m2l_ops_tc(ctx, N, &t_inv);
 				if (!tc) return ERR_OOM;
 				if ((st = m2l_gemm_tc(ctx, plan, tc, reinterpret_cast<const float*>(mL), reinterpret_cast<float*>(lL), N,
-				                      level_N ? level_N[L] : 0)))
+				                      level_N ? level_N[L] : 0, t_inv)))
 					return st;
 			} else {
 				if ((st = m2l_gemm<real>(ctx, plan, ops, mL, lL, N))) return st;

@@ -21,8 +21,10 @@
 // DEV_ERR_TIMEOUT, waits (bounded) for its copies and MMAs in flight, frees
 // TMEM and returns.
 #include "m2l_tc.cuh"
+#include <cuda_fp16.h>
 #include "fmm3d.cuh"
 #include <mutex>
+#include <cstring>
 #include <cmath>
 
 namespace lfmm {
@@ -60,52 +62,42 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
 	return d;
 }
 
-// D (+)= A B^T with A read from tensor memory (M lanes x K columns of TF32)
-template <int NC>
-__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate)
+// Instruction descriptor: D FP32, A and B both TF32 (kind::tf32) or both FP16
+// (kind::f16), K-major, M = TC_M, N = n (a multiple of 16 in [16, 256]).
+template <bool F16>
+__host__ __device__ constexpr uint32_t idesc_of(int n)
 {
-	constexpr uint32_t IDESC = (1u << 4)                     // D: FP32
-	                         | (2u << 7)                     // A: TF32
-	                         | (2u << 10)                    // B: TF32
-	                         | ((uint32_t)(NC >> 3) << 17)   // N
-	                         | ((uint32_t)(TC_M >> 4) << 24); // M
-	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
-	             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(IDESC), "r"(accumulate));
+	return (1u << 4) | ((F16 ? 0u : 2u) << 7) | ((F16 ? 0u : 2u) << 10) | ((uint32_t)(n >> 3) << 17) |
+	       ((uint32_t)(TC_M >> 4) << 24);
 }
 
-template <int NC>
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+// D (+)= A B^T, one K step (32 bytes of each row: 8 TF32 or 16 FP16 inputs),
+// A read from tensor memory (M lanes x 8 columns)
+template <bool F16>
+__device__ __forceinline__ void mma_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t accumulate)
 {
-	constexpr uint32_t IDESC = (1u << 4)                     // D: FP32
-	                         | (2u << 7)                     // A: TF32
-	                         | (2u << 10)                    // B: TF32
-	                         | ((uint32_t)(NC >> 3) << 17)   // N
-	                         | ((uint32_t)(TC_M >> 4) << 24); // M
-	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate));
+	if constexpr (F16)
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		             "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n"
+		             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
+	else
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		             "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+		             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
-// Runtime-N forms (N a multiple of 16 in [16, 256]).
-__device__ __forceinline__ uint32_t idesc_tf32(int n)
+// the same with A in shared memory
+template <bool F16>
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
 {
-	return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_tf32_ta_n(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
-                                              uint32_t accumulate)
-{
-	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
-	             :: "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_tf32_n(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
-{
-	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-	             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+	if constexpr (F16)
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+		             :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+	else
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+		             :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar)
@@ -229,11 +221,18 @@ __device__ __forceinline__ void tmem_accumulate(uint32_t taddr, float (&acc)[W])
 // of the drained columns (NA x 128 bytes) and the sources' lo block.
 //
 // TMEM_HI = false keeps the sources' hi parts in shared memory (the L2L
-// mode: one slot of few K blocks per tile leaves the TMEM stores' waits exposed)
-template <int NC, int NA, bool TMEM_HI = true>
+// mode: one slot of few K blocks per tile leaves the TMEM stores' waits exposed).
+// F16: the operands are FP16 hi / lo pairs (kind::f16, twice the TF32 rate;
+// the same 11-bit significands, the range kept by exact power-of-two scales of
+// the operators and of each level's multipoles): a 128-byte row holds 64
+// inputs instead of 32, so a K block covers 64 inputs with the same bytes,
+// descriptors and TMEM columns.
+template <int NC, int NA, bool TMEM_HI = true, bool F16 = false>
 struct TcCfg {
-	static constexpr int KB = (NC + 31) / 32;           // K blocks of 32 inputs
-	static constexpr int KBC = (NA + 31) / 32;          // K blocks with corrections
+	static constexpr int EPB = F16 ? 64 : 32;           // inputs per 128-byte row (K block)
+	static constexpr int UPB = EPB / 32;                // 32-input gather units per K block
+	static constexpr int KB = (NC + EPB - 1) / EPB;     // K blocks
+	static constexpr int KBC = (NA + EPB - 1) / EPB;    // K blocks with corrections
 	static constexpr int HI_BYTES = NC * 128;           // operator hi rows of a K block
 	static constexpr int LO_BYTES = NA * 128;           // operator lo rows (drained columns) of a K block
 	static constexpr int A_BYTES = TC_M * 128;          // one 32-wide K block of the multipoles (hi or lo)
@@ -251,6 +250,9 @@ struct TcCfg {
 	static __host__ __device__ __forceinline__ uint32_t op_bytes(int kb)
 	{ return (uint32_t)(HI_BYTES + (kb < KBC ? LO_BYTES : 0)); }
 	static __device__ __forceinline__ uint32_t hi_col(uint32_t s) { return (uint32_t)(NC + NA) + 32u * s; }
+	// K steps (32 bytes of a row each) of K block kb holding inputs below NC
+	static __host__ __device__ __forceinline__ int ksteps(int kb)
+	{ const int left = NC - kb * EPB; return left >= EPB ? 4 : (left + EPB / 4 - 1) / (EPB / 4); }
 	static_assert(NC % 16 == 0 && NC >= 16 && NC <= 352, "operator rows");
 	static_assert(NA % 16 == 0 && NA >= 16 && NA <= NC && NA <= 256 && NC - NA <= 256, "MMA N");
 	static_assert(NC + NA <= (int)TMEM_COLS, "TMEM columns");
@@ -290,15 +292,60 @@ __device__ __forceinline__ int dir_d2(int dir)
 // The K blocks of a slot are fed from the highest degrees down, so the
 // dominant low-degree products enter each FP32 accumulator last, when the
 // accumulator's own rounding has least left to act on.
-template <int NC, int NA, int SLOTS, int MODE, bool PERSIST>
+// The exponent e of the FP16 multipole scale 2^e for a level whose largest
+// magnitude has the float bits mb: 2^e mb in [2^14, 2^15).
+__host__ __device__ __forceinline__ int f16_exponent(uint32_t mb)
+{
+	const int e = mb ? 14 - ((int)((mb >> 23) & 255u) - 127) : 0;
+	return e < -126 ? -126 : (e > 126 ? 126 : e);
+}
+
+// The M2L's FP16 sources: each cell's multipole (R floats) x 2^e split into
+// FP16 hi and lo (the residual), as rows of KB blocks of 64 (hi; zero past
+// R) and of KBC blocks (lo), FP16 pairs with the lower input in the low half.
+// One thread per (cell, 8 inputs).
+__global__ void stage_f16_kernel(const float* __restrict__ mult, size_t cells, int R, int KB, int KBC,
+                                 const unsigned* __restrict__ bmax, uint4* __restrict__ hi, uint4* __restrict__ lo)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= cells * (size_t)KB * 8) return;
+	const size_t cell = i / ((size_t)KB * 8);
+	const int c = (int)(i % ((size_t)KB * 8));
+	const float sc = __uint_as_float((uint32_t)(127 + f16_exponent(*bmax)) << 23);
+	const float2* row = reinterpret_cast<const float2*>(mult + cell * (size_t)R);
+	uint32_t h[4], l[4];
+#pragma unroll
+	for (int q = 0; q < 4; ++q) {
+		const int k = c * 8 + 2 * q;                 // R is even: a pair is in or out
+		const float2 x = k < R ? row[k / 2] : make_float2(0.f, 0.f);
+		const float x0 = x.x * sc, x1 = x.y * sc;
+		const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+		const __half l0 = __float2half_rn(x0 - __half2float(h0)), l1 = __float2half_rn(x1 - __half2float(h1));
+		h[q] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+		l[q] = (uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
+	}
+	hi[i] = make_uint4(h[0], h[1], h[2], h[3]);
+	if (c < KBC * 8) lo[cell * (size_t)KBC * 8 + c] = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// F16 (M2L only): the sources come split already (stage_f16_kernel): shi /
+// slo hold each source cell's multipole scaled by 2^e, with e such that the
+// level's largest magnitude (*bmax, the bits of a positive float) lands in
+// [2^14, 2^15), as FP16 hi / lo rows of KB (lo: KBC) blocks of 64; the
+// results are scaled by 2^-e t_inv (t_inv: the inverse of the operators'
+// scale); both exact.
+template <int NC, int NA, int SLOTS, int MODE, bool PERSIST, bool F16>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
               const float* __restrict__ diag, unsigned* flags, const TcTrunc trunc, size_t src_cells, int ndir,
-              unsigned* __restrict__ work, int S, unsigned total)
+              unsigned* __restrict__ work, int S, unsigned total, const unsigned* __restrict__ bmax, float t_inv,
+              const uint4* __restrict__ shi, const uint4* __restrict__ slo)
 {
-	using C = TcCfg<NC, NA, MODE != TC_L2L>;
+	static_assert(!F16 || MODE == TC_M2L, "FP16 operands: M2L only");
+	using C = TcCfg<NC, NA, MODE != TC_L2L, F16>;
+	constexpr int UPB = C::UPB;
 	extern __shared__ uint8_t dsm[];
 	constexpr int NSTAGE = C::NSTAGE;
 	constexpr int KB = C::KB, KBC = C::KBC;
@@ -325,6 +372,9 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 	const uint32_t tmem = tmem_sh;
+	// the FP16 outputs' scale 2^-e t_inv
+	float out_scale = 1.f;
+	if constexpr (F16) out_scale = __uint_as_float((uint32_t)(127 - f16_exponent(*bmax)) << 23) * t_inv;
 
 	for (int round = 0;; ++round) {
 	uint32_t witem;
@@ -405,19 +455,35 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 		// comparable with one K block of MMAs).
 		const int myt = tgt[tid];
 		uint32_t it = 0;
-		// the gather of K block kb of slot active[j] into w[16]
-		auto gather = [&](int j, int kb, float2 (&w)[16]) {
+		// the gather of 32-input unit g (inputs [32 g, 32 g + 32)) of slot
+		// active[j] into w: TF32, the 32 multipole floats (bits); F16, the staged
+		// hi words (w[0, 16)) and, in corrected K blocks, lo words (w[16, 32))
+		auto gather = [&](int j, int g, uint32_t (&w)[32]) {
 			const int slot = active[j];
 			int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
 			if (src >= 0 && (size_t)src >= src_cells) {    // a source outside the level: skipped, reported
 				atomicOr(flags, DEV_ERR_RANGE);
 				src = -1;
 			}
-			const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
+			if constexpr (F16) {
+				const bool corr = g / UPB < KBC;
+				const uint4* hp = shi + (size_t)(src >= 0 ? src : 0) * (KB * 8) + g * 4;
+				const uint4* lp = slo + (size_t)(src >= 0 ? src : 0) * (KBC * 8) + g * 4;
 #pragma unroll
-			for (int q = 0; q < 16; ++q) {
-				const int k = kb * 32 + 2 * q;               // R is even: a pair is in or out
-				w[q] = (src >= 0 && k < R) ? mp[kb * 16 + q] : make_float2(0.f, 0.f);
+				for (int q = 0; q < 4; ++q) {
+					const uint4 a = src >= 0 ? hp[q] : make_uint4(0u, 0u, 0u, 0u);
+					const uint4 b = src >= 0 && corr ? lp[q] : make_uint4(0u, 0u, 0u, 0u);
+					w[4 * q] = a.x; w[4 * q + 1] = a.y; w[4 * q + 2] = a.z; w[4 * q + 3] = a.w;
+					w[16 + 4 * q] = b.x; w[16 + 4 * q + 1] = b.y; w[16 + 4 * q + 2] = b.z; w[16 + 4 * q + 3] = b.w;
+				}
+			} else {
+				const float2* mp = reinterpret_cast<const float2*>(mult + (size_t)(src >= 0 ? src : 0) * R);
+#pragma unroll
+				for (int q = 0; q < 16; ++q) {
+					const int k = g * 32 + 2 * q;            // R is even: a pair is in or out
+					const float2 x = (src >= 0 && k < R) ? mp[g * 16 + q] : make_float2(0.f, 0.f);
+					w[2 * q] = __float_as_uint(x.x); w[2 * q + 1] = __float_as_uint(x.y);
+				}
 			}
 		};
 		// the high-degree columns accumulate over slots of different widths:
@@ -432,8 +498,8 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 		}
-		float2 nxt[16];
-		if (nact > 0) gather(0, active_kb[0] - 1, nxt);
+		uint32_t nxt[32];
+		if (nact > 0) gather(0, (active_kb[0] - 1) * UPB, nxt);
 		for (int j = 0; j < nact; ++j) {
 			const int slot = active[j];
 			int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
@@ -442,59 +508,84 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				dir = 0;
 			}
 			const int kbs = active_kb[j];
-			const uint32_t hi_bytes = (uint32_t)min(NC, 32 * kbs) * 128u;    // the slot's output columns
+			const uint32_t hi_bytes = (uint32_t)min(NC, C::EPB * kbs) * 128u;    // the slot's output columns
 			bool ok = true;
 			for (int kq = 0; kq < kbs; ++kq, ++it) {
 				const int kb = kbs - 1 - kq;                 // highest degrees first
 				const bool corr = kb < KBC;
 				const uint32_t st = it % NSTAGE;
-				float v[32];
-#pragma unroll
-				for (int q = 0; q < 16; ++q) { v[2 * q] = nxt[q].x; v[2 * q + 1] = nxt[q].y; }
-				if (kq + 1 < kbs) gather(j, kb - 1, nxt);
-				else if (j + 1 < nact) gather(j + 1, active_kb[j + 1] - 1, nxt);
-				// the TMEM stores below are warp-collective: the warp gives up as one
-				const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
-				if (!__all_sync(0xffffffffu, got)) {
-					ok = false;
-					break;
-				}
-				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 				uint8_t* stage = base + st * C::STAGE;
-				if (tid == 0) {
-					// the hi rows of the slot's output columns, and the lo rows
-					const uint8_t* blk = ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb);
-					mbar_expect_tx(smem_u32(&full_bar[st]), hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u));
-					bulk_g2s(smem_u32(stage), blk, hi_bytes, smem_u32(&full_bar[st]));
-					if (corr)
-						bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES, smem_u32(&full_bar[st]));
-				}
 				// lo (corrected K blocks only) to the stage's swizzled row tid;
 				// hi to TMEM columns [hi_col(st), +32) of lane tid (or to the row after lo's)
 				const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + C::hi_col(st);
 				uint8_t* rl = stage + C::HI_BYTES + C::LO_BYTES + tid * 128;
 				uint8_t* rh = rl + C::A_BYTES;
+				for (int u = 0; u < UPB; ++u) {
+					uint32_t v[32];
 #pragma unroll
-				for (int hf = 0; hf < 2; ++hf) {
-					uint32_t h[16], l[16];
-#pragma unroll
-					for (int e = 0; e < 16; ++e) {
-						const float x = v[16 * hf + e];
-						h[e] = tf32_rna(x);
-						l[e] = tf32_rna(x - __uint_as_float(h[e]));
+					for (int q = 0; q < 32; ++q) v[q] = nxt[q];
+					if (u + 1 < UPB) gather(j, kb * UPB + u + 1, nxt);
+					else if (kq + 1 < kbs) gather(j, (kb - 1) * UPB, nxt);
+					else if (j + 1 < nact) gather(j + 1, (active_kb[j + 1] - 1) * UPB, nxt);
+					if (u == 0) {
+						// the TMEM stores below are warp-collective: the warp gives up as one
+						const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
+						if (!__all_sync(0xffffffffu, got)) {
+							ok = false;
+							break;
+						}
+						asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+						if (tid == 0) {
+							// the hi rows of the slot's output columns, and the lo rows
+							const uint8_t* blk = ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb);
+							mbar_expect_tx(smem_u32(&full_bar[st]), hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u));
+							bulk_g2s(smem_u32(stage), blk, hi_bytes, smem_u32(&full_bar[st]));
+							if (corr)
+								bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES,
+								         smem_u32(&full_bar[st]));
+						}
 					}
-					if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * hf, h);
+					if constexpr (F16) {
+						// unit u: 16 words of FP16 pairs each, hi to TMEM columns [16 u, +16),
+						// lo to chunks [4 u, +4)
+						const uint32_t* h = v;
+						const uint32_t* l = v + 16;
+						if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * u, h);
 #pragma unroll
-					for (int c = 0; c < 4; ++c) {
-						const int pc = (4 * hf + c) ^ (tid & 7);
-						if (corr)
-							*reinterpret_cast<uint4*>(rl + pc * 16) =
-								make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
-						if constexpr (!C::HI_TMEM)
-							*reinterpret_cast<uint4*>(rh + pc * 16) =
-								make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+						for (int c = 0; c < 4; ++c) {
+							const int pc = (4 * u + c) ^ (tid & 7);
+							if (corr)
+								*reinterpret_cast<uint4*>(rl + pc * 16) =
+									make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
+							if constexpr (!C::HI_TMEM)
+								*reinterpret_cast<uint4*>(rh + pc * 16) =
+									make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+						}
+					} else {
+#pragma unroll
+						for (int hf = 0; hf < 2; ++hf) {
+							uint32_t h[16], l[16];
+#pragma unroll
+							for (int e = 0; e < 16; ++e) {
+								const float x = __uint_as_float(v[16 * hf + e]);
+								h[e] = tf32_rna(x);
+								l[e] = tf32_rna(x - __uint_as_float(h[e]));
+							}
+							if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * hf, h);
+#pragma unroll
+							for (int c = 0; c < 4; ++c) {
+								const int pc = (4 * hf + c) ^ (tid & 7);
+								if (corr)
+									*reinterpret_cast<uint4*>(rl + pc * 16) =
+										make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
+								if constexpr (!C::HI_TMEM)
+									*reinterpret_cast<uint4*>(rh + pc * 16) =
+										make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+							}
+						}
 					}
 				}
+				if (!ok) break;
 				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 				if constexpr (C::HI_TMEM) {
 					asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -521,38 +612,40 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				if (j > 0 && !mbar_wait(smem_u32(&tempty_bar), (j - 1) & 1u, abort)) { ok = false; break; }
 				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 				const int kbs = active_kb[j];
-				const int nq = min(NC, 32 * kbs) - NA;      // the slot's high-degree columns
-				const uint32_t idq = nq > 0 ? idesc_tf32(nq) : 0u;
+				const int nq = min(NC, C::EPB * kbs) - NA;  // the slot's high-degree columns
+				const uint32_t idq = nq > 0 ? idesc_of<F16>(nq) : 0u;
+				constexpr uint32_t IDA = idesc_of<F16>(NA);
 				for (int kq = 0; kq < kbs; ++kq, ++it) {
 					const int kb = kbs - 1 - kq;
+					const int k0 = 4 - C::ksteps(kb);           // the K steps past NC hold only padding
 					const uint32_t st = it % NSTAGE;
 					if (!mbar_wait(smem_u32(&full_bar[st]), (it / NSTAGE) & 1u, abort)) { ok = false; break; }
 					asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 					const uint32_t sb = smem_u32(base + st * C::STAGE);
 					const uint32_t op_hi = sb, op_lo = sb + C::HI_BYTES, a_lo = sb + C::HI_BYTES + C::LO_BYTES;
 					const uint32_t a_hi_t = tmem + C::hi_col(st), a_hi_s = a_lo + C::A_BYTES;
-#pragma unroll
-					for (int kk = 0; kk < 4; ++kk) {
+					for (int kk = k0; kk < 4; ++kk) {
 						const int ks = 3 - kk;
-						const uint32_t first = kq == 0 && kk == 0;          // first MMA of the slot
+						const uint32_t first = kq == 0 && kk == k0;         // first MMA of the slot
 						const uint64_t bh = desc_sw128(op_hi + ks * 32);
 						const uint64_t bq = desc_sw128(op_hi + NA * 128 + ks * 32);
 						if constexpr (C::HI_TMEM) {
 							const uint32_t ah = a_hi_t + 8u * ks;
-							mma_tf32_ta<NA>(tmem, ah, bh, !first);
-							if (nq > 0) mma_tf32_ta_n(tmem + C::Q_COL, ah, bq, idq, 1u);
+							mma_ta<F16>(tmem, ah, bh, IDA, !first);
+							if (nq > 0) mma_ta<F16>(tmem + C::Q_COL, ah, bq, idq, 1u);
 						} else {
 							const uint64_t ah = desc_sw128(a_hi_s + ks * 32);
-							mma_tf32<NA>(tmem, ah, bh, !first);
-							if (nq > 0) mma_tf32_n(tmem + C::Q_COL, ah, bq, idq, 1u);
+							mma_ss<F16>(tmem, ah, bh, IDA, !first);
+							if (nq > 0) mma_ss<F16>(tmem + C::Q_COL, ah, bq, idq, 1u);
 						}
 						if (kb < KBC) {
-							// the first correction of the tile: highest corrected block, ks = 3, slot 0
-							const uint32_t cfirst = j == 0 && kb == KBC - 1 && kk == 0;
+							// the first correction of the tile: highest corrected block, its
+							// first K step, slot 0
+							const uint32_t cfirst = j == 0 && kb == KBC - 1 && kk == k0;
 							const uint64_t bl = desc_sw128(op_lo + ks * 32), al = desc_sw128(a_lo + ks * 32);
-							if constexpr (C::HI_TMEM) mma_tf32_ta<NA>(tmem + C::C_COL, a_hi_t + 8u * ks, bl, !cfirst);
-							else mma_tf32<NA>(tmem + C::C_COL, desc_sw128(a_hi_s + ks * 32), bl, !cfirst);
-							mma_tf32<NA>(tmem + C::C_COL, al, bh, 1u);
+							if constexpr (C::HI_TMEM) mma_ta<F16>(tmem + C::C_COL, a_hi_t + 8u * ks, bl, IDA, !cfirst);
+							else mma_ss<F16>(tmem + C::C_COL, desc_sw128(a_hi_s + ks * 32), bl, IDA, !cfirst);
+							mma_ss<F16>(tmem + C::C_COL, al, bh, IDA, 1u);
 						}
 					}
 					mma_commit(smem_u32(&empty_bar[st]));
@@ -619,6 +712,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 				for (int c = 0; c < W; ++c)
 					if (c < lim) {
 						if (MODE == TC_L2L) o[c] += acc[c] + dg[c0 + c] * xs[c0 + c];
+						else if constexpr (F16) o[c] = acc[c] * out_scale;
 						else o[c] = acc[c];
 					}
 			}
@@ -641,6 +735,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 						for (int e = 0; e < 8; ++e)
 							if (c0 + c + e < R) {
 								if (MODE == TC_L2L) o[e] += v[e] + dg[c0 + c + e] * xs[c0 + c + e];
+								else if constexpr (F16) o[e] = v[e] * out_scale;
 								else o[e] = v[e];
 							}
 					}
@@ -696,6 +791,49 @@ __global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, 
 	if (kb < KBC && row < NA) out[blk + (size_t)NC * 32 + (size_t)row * 32 + in_row] = lo;
 }
 
+// The FP16 layout of the same: FP64 operators x scale -> per (direction, K
+// block of 64 inputs): the hi rows of every output column, then (K blocks
+// below KBC) the lo rows of the drained columns; FP16 pairs (the lower input
+// in the low half), 16-byte chunk c (8 inputs) of row r at c ^ (r & 7).  One
+// thread per (direction, K block, row, input pair).
+__global__ void build_tc16_ops_kernel(const double* __restrict__ ops64, int ndir, int NC, int NA, int R, int KB,
+                                      double scale, uint32_t* __restrict__ out)
+{
+	const size_t total = (size_t)ndir * KB * NC * 32;
+	const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= total) return;
+	const int jp = (int)(e % 32);
+	size_t rest = e / 32;
+	const int row = (int)(rest % NC); rest /= NC;
+	const int kb = (int)(rest % KB);
+	const int dir = (int)(rest / KB);
+	const int KBC = (NA + 63) / 64;
+	const int k = kb * 64 + 2 * jp;
+	const double* src = ops64 + ((size_t)dir * NC + row) * NC;
+	const double v0 = (row < R && k < R) ? src[k] * scale : 0.0;
+	const double v1 = (row < R && k + 1 < R) ? src[k + 1] * scale : 0.0;
+	const __half h0 = __float2half_rn((float)v0), h1 = __float2half_rn((float)v1);
+	const __half l0 = __float2half_rn((float)(v0 - (double)__half2float(h0)));
+	const __half l1 = __float2half_rn((float)(v1 - (double)__half2float(h1)));
+	const size_t dir_words = ((size_t)KB * NC + (size_t)KBC * NA) * 32;
+	const size_t blk = (size_t)dir * dir_words + ((size_t)kb * NC + (size_t)min(kb, KBC) * NA) * 32;
+	const size_t in_row = (size_t)(((jp >> 2) ^ (row & 7)) * 4) + (jp & 3);
+	out[blk + (size_t)row * 32 + in_row] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+	if (kb < KBC && row < NA)
+		out[blk + (size_t)NC * 32 + (size_t)row * 32 + in_row] =
+			(uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
+}
+
+// *out = max |x| over x[0, n) as the bits of a non-negative double (out zeroed before)
+__global__ void absmax64_kernel(const double* __restrict__ x, size_t n, unsigned long long* __restrict__ out)
+{
+	unsigned long long m = 0;
+	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+		m = max(m, (unsigned long long)__double_as_longlong(fabs(x[i])));
+	for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+	if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 // K blocks per far slot by |d|^2 for order N and KB K blocks: the offsets
 // with |d|^2 < 8 (|d| = 2, sqrt 5, sqrt 6: worst-case ratios 0.87 to 0.71)
 // keep every degree; the farther classes [8, 9], [10, 13], [14, 19], [20, 27]
@@ -704,24 +842,36 @@ __global__ void build_tc_ops_kernel(const double* __restrict__ ops64, int ndir, 
 // clustered set at N = 16: potential 3.31e-7 -> 3.27e-7, field 6.47e-7 ->
 // 6.44e-7 against the FP64 direct sum, M2L kernel 99.4 -> 73.4 ms; one
 // degree off the |d|^2 = 5, 6 class already raised the field to 6.99e-7.
-TcTrunc tc_trunc(int N, int KB)
+TcTrunc tc_trunc(int N, int KB, int EPB)
 {
 	TcTrunc t;
 	for (int d2 = 0; d2 < 28; ++d2) {
 		const int r = d2 < 8 ? 0 : d2 < 10 ? 3 : d2 < 14 ? 4 : d2 < 20 ? 5 : 6;
 		const int Nd = std::max(1, N - r);
-		t.kb[d2] = (uint8_t)std::min(KB, (Nd * (Nd + 1) + 31) / 32);
+		t.kb[d2] = (uint8_t)std::min(KB, (Nd * (Nd + 1) + EPB - 1) / EPB);
 	}
 	return t;
 }
 
+// *out = max |x| over x[0, n) as the bits of a positive float (out zeroed
+// before the launch): the FP16 M2L's multipole scale.
+__global__ void absmax_kernel(const float* __restrict__ x, size_t n, unsigned* __restrict__ out)
+{
+	unsigned m = 0;
+	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+		m = max(m, __float_as_uint(fabsf(x[i])));
+	for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+	if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 // persistent: about one block per SM taking items from the counter; else one
 // block per item (the hardware's block scheduler hands them out).
-template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L>
+template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L, bool F16 = false>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
-           bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0, bool persistent = true)
+           bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0, bool persistent = true,
+           const unsigned* bmax = nullptr, float t_inv = 1.f, const uint4* shi = nullptr, const uint4* slo = nullptr)
 {
-	using C = TcCfg<NC, NA, MODE != TC_L2L>;
+	using C = TcCfg<NC, NA, MODE != TC_L2L, F16>;
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	const unsigned total = tiles * (unsigned)S;
 	unsigned* work = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
@@ -731,15 +881,18 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 	timed = timed && ctx.timing && ctx.kev_used + 2 <= 32;
 	if (timed) LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used], ctx.stream));
 	const TcTrunc tr =
-		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB);
+		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB,
+		         C::EPB);
 	if (persistent)
-		m2l_tc_kernel<NC, NA, SLOTS, MODE, true><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, true, F16><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
-			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total);
+			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total, bmax, t_inv,
+			shi, slo);
 	else
-		m2l_tc_kernel<NC, NA, SLOTS, MODE, false><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, false, F16><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
-			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total);
+			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total, bmax, t_inv,
+			shi, slo);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
 		ctx.kev_used += 2;
@@ -761,21 +914,39 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 // {persistent, one block per item} with CUDA events and keeps the fastest
 // for the context (stored as S | 16 for persistent; the chosen pair runs
 // last, so the level's result always comes from it).
-template <int NC, int NA>
-int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int n_src)
+template <int NC, int NA, bool F16>
+int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int n_src,
+              float t_inv)
 {
-	using C = TcCfg<NC, NA>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, true>,
+	using C = TcCfg<NC, NA, true, F16>;
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, true, F16>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, false>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, false, F16>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+	unsigned* bmax = nullptr;
+	uint4 *shi = nullptr, *slo = nullptr;
+	if (F16) {
+		// the level's largest multipole magnitude (the sources' scale), then
+		// the sources split once into FP16 hi / lo rows
+		bmax = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
+		shi = static_cast<uint4*>(ctx.arena.take(plan.cells * (size_t)C::KB * 128));
+		slo = static_cast<uint4*>(ctx.arena.take(plan.cells * (size_t)C::KBC * 128));
+		if (!bmax || !shi || !slo) { ctx.last_error = "tensor-core M2L: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(ctx, cudaMemsetAsync(bmax, 0, sizeof(unsigned), ctx.stream));
+		const size_t n = plan.cells * (size_t)R;
+		absmax_kernel<<<(unsigned)std::min<size_t>(div_up(n, 256), 8 * (size_t)ctx.num_sms), 256, 0, ctx.stream>>>(
+			mult, n, bmax);
+		const size_t chunks = plan.cells * (size_t)C::KB * 8;
+		stage_f16_kernel<<<div_up(chunks, 256), 256, 0, ctx.stream>>>(mult, plan.cells, R, C::KB, C::KBC, bmax, shi,
+		                                                              slo);
+	}
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	int S = 1;
 	while (S < 8 && tiles * S < 2u * (unsigned)ctx.num_sms) S *= 2;
 	int bucket = 0;
 	while ((1u << bucket) < tiles && bucket < 32) ++bucket;
 	static_assert(NC / 16 < Context::SPLIT_ROWS, "autotuner table");
-	int& tuned = ctx.m2l_split[NC / 16][bucket];
+	int& tuned = ctx.m2l_split[F16 ? 1 : 0][NC / 16][bucket];
 	const bool tune = ctx.tune_m2l && tuned == 0;
 	bool pers = false;
 	if (ctx.tune_m2l && !tune) { S = tuned & 15; pers = (tuned & 16) != 0; }
@@ -800,8 +971,9 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		for (int mode = 0; mode < 2; ++mode)
 			for (int cand = 1; cand <= maxS; cand *= 2) {
 				LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-				int st = run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, cand, part, false, plan.cells, nullptr, n_src,
-				                        mode == 0);
+				int st = run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16>(ctx, plan, ops, mult, loc, R, cand, part, false,
+				                                                plan.cells, nullptr, n_src, mode == 0, bmax, t_inv,
+				                                                shi, slo);
 				if (st) return st;
 				LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
 				LFMM_CUDA(ctx, cudaEventSynchronize(e1));
@@ -815,7 +987,8 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		S = bestS;
 		pers = bestP;
 	}
-	return run_tc<NC, NA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr, n_src, pers);
+	return run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr,
+	                                              n_src, pers, bmax, t_inv, shi, slo);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
@@ -826,12 +999,12 @@ int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* op
 	using C = TcCfg<NC, NA>;
 	using CL = TcCfg<NC, NA, false>;
 	if (mode == TC_M2M) {
-		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M, false>,
+		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M, false, false>,
 		                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, nullptr, 0,
 		                                 false);
 	}
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L, false>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L, false, false>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
 	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + 8 * C::DIR_BYTES);
@@ -855,30 +1028,72 @@ int upload_slot_dirs(Context& ctx)
 
 } // namespace
 
-const uint4* m2l_ops_tc(Context& ctx, int N)
+const uint4* m2l_ops_tc(Context& ctx, int N, float* t_inv)
 {
+	const bool f16 = ctx.m2l_f16 != 0;
+	const int prec = f16 ? 4 : 3;
 	for (auto& e : ctx.opcache)
-		if (e.N == N && e.prec == 3) { e.stamp = ++ctx.opcache_clock; return static_cast<const uint4*>(e.ptr); }
+		if (e.N == N && e.prec == prec) {
+			e.stamp = ++ctx.opcache_clock;
+			if (t_inv) *t_inv = e.aux;
+			return static_cast<const uint4*>(e.ptr);
+		}
 	const double* d = m2l_ops_fp64(ctx, N, 1.0);
 	if (!d) return nullptr;
-	const int NC = m2l_padded(N), R = N * (N + 1), KB = m2l_tc_kblocks(N), NA = m2l_tc_drained(N);
-	const size_t bytes = tc_ops_bytes(343, N);
+	const int NC = m2l_padded(N), R = N * (N + 1), NA = m2l_tc_drained(N);
+	const int KB = f16 ? (NC + 63) / 64 : m2l_tc_kblocks(N);
 	OpCacheEntry e;
-	e.N = N; e.prec = 3; e.h = 1.0; e.bytes = bytes; e.stamp = ++ctx.opcache_clock;
+	e.N = N; e.prec = prec; e.h = 1.0; e.stamp = ++ctx.opcache_clock;
+	double scale = 1.0;
+	if (f16) {
+		// the largest operator magnitude scaled into [2^14, 2^15)
+		unsigned long long* mx = static_cast<unsigned long long*>(ctx.arena.take(sizeof(unsigned long long)));
+		if (!mx) { ctx.last_error = "tensor-core operators: allocation failed"; return nullptr; }
+		const size_t n = (size_t)343 * NC * NC;
+		unsigned long long hb = 0;
+		if (cudaMemsetAsync(mx, 0, sizeof(hb), ctx.stream) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+		absmax64_kernel<<<(unsigned)std::min<size_t>(div_up(n, 256), 8 * (size_t)ctx.num_sms), 256, 0, ctx.stream>>>(
+			d, n, mx);
+		if (cudaMemcpyAsync(&hb, mx, sizeof(hb), cudaMemcpyDeviceToHost, ctx.stream) != cudaSuccess ||
+		    cudaStreamSynchronize(ctx.stream) != cudaSuccess) {
+			cudaGetLastError();
+			ctx.last_error = "tensor-core operators: scale reduction failed";
+			return nullptr;
+		}
+		double m;
+		std::memcpy(&m, &hb, sizeof(m));
+		const int ex = m > 0.0 ? std::ilogb(m) : 0;
+		scale = std::ldexp(1.0, 14 - ex);
+		e.aux = (float)std::ldexp(1.0, ex - 14);
+	}
+	e.bytes = f16 ? tc16_ops_bytes(343, N) : tc_ops_bytes(343, N);
 	if (cudaMalloc(&e.ptr, e.bytes) != cudaSuccess) {
 		cudaGetLastError();
 		ctx.last_error = "tensor-core operators: out of memory";
 		return nullptr;
 	}
 	const size_t threads = (size_t)343 * KB * NC * 32;
-	build_tc_ops_kernel<<<div_up(threads, 256), 256, 0, ctx.stream>>>(d, 343, NC, NA, R, KB, static_cast<uint32_t*>(e.ptr));
+	if (f16)
+		build_tc16_ops_kernel<<<div_up(threads, 256), 256, 0, ctx.stream>>>(d, 343, NC, NA, R, KB, scale,
+		                                                                    static_cast<uint32_t*>(e.ptr));
+	else
+		build_tc_ops_kernel<<<div_up(threads, 256), 256, 0, ctx.stream>>>(d, 343, NC, NA, R, KB,
+		                                                                  static_cast<uint32_t*>(e.ptr));
 	if (cudaGetLastError() != cudaSuccess) {
 		cudaFree(e.ptr);
 		ctx.last_error = "tensor-core operators: launch failed";
 		return nullptr;
 	}
 	ctx.opcache.push_back(e);
+	if (t_inv) *t_inv = e.aux;
 	return static_cast<const uint4*>(e.ptr);
+}
+
+size_t tc16_ops_bytes(int ndir, int N)
+{
+	const int NC = m2l_padded(N), NA = m2l_tc_drained(N);
+	const size_t KB = (size_t)(NC + 63) / 64, KBC = (size_t)(NA + 63) / 64;
+	return (size_t)ndir * (KB * NC + KBC * NA) * 128;
 }
 
 size_t tc_ops_bytes(int ndir, int N)
@@ -914,12 +1129,16 @@ int shift_gemm_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* ops,
 	return ERR_UNSUPPORTED;
 }
 
-int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N, int n_src)
+int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N, int n_src,
+                float t_inv)
 {
 	if (int st = upload_slot_dirs(ctx)) return st;
 	const int R = N * (N + 1), NC = m2l_padded(N), NA = m2l_tc_drained(N);
 	const int ns = n_src > 0 && n_src < N ? n_src : 0;
-#define LFMM_TC_M2L(nc, na) if (NC == nc && NA == na) return launch_tc<nc, na>(ctx, plan, ops, mult, loc, R, ns);
+#define LFMM_TC_M2L(nc, na)                                                                                   \
+	if (NC == nc && NA == na)                                                                                 \
+		return ctx.m2l_f16 ? launch_tc<nc, na, true>(ctx, plan, ops, mult, loc, R, ns, t_inv)                 \
+		                   : launch_tc<nc, na, false>(ctx, plan, ops, mult, loc, R, ns, 1.f);
 	LFMM_TC_ORDERS(LFMM_TC_M2L)
 #undef LFMM_TC_M2L
 	ctx.last_error = "tensor-core M2L: unsupported order";

@@ -1,5 +1,5 @@
 // tcgen05 (5th-generation tensor core) form of the direction-grouped M2L
-// GEMM for the FP32 levels, TF32 with a hi + lo split of both operands:
+// GEMM for the FP32 levels, FP16 (or TF32) with a hi + lo split of both operands:
 //   D = B T^T ~= B_hi T_hi + (B_hi T_lo + B_lo T_hi)
 // with D[targets][output coefficients], B the gathered source multipoles and
 // T the offset's operator.  The three products of each far slot are summed
@@ -30,15 +30,19 @@ inline int m2l_tc_drained(int N) { return m2l_padded(N) <= 160 ? m2l_padded(N) :
 // columns' source degrees, the lo rows of the m2l_tc_drained(N) drained
 // columns; rows of 128 bytes, 128-byte swizzled (16-byte chunk c of row r
 // stored at chunk c ^ (r & 7)); built from the FP64 scaled operators, cached
-// per context.
-const uint4* m2l_ops_tc(Context& ctx, int N);
+// per context.  The context's operand type (Context::m2l_f16): TF32 pairs,
+// K blocks of 32 inputs, or FP16 pairs of the operators scaled by a power of
+// two (*t_inv: its inverse), K blocks of 64 inputs.
+const uint4* m2l_ops_tc(Context& ctx, int N, float* t_inv = nullptr);
+size_t tc16_ops_bytes(int ndir, int N);
 
 // loc = sum over slots of T_dir mult[src] for every cell of the level (FP32).
 // n_src in (0, N): the level's M2L order, the degrees of the sources it uses
 // (the nearest offsets use n_src degrees, the farther ones the truncation
-// rule's fewer, never below the corrected K blocks); 0: N.
+// rule's fewer, never below the corrected K blocks); 0: N.  ops and t_inv from
+// m2l_ops_tc (the context's operand type).
 int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int N,
-                int n_src = 0);
+                int n_src = 0, float t_inv = 1.f);
 
 // The same engine for the level-to-level shifts, whose scaled operators are
 // one per child octant:

@@ -1,7 +1,8 @@
-"""tcgen05 engine (TF32 hi/lo split, per-slot FP32 flush; the default for the
-mixed form's M2L, M2M and L2L) against the SIMT FP32 engine (SIMT GEMM M2L,
-rotation M2M / L2L) and the FP64 form.  Both mixed engines must stay within
-the mixed form's 1e-6 of the FP64 form (measured: 3-5e-7 for the tensor-core
+"""tcgen05 engine (hi/lo split, per-slot FP32 flush; the default for the
+mixed form's M2L, M2M and L2L: FP16 operands for the M2L, TF32 for the
+shifts) against the SIMT FP32 engine (SIMT GEMM M2L, rotation M2M / L2L), the
+TF32-operand M2L and the FP64 form.  The mixed engines must stay within the
+mixed form's 1e-6 of the FP64 form (measured: 3-5e-7 for the tensor-core
 engine; 1.1e-6 before L2L's diagonal moved out of the TF32 operators)."""
 import os
 
@@ -14,12 +15,12 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def engine_context(name):
-    os.environ["LFMM_M2L"] = name
+def engine_context(name, var="LFMM_M2L"):
+    os.environ[var] = name
     try:
         return Context(0)
     finally:
-        del os.environ["LFMM_M2L"]
+        del os.environ[var]
 
 
 @pytest.fixture(scope="module")
@@ -36,8 +37,37 @@ def simt():
     c.close()
 
 
+@pytest.fixture(scope="module")
+def tf32():
+    c = engine_context("tf32", "LFMM_M2L_TYPE")
+    yield c
+    c.close()
+
+
 def noself(p, q):
     return p - q * 1e4
+
+
+@pytest.mark.parametrize("N,depth,gen", [(16, 10, "plummer"), (17, 10, "plummer"), (12, 6, "uniform"),
+                                         (15, 6, "uniform")])
+def test_f16_and_tf32_operands_agree(tc, tf32, ctx, N, depth, gen):
+    """The FP16 hi/lo M2L (operators and each level's multipoles scaled by
+    powers of two into FP16's range, sources split once per level) against the
+    TF32 hi/lo M2L: the same 22-bit operand splits, so both land equally close
+    to the FP64 form and within a few 1e-7 of each other."""
+    src, q = (plummer_mix3d if gen == "plummer" else uniform3d)(300000, seed=70 + N)
+    kw = dict(N=N, tree_depth=depth, precision="mixed")
+    if gen == "plummer":
+        kw["max_leaf"] = 64
+    a = FastMultipole3d((src, q), ctx=tc, **kw)
+    b = FastMultipole3d((src, q), ctx=tf32, **kw)
+    c = FastMultipole3d((src, q), ctx=ctx, **{k: v for k, v in kw.items() if k != "precision"})
+    ea = rel_l2(noself(a.potentials, q), noself(c.potentials, q))
+    eb = rel_l2(noself(b.potentials, q), noself(c.potentials, q))
+    fa, fb = rel_l2(a.forces, c.forces), rel_l2(b.forces, c.forces)
+    assert ea < TOL and fa < TOL
+    assert ea < 1.3 * eb + 1e-8 and fa < 1.3 * fb + 1e-8
+    assert rel_l2(noself(a.potentials, q), noself(b.potentials, q)) < 5e-7
 
 
 @pytest.mark.parametrize("N", [13, 9, 7, 11, 14, 15, 16])
