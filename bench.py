@@ -553,28 +553,36 @@ def m2l_flops(N):
     return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
 
 
-# DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode), from an ncu
-# capture of a 2,097,152-particle case of the default workload at N = 16
-# (788.5 MB read + written over 4.365 ms in 4 launches); the kernel's traffic
-# grows with its work, so a full launch's traffic is this rate times its
-# duration.
-M2L_TC_DRAM_BYTES_PER_MS = 788.5e6 / 4.365
+# DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode, FP16 operands),
+# from an ncu capture of a 2,097,152-particle case of the default workload at
+# N = 17 (185.6 MB read + 71.9 MB written in one 1.572 ms launch); the
+# kernel's traffic grows with its work, so a full launch's traffic is this
+# rate times its duration.
+M2L_TC_DRAM_BYTES_PER_MS = (185.6e6 + 71.9e6) / 1.572
 
 
 def padded(N):
     return (N * (N + 1) + 15) // 16 * 16
 
 
-def tc_executed_per_pair(N):
+def tc_executed_per_pair(N, epb=64):
     """Tensor flops the tcgen05 M2L executes per V pair, averaged over the 189
-    far offsets of an octant class: B_hi T_hi over the slot's K blocks and
-    output columns, plus the two hi/lo corrections over the drained columns
-    (degrees < 12) and their K blocks; a slot of |d|^2 >= 8 is truncated by 3,
-    4, 5, 6 degrees for |d|^2 in [8, 9], [10, 13], [14, 19], [20, 27], never
-    below the drained columns (csrc/m2l_tc.cu, tc_trunc)."""
+    far offsets of an octant class: B_hi T_hi over the slot's K blocks (epb
+    inputs each: 64 for FP16 operands, 32 for TF32; a partial last block runs
+    only its K steps below the padded row count) and output columns, plus the
+    two hi/lo corrections over the drained columns (degrees < 12) and their K
+    blocks; a slot of |d|^2 >= 8 is truncated by 3, 4, 5, 6 degrees for |d|^2
+    in [8, 9], [10, 13], [14, 19], [20, 27], never below the drained columns
+    (csrc/m2l_tc.cu, tc_trunc)."""
     nc = padded(N)
     na = nc if nc <= 160 else 160
-    kb_all, kbc = (nc + 31) // 32, (na + 31) // 32
+    kb_all, kbc = (nc + epb - 1) // epb, (na + epb - 1) // epb
+    step = epb // 4
+
+    def k_in(b):
+        left = nc - b * epb
+        return epb if left >= epb else (left + step - 1) // step * step
+
     tot = 0.0
     offs = [(x, y, z) for x in range(-2, 4) for y in range(-2, 4) for z in range(-2, 4)
             if max(abs(x), abs(y), abs(z)) > 1]
@@ -582,9 +590,9 @@ def tc_executed_per_pair(N):
         d2 = x * x + y * y + z * z
         r = 0 if d2 < 8 else 3 if d2 < 10 else 4 if d2 < 14 else 5 if d2 < 20 else 6
         nd = max(1, N - r)
-        kb = max(kbc, min(kb_all, (nd * (nd + 1) + 31) // 32))
-        cols = min(nc, 32 * kb)
-        tot += 2.0 * cols * 32 * kb + 2 * 2.0 * na * 32 * kbc
+        kb = max(kbc, min(kb_all, (nd * (nd + 1) + epb - 1) // epb))
+        cols = min(nc, epb * kb)
+        tot += sum(2.0 * cols * k_in(b) for b in range(kb)) + sum(2 * 2.0 * na * k_in(b) for b in range(kbc))
     return tot / len(offs)
 
 
@@ -624,14 +632,13 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
         tensor = tc_executed_per_pair(N) * stats["n_far_pairs"]
         achieved = flops / (ms * 1e-3) / 1e12
         bf16 = peaks["bf16_tflops"]
-        return {"kernel": "m2l_tc_kernel (tcgen05 TF32 hi/lo, direction-grouped)", "bound": "tensor",
+        return {"kernel": "m2l_tc_kernel (tcgen05 FP16 hi/lo, direction-grouped)", "bound": "tensor",
                 "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-                "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({peaks['source']}); the kernel runs TF32 MMAs, "
-                               "whose dense rate is half of bf16's: frac_tf32 uses the TF32 cuBLAS GEMM peak "
-                               "measured in this run",
-                "frac_tf32": achieved / tf32_tflops, "tf32_peak": tf32_tflops, "algorithmic_flops": flops,
+                "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({peaks['source']}); the kernel runs FP16 MMAs, "
+                               "whose dense rate is bf16's",
+                "algorithmic_flops": flops,
                 "executed_tensor_flops": tensor, "executed_tensor_tflops": tensor / (ms * 1e-3) / 1e12,
-                "executed_frac_tf32": tensor / (ms * 1e-3) / 1e12 / tf32_tflops,
+                "executed_frac": tensor / (ms * 1e-3) / 1e12 / bf16,
                 "kernel_ms": ms, "kernel_launches": stats["n_m2l_kernel"], "phase_ms": phases["m2l"],
                 "traffic": M2L_TC_DRAM_BYTES_PER_MS * ms / stats["n_m2l_kernel"],
                 "traffic_unit": "bytes per launch (ncu capture of a 2M-particle case, scaled by kernel time)"}
