@@ -362,10 +362,12 @@ int lfmm_create(lfmm_ctx** out, const lfmm_options* opt)
 	// M2L engine (LFMM_M2L): tc (default) = tcgen05 hi/lo GEMMs on the FP32
 	// levels and SIMT GEMMs elsewhere; simt = SIMT GEMMs only; rotation =
 	// per-pair rotations on the plain path.  LFMM_M2L_TYPE: f16 (default) or
-	// tf32, the tcgen05 M2L's operand type.
+	// tf32, the tcgen05 M2L's operand type; LFMM_M2L_GATHER: tma (default) or
+	// ldg, how the FP16 form's producers bring the sources in.
 	c.m2l_engine = 3;
 	if (const char* e = std::getenv("LFMM_M2L_TUNE")) c.tune_m2l = std::strcmp(e, "0") != 0;
 	if (const char* e = std::getenv("LFMM_M2L_TYPE")) c.m2l_f16 = std::strcmp(e, "tf32") != 0;
+	if (const char* e = std::getenv("LFMM_M2L_GATHER")) c.m2l_tma = std::strcmp(e, "ldg") != 0;
 	if (const char* e = std::getenv("LFMM_M2L"))
 		c.m2l_engine = std::strcmp(e, "rotation") == 0 ? 1 : (std::strcmp(e, "simt") == 0 ? 0 : 3);
 	int ndev = 0;

@@ -106,11 +106,14 @@ struct Context {
 	// tcgen05 M2L operands: FP16 hi / lo pairs (1, the default) or TF32 hi / lo
 	// pairs (0; LFMM_M2L_TYPE=tf32)
 	int m2l_f16 = 1;
-	// M2L autotuner: slot split chosen per (operand type, operator rows / 16,
+	// FP16 M2L sources gathered by TMA row gathers (1, the default) or by the
+	// producers' loads (0; LFMM_M2L_GATHER=ldg)
+	int m2l_tma = 1;
+	// M2L autotuner: slot split chosen per (operand type and gather, operator rows / 16,
 	// level-size bucket); 0 = not tuned yet.  tune_m2l = 0 (LFMM_M2L_TUNE=0):
 	// the fixed rule.  Operator rows reach 352 (N = 18): 23 row classes.
 	static constexpr int SPLIT_ROWS = 352 / 16 + 1;
-	int m2l_split[2][SPLIT_ROWS][33] = {};
+	int m2l_split[3][SPLIT_ROWS][33] = {};
 	int tune_m2l = 1;
 	int timing = 0;
 };

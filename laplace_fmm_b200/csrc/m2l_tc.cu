@@ -21,6 +21,8 @@
 // DEV_ERR_TIMEOUT, waits (bounded) for its copies and MMAs in flight, frees
 // TMEM and returns.
 #include "m2l_tc.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include "fmm3d.cuh"
 #include <mutex>
@@ -134,6 +136,23 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 	return false;
 }
 
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+
+// Rows y0..y3 of a 2D tensor map (box: one row of 64 FP16 = 128 bytes, 128-byte
+// swizzle) from column x into 4 consecutive 128-byte rows at dst.
+__device__ __forceinline__ void gather4_g2s(uint32_t dst, const CUtensorMap* map, int x, int y0, int y1, int y2, int y3,
+                                            uint32_t bar)
+{
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+	             " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+	             :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3),
+	                "r"(bar)
+	             : "memory");
+}
+
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
 {
 	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -240,8 +259,9 @@ struct TcCfg {
 	static constexpr uint32_t Q_COL = NA, C_COL = NC;
 	static constexpr int FREE = (int)TMEM_COLS - NC - NA;
 	static constexpr bool HI_TMEM = TMEM_HI && FREE >= 64; // B_hi in TMEM (else in shared memory)
-	static constexpr int NSTAGE = HI_TMEM ? (FREE / 32 < NSTAGE_MAX ? FREE / 32 : NSTAGE_MAX) : 2;
 	static constexpr int STAGE = HI_BYTES + LO_BYTES + (HI_TMEM ? 1 : 2) * A_BYTES;
+	static constexpr int NSTAGE = HI_TMEM ? (FREE / 32 < NSTAGE_MAX ? FREE / 32 : NSTAGE_MAX)
+	                                      : ((227 * 1024 - 1024) / STAGE >= 3 ? 3 : 2);
 	static constexpr int HALF = NA / 2;                 // drained columns per epilogue warp
 	static constexpr int HQ = (NC - NA) / 2;            // high-degree columns per epilogue warp
 	static constexpr int SMEM = NSTAGE * STAGE + 1024;
@@ -334,17 +354,23 @@ __global__ void stage_f16_kernel(const float* __restrict__ mult, size_t cells, i
 // [2^14, 2^15), as FP16 hi / lo rows of KB (lo: KBC) blocks of 64; the
 // results are scaled by 2^-e t_inv (t_inv: the inverse of the operators'
 // scale); both exact.
-template <int NC, int NA, int SLOTS, int MODE, bool PERSIST, bool F16>
+// TMA (with F16): the producers gather the staged rows with tile::gather4
+// (tm_hi / tm_lo: the staged hi / lo arrays, one row per source cell and a
+// zero row zero_row for targets without a source in the slot) straight into
+// the stage's swizzled A rows; the MMAs read both A parts from shared memory.
+template <int NC, int NA, int SLOTS, int MODE, bool PERSIST, bool F16, bool TMA>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, float* __restrict__ loc,
               const int32_t* __restrict__ vtab, const int32_t* __restrict__ order,
               const uint32_t* __restrict__ oct_count, int R, float* __restrict__ part, size_t cells,
               const float* __restrict__ diag, unsigned* flags, const TcTrunc trunc, size_t src_cells, int ndir,
               unsigned* __restrict__ work, int S, unsigned total, const unsigned* __restrict__ bmax, float t_inv,
-              const uint4* __restrict__ shi, const uint4* __restrict__ slo)
+              const uint4* __restrict__ shi, const uint4* __restrict__ slo,
+              const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, int zero_row)
 {
 	static_assert(!F16 || MODE == TC_M2L, "FP16 operands: M2L only");
-	using C = TcCfg<NC, NA, MODE != TC_L2L, F16>;
+	static_assert(!TMA || F16, "TMA row gathers: FP16 staged sources only");
+	using C = TcCfg<NC, NA, MODE != TC_L2L && !TMA, F16>;
 	constexpr int UPB = C::UPB;
 	extern __shared__ uint8_t dsm[];
 	constexpr int NSTAGE = C::NSTAGE;
@@ -413,7 +439,7 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 	if (tid < TC_M) tgt[tid] = tid < s_n ? order[s_start + tid] : -1;
 	if (tid == 0) {
 		for (int s = 0; s < NSTAGE; ++s) {
-			mbar_init(smem_u32(&full_bar[s]), TC_M);
+			mbar_init(smem_u32(&full_bar[s]), TMA ? 4 : TC_M);    // TMA: one arrival per producer warp
 			mbar_init(smem_u32(&empty_bar[s]), 1);
 		}
 		mbar_init(smem_u32(&tfull_bar), 1);
@@ -498,83 +524,122 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 			asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 		}
-		uint32_t nxt[32];
-		if (nact > 0) gather(0, (active_kb[0] - 1) * UPB, nxt);
-		for (int j = 0; j < nact; ++j) {
-			const int slot = active[j];
-			int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
-			if (dir < 0 || dir >= ndir) {                   // an operator outside the set: reported
-				if (tid == 0) atomicOr(flags, DEV_ERR_RANGE);
-				dir = 0;
-			}
-			const int kbs = active_kb[j];
-			const uint32_t hi_bytes = (uint32_t)min(NC, C::EPB * kbs) * 128u;    // the slot's output columns
-			bool ok = true;
-			for (int kq = 0; kq < kbs; ++kq, ++it) {
-				const int kb = kbs - 1 - kq;                 // highest degrees first
-				const bool corr = kb < KBC;
-				const uint32_t st = it % NSTAGE;
-				uint8_t* stage = base + st * C::STAGE;
-				// lo (corrected K blocks only) to the stage's swizzled row tid;
-				// hi to TMEM columns [hi_col(st), +32) of lane tid (or to the row after lo's)
-				const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + C::hi_col(st);
-				uint8_t* rl = stage + C::HI_BYTES + C::LO_BYTES + tid * 128;
-				uint8_t* rh = rl + C::A_BYTES;
-				for (int u = 0; u < UPB; ++u) {
-					uint32_t v[32];
-#pragma unroll
-					for (int q = 0; q < 32; ++q) v[q] = nxt[q];
-					if (u + 1 < UPB) gather(j, kb * UPB + u + 1, nxt);
-					else if (kq + 1 < kbs) gather(j, (kb - 1) * UPB, nxt);
-					else if (j + 1 < nact) gather(j + 1, (active_kb[j + 1] - 1) * UPB, nxt);
-					if (u == 0) {
-						// the TMEM stores below are warp-collective: the warp gives up as one
-						const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
-						if (!__all_sync(0xffffffffu, got)) {
-							ok = false;
-							break;
-						}
-						asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-						if (tid == 0) {
-							// the hi rows of the slot's output columns, and the lo rows
+		if constexpr (TMA) {
+			// per slot each lane finds its row's source cell (or the zero row);
+			// per K block lane 0 arrives with the warp's byte count (warp 0:
+			// and the operator's) and lanes 0-7 gather the warp's 32 rows, four
+			// per tile::gather4, hi (and lo in corrected blocks)
+			for (int j = 0; j < nact; ++j) {
+				const int slot = active[j];
+				int dir = c_tc_slot_dir[oct][slot];
+				if (dir < 0 || dir >= ndir) {               // an operator outside the set: reported
+					if (tid == 0) atomicOr(flags, DEV_ERR_RANGE);
+					dir = 0;
+				}
+				int src = myt >= 0 ? vtab[(size_t)myt * SLOTS + slot] : -1;
+				if (src >= 0 && (size_t)src >= src_cells) {  // a source outside the level: skipped, reported
+					atomicOr(flags, DEV_ERR_RANGE);
+					src = -1;
+				}
+				const int y = src >= 0 ? src : zero_row;
+				const int l4 = (4 * lane) & 31;
+				const int y0 = __shfl_sync(0xffffffffu, y, l4), y1 = __shfl_sync(0xffffffffu, y, l4 + 1);
+				const int y2 = __shfl_sync(0xffffffffu, y, l4 + 2), y3 = __shfl_sync(0xffffffffu, y, l4 + 3);
+				const int kbs = active_kb[j];
+				const uint32_t hi_bytes = (uint32_t)min(NC, C::EPB * kbs) * 128u;
+				bool ok = true;
+				for (int kq = 0; kq < kbs; ++kq, ++it) {
+					const int kb = kbs - 1 - kq;
+					const bool corr = kb < KBC;
+					const uint32_t st = it % NSTAGE;
+					uint8_t* stage = base + st * C::STAGE;
+					const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
+					if (!__all_sync(0xffffffffu, got)) {
+						ok = false;
+						break;
+					}
+					const uint32_t fb = smem_u32(&full_bar[st]);
+					if (lane == 0) {
+						uint32_t bytes = 32u * 128u * (corr ? 2u : 1u);
+						if (warp == 0) bytes += hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u);
+						mbar_arrive_expect_tx(fb, bytes);
+						if (warp == 0) {
 							const uint8_t* blk = ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb);
-							mbar_expect_tx(smem_u32(&full_bar[st]), hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u));
-							bulk_g2s(smem_u32(stage), blk, hi_bytes, smem_u32(&full_bar[st]));
-							if (corr)
-								bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES,
-								         smem_u32(&full_bar[st]));
+							bulk_g2s(smem_u32(stage), blk, hi_bytes, fb);
+							if (corr) bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES, fb);
 						}
 					}
-					if constexpr (F16) {
-						// unit u: 16 words of FP16 pairs each, hi to TMEM columns [16 u, +16),
-						// lo to chunks [4 u, +4)
-						const uint32_t* h = v;
-						const uint32_t* l = v + 16;
-						if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * u, h);
-#pragma unroll
-						for (int c = 0; c < 4; ++c) {
-							const int pc = (4 * u + c) ^ (tid & 7);
-							if (corr)
-								*reinterpret_cast<uint4*>(rl + pc * 16) =
-									make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
-							if constexpr (!C::HI_TMEM)
-								*reinterpret_cast<uint4*>(rh + pc * 16) =
-									make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
-						}
-					} else {
-#pragma unroll
-						for (int hf = 0; hf < 2; ++hf) {
-							uint32_t h[16], l[16];
-#pragma unroll
-							for (int e = 0; e < 16; ++e) {
-								const float x = __uint_as_float(v[16 * hf + e]);
-								h[e] = tf32_rna(x);
-								l[e] = tf32_rna(x - __uint_as_float(h[e]));
+					__syncwarp();
+					if (lane < 8) {
+						const uint32_t row = (uint32_t)(32 * warp + 4 * lane) * 128u;
+						uint8_t* a_lo = stage + C::HI_BYTES + C::LO_BYTES;
+						gather4_g2s(smem_u32(a_lo + C::A_BYTES) + row, &tm_hi, kb * C::EPB, y0, y1, y2, y3, fb);
+						if (corr) gather4_g2s(smem_u32(a_lo) + row, &tm_lo, kb * C::EPB, y0, y1, y2, y3, fb);
+					}
+				}
+				if (!ok) {
+					*abort = 1;
+					atomicOr(flags, DEV_ERR_TIMEOUT);
+					break;
+				}
+			}
+		} else {
+			uint32_t nxt[32];
+			if (nact > 0) gather(0, (active_kb[0] - 1) * UPB, nxt);
+			for (int j = 0; j < nact; ++j) {
+				const int slot = active[j];
+				int dir = MODE == TC_M2L ? c_tc_slot_dir[oct][slot] : MODE == TC_M2M ? slot : oct;
+				if (dir < 0 || dir >= ndir) {                   // an operator outside the set: reported
+					if (tid == 0) atomicOr(flags, DEV_ERR_RANGE);
+					dir = 0;
+				}
+				const int kbs = active_kb[j];
+				const uint32_t hi_bytes = (uint32_t)min(NC, C::EPB * kbs) * 128u;    // the slot's output columns
+				bool ok = true;
+				for (int kq = 0; kq < kbs; ++kq, ++it) {
+					const int kb = kbs - 1 - kq;                 // highest degrees first
+					const bool corr = kb < KBC;
+					const uint32_t st = it % NSTAGE;
+					uint8_t* stage = base + st * C::STAGE;
+					// lo (corrected K blocks only) to the stage's swizzled row tid;
+					// hi to TMEM columns [hi_col(st), +32) of lane tid (or to the row after lo's)
+					const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + C::hi_col(st);
+					uint8_t* rl = stage + C::HI_BYTES + C::LO_BYTES + tid * 128;
+					uint8_t* rh = rl + C::A_BYTES;
+					for (int u = 0; u < UPB; ++u) {
+						uint32_t v[32];
+	#pragma unroll
+						for (int q = 0; q < 32; ++q) v[q] = nxt[q];
+						if (u + 1 < UPB) gather(j, kb * UPB + u + 1, nxt);
+						else if (kq + 1 < kbs) gather(j, (kb - 1) * UPB, nxt);
+						else if (j + 1 < nact) gather(j + 1, (active_kb[j + 1] - 1) * UPB, nxt);
+						if (u == 0) {
+							// the TMEM stores below are warp-collective: the warp gives up as one
+							const bool got = it < NSTAGE || mbar_wait(smem_u32(&empty_bar[st]), ((it / NSTAGE) - 1) & 1u, abort);
+							if (!__all_sync(0xffffffffu, got)) {
+								ok = false;
+								break;
 							}
-							if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * hf, h);
-#pragma unroll
+							asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+							if (tid == 0) {
+								// the hi rows of the slot's output columns, and the lo rows
+								const uint8_t* blk = ops + (size_t)dir * C::DIR_BYTES + C::op_off(kb);
+								mbar_expect_tx(smem_u32(&full_bar[st]), hi_bytes + (corr ? (uint32_t)C::LO_BYTES : 0u));
+								bulk_g2s(smem_u32(stage), blk, hi_bytes, smem_u32(&full_bar[st]));
+								if (corr)
+									bulk_g2s(smem_u32(stage + C::HI_BYTES), blk + C::HI_BYTES, C::LO_BYTES,
+									         smem_u32(&full_bar[st]));
+							}
+						}
+						if constexpr (F16) {
+							// unit u: 16 words of FP16 pairs each, hi to TMEM columns [16 u, +16),
+							// lo to chunks [4 u, +4)
+							const uint32_t* h = v;
+							const uint32_t* l = v + 16;
+							if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * u, h);
+	#pragma unroll
 							for (int c = 0; c < 4; ++c) {
-								const int pc = (4 * hf + c) ^ (tid & 7);
+								const int pc = (4 * u + c) ^ (tid & 7);
 								if (corr)
 									*reinterpret_cast<uint4*>(rl + pc * 16) =
 										make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
@@ -582,21 +647,43 @@ m2l_tc_kernel(const uint8_t* __restrict__ ops, const float* __restrict__ mult, f
 									*reinterpret_cast<uint4*>(rh + pc * 16) =
 										make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
 							}
+						} else {
+	#pragma unroll
+							for (int hf = 0; hf < 2; ++hf) {
+								uint32_t h[16], l[16];
+	#pragma unroll
+								for (int e = 0; e < 16; ++e) {
+									const float x = __uint_as_float(v[16 * hf + e]);
+									h[e] = tf32_rna(x);
+									l[e] = tf32_rna(x - __uint_as_float(h[e]));
+								}
+								if constexpr (C::HI_TMEM) tmem_st16(ta + 16u * hf, h);
+	#pragma unroll
+								for (int c = 0; c < 4; ++c) {
+									const int pc = (4 * hf + c) ^ (tid & 7);
+									if (corr)
+										*reinterpret_cast<uint4*>(rl + pc * 16) =
+											make_uint4(l[4 * c], l[4 * c + 1], l[4 * c + 2], l[4 * c + 3]);
+									if constexpr (!C::HI_TMEM)
+										*reinterpret_cast<uint4*>(rh + pc * 16) =
+											make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+								}
+							}
 						}
 					}
+					if (!ok) break;
+					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+					if constexpr (C::HI_TMEM) {
+						asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+						asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+					}
+					mbar_arrive(smem_u32(&full_bar[st]));
 				}
-				if (!ok) break;
-				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-				if constexpr (C::HI_TMEM) {
-					asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-					asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+				if (!ok) {
+					*abort = 1;
+					atomicOr(flags, DEV_ERR_TIMEOUT);
+					break;
 				}
-				mbar_arrive(smem_u32(&full_bar[st]));
-			}
-			if (!ok) {
-				*abort = 1;
-				atomicOr(flags, DEV_ERR_TIMEOUT);
-				break;
 			}
 		}
 		// the operator copies still in flight land before the block exits
@@ -864,14 +951,48 @@ __global__ void absmax_kernel(const float* __restrict__ x, size_t n, unsigned* _
 	if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+// A 2D tensor map over rows of cols FP16 values (row pitch cols * 2 bytes),
+// read one row of 64 values (128 bytes, 128-byte swizzle) at a time: the
+// staged sources for the TMA row gathers.  cuTensorMapEncodeTiled comes from
+// the driver through the runtime's entry-point query.
+int row_map(Context& ctx, CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows)
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void* fn = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+		        cudaSuccess && q == cudaDriverEntryPointSuccess)
+			encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+		else
+			cudaGetLastError();
+	});
+	if (!encode) { ctx.last_error = "tensor-core M2L: cuTensorMapEncodeTiled unavailable"; return ERR_CUDA; }
+	const cuuint64_t dims[2] = {cols, rows};
+	const cuuint64_t strides[1] = {cols * 2};
+	const cuuint32_t box[2] = {64, 1};
+	const cuuint32_t estr[2] = {1, 1};
+	const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+	                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+	                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS) { ctx.last_error = "tensor-core M2L: tensor map encoding failed"; return ERR_CUDA; }
+	return OK;
+}
+
 // persistent: about one block per SM taking items from the counter; else one
 // block per item (the hardware's block scheduler hands them out).
-template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L, bool F16 = false>
+template <int NC, int NA, int SLOTS = M2L_SLOTS, int MODE = TC_M2L, bool F16 = false, bool TMA = false>
 int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int S, float* part,
            bool timed, size_t src_cells, const float* diag = nullptr, int n_src = 0, bool persistent = true,
-           const unsigned* bmax = nullptr, float t_inv = 1.f, const uint4* shi = nullptr, const uint4* slo = nullptr)
+           const unsigned* bmax = nullptr, float t_inv = 1.f, const uint4* shi = nullptr, const uint4* slo = nullptr,
+           const CUtensorMap* maps = nullptr)
 {
-	using C = TcCfg<NC, NA, MODE != TC_L2L, F16>;
+	using C = TcCfg<NC, NA, MODE != TC_L2L && !TMA, F16>;
+	CUtensorMap m_hi, m_lo;
+	std::memset(&m_hi, 0, sizeof(m_hi));
+	std::memset(&m_lo, 0, sizeof(m_lo));
+	if (maps) { m_hi = maps[0]; m_lo = maps[1]; }
 	const unsigned tiles = (unsigned)(plan.cells / TC_M + 8);
 	const unsigned total = tiles * (unsigned)S;
 	unsigned* work = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
@@ -884,15 +1005,15 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 		tc_trunc(n_src > 0 ? n_src : R > 0 ? (int)std::lround((std::sqrt(4.0 * R + 1.0) - 1.0) / 2.0) : 0, C::KB,
 		         C::EPB);
 	if (persistent)
-		m2l_tc_kernel<NC, NA, SLOTS, MODE, true, F16><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, true, F16, TMA><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
 			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total, bmax, t_inv,
-			shi, slo);
+			shi, slo, m_hi, m_lo, (int)src_cells);
 	else
-		m2l_tc_kernel<NC, NA, SLOTS, MODE, false, F16><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
+		m2l_tc_kernel<NC, NA, SLOTS, MODE, false, F16, TMA><<<grid, TC_THREADS, C::SMEM, ctx.stream>>>(
 			reinterpret_cast<const uint8_t*>(ops), mult, loc, plan.vtab, plan.order, plan.oct_count, R, part,
 			plan.cells, diag, ctx.dev_flags, tr, src_cells, MODE == TC_M2L ? 343 : 8, work, S, total, bmax, t_inv,
-			shi, slo);
+			shi, slo, m_hi, m_lo, (int)src_cells);
 	if (timed) {
 		LFMM_CUDA(ctx, cudaEventRecord(ctx.kev[ctx.kev_used + 1], ctx.stream));
 		ctx.kev_used += 2;
@@ -914,24 +1035,33 @@ int run_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mul
 // {persistent, one block per item} with CUDA events and keeps the fastest
 // for the context (stored as S | 16 for persistent; the chosen pair runs
 // last, so the level's result always comes from it).
-template <int NC, int NA, bool F16>
+template <int NC, int NA, bool F16, bool TMA>
 int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* mult, float* loc, int R, int n_src,
               float t_inv)
 {
-	using C = TcCfg<NC, NA, true, F16>;
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, true, F16>,
+	using C = TcCfg<NC, NA, !TMA, F16>;
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, true, F16, TMA>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, false, F16>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, M2L_SLOTS, TC_M2L, false, F16, TMA>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 	unsigned* bmax = nullptr;
 	uint4 *shi = nullptr, *slo = nullptr;
+	CUtensorMap maps[2];
 	if (F16) {
 		// the level's largest multipole magnitude (the sources' scale), then
-		// the sources split once into FP16 hi / lo rows
+		// the sources split once into FP16 hi / lo rows, and a zero row after
+		// them (the TMA gathers' row for a target without a source)
+		const size_t rows = plan.cells + 1;
 		bmax = static_cast<unsigned*>(ctx.arena.take(sizeof(unsigned)));
-		shi = static_cast<uint4*>(ctx.arena.take(plan.cells * (size_t)C::KB * 128));
-		slo = static_cast<uint4*>(ctx.arena.take(plan.cells * (size_t)C::KBC * 128));
+		shi = static_cast<uint4*>(ctx.arena.take(rows * (size_t)C::KB * 128));
+		slo = static_cast<uint4*>(ctx.arena.take(rows * (size_t)C::KBC * 128));
 		if (!bmax || !shi || !slo) { ctx.last_error = "tensor-core M2L: allocation failed"; return ERR_OOM; }
+		LFMM_CUDA(ctx, cudaMemsetAsync(shi + plan.cells * (size_t)C::KB * 8, 0, (size_t)C::KB * 128, ctx.stream));
+		LFMM_CUDA(ctx, cudaMemsetAsync(slo + plan.cells * (size_t)C::KBC * 8, 0, (size_t)C::KBC * 128, ctx.stream));
+		if (TMA) {
+			if (int st = row_map(ctx, &maps[0], shi, (uint64_t)C::KB * 64, rows)) return st;
+			if (int st = row_map(ctx, &maps[1], slo, (uint64_t)C::KBC * 64, rows)) return st;
+		}
 		LFMM_CUDA(ctx, cudaMemsetAsync(bmax, 0, sizeof(unsigned), ctx.stream));
 		const size_t n = plan.cells * (size_t)R;
 		absmax_kernel<<<(unsigned)std::min<size_t>(div_up(n, 256), 8 * (size_t)ctx.num_sms), 256, 0, ctx.stream>>>(
@@ -946,7 +1076,7 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 	int bucket = 0;
 	while ((1u << bucket) < tiles && bucket < 32) ++bucket;
 	static_assert(NC / 16 < Context::SPLIT_ROWS, "autotuner table");
-	int& tuned = ctx.m2l_split[F16 ? 1 : 0][NC / 16][bucket];
+	int& tuned = ctx.m2l_split[F16 ? (TMA ? 2 : 1) : 0][NC / 16][bucket];
 	const bool tune = ctx.tune_m2l && tuned == 0;
 	bool pers = false;
 	if (ctx.tune_m2l && !tune) { S = tuned & 15; pers = (tuned & 16) != 0; }
@@ -971,9 +1101,9 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		for (int mode = 0; mode < 2; ++mode)
 			for (int cand = 1; cand <= maxS; cand *= 2) {
 				LFMM_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
-				int st = run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16>(ctx, plan, ops, mult, loc, R, cand, part, false,
-				                                                plan.cells, nullptr, n_src, mode == 0, bmax, t_inv,
-				                                                shi, slo);
+				int st = run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16, TMA>(ctx, plan, ops, mult, loc, R, cand, part, false,
+				                                                     plan.cells, nullptr, n_src, mode == 0, bmax, t_inv,
+				                                                     shi, slo, TMA ? maps : nullptr);
 				if (st) return st;
 				LFMM_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
 				LFMM_CUDA(ctx, cudaEventSynchronize(e1));
@@ -987,8 +1117,9 @@ int launch_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float* 
 		S = bestS;
 		pers = bestP;
 	}
-	return run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells, nullptr,
-	                                              n_src, pers, bmax, t_inv, shi, slo);
+	return run_tc<NC, NA, M2L_SLOTS, TC_M2L, F16, TMA>(ctx, plan, ops, mult, loc, R, S, part, true, plan.cells,
+	                                                   nullptr, n_src, pers, bmax, t_inv, shi, slo,
+	                                                   TMA ? maps : nullptr);
 }
 
 // M2M (8 slots, stored) or L2L (1 slot, added) of one level: S = 1.
@@ -999,12 +1130,12 @@ int launch_shift_tc(Context& ctx, int mode, const M2LPlan& plan, const uint4* op
 	using C = TcCfg<NC, NA>;
 	using CL = TcCfg<NC, NA, false>;
 	if (mode == TC_M2M) {
-		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M, false, false>,
+		LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 8, TC_M2M, false, false, false>,
 		                                    cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
 		return run_tc<NC, NA, 8, TC_M2M>(ctx, plan, ops, src, dst, R, 1, nullptr, false, src_cells, nullptr, 0,
 		                                 false);
 	}
-	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L, false, false>,
+	LFMM_CUDA(ctx, cudaFuncSetAttribute(m2l_tc_kernel<NC, NA, 1, TC_L2L, false, false, false>,
 	                                    cudaFuncAttributeMaxDynamicSharedMemorySize, CL::SMEM));
 	// the diagonal [8][NC] follows the 8 operators
 	const float* diag = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(ops) + 8 * C::DIR_BYTES);
@@ -1137,8 +1268,9 @@ int m2l_gemm_tc(Context& ctx, const M2LPlan& plan, const uint4* ops, const float
 	const int ns = n_src > 0 && n_src < N ? n_src : 0;
 #define LFMM_TC_M2L(nc, na)                                                                                   \
 	if (NC == nc && NA == na)                                                                                 \
-		return ctx.m2l_f16 ? launch_tc<nc, na, true>(ctx, plan, ops, mult, loc, R, ns, t_inv)                 \
-		                   : launch_tc<nc, na, false>(ctx, plan, ops, mult, loc, R, ns, 1.f);
+		return !ctx.m2l_f16 ? launch_tc<nc, na, false, false>(ctx, plan, ops, mult, loc, R, ns, 1.f)          \
+		       : ctx.m2l_tma ? launch_tc<nc, na, true, true>(ctx, plan, ops, mult, loc, R, ns, t_inv)          \
+		                     : launch_tc<nc, na, true, false>(ctx, plan, ops, mult, loc, R, ns, t_inv);
 	LFMM_TC_ORDERS(LFMM_TC_M2L)
 #undef LFMM_TC_M2L
 	ctx.last_error = "tensor-core M2L: unsupported order";

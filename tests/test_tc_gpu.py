@@ -44,17 +44,28 @@ def tf32():
     c.close()
 
 
+@pytest.fixture(scope="module")
+def ldg():
+    c = engine_context("ldg", "LFMM_M2L_GATHER")
+    yield c
+    c.close()
+
+
 def noself(p, q):
     return p - q * 1e4
 
 
 @pytest.mark.parametrize("N,depth,gen", [(16, 10, "plummer"), (17, 10, "plummer"), (12, 6, "uniform"),
                                          (15, 6, "uniform")])
-def test_f16_and_tf32_operands_agree(tc, tf32, ctx, N, depth, gen):
+def test_f16_and_tf32_operands_agree(tc, tf32, ldg, ctx, N, depth, gen):
     """The FP16 hi/lo M2L (operators and each level's multipoles scaled by
-    powers of two into FP16's range, sources split once per level) against the
-    TF32 hi/lo M2L: the same 22-bit operand splits, so both land equally close
-    to the FP64 form and within a few 1e-7 of each other."""
+    powers of two into FP16's range, sources split once per level; rows
+    brought in by TMA gathers, the default, or by the producers' loads)
+    against the TF32 hi/lo M2L: the same 22-bit operand splits, so all land
+    equally close to the FP64 form and within a few 1e-7 of each other; the
+    two FP16 forms multiply the same staged values (the autotuner may pick
+    different slot splits for them, whose partial sums round differently in
+    FP32: measured 1.4e-7 apart on the potential)."""
     src, q = (plummer_mix3d if gen == "plummer" else uniform3d)(300000, seed=70 + N)
     kw = dict(N=N, tree_depth=depth, precision="mixed")
     if gen == "plummer":
@@ -68,6 +79,9 @@ def test_f16_and_tf32_operands_agree(tc, tf32, ctx, N, depth, gen):
     assert ea < TOL and fa < TOL
     assert ea < 1.3 * eb + 1e-8 and fa < 1.3 * fb + 1e-8
     assert rel_l2(noself(a.potentials, q), noself(b.potentials, q)) < 5e-7
+    d = FastMultipole3d((src, q), ctx=ldg, **kw)
+    assert rel_l2(noself(a.potentials, q), noself(d.potentials, q)) < 3e-7
+    assert rel_l2(a.forces, d.forces) < 3e-7
 
 
 @pytest.mark.parametrize("N", [13, 9, 7, 11, 14, 15, 16])
