@@ -256,41 +256,42 @@ __global__ void x_kernel(DevTree a, int pass, uint32_t* __restrict__ xcnt)
 }
 
 // Candidate thresholds' counts for the uniform cells of level L (see
-// LeafChooser); acc [K][LEAF_STATS].
+// LeafChooser); acc [K][LEAF_STATS].  Block row blockIdx.y = candidate k;
+// each thread sums its cells (grid-stride) in registers, then one warp
+// reduction and one atomic per statistic and warp.
 __global__ void leaf_candidates_kernel(DevTree u, int L, const uint32_t* __restrict__ pb,
                                        const uint32_t* __restrict__ pe, const int* __restrict__ cand, int K,
                                        unsigned long long* __restrict__ acc)
 {
-	const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-	const bool valid = c < u.lsize[L];
-	unsigned long long n = 0, np = 0;
-	if (valid) {
+	const int k = blockIdx.y;
+	const unsigned long long m = (unsigned long long)cand[k];
+	const bool last = L == u.depth - 1;
+	unsigned long long v[LEAF_STATS] = {};
+	for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < u.lsize[L]; c += (size_t)gridDim.x * blockDim.x) {
 		const size_t g = u.loff[L] + c;
-		n = pe[g] - pb[g];
+		const unsigned long long n = pe[g] - pb[g];
+		unsigned long long np = 0;
 		if (L > 0) {
 			const size_t gp = u.loff[L - 1] + (size_t)u.parent[g];
 			np = pe[gp] - pb[gp];
 		}
+		const bool kept = L == 0 || np > m;
+		if (!kept) continue;
+		const bool leaf = n <= m || last;
+		v[0] += 1; v[1] += leaf; v[2] += L >= 2; v[3] += L >= 4;
+		if (leaf) { v[4] += n * n; v[5] += n * np; v[6] += last ? n : 0; v[8] = v[8] > n ? v[8] : n; }
+		v[7] = (unsigned long long)L;
 	}
-	const bool last = L == u.depth - 1;
-	for (int k = 0; k < K; ++k) {
-		const unsigned long long m = (unsigned long long)cand[k];
-		const bool kept = valid && (L == 0 || np > m);
-		const bool leaf = kept && (n <= m || last);
-		unsigned long long v[LEAF_STATS] = {kept, leaf, kept && L >= 2, kept && L >= 4, leaf ? n * n : 0,
-		                                    leaf ? n * np : 0, leaf && last ? n : 0, kept ? (unsigned long long)L : 0,
-		                                    leaf ? n : 0};
 #pragma unroll
-		for (int j = 0; j < LEAF_STATS; ++j) {
-			unsigned long long x = v[j];
-			for (int o = 16; o; o >>= 1) {
-				const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
-				x = j >= 7 ? (x > y ? x : y) : x + y;
-			}
-			if ((threadIdx.x & 31) == 0 && x) {
-				if (j >= 7) atomicMax(&acc[k * LEAF_STATS + j], x);
-				else atomicAdd(&acc[k * LEAF_STATS + j], x);
-			}
+	for (int j = 0; j < LEAF_STATS; ++j) {
+		unsigned long long x = v[j];
+		for (int o = 16; o; o >>= 1) {
+			const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+			x = j >= 7 ? (x > y ? x : y) : x + y;
+		}
+		if ((threadIdx.x & 31) == 0 && x) {
+			if (j >= 7) atomicMax(&acc[k * LEAF_STATS + j], x);
+			else atomicAdd(&acc[k * LEAF_STATS + j], x);
 		}
 	}
 }
@@ -355,7 +356,10 @@ int candidate_counts(Context& ctx, const DevTree& u, const uint32_t* pb, const u
 	LFMM_CUDA(ctx, cudaMemcpyAsync(dc, cand, sizeof(int) * K, cudaMemcpyHostToDevice, s));
 	LFMM_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * K * LEAF_STATS, s));
 	for (int L = 0; L < u.depth; ++L)
-		if (u.lsize[L]) leaf_candidates_kernel<<<div_up(u.lsize[L], 256), 256, 0, s>>>(u, L, pb, pe, dc, K, acc);
+		if (u.lsize[L]) {
+			const dim3 grid((unsigned)std::min<size_t>(div_up(u.lsize[L], 256), 2 * (size_t)ctx.num_sms), (unsigned)K);
+			leaf_candidates_kernel<<<grid, 256, 0, s>>>(u, L, pb, pe, dc, K, acc);
+		}
 	LFMM_CUDA(ctx, cudaMemcpyAsync(stats, acc, sizeof(unsigned long long) * K * LEAF_STATS, cudaMemcpyDeviceToHost, s));
 	LFMM_CUDA(ctx, cudaStreamSynchronize(s));
 	return OK;
