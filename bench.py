@@ -553,12 +553,12 @@ def m2l_flops(N):
     return 2 * sum((n + 1) * (4 * n + 2) for n in range(N)) + 4 * sum(m * m for m in range(1, N + 1)) + 12 * nx2
 
 
-# DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode, FP16 operands),
-# from an ncu capture of a 2,097,152-particle case of the default workload at
-# N = 17 (185.6 MB read + 71.9 MB written in one 1.572 ms launch); the
-# kernel's traffic grows with its work, so a full launch's traffic is this
-# rate times its duration.
-M2L_TC_DRAM_BYTES_PER_MS = (185.6e6 + 71.9e6) / 1.572
+# DRAM bytes per millisecond of m2l_tc_kernel time (M2L mode, FP16 operands
+# gathered by TMA), from an ncu capture of a 2,097,152-particle case of the
+# default workload at N = 17 (176.6 MB read + 73.4 MB written in one 1.061 ms
+# launch); the kernel's traffic grows with its work, so a full launch's
+# traffic is this rate times its duration.
+M2L_TC_DRAM_BYTES_PER_MS = (176.6e6 + 73.4e6) / 1.061
 
 
 def padded(N):
