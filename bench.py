@@ -455,8 +455,14 @@ def run_ours(args, cfg, rank, world, local_rank):
             t1.record()
         t1.synchronize()
         fms = t0.elapsed_time(t1) / reps
+        # its phases (one more solve with the phase events): the tree phase here is
+        # the tree build alone, without the learned solve's prediction and check
+        stf = LfmmStats()
+        call(ctx_t, True, prec, stats=stf, tree=ft)
+        torch.cuda.synchronize()
         mixed_fixed = {"value": n / (fms * 1e-3) / 1e6, "unit": "Mparticles/s", "ms_per_step": fms,
                        "precision": cfg["precision"], "N_degrees": N, "max_leaf": max_leaf,
+                       "phases_ms": {k: v for k, v in stf.as_dict().items() if k.startswith("ms_")},
                        "what": "the mixed form at the fixed order and leaf size, no prediction or check"}
     # 2D: the reference's uniform quadtree on the same particles beside the adaptive one
     if dim == 2 and max_leaf > 0 and cfg.get("uniform_depth") and not args.no_plain:

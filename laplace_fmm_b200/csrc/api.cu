@@ -546,12 +546,15 @@ int lfmm3d_solve_levels_device(lfmm_ctx* ctx, size_t ns, const double* src, cons
 	return st;
 }
 
-int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt,
-                               const double* tgt, const lfmm_solve_opts* o, double* field, lfmm_stats* stats)
+namespace {
+
+// The vector solve on device buffers.  own_arena: reset the context's arena
+// before and settle it after (the device entry point); false when the host
+// entry point already took its copies of the inputs from the arena.
+int vector_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt, const double* tgt,
+                  const lfmm_solve_opts* o, double* field, lfmm_stats* stats, bool own_arena)
 {
-	if (!ctx || !o) return LFMM_ERR_ARG;
 	Context& c = ctx->c;
-	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	if (ns == 0 && nt == 0) { c.last_error = "no particles"; return LFMM_ERR_ARG; }
 	if ((ns && (!src || !q3)) || (nt && !tgt) || !field) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
 	if (o->precision != LFMM_PRECISION_FP64 && o->precision != LFMM_PRECISION_MIXED) {
@@ -560,7 +563,7 @@ int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, cons
 	}
 	const int Nr = resolve_order(3, o->N, o->eps), Dr = resolve_depth(3, o->tree_depth, ns + nt);
 	if (Nr < 1 || Dr < 1) { c.last_error = "order and tree depth must be >= 1"; return LFMM_ERR_ARG; }
-	c.arena.reset();
+	if (own_arena) c.arena.reset();
 	ctx->has_tree = false;
 	ParticleInput in;
 	in.dim = 3; in.ns = ns; in.nt = nt; in.src = src; in.srcq = q3; in.tgt = tgt;
@@ -570,8 +573,18 @@ int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, cons
 		fill_stats(stats, ss);
 		st = check_flags(c);
 	}
-	c.arena.settle();
+	if (own_arena) c.arena.settle();
 	return st;
+}
+
+} // namespace
+
+int lfmm3d_solve_vector_device(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt,
+                               const double* tgt, const lfmm_solve_opts* o, double* field, lfmm_stats* stats)
+{
+	if (!ctx || !o) return LFMM_ERR_ARG;
+	if (select_device(ctx)) return LFMM_ERR_CUDA;
+	return vector_device(ctx, ns, src, q3, nt, tgt, o, field, stats, true);
 }
 
 int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t ns, const double* src, const double* q3, size_t nt, const double* tgt,
@@ -582,33 +595,29 @@ int lfmm3d_solve_vector(lfmm_ctx* ctx, size_t ns, const double* src, const doubl
 	if (select_device(ctx)) return LFMM_ERR_CUDA;
 	if ((ns && (!src || !q3)) || (nt && !tgt) || !field) { c.last_error = "null buffer"; return LFMM_ERR_ARG; }
 	const size_t nout = nt ? nt : ns;
-	// the device copies live outside the solve's arena (it resets it)
-	double *dsrc = nullptr, *dq = nullptr, *dtgt = nullptr, *dfld = nullptr;
-	auto release = [&] { cudaFree(dsrc); cudaFree(dq); cudaFree(dtgt); cudaFree(dfld); };
-	if ((ns && (cudaMalloc(&dsrc, sizeof(double) * 3 * ns) != cudaSuccess ||
-	            cudaMalloc(&dq, sizeof(double) * 3 * ns) != cudaSuccess)) ||
-	    (nt && cudaMalloc(&dtgt, sizeof(double) * 3 * nt) != cudaSuccess) ||
-	    (nout && cudaMalloc(&dfld, sizeof(double) * 3 * nout) != cudaSuccess)) {
-		cudaGetLastError();
-		release();
-		c.last_error = "device allocation failed";
-		return LFMM_ERR_OOM;
-	}
-	cudaStream_t s = c.stream;
+	// the device copies come from the context's arena (kept across the solve,
+	// which then does not reset it), as in the scalar host entry points
+	c.arena.reset();
+	double* dsrc = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dq = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(ns, 1)));
+	double* dtgt = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nt, 1)));
+	double* dfld = static_cast<double*>(c.arena.take(sizeof(double) * 3 * std::max<size_t>(nout, 1)));
 	int st = OK;
+	if (!dsrc || !dq || !dtgt || !dfld) { c.last_error = "device allocation failed"; st = LFMM_ERR_OOM; }
+	cudaStream_t s = c.stream;
 	cudaError_t e = cudaSuccess;
-	if (ns) e = cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
-	if (e == cudaSuccess && ns) e = cudaMemcpyAsync(dq, q3, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
-	if (e == cudaSuccess && nt) e = cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s);
+	if (st == OK && ns) e = cudaMemcpyAsync(dsrc, src, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
+	if (st == OK && e == cudaSuccess && ns) e = cudaMemcpyAsync(dq, q3, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s);
+	if (st == OK && e == cudaSuccess && nt) e = cudaMemcpyAsync(dtgt, tgt, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s);
 	if (e != cudaSuccess) st = cuda_fail(c, e, "vector solve: copy in");
-	if (st == OK) st = lfmm3d_solve_vector_device(ctx, ns, dsrc, dq, nt, dtgt, o, dfld, stats);
+	if (st == OK) st = vector_device(ctx, ns, dsrc, dq, nt, dtgt, o, dfld, stats, false);
 	if (st == OK) {
 		e = cudaMemcpyAsync(field, dfld, sizeof(double) * 3 * nout, cudaMemcpyDeviceToHost, s);
 		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
 		if (e != cudaSuccess) st = cuda_fail(c, e, "vector solve: copy out");
 	}
 	cudaStreamSynchronize(s);
-	release();
+	c.arena.settle();
 	return st;
 }
 
