@@ -1,25 +1,35 @@
-// tcgen05 M2L engine (m2l_tc.cuh).  One CTA per tile of 128 targets of one
-// octant class; D[128 targets][NC coefficients] in TMEM.  Warp roles:
-//   warps 0-3  producers: thread t gathers target t's source multipole for
-//              the K block and splits it into TF32 hi / lo: hi into TMEM lane
-//              t (read by two MMAs straight from tensor memory), lo into the
-//              stage's shared memory as a 128-byte swizzled row (read by
-//              one); thread 0 also starts the bulk copy of the operator block
-//              (hi and lo, stored pre-swizzled) into the stage.
-//   warp 4     TMEM owner; lane 0 issues the MMAs (M=128, N=NC, K=8):
-//              main = B_hi T_hi (fresh per slot), corr += B_hi T_lo + B_lo T_hi.
+// tcgen05 M2L engine (m2l_tc.cuh).  One CTA per work item (a tile of 128
+// targets of one octant class and a share of its far slots); D[128 targets][NC
+// coefficients] in TMEM.  Operands are hi / lo pairs: FP16 for the M2L (the
+// default; operators and each level's multipoles scaled by exact powers of
+// two), TF32 for the M2M / L2L shifts and the LFMM_M2L_TYPE=tf32 M2L.  Warp roles:
+//   warps 0-3  producers, one target row per thread.  FP16 with TMA (the
+//              default M2L): the sources are split once per level into staged
+//              FP16 hi / lo rows (stage_f16_kernel); per K block lanes 0-7 of
+//              each warp gather the warp's rows with tile::gather4 copies
+//              straight into the stage's 128-byte swizzled rows, and lane 0
+//              arrives with the warp's byte count.  Otherwise thread t loads
+//              target t's source K block (staged FP16 rows, or the FP32
+//              multipole it splits into TF32 hi / lo), stores hi into TMEM
+//              lane t (read by two MMAs from tensor memory) and lo into the
+//              stage's shared memory as a swizzled row (read by one).  Warp
+//              0's lane 0 (thread 0) also starts the bulk copy of the
+//              operator block (hi and lo rows, stored pre-swizzled).
+//   warp 4     TMEM owner; lane 0 issues the MMAs (M = 128, K steps of 32
+//              bytes): main = B_hi T_hi (fresh per slot), corr += B_hi T_lo +
+//              B_lo T_hi.
 //   warps 5-12 epilogue: after each slot, add main to FP32 registers (warp w
 //              reads TMEM lanes 32 (w % 4) .. +31, half of the columns each).
-// TMEM: main at columns [0, NC), corr at [256, 256 + NC), the stages' B_hi
-// (32 columns each) in the gaps [NC, 256) and [256 + NC, 512).  The two
-// accumulators stay apart: each tensor-core accumulate rounds at its
-// accumulator's ulp, and the corrections summed into main (measured) doubled
-// the mixed form's error on clustered sets.  With no 32-column gap (NC = 240)
-// B_hi goes to shared memory beside B_lo.  Stages (full: 128 arrivals +
-// operator bytes; empty: MMA commit): up to three; one main accumulator
-// (full: MMA commit after the slot; empty: 256 epilogue arrivals).  Every wait is bounded; on expiry the kernel sets
-// DEV_ERR_TIMEOUT, waits (bounded) for its copies and MMAs in flight, frees
-// TMEM and returns.
+// TMEM: main, the high-degree columns and the corrections (TcCfg), and, when
+// two or more fit, the stages' B_hi blocks (32 columns each); else B_hi sits in
+// shared memory beside B_lo.  The two accumulators stay apart: each
+// tensor-core accumulate rounds at its accumulator's ulp, and the corrections
+// summed into main (measured) doubled the mixed form's error on clustered
+// sets.  Stages (full: 128 producer arrivals, or 4 with TMA, plus the copies'
+// bytes; empty: MMA commit): two to three; one main accumulator (full: MMA
+// commit after the slot; empty: 256 epilogue arrivals).  Every wait is
+// bounded; on expiry the kernel sets DEV_ERR_TIMEOUT, waits (bounded) for its
+// copies and MMAs in flight, frees TMEM and returns.
 #include "m2l_tc.cuh"
 #include <cuda.h>
 #include <cudaTypedefs.h>
