@@ -18,17 +18,20 @@ static_assert(NPARAM == LFMM_MLP_PARAMS, "parameter count");
 constexpr int MT = 32;   // rows (samples) per block (static shared memory <= 48 KB)
 
 // Forward for a block of 32 samples; thread t < 64 computes hidden unit t for
-// every sample of the block (weights in shared memory, activations too).
+// every sample of the block (weights in shared memory, activations too).  The
+// first two layers' weights are stored transposed ([input][unit]), so a warp's
+// reads of one input's weights fall in distinct banks (row-major, units 64
+// floats apart all hit one bank); the same values in the same order.
 __global__ void __launch_bounds__(64) mlp_forward_kernel(const float* __restrict__ P, int n, const float* __restrict__ X,
                                                          float* __restrict__ Y, float* __restrict__ A1,
                                                          float* __restrict__ A2)
 {
-	__shared__ float sW1[H * F], sb1[H], sW2[H * H], sb2[H], sW3[O * H], sb3[O];
+	__shared__ float sW1t[F * H], sb1[H], sW2t[H * H], sb2[H], sW3[O * H], sb3[O];
 	__shared__ float sX[MT][F];
 	__shared__ float sA1[MT][H + 1], sA2[MT][H + 1];
 	const int t = threadIdx.x;
-	for (int i = t; i < H * F; i += 64) sW1[i] = P[OFF_W1 + i];
-	for (int i = t; i < H * H; i += 64) sW2[i] = P[OFF_W2 + i];
+	for (int i = t; i < H * F; i += 64) sW1t[(i % F) * H + i / F] = P[OFF_W1 + i];
+	for (int i = t; i < H * H; i += 64) sW2t[(i % H) * H + i / H] = P[OFF_W2 + i];
 	for (int i = t; i < O * H; i += 64) sW3[i] = P[OFF_W3 + i];
 	sb1[t] = P[OFF_B1 + t]; sb2[t] = P[OFF_B2 + t];
 	if (t < O) sb3[t] = P[OFF_B3 + t];
@@ -40,13 +43,13 @@ __global__ void __launch_bounds__(64) mlp_forward_kernel(const float* __restrict
 	__syncthreads();
 	for (int r = 0; r < MT; ++r) {
 		float a = sb1[t];
-		for (int c = 0; c < F; ++c) a = fmaf(sW1[t * F + c], sX[r][c], a);
+		for (int c = 0; c < F; ++c) a = fmaf(sW1t[c * H + t], sX[r][c], a);
 		sA1[r][t] = fmaxf(a, 0.f);
 	}
 	__syncthreads();
 	for (int r = 0; r < MT; ++r) {
 		float a = sb2[t];
-		for (int c = 0; c < H; ++c) a = fmaf(sW2[t * H + c], sA1[r][c], a);
+		for (int c = 0; c < H; ++c) a = fmaf(sW2t[c * H + t], sA1[r][c], a);
 		sA2[r][t] = fmaxf(a, 0.f);
 	}
 	__syncthreads();
