@@ -567,6 +567,14 @@ def m2l_flops(N):
 M2L_TC_DRAM_BYTES_PER_MS = (176.6e6 + 73.4e6) / 1.061
 
 
+# DRAM bytes per particle of p2p_f32_kernel (mixed 3D form), from an ncu
+# capture of a 2,097,152-particle case of the default workload (146.5 MB read
+# + 83.0 MB written in one launch): the kernel reads the particle arrays
+# (repeated source reads hit L2) and writes the outputs, so its traffic grows
+# with the particles.
+P2P_DRAM_BYTES_PER_PARTICLE = (146.5e6 + 83.0e6) / 2097152
+
+
 def padded(N):
     return (N * (N + 1) + 15) // 16 * 16
 
@@ -653,9 +661,18 @@ def roofline(cfg, stats, peaks, fp64_tflops, fp32_tflops, tf32_tflops, phase=Non
     if dom == "leaves":
         flops = 20.0 * stats["n_p2p_pairs"]     # 2D: 20 flops and one FP64 log per pair
         achieved = flops / (ms * 1e-3) / 1e12
-        return {"kernel": "leaves kernel (P2P + M2P + L2P)", "bound": "fp64" if fp64 else "fp32",
+        line = {"kernel": "leaves kernel (P2P + M2P + L2P)", "bound": "fp64" if fp64 else "fp32",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": src, "algorithmic_flops": flops, "phase_ms": ms, "traffic": None}
+                "peak_source": src, "algorithmic_flops": flops, "phase_ms": ms, "traffic": None,
+                "flop_model": "20 flops per near-field (target, source) pair; the phase time also holds "
+                              "the expansions' evaluation at the targets (M2P over W, L2P)"}
+        if cfg["dim"] == 3 and not fp64 and stats.get("n_particles"):
+            # the near-field kernel's DRAM bytes: P2P_DRAM_BYTES_PER_PARTICLE x particles
+            line["kernel"] = "p2p_f32_kernel (near field) + eval_scaled_kernel (M2P, L2P)"
+            line["traffic"] = P2P_DRAM_BYTES_PER_PARTICLE * stats["n_particles"]
+            line["traffic_unit"] = ("bytes of the near-field launch (ncu capture of a 2M-particle case, "
+                                    "scaled by particles)")
+        return line
     if dom == "m2l":
         Nd = stats.get("order_N") or cfg["N"]
         flops = float(m2l_flops(Nd)) * stats["n_far_pairs"]
