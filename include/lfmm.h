@@ -83,6 +83,13 @@ typedef struct {
 	int n_m2l_kernel;       /* M2L GEMMs timed */
 } lfmm_stats;
 
+/* A context: its own stream, device arena and caches, on opt->device.  The
+ * M2L engine is read from the environment when the context is created:
+ * LFMM_M2L = tc (default; tcgen05 on the mixed form's FP32 levels), simt or
+ * rotation; LFMM_M2L_TYPE = f16 (default; FP16 hi / lo operands) or tf32;
+ * LFMM_M2L_GATHER = tma (default; the staged FP16 sources gathered by
+ * tile::gather4) or ldg (loaded by the producer warps); LFMM_M2L_TUNE = 0
+ * keeps the fixed launch rule instead of the autotuner. */
 int lfmm_create(lfmm_ctx** ctx, const lfmm_options* opt);
 void lfmm_destroy(lfmm_ctx* ctx);
 const char* lfmm_last_error(const lfmm_ctx* ctx);
